@@ -1,0 +1,323 @@
+"""bench.py -- throughput of the batched path stage on B200 in path·k-points/s.
+
+Workload (one GPU): the Fe K-edge stage of a seeded random packing of 3000 atoms (Fe/O/Pt, minimum separation
+1.8 A, 0.08 atoms/A^3), the two most central Fe absorbers, paths of 2-8 legs to 8 A with the reference path
+finder's leg-count histogram for that structure (2.02e5 paths, drawn synthetically), phase tables lmax 24 of the
+reference's own phase-shift stage resampled to 401 k points (0-20 1/A), output chi(k) on the same 401 points.
+One step = the whole stage over that batch: geometry, rotation matrices, scattering-matrix chain, termination,
+cfac, fine-grid signal and the deterministic degeneracy-weighted sum into the two absorbers' rows, in the
+mixed precision form (FP32 complex chain, FP64 phase argument and sums).  Under torchrun every rank evaluates its
+own two absorbers (weak scaling, no collective on the data path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's path stage on the CPU (the FP64 oracle port of its algorithm with all host
+threads) on a bounded stratified sample of the same workload, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+NK = 401
+Q = np.arange(NK) * 0.05
+METRIC = "path·k-points/s fwd and fwd+bwd vs plain FP64 on same B200 at R<=1e-6"
+UNIT = "path·k/s"
+
+
+# ------------------------------------------------------------------------------------------------ workload
+def workload(rank: int, world: int):
+    from feffgpu_b200 import workloads as W
+    from feffgpu_b200.pad import phase_from_npz, resample_phase
+    z = np.load(ROOT / "tests" / "golden" / "cfg2_phase.npz")
+    P = resample_phase(phase_from_npz(z, prefix="ph_"), Q)
+    pos, lab, box = W.random_packing(3000, 0.08, 1.8, seed=2024)
+    absorbers = W.central_atom(pos, box, lab, "Fe", 2 * world)[2 * rank:2 * rank + 2]
+    ipot_of = np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
+    groups = []
+    for i, ab in enumerate(absorbers):
+        paths = W.random_paths(pos, box, int(ab), W.FEOPT_LEG_COUNTS, rmax=8.0, seed=1000 + int(ab), ipot_of=ipot_of)
+        for nleg, (c, ip, _atoms) in paths.items():
+            groups.append((c, ip, None, np.full(len(c), i)))
+    return P, groups
+
+
+# ------------------------------------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi samples of the GPU's clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid, self.proc, self.lines = uuid, None, []
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
+        if self.uuid:
+            cmd.insert(1, f"--id={self.uuid}")
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for l in self.lines:
+            p = [v.strip() for v in l.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                rows.append((float(p[0]), float(p[1]), float(p[2]), p[3], p[4], p[5], p[6], p[7]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [r for r in rows if r[2] > 200.0] or rows
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in load for n, v in zip(names, r[4:]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in load])), "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows), "samples": len(load), "reasons": reasons}
+
+
+# ------------------------------------------------------------------------------------------------ CPU legs
+def cpu_sample(P, groups, budget_s: float, nthreads: int):
+    """The oracle (FP64, C, pthreads) on a stratified sample of every leg count, extrapolated to the workload:
+    cchi of the sampled paths, their fine-grid signal and weighted sum.  Returns (path·k/s, description)."""
+    from oracle import oracle as O
+    orc = O.Oracle(P)
+    S = orc.linear_matrix(Q)
+    by_leg: dict = {}
+    for c, ip, _deg, _row in groups:
+        by_leg.setdefault(c.shape[1], []).append((c, ip))
+    counts = {n: sum(len(c) for c, _ in v) for n, v in by_leg.items()}
+    rng = np.random.default_rng(0)
+
+    def run(n, m):
+        c = np.concatenate([x[0] for x in by_leg[n]])
+        ip = np.concatenate([x[1] for x in by_leg[n]])
+        sel = rng.choice(len(c), size=min(m, len(c)), replace=False)
+        t = time.perf_counter()
+        cc, rf = orc.cchi(c[sel], ip[sel], nthreads=nthreads)
+        chi = O.chi_fine(cc, rf, Q, S).sum(0)
+        return (time.perf_counter() - t) / len(sel), len(sel), chi
+
+    # calibrate with two paths per leg count, then spend the budget in proportion to each bucket's total time
+    per = {n: run(n, 2)[0] for n in counts}
+    full = sum(counts[n] * per[n] for n in counts)
+    scale = budget_s / max(full, 1e-9)
+    t_total, sampled = 0.0, 0
+    for n in sorted(counts):
+        m = max(4, int(counts[n] * scale))
+        tp, got, _ = run(n, m)
+        t_total += counts[n] * tp
+        sampled += got
+    n_paths = sum(counts.values())
+    return n_paths * NK / t_total, f"stratified sample of {sampled} of {n_paths} paths (every leg count), " \
+                                    f"timed per leg count and extrapolated to the full batch"
+
+
+# ------------------------------------------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work for the CPU baseline")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    nthreads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        P, groups = workload(0, 1)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, desc = cpu_sample(P, groups, budget_s=max(2.0, args.cpu_budget / 3), nthreads=nthreads)
+            if i >= args.warmup:
+                vals.append(v)
+        v = float(np.median(vals))
+        n_paths = sum(len(g[0]) for g in groups)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": n_paths * NK / v * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+            "config": {"workload": f"Fe/O/Pt packing 3000 atoms, 2 Fe K absorbers, rmax 8 A, 2-8 legs, {n_paths} paths, "
+                                   f"lmax 24 x {NK} k", "impl": "FP64 C port of the reference's path stage (oracle)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    import torch.distributed as dist
+    from feffgpu_b200 import GPUPathStage, PathBatch, _lib
+    from feffgpu_b200.roofline import batch_flops
+
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+    P, groups = workload(rank, world)
+    stage = GPUPathStage(P, device=dev, dtype=torch.complex64)
+    batch = PathBatch(groups, nrows=2, device=dev)
+    S = stage.linear_matrix(Q)
+    lib = _lib.load()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2, written between steps
+    n_paths = batch.n
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def timed(fn, steps, warmup, kernel_time=False):
+        for _ in range(warmup):
+            fn()
+        barrier()
+        total, kern = 0.0, []
+        if kernel_time:
+            lib.fg_set_kernel_timing(1)
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+            if kernel_time:
+                import ctypes
+                ms = ctypes.c_float()
+                _lib.check(lib.fg_kernel_time_ms(ctypes.byref(ms)))
+                kern.append(ms.value)
+        if kernel_time:
+            lib.fg_set_kernel_timing(0)
+        barrier()
+        t = torch.tensor([total], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()) / steps, kern
+
+    # the headline: fused forward with the inputs resident
+    uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    uuid = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
+    with torch.no_grad():
+        with Clocks(uuid) as clk:
+            ms, kern = timed(lambda: stage.chi_reduce(batch, Q, S), args.steps, args.warmup, kernel_time=True)
+    value = world * n_paths * NK / (ms * 1e-3)
+
+    # end to end through the public API: coordinates from pinned host memory, rows back to the host, every step
+    coords_h = batch.coords.cpu().pin_memory()
+    coords_d = torch.empty_like(batch.coords)
+    rows_h = torch.empty(batch.nrows, NK, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        coords_d.copy_(coords_h, non_blocking=True)
+        rows = stage.chi_reduce(batch, Q, S, coords=coords_d)
+        rows_h.copy_(rows, non_blocking=True)
+
+    with torch.no_grad():
+        ms_e2e, _ = timed(e2e_step, args.steps, 1)
+    e2e = {"value": world * n_paths * NK / (ms_e2e * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": int(coords_h.numel() * coords_h.element_size()),
+           "d2h_bytes_per_step": int(rows_h.numel() * rows_h.element_size())}
+
+    # forward + backward (gradients with respect to every path coordinate and per-path sigma^2)
+    fwd_bwd = None
+    try:
+        s2 = torch.zeros(n_paths, dtype=torch.float64, device=dev, requires_grad=True)
+        cg = batch.coords.clone().requires_grad_(True)
+        w = torch.randn(batch.nrows, NK, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
+
+        def fb():
+            rows = stage.chi_reduce(batch, Q, S, coords=cg, sigma2=s2)
+            (rows * w).sum().backward()
+
+        ms_fb, _ = timed(fb, max(2, args.steps // 2), 1)
+        fwd_bwd = {"value": world * n_paths * NK / (ms_fb * 1e-3), "unit": UNIT, "ms_per_step": ms_fb}
+    except NotImplementedError as err:
+        fwd_bwd = {"value": None, "unit": UNIT, "note": f"not available: {err}"}
+
+    # the plain FP64 drop-in (complex128) on the same batch
+    stage64 = GPUPathStage(P, device=dev, dtype=torch.complex128)
+    with torch.no_grad():
+        ms64, _ = timed(lambda: stage64.chi_reduce(batch, Q, S), 2, 1)
+    plain = {"value": world * n_paths * NK / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
+             "speedup_mixed_over_fp64": ms64 / ms}
+
+    # roofline of the dominant kernel (the fused per-path kernel): algorithmic FLOPs of the reference's loops
+    import ctypes
+    peak = ctypes.c_double()
+    _lib.check(lib.fg_fp32_fma_peak(ctypes.byref(peak), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+    flops = batch_flops(batch.nleg.cpu().numpy(), batch.ipots.cpu().numpy(), stage.lmax.cpu().numpy())
+    kern_ms = float(np.mean(kern)) if kern else None
+    achieved = flops / (kern_ms * 1e-3) / 1e12 if kern_ms else None
+    traffic = None
+    tf = ROOT / "profiles" / "k_fused_feopt_traffic.txt"
+    if tf.exists():
+        for line in tf.read_text().splitlines():
+            if line.startswith("bytes_per_launch"):
+                traffic = float(line.split("=")[1])
+    roof = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+            "frac": achieved / peak.value if achieved else None, "traffic": traffic,
+            "kernel": "k_fused (per-path signal, all leg counts, one persistent launch)",
+            "kernel_ms": kern_ms, "flops_per_launch": flops,
+            "peak_source": "measured on this GPU by fg_fp32_fma_peak (FFMA chains on every SM); "
+                           "MEASURED_PEAKS.json holds no FP32 figure"}
+
+    cpu = None
+    if rank == 0:
+        v, desc = cpu_sample(P, groups, budget_s=args.cpu_budget, nthreads=nthreads)
+        cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32 (complex chain) + fp64 (phase argument, sums)", "data": "synthetic",
+        "config": {"workload": f"Fe/O/Pt packing 3000 atoms, 2 Fe K absorbers per GPU, rmax 8 A, 2-8 legs, "
+                               f"{n_paths} paths per GPU, lmax 24 x {NK} k, chi on {NK} k",
+                   "paths_per_gpu": n_paths, "legs": batch.counts, "energies": stage.E, "nk": NK,
+                   "l2": "flushed between steps (256 MB write)", "parallelism": f"dp{world} (absorbers per rank)"},
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "fwd_bwd": fwd_bwd, "plain_fp64": plain,
+        "gpu_launches": 3 * args.steps, "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

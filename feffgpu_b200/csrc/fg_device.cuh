@@ -1,0 +1,244 @@
+// fg_device.cuh -- device-side building blocks of the B200 path stage.
+//
+// Work decomposition: one warp owns one path at a time; its lanes own 32 consecutive energies of the phase file's
+// real-axis grid and loop over the grid in chunks of 32.  Everything that depends on the path only (leg geometry,
+// rotation matrices, Euler phases) is computed once per path by the warp into its own shared-memory slice; the
+// energy-dependent work (spherical-wave recursions, scattering matrices, chain product, termination, cfac) runs
+// per lane in registers.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace fg {
+
+constexpr double kBohr = 0.52917721067;   // pad.py:13
+constexpr int kMaxLeg = 9;                 // pathfinder.py:26 (NLEG_MAX)
+constexpr int kLamTot = 15;                // genfmt.py:18
+
+// ------------------------------------------------------------------------------------------------ complex helpers
+template <typename R> struct C2 { R x, y; };
+
+template <typename R> __device__ __forceinline__ C2<R> cz() { return C2<R>{R(0), R(0)}; }
+template <typename R> __device__ __forceinline__ C2<R> cadd(C2<R> a, C2<R> b) { return C2<R>{a.x + b.x, a.y + b.y}; }
+template <typename R> __device__ __forceinline__ C2<R> csub(C2<R> a, C2<R> b) { return C2<R>{a.x - b.x, a.y - b.y}; }
+template <typename R> __device__ __forceinline__ C2<R> cmul(C2<R> a, C2<R> b)
+{
+    return C2<R>{fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x)};
+}
+template <typename R> __device__ __forceinline__ C2<R> cscl(C2<R> a, R r) { return C2<R>{a.x * r, a.y * r}; }
+template <typename R> __device__ __forceinline__ C2<R> cconj(C2<R> a) { return C2<R>{a.x, -a.y}; }
+// acc + a b
+template <typename R> __device__ __forceinline__ C2<R> cfma(C2<R> a, C2<R> b, C2<R> acc)
+{
+    return C2<R>{fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y))};
+}
+// acc - a b
+template <typename R> __device__ __forceinline__ C2<R> cfms(C2<R> a, C2<R> b, C2<R> acc)
+{
+    return C2<R>{fma(-a.x, b.x, fma(a.y, b.y, acc.x)), fma(-a.x, b.y, fma(-a.y, b.x, acc.y))};
+}
+// acc + a r
+template <typename R> __device__ __forceinline__ C2<R> cfmr(C2<R> a, R r, C2<R> acc)
+{
+    return C2<R>{fma(a.x, r, acc.x), fma(a.y, r, acc.y)};
+}
+// acc + conj(a) b
+template <typename R> __device__ __forceinline__ C2<R> cfmac(C2<R> a, C2<R> b, C2<R> acc)
+{
+    return C2<R>{fma(a.x, b.x, fma(a.y, b.y, acc.x)), fma(a.x, b.y, fma(-a.y, b.x, acc.y))};
+}
+template <typename R> __device__ __forceinline__ C2<R> cinv(C2<R> a)
+{
+    R d = R(1) / fma(a.x, a.x, a.y * a.y);
+    return C2<R>{a.x * d, -a.y * d};
+}
+// -i / rho, the argument of FEFF's spherical-wave factors (genfmt.py:210)
+template <typename R> __device__ __forceinline__ C2<R> zfac(C2<R> rho)
+{
+    R d = R(1) / fma(rho.x, rho.x, rho.y * rho.y);
+    return C2<R>{-rho.y * d, -rho.x * d};
+}
+
+// ------------------------------------------------------------------------------------------------ lambda sets
+// The lambda index sets of setlam (genfmt.py:115-153) in the order setlam leaves them: the laml0x entries that
+// reach the final state lead.  kind 0: K edge, two or more scatterers; 1: L and M edges, two or more scatterers
+// (iorder 2 gives the same six entries, all of them within the final state); 2/3/4: single scattering at K/L/M
+// edges (mmax = nmax = l_init + 1, FEFF's LAMTOT = 15 truncates the M set).
+struct LamTab {
+    int N, N0, MM, CI, CO;
+    int m[kLamTot], n[kLamTot];
+};
+
+__host__ __device__ constexpr LamTab lamtab(int kind)
+{
+    LamTab t{};
+    if (kind == 0 || kind == 1 || kind == 2) {
+        const int mK[6] = {0, -1, 1, 0, -2, 2}, nK[6] = {0, 0, 0, 1, 0, 0};
+        const int mL[6] = {0, -1, 1, -2, 2, 0}, nL[6] = {0, 0, 0, 0, 0, 1};
+        const int mS[6] = {0, -1, 1, 0, -1, 1}, nS[6] = {0, 0, 0, 1, 1, 1};
+        t.N = 6;
+        t.N0 = kind == 0 ? 4 : 6;
+        for (int i = 0; i < 6; ++i) {
+            t.m[i] = kind == 0 ? mK[i] : (kind == 1 ? mL[i] : mS[i]);
+            t.n[i] = kind == 0 ? nK[i] : (kind == 1 ? nL[i] : nS[i]);
+        }
+    } else {
+        const int mmax = kind == 3 ? 2 : 3;
+        int c = 0;
+        for (int n = 0; n <= mmax && c < kLamTot; ++n)
+            for (int m = 0; m <= mmax && c < kLamTot; ++m) {
+                if (2 * n + m > 3 * (kind - 1)) continue;
+                t.m[c] = -m; t.n[c] = n; ++c;
+                if (m == 0 || c >= kLamTot) continue;
+                t.m[c] = m; t.n[c] = n; ++c;
+            }
+        t.N = c;
+        t.N0 = c;
+    }
+    t.MM = 0; t.CI = 0; t.CO = 0;
+    for (int i = 0; i < t.N; ++i) {
+        int am = t.m[i] < 0 ? -t.m[i] : t.m[i];
+        if (am > t.MM) t.MM = am;
+        if (am + t.n[i] + 1 > t.CI) t.CI = am + t.n[i] + 1;
+        if (t.n[i] + 1 > t.CO) t.CO = t.n[i] + 1;
+    }
+    return t;
+}
+
+__host__ __device__ constexpr bool canonical(int m1, int m2) { return m1 > 0 || (m1 == 0 && m2 >= 0); }
+// Canonical (m1, m2) pairs are stored; d_{-m1,-m2} = (-1)^(m1-m2) d_{m1,m2} gives the others.
+__host__ __device__ constexpr int dcanon(int MM, int m1, int m2)
+{
+    return m1 == 0 ? m2 : (MM + 1) + (m1 - 1) * (2 * MM + 1) + (m2 + MM);
+}
+__host__ __device__ constexpr int ncanon(int MM) { return (MM + 1) + MM * (2 * MM + 1); }
+__host__ __device__ constexpr int dstride(int MM) { return MM <= 2 ? 16 : 32; }
+
+// Representatives of the scattering-matrix entries (lam1 < NR, lam2 < NC) under the flip (m1, m2) -> (-m1, -m2):
+// the pre-phase matrix obeys F~[flip] = (-1)^(m1-m2) F~ because the spherical-wave factors depend on |m| only and
+// the rotation matrix has that symmetry; only canonical entries are accumulated.
+template <int KIND, int NR, int NC> struct RepTab {
+    int n;
+    int a[kLamTot * kLamTot], b[kLamTot * kLamTot], d[kLamTot * kLamTot], ci[kLamTot * kLamTot],
+        co[kLamTot * kLamTot];
+    int rep[kLamTot][kLamTot], sg[kLamTot][kLamTot];
+    __host__ __device__ constexpr RepTab() : n(0), a{}, b{}, d{}, ci{}, co{}, rep{}, sg{}
+    {
+        const LamTab L = lamtab(KIND);
+        for (int i = 0; i < NR; ++i)
+            for (int j = 0; j < NC; ++j)
+                if (canonical(L.m[i], L.m[j])) {
+                    const int am = L.m[i] < 0 ? -L.m[i] : L.m[i];
+                    a[n] = i; b[n] = j; d[n] = dcanon(L.MM, L.m[i], L.m[j]);
+                    ci[n] = am + L.n[i] + 1; co[n] = L.n[j] + 1;
+                    rep[i][j] = n; sg[i][j] = 1;
+                    ++n;
+                }
+        for (int i = 0; i < NR; ++i)
+            for (int j = 0; j < NC; ++j)
+                if (!canonical(L.m[i], L.m[j])) {
+                    int fi = 0, fj = 0;
+                    for (int k = 0; k < L.N; ++k) {
+                        if (L.m[k] == -L.m[i] && L.n[k] == L.n[i]) fi = k;
+                        if (L.m[k] == -L.m[j] && L.n[k] == L.n[j]) fj = k;
+                    }
+                    rep[i][j] = rep[fi][fj];
+                    sg[i][j] = ((L.m[i] - L.m[j]) & 1) ? -1 : 1;
+                }
+    }
+};
+
+// ------------------------------------------------------------------------------------------------ stage tables
+// Device tables of one phase file (built by fg_stage_create).
+template <typename R> struct Tables {
+    int E, nph1, L1, nterm, MMd;
+    int term_l[2];              // l of the termination terms (distinct final-state l of bcoef, genfmt.py:230)
+    const C2<R> *tl;            // (nph1, L1+1, E) j-averaged t-matrix, index il = l + 1 (stage.py:111-118)
+    const int *lmax;            // (nph1, E)
+    const C2<R> *ck;            // (E) complex momentum, bohr^-1
+    const double2 *dk;          // (E) ck - xk in FP64 (the cfac argument, stage.py:336-337)
+    const C2<R> *wt;            // (nterm, E) sum over k with lind_k = l of bdiag_k rkk_k^2 (mmtrxi, genfmt.py:378)
+    const double *xfac;         // (L1+2, 7, 7) xnlm(il,|m1|+1) (-1)^|m1| / xnlm(il,|m2|+1), 0 where |m| >= il
+    const double *xnlm;         // (L1+2, 8) Legendre normalisation, snlm (genfmt.py:41-53)
+    const double *rc;           // (L1+1, 7, 7, 3) three-term recursion coefficients for d^{l+1} (stage.py:80-86)
+};
+
+// ------------------------------------------------------------------------------------------------ geometry
+// trig.f, as stage.py:148-157 and genfmt.py:56-69
+__device__ __forceinline__ void trig(double x, double y, double z, double &ct, double &st, double &cp, double &sp)
+{
+    const double r = sqrt(x * x + y * y + z * z), rxy = sqrt(x * x + y * y);
+    const bool sr = r < 1e-6, sxy = rxy < 1e-6;
+    ct = sr ? 1.0 : z / r;
+    st = sr ? 0.0 : rxy / r;
+    cp = sxy ? (ct < 0 ? -1.0 : 1.0) : x / rxy;
+    sp = sxy ? 0.0 : y / rxy;
+}
+
+// arg with FEFF's 1e-6 thresholds (stage.py:160-168)
+__device__ __forceinline__ double arg_fi(double x, double y, double fi)
+{
+    x = fabs(x) < 1e-6 ? 0.0 : x;
+    y = fabs(y) < 1e-6 ? 0.0 : y;
+    return (x == 0.0 && y == 0.0) ? fi : atan2(y, x);
+}
+
+// Leg j (1-based) of a path: length (bohr), scattering angle beta and the Euler angles alpha, gamma
+// (pathgeom, stage.py:170-206).  rat(j) returns atom j in bohr; atom 0 and atom nleg are the absorber.
+struct LegGeom { double ri, beta, alpha, gamma; };
+
+template <class Rat> __device__ __forceinline__ LegGeom leg_geometry(const Rat &rat, int j, int nleg)
+{
+    const int nsc = nleg - 1;
+    int i, ip1, im1;
+    if (j == nsc + 1) { i = 0; ip1 = 1; im1 = nsc; } else { i = j; ip1 = j + 1; im1 = j - 1; }
+    double ai[3], bi[3], ci[3];
+    rat(i, ai); rat(ip1, bi); rat(im1, ci);
+    double ctp, stp, cpp, spp, ct, st, cp, sp;
+    trig(bi[0] - ai[0], bi[1] - ai[1], bi[2] - ai[2], ctp, stp, cpp, spp);
+    trig(ai[0] - ci[0], ai[1] - ci[1], ai[2] - ci[2], ct, st, cp, sp);
+    const double cppp = cp * cpp + sp * spp, sppp = spp * cp - cpp * sp;
+    const double phi = atan2(sp, cp), phip = atan2(spp, cpp);
+    const double ax = -(st * ctp - ct * stp * cppp), ay = stp * sppp;
+    double b = ct * ctp + st * stp * cppp;
+    b = fmin(1.0, fmax(-1.0, b));
+    const double u1x = st * cp, u1y = st * sp, u1z = ct, u2x = stp * cpp, u2y = stp * spp, u2z = ctp;
+    const double wx = u1y * u2z - u1z * u2y, wy = u1z * u2x - u1x * u2z, wz = u1x * u2y - u1y * u2x;
+    const double sb2 = wx * wx + wy * wy + wz * wz;
+    const double gx = -(st * ctp * cppp - ct * stp), gy = -st * sppp;
+    const double a_j = arg_fi(ax, ay, phip - phi);
+    const double g_j = arg_fi(gx, gy, 0.0);
+    LegGeom g;
+    g.alpha = M_PI - g_j;
+    g.gamma = M_PI - a_j;
+    g.beta = atan2(sqrt(sb2 + 1e-30), b);
+    const double dx = ai[0] - ci[0], dy = ai[1] - ci[1], dz = ai[2] - ci[2];
+    g.ri = sqrt(dx * dx + dy * dy + dz * dz);
+    return g;
+}
+
+// ------------------------------------------------------------------------------------------------ rotation matrices
+// d^l_{mn}(beta) for l <= 3 from Wigner's explicit sum (the seeds; stage.py:26-38 and the closed forms of
+// stage.py:52-76 are its l = 1, 2 cases).
+__device__ __forceinline__ double wigner_small(int l, int m, int n, double c2, double s2)
+{
+    if (abs(m) > l || abs(n) > l) return 0.0;
+    const double f[8] = {1, 1, 2, 6, 24, 120, 720, 5040};
+    const double pref = sqrt(f[l + m] * f[l - m] * f[l + n] * f[l - n]);
+    double out = 0.0;
+    for (int k = 0; k <= 2 * l; ++k) {
+        const int a = l + n - k, b = k, c = m - n + k, d = l - m - k;
+        if (a < 0 || b < 0 || c < 0 || d < 0) continue;
+        double term = pref / (f[a] * f[b] * f[c] * f[d]);
+        if ((m - n + k) & 1) term = -term;
+        const int pc = 2 * l + n - m - 2 * k, ps = m - n + 2 * k;
+        double pw = 1.0;
+        for (int q = 0; q < pc; ++q) pw *= c2;
+        for (int q = 0; q < ps; ++q) pw *= s2;
+        out += term * pw;
+    }
+    return out;
+}
+
+}  // namespace fg

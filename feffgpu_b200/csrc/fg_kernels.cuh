@@ -1,0 +1,303 @@
+// fg_kernels.cuh -- forward kernels and their launches (included by the fg_inst_*.cu translation units).
+#pragma once
+#include <algorithm>
+#include <string>
+
+#include "fg_forward.cuh"
+#include "fg_launch.h"
+
+namespace fg {
+
+template <typename R> __host__ __device__ constexpr size_t geo_bytes() { return (sizeof(WarpPath<R>) + 15) / 16 * 16; }
+
+// Per-warp shared memory: the path state, the rotation tables of nsc legs and (fused kernels) the path's signal
+// and unwrapped phase.
+template <typename R> inline size_t warp_bytes(int L1, int nsc_max, int MM, int E, bool with_signal)
+{
+    size_t b = geo_bytes<R>() + align_up((size_t)nsc_max * (L1 + 1) * dstride(MM) * sizeof(R), 16);
+    if (with_signal) b += align_up((size_t)E * sizeof(C2<R>), 16) + align_up((size_t)E * sizeof(double), 16);
+    return b;
+}
+
+template <int EDGE> struct Kinds {
+    static constexpr int MS = EDGE == 1 ? 0 : 1;
+    static constexpr int SS = EDGE + 1;
+    static constexpr int MMMS = lamtab(MS).MM;
+    static constexpr int MMSS = lamtab(SS).MM;
+    static constexpr int MM = MMMS > MMSS ? MMMS : MMSS;
+};
+
+template <typename R, int EDGE>
+__device__ __forceinline__ C2<R> path_energy(const WarpPath<R> &g, const R *dh, const Tables<R> &T, int e, int nleg)
+{
+    using K = Kinds<EDGE>;
+    if (nleg == 2) {
+        if constexpr (EDGE == 1)
+            return energy_ss_sym<R, K::SS>(g, dh, T, e);
+        else
+            return energy_ss_col<R, K::SS>(g, dh, T, e);
+    }
+    return energy_ms<R, K::MS>(g, dh, T, e, nleg);
+}
+
+// One warp per path, grid-stride over the paths of one leg count: cchi (B, E) and reff (B).
+template <typename R, int EDGE, typename CT>
+__global__ void __launch_bounds__(256) k_cchi(Tables<R> T, const CT *__restrict__ coords,
+                                               const int64_t *__restrict__ ipots, int64_t B, int nleg,
+                                               C2<R> *__restrict__ out, R *__restrict__ reff, int *bad, size_t wbytes)
+{
+    using K = Kinds<EDGE>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    unsigned char *base = smem + (size_t)w * wbytes;
+    WarpPath<R> &g = *reinterpret_cast<WarpPath<R> *>(base);
+    R *dh = reinterpret_cast<R *>(base + geo_bytes<R>());
+    const int E = T.E;
+    const int MM = nleg == 2 ? K::MMSS : K::MMMS;
+    for (int64_t p = (int64_t)blockIdx.x * nw + w; p < B; p += (int64_t)gridDim.x * nw) {
+        path_setup<R, CT>(g, dh, T, coords + p * nleg * 3, ipots + p * nleg, nleg, lane, bad, MM);
+        for (int e0 = 0; e0 < E; e0 += 32) {
+            const int e = e0 + lane;
+            if (e < E) out[p * E + e] = path_energy<R, EDGE>(g, dh, T, e, nleg);
+        }
+        if (lane == 0) reff[p] = (R)(g.reff * kBohr);
+        __syncwarp();
+    }
+}
+
+// Amplitude and unwrapped phase of one path's signal (stage.py:366-370, 380-384), one warp: differences brought
+// into (-pi, pi] with round-half-even (torch.round) and summed in FP64.  amp may be null.
+template <typename R, class Load>
+__device__ __forceinline__ void amp_phase(int E, int lane, const Load &load, R *amp, double *pha)
+{
+    double carry = 0.0, prev_raw = 0.0;
+    for (int e0 = 0; e0 < E; e0 += 32) {
+        const int e = e0 + lane;
+        double a = 0.0, ang = 0.0;
+        if (e < E) {
+            const C2<R> c = load(e);
+            const double x = (double)c.x, y = (double)c.y;
+            a = sqrt(x * x + y * y + 1e-30);
+            ang = a >= 1e-16 ? atan2(y, x) : 0.0;
+        }
+        double prev = __shfl_up_sync(0xffffffffu, ang, 1);
+        if (lane == 0) prev = prev_raw;
+        double dlt = (e == 0 || e >= E) ? 0.0 : ang - prev;
+        dlt -= 6.283185307179586 * rint(dlt / 6.283185307179586);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double v = __shfl_up_sync(0xffffffffu, dlt, o);
+            if (lane >= o) dlt += v;
+        }
+        const double base = e0 == 0 ? __shfl_sync(0xffffffffu, ang, 0) : carry;
+        const double u = base + dlt;
+        if (e < E) {
+            if (amp) amp[e] = (R)a;
+            pha[e] = u;
+        }
+        carry = __shfl_sync(0xffffffffu, u, 31);
+        prev_raw = __shfl_sync(0xffffffffu, ang, 31);
+    }
+}
+
+// sin of an FP64 argument: FP64 for the plain form, FP64 range reduction then FP32 sine for the mixed form
+template <typename R> __device__ __forceinline__ double sin_arg(double arg)
+{
+    if constexpr (sizeof(R) == 4) {
+        arg -= 6.283185307179586 * rint(arg * 0.15915494309189535);
+        return (double)sinf((float)arg);
+    } else {
+        return sin(arg);
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_chi_fine(int64_t B, int E, const C2<R> *__restrict__ cchi,
+                                                   const R *__restrict__ reff, int NK, const R *__restrict__ q,
+                                                   const R *__restrict__ S, const int *__restrict__ span,
+                                                   R *__restrict__ chi, size_t wbytes)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    R *amp = reinterpret_cast<R *>(smem + (size_t)w * wbytes);
+    double *pha = reinterpret_cast<double *>(smem + (size_t)w * wbytes + align_up((size_t)E * sizeof(R), 16));
+    for (int64_t p = (int64_t)blockIdx.x * nw + w; p < B; p += (int64_t)gridDim.x * nw) {
+        const C2<R> *c = cchi + p * E;
+        amp_phase<R>(E, lane, [&](int e) { return c[e]; }, amp, pha);
+        __syncwarp();
+        const double rf = (double)reff[p];
+        for (int k0 = 0; k0 < NK; k0 += 32) {
+            const int k = k0 + lane;
+            if (k < NK) {
+                const int lo = span[2 * k], hi = span[2 * k + 1];
+                double a = 0.0, ph = 0.0;
+                for (int j = lo; j < hi; ++j) {
+                    const double sv = (double)S[(size_t)k * E + j];
+                    a += sv * (double)amp[j];
+                    ph += sv * pha[j];
+                }
+                chi[p * NK + k] = (R)(a * sin_arg<R>(ph + 2.0 * (double)q[k] * rf));
+            }
+        }
+        __syncwarp();
+    }
+}
+
+struct PathsDev {
+    int64_t n;
+    int nleg_max;
+    const double *coords;
+    const int64_t *ipots;
+    const int *nleg;
+    const double *deg;
+    const double *sigma2;
+    const int *order;
+};
+
+// Fused forward: every path of the batch, all leg counts, from one work queue (costliest first); per path the
+// signal at all E, its amplitude and unwrapped phase, and the weighted fine-grid terms
+// deg exp(-2 sigma2 q^2) a(q) sin(phi(q) + 2 q reff) for the deterministic reduction that follows.
+template <typename R, int EDGE>
+__global__ void __launch_bounds__(256) k_fused(Tables<R> T, PathsDev P, int NK, const double *__restrict__ q,
+                                                const double *__restrict__ S, const int *__restrict__ span,
+                                                double *__restrict__ terms, C2<R> *__restrict__ cchi_save,
+                                                double *__restrict__ reff_save, unsigned long long *counter, int *bad,
+                                                int nsc_max, size_t wbytes)
+{
+    using K = Kinds<EDGE>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int E = T.E, L1 = T.L1;
+    unsigned char *base = smem + (size_t)w * wbytes;
+    WarpPath<R> &g = *reinterpret_cast<WarpPath<R> *>(base);
+    R *dh = reinterpret_cast<R *>(base + geo_bytes<R>());
+    unsigned char *sig = base + geo_bytes<R>() + align_up((size_t)nsc_max * (L1 + 1) * dstride(K::MM) * sizeof(R), 16);
+    C2<R> *cbuf = reinterpret_cast<C2<R> *>(sig);
+    double *pha = reinterpret_cast<double *>(sig + align_up((size_t)E * sizeof(C2<R>), 16));
+    for (;;) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(counter, 1ull);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= (unsigned long long)P.n) break;
+        const int64_t p = P.order[t];
+        const int nleg = P.nleg[p];
+        path_setup<R, double>(g, dh, T, P.coords + p * P.nleg_max * 3, P.ipots + p * P.nleg_max, nleg, lane, bad,
+                              nleg == 2 ? K::MMSS : K::MMMS);
+        for (int e0 = 0; e0 < E; e0 += 32) {
+            const int e = e0 + lane;
+            if (e < E) {
+                const C2<R> v = path_energy<R, EDGE>(g, dh, T, e, nleg);
+                cbuf[e] = v;
+                if (cchi_save) cchi_save[p * E + e] = v;
+            }
+        }
+        __syncwarp();
+        amp_phase<R>(E, lane, [&](int e) { return cbuf[e]; }, static_cast<R *>(nullptr), pha);
+        __syncwarp();
+        const double rf = g.reff * kBohr, wdeg = P.deg[p], s2 = P.sigma2 ? P.sigma2[p] : 0.0;
+        for (int k0 = 0; k0 < NK; k0 += 32) {
+            const int k = k0 + lane;
+            if (k < NK) {
+                const int lo = span[2 * k], hi = span[2 * k + 1];
+                double a = 0.0, ph = 0.0;
+                for (int j = lo; j < hi; ++j) {
+                    const double sv = S[(size_t)k * E + j];
+                    const C2<R> c = cbuf[j];
+                    a += sv * sqrt((double)c.x * c.x + (double)c.y * c.y + 1e-30);
+                    ph += sv * pha[j];
+                }
+                const double qk = q[k];
+                terms[p * NK + k] = wdeg * a * sin_arg<R>(ph + 2.0 * qk * rf) * exp(-2.0 * s2 * qk * qk);
+            }
+        }
+        if (lane == 0 && reff_save) reff_save[p] = rf;
+        __syncwarp();
+    }
+}
+
+template <typename KernelT>
+inline fg_status grid_for(KernelT kern, int threads, size_t smem, int num_sms, int64_t work_warps, int &blocks)
+{
+    if (smem > 48 * 1024) FG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    FG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    if (per_sm < 1) return fail(FG_ERR_VALUE, "the kernel does not fit on an SM (shared memory " + std::to_string(smem) + " B)");
+    const int64_t need = (work_warps + threads / 32 - 1) / (threads / 32);
+    blocks = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)per_sm * num_sms));
+    return FG_OK;
+}
+
+template <typename R, int EDGE>
+fg_status Launch<R, EDGE>::cchi(const StageView &sv, const Tables<R> &T, int64_t B, int nleg, const void *coords,
+                                int coords_f64, const int64_t *ipots, void *cchi, void *reff, int *bad, int warps,
+                                cudaStream_t st)
+{
+    using K = Kinds<EDGE>;
+    const int threads = warps * 32;
+    const int MM = nleg == 2 ? K::MMSS : K::MMMS;
+    const size_t wb = warp_bytes<R>(sv.L1, nleg - 1, MM, sv.E, false);
+    const size_t smem = wb * warps;
+    int blocks = 0;
+    if (coords_f64) {
+        auto kern = k_cchi<R, EDGE, double>;
+        if (fg_status rc = grid_for(kern, threads, smem, sv.num_sms, B, blocks)) return rc;
+        timer_begin(st);
+        kern<<<blocks, threads, smem, st>>>(T, static_cast<const double *>(coords), ipots, B, nleg,
+                                            static_cast<C2<R> *>(cchi), static_cast<R *>(reff), bad, wb);
+    } else {
+        auto kern = k_cchi<R, EDGE, float>;
+        if (fg_status rc = grid_for(kern, threads, smem, sv.num_sms, B, blocks)) return rc;
+        timer_begin(st);
+        kern<<<blocks, threads, smem, st>>>(T, static_cast<const float *>(coords), ipots, B, nleg,
+                                            static_cast<C2<R> *>(cchi), static_cast<R *>(reff), bad, wb);
+    }
+    timer_end(st);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+template <typename R, int EDGE>
+fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const fg_paths *P, int NK, const double *q,
+                                 const double *S, const int *span, double *rows, void *cchi_save, double *reff_save,
+                                 unsigned char *ws, int warps, cudaStream_t st)
+{
+    using K = Kinds<EDGE>;
+    unsigned long long *counter = reinterpret_cast<unsigned long long *>(ws);
+    int *bad = reinterpret_cast<int *>(ws + 64);
+    double *terms = reinterpret_cast<double *>(ws + kCounterBytes);
+    double *partial = reinterpret_cast<double *>(ws + kCounterBytes + align_up((size_t)P->n * NK * sizeof(double), 256));
+    FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes, st));
+    if (P->n > 0) {
+        const int threads = warps * 32;
+        const int nsc_max = P->nleg_max - 1;
+        const size_t wb = warp_bytes<R>(sv.L1, nsc_max, K::MM, sv.E, true);
+        auto kern = k_fused<R, EDGE>;
+        int blocks = 0;
+        if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, P->n, blocks)) return rc;
+        PathsDev pd{P->n, P->nleg_max, P->coords, P->ipots, P->nleg, P->deg, P->sigma2, P->order};
+        timer_begin(st);
+        kern<<<blocks, threads, wb * warps, st>>>(T, pd, NK, q, S, span, terms, static_cast<C2<R> *>(cchi_save),
+                                                  reff_save, counter, bad, nsc_max, wb);
+        timer_end(st);
+        FG_CUDA(cudaGetLastError());
+    }
+    return launch_reductions(P, NK, terms, partial, rows, st);
+}
+
+template <typename R>
+fg_status LaunchCommon<R>::chi_fine(const StageView &sv, int64_t B, const void *cchi, const void *reff, int NK,
+                                    const void *q, const void *S, const int *span, void *chi, cudaStream_t st)
+{
+    const int warps = 8, threads = warps * 32;
+    const size_t wb = align_up((size_t)sv.E * sizeof(R), 16) + align_up((size_t)sv.E * sizeof(double), 16);
+    auto kern = k_chi_fine<R>;
+    int blocks = 0;
+    if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;
+    kern<<<blocks, threads, wb * warps, st>>>(B, sv.E, static_cast<const C2<R> *>(cchi), static_cast<const R *>(reff),
+                                              NK, static_cast<const R *>(q), static_cast<const R *>(S), span,
+                                              static_cast<R *>(chi), wb);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+}  // namespace fg

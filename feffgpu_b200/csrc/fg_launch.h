@@ -1,0 +1,68 @@
+// fg_launch.h -- host-side interface between the C ABI (fg_api.cu) and the kernel translation units
+// (fg_inst_*.cu, one per precision and initial-state class, compiled in parallel).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "feffgpu_b200.h"
+#include "fg_device.cuh"
+
+namespace fg {
+
+fg_status fail(fg_status s, const std::string &m);  // records the message for fg_last_error (fg_api.cu)
+
+__host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+constexpr size_t kCounterBytes = 256;   // head of every fused workspace: work-queue counters and flags
+
+// What the launches need to know about a stage.
+struct StageView {
+    int E, L1, nph1, num_sms, ilinit;
+};
+
+// Per precision R and initial-state class EDGE (l_init + 1 = 1, 2, 3: K/L1, L2/L3/M2/M3, M4/M5/N4/N5 edges).
+template <typename R, int EDGE> struct Launch {
+    static fg_status cchi(const StageView &sv, const Tables<R> &T, int64_t B, int nleg, const void *coords,
+                          int coords_f64, const int64_t *ipots, void *cchi, void *reff, int *bad, int warps,
+                          cudaStream_t st);
+    static fg_status fused(const StageView &sv, const Tables<R> &T, const fg_paths *P, int NK, const double *q,
+                           const double *S, const int *span, double *rows, void *cchi_save, double *reff_save,
+                           unsigned char *ws, int warps, cudaStream_t st);
+    static fg_status cchi_bwd(const StageView &sv, const Tables<R> &T, int64_t B, int nleg, const void *coords,
+                              int coords_f64, const int64_t *ipots, const void *grad_cchi, const void *grad_reff,
+                              void *grad_coords, unsigned char *ws, int warps, cudaStream_t st);
+    static fg_status fused_bwd(const StageView &sv, const Tables<R> &T, const fg_paths *P, int NK, const double *q,
+                               const double *S, const int *span, const double *grad_rows, const void *cchi_saved,
+                               const double *reff_saved, double *grad_coords, double *grad_sigma2, unsigned char *ws,
+                               int warps, cudaStream_t st);
+};
+
+// Precision-only launches (no lambda-set dependence).
+template <typename R> struct LaunchCommon {
+    static fg_status chi_fine(const StageView &sv, int64_t B, const void *cchi, const void *reff, int NK,
+                              const void *q, const void *S, const int *span, void *chi, cudaStream_t st);
+    static fg_status chi_fine_bwd(const StageView &sv, int64_t B, const void *cchi, const void *reff, int NK,
+                                  const void *q, const void *S, const int *span, const void *grad_chi,
+                                  void *grad_cchi, void *grad_reff, cudaStream_t st);
+};
+
+// Fused reduction kernels (precision independent, FP64).
+fg_status launch_reductions(const fg_paths *P, int NK, const double *terms, double *partial, double *rows,
+                            cudaStream_t st);
+
+// Events around the main kernel of a call when kernel timing is on (fg_set_kernel_timing)
+void timer_begin(cudaStream_t st);
+void timer_end(cudaStream_t st);
+
+size_t fused_workspace(const fg_paths *P, int NK);
+size_t fused_bwd_workspace(const fg_paths *P, int NK);
+size_t cchi_bwd_workspace(int64_t B, int nleg);
+
+}  // namespace fg
+
+#define FG_CUDA(call)                                                                                         \
+    do {                                                                                                      \
+        cudaError_t e_ = (call);                                                                              \
+        if (e_ != cudaSuccess) return ::fg::fail(FG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)

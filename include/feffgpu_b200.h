@@ -1,0 +1,170 @@
+/*
+ * feffgpu_b200.h -- C ABI of the B200 path stage.
+ *
+ * The library evaluates the Rehr-Albers path stage of FEFF 8.5L (as nmarcella/feffGPU implements it in
+ * src/feffgpu/stage.py:96-388) on an sm_100a GPU: per-path complex signals on the phase file's real-axis
+ * energy grid, the fine-grid signal, and the degeneracy-weighted sum of paths into rows of chi(k), with the
+ * hand-written adjoints of all three.
+ *
+ * Conventions shared by every entry point:
+ *   - device pointers for arrays, host pointers for the phase description; no allocation on the caller's behalf
+ *     beyond the stage's own tables (fg_stage_create) -- scratch memory is passed in as `workspace`;
+ *   - `stream` is a cudaStream_t (NULL = the legacy default stream); every call is asynchronous on it;
+ *   - coordinates are in angstrom, absorber first (translation invariant), shape (B, nleg, 3), row-major;
+ *   - complex arrays are interleaved (re, im) of the precision's real type;
+ *   - precision FG_MIXED: complex64 outputs (the reference's torch.complex64 mode), FP32 scattering-matrix chain,
+ *     FP64 geometry, FP64 2kR + phase argument and FP64 cross-path sums; FG_FP64: complex128 throughout;
+ *   - every entry point returns an fg_status; fg_last_error() gives a message for the calling thread.
+ */
+#ifndef FEFFGPU_B200_H
+#define FEFFGPU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FG_API __attribute__((visibility("default")))
+#else
+#define FG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fg_status {
+    FG_OK = 0,
+    FG_ERR_VALUE = 1,           /* bad argument: maps to ValueError (genfmt.py:151-152 raises it for lambda sets) */
+    FG_ERR_NOT_IMPLEMENTED = 2, /* nsp != 1 (stage.py:99-100), icalc >= 10 (genfmt.py:123): NotImplementedError */
+    FG_ERR_CUDA = 3,            /* a CUDA runtime error: RuntimeError */
+    FG_ERR_WORKSPACE = 4        /* workspace too small: ValueError */
+} fg_status;
+
+typedef enum fg_precision { FG_MIXED = 0, FG_FP64 = 1 } fg_precision;
+
+/* Phase tables of one FEFF phase file, host memory (src/feffgpu/pad.py:69-121, PhaseData).  Only the first
+ * ne1 (real-axis) energies and spin 0 are read, as GPUPathStage does. */
+typedef struct fg_phase_desc {
+    int32_t ne1;          /* real-axis energies E */
+    int32_t nph;          /* unique potentials 0..nph */
+    int32_t ltot;         /* ph index offset: entry l + ltot holds l = -lmax0..lmax0 */
+    int32_t nsp;          /* spin channels; only 1 is supported */
+    int32_t ihole;        /* FEFF hole index (1 = K, 4 = L3, 9 = M5, ...) */
+    int32_t iorder;       /* lambda-set order, 2 by default (GPUPathStage's iorder) */
+    double edge;          /* edge energy (hartree), for xk */
+    const int32_t *lmax0; /* (nph+1) partial waves stored per potential */
+    const double *em;     /* (ne1) complex energies (hartree), interleaved */
+    const double *eref;   /* (ne1) complex energy reference of spin 0, interleaved */
+    const double *ph;     /* (ne1, 2*ltot+1, nph+1) complex phase shifts of spin 0, interleaved */
+    const double *rkk;    /* (ne1, 8) complex reduced matrix elements of spin 0, interleaved */
+} fg_phase_desc;
+
+typedef struct fg_stage fg_stage;
+
+typedef struct fg_stage_info {
+    int32_t E;            /* energies of the stage (ne1) */
+    int32_t L1;           /* largest lmax + 1 (GPUPathStage.L1, stage.py:105) */
+    int32_t nph;
+    int32_t kinit, ilinit;
+    int32_t lamx_ss, laml0x_ss;   /* lambda-set sizes of two-leg paths */
+    int32_t lamx_ms, laml0x_ms;   /* ... and of paths with two or more scatterers */
+    int32_t device;
+} fg_stage_info;
+
+/* Build the device tables of one phase file on `device` (replaces GPUPathStage.__init__, stage.py:97-125).
+ * Allocates the stage's tables (a few hundred KB) with cudaMalloc; fg_stage_destroy frees them. */
+FG_API fg_status fg_stage_create(const fg_phase_desc *desc, int device, fg_stage **out);
+FG_API void fg_stage_destroy(fg_stage *stage);
+FG_API fg_status fg_stage_get_info(const fg_stage *stage, fg_stage_info *info);
+/* lmax(ie, iph) as the stage uses it (pad.py:93-106), host output (E, nph+1). */
+FG_API fg_status fg_stage_lmax(const fg_stage *stage, int32_t *lmax_out);
+/* Real-axis momenta xk (E) in bohr^-1 (pad.py:111-115), host output. */
+FG_API fg_status fg_stage_xk(const fg_stage *stage, double *xk_out);
+
+/* Message of the last failed call on this thread ("" if none). */
+FG_API const char *fg_last_error(void);
+
+/* Per-path complex signal cchi (B, E) and effective half path length reff (B) in angstrom: replaces
+ * GPUPathStage.cchi (stage.py:235-338).  coords (B, nleg, 3) as float (coords_f64 = 0) or double; ipots (B, nleg)
+ * int64 with the absorber's potential first; 2 <= nleg <= 9.  cchi: complex64 (FG_MIXED) or complex128 (FG_FP64);
+ * reff: float or double likewise.  ipots outside 0..nph are clamped and reported through *bad_ipot if non-NULL
+ * (a device int32, left untouched when every index is valid). */
+FG_API fg_status fg_cchi(const fg_stage *stage, fg_precision prec, int64_t B, int32_t nleg, const void *coords,
+                  int32_t coords_f64, const int64_t *ipots, void *cchi, void *reff, int32_t *bad_ipot, void *stream);
+
+/* Adjoint of fg_cchi: grad_coords (B, nleg, 3) = d(loss)/d(coords) from grad_cchi (B, E) complex with PyTorch's
+ * convention d(loss)/d(Re) + i d(loss)/d(Im), and grad_reff (B) (may be NULL).  grad_coords has the precision's
+ * real type.  Recomputes the per-leg scattering matrices (no forward state is kept).  `workspace` must hold
+ * fg_cchi_backward_workspace(...) bytes. */
+FG_API size_t fg_cchi_backward_workspace(const fg_stage *stage, int64_t B, int32_t nleg);
+FG_API fg_status fg_cchi_backward(const fg_stage *stage, fg_precision prec, int64_t B, int32_t nleg, const void *coords,
+                           int32_t coords_f64, const int64_t *ipots, const void *grad_cchi, const void *grad_reff,
+                           void *grad_coords, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Fine-grid signal chi (B, NK) = a(q) sin(phi(q) + 2 q reff), with the amplitude and the unwrapped phase of cchi
+ * interpolated by S (NK, E): replaces GPUPathStage.chi_fine (stage.py:372-388).  S is dense in the precision's
+ * real type; span (NK, 2) int32 gives each row's non-zero column range [lo, hi) (the full row is always valid).
+ * q (NK) and reff (B) have the precision's real type. */
+FG_API fg_status fg_chi_fine(const fg_stage *stage, fg_precision prec, int64_t B, const void *cchi, const void *reff,
+                      int32_t NK, const void *q, const void *S, const int32_t *span, void *chi, void *stream);
+/* Adjoint of fg_chi_fine: grad_cchi (B, E) complex (PyTorch convention) and grad_reff (B) from grad_chi (B, NK). */
+FG_API fg_status fg_chi_fine_backward(const fg_stage *stage, fg_precision prec, int64_t B, const void *cchi,
+                               const void *reff, int32_t NK, const void *q, const void *S, const int32_t *span,
+                               const void *grad_chi, void *grad_cchi, void *grad_reff, void *stream);
+
+/* A batch of paths with mixed leg counts for the fused stage (one persistent launch over every leg count). */
+typedef struct fg_paths {
+    int64_t n;               /* paths */
+    int32_t nleg_max;        /* leg dimension of coords and ipots (<= 9) */
+    int32_t nrows;           /* output rows */
+    const double *coords;    /* (n, nleg_max, 3) angstrom, absorber first; legs past nleg[p] are ignored */
+    const int64_t *ipots;    /* (n, nleg_max) */
+    const int32_t *nleg;     /* (n) legs of each path, 2..9 */
+    const double *deg;       /* (n) degeneracy weight */
+    const double *sigma2;    /* (n) per-path sigma^2 in A^2, or NULL (no damping) */
+    const int32_t *row;      /* (n) output row of each path, 0..nrows-1 */
+    const int32_t *order;    /* (n) launch order: a permutation of 0..n-1, costliest paths first */
+    const int32_t *sorted;   /* (n) path indices grouped by row: the fixed summation order */
+    const int64_t *chunk_bounds; /* (nchunks+1) offsets into `sorted`; each chunk lies within one row */
+    const int64_t *row_chunks;   /* (nrows+1) offsets into the chunks: row r owns chunks row_chunks[r]..[r+1]-1 */
+    int64_t nchunks;
+} fg_paths;
+
+/* Workspace of the fused calls: a work-queue counter, per-path fine-grid terms and per-chunk partial sums. */
+FG_API size_t fg_chi_reduce_workspace(const fg_stage *stage, const fg_paths *paths, int32_t NK);
+
+/* rows (nrows, NK) FP64 = sum over paths p of deg_p exp(-2 sigma2_p q^2) chi_p(q), chi_p from cchi and chi_fine
+ * as above, summed in a fixed order (deterministic).  Fuses GPUPathStage.cchi + chi_fine with the reduction
+ * of the callers (chain.py:48-49, exafs/forward.py:162, md/spectrum.py:298).  q (NK), S (NK, E) and span as in
+ * fg_chi_fine but always FP64.  If cchi_save (n, E complex of the precision) and reff_save (n, FP64) are non-NULL
+ * the per-path signals are kept for fg_chi_reduce_backward. */
+FG_API fg_status fg_chi_reduce(const fg_stage *stage, fg_precision prec, const fg_paths *paths, int32_t NK, const double *q,
+                        const double *S, const int32_t *span, double *rows, void *cchi_save, double *reff_save,
+                        void *workspace, size_t workspace_bytes, void *stream);
+
+/* Adjoint of fg_chi_reduce: grad_coords (n, nleg_max, 3) FP64 and grad_sigma2 (n) FP64 (may be NULL) from
+ * grad_rows (nrows, NK), using the saved cchi and reff.  No reference counterpart for sigma^2 (a new input). */
+FG_API size_t fg_chi_reduce_backward_workspace(const fg_stage *stage, const fg_paths *paths, int32_t NK);
+FG_API fg_status fg_chi_reduce_backward(const fg_stage *stage, fg_precision prec, const fg_paths *paths, int32_t NK,
+                                 const double *q, const double *S, const int32_t *span, const double *grad_rows,
+                                 const void *cchi_saved, const double *reff_saved, double *grad_coords,
+                                 double *grad_sigma2, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Device timing of the library's main kernel (the per-path kernel of each call), for profiling and autotuning:
+ * while enabled, every call records CUDA events around its main kernel on the call's stream; fg_kernel_time_ms
+ * waits for the last recorded end event and returns the elapsed milliseconds. */
+FG_API fg_status fg_set_kernel_timing(int32_t enable);
+FG_API fg_status fg_kernel_time_ms(float *ms);
+
+/* Measured FP32 FMA throughput of this GPU (TFLOP/s): a calibration kernel of independent FFMA chains on every SM,
+ * timed with CUDA events on `stream` (the roofline denominator of the FP32 CUDA-core kernels). */
+FG_API fg_status fg_fp32_fma_peak(double *tflops, void *stream);
+
+/* Launch tuning (set by the autotuner): warps per block for the forward and the adjoint kernels (1..8),
+ * 0 = the built-in default. */
+FG_API fg_status fg_set_launch(int32_t fwd_warps, int32_t bwd_warps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FEFFGPU_B200_H */

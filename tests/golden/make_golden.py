@@ -1,0 +1,288 @@
+"""Generates the golden fixtures of tests/golden/ from the reference implementation (nmarcella/feffGPU).
+
+Run in a container where the reference is mounted (default /root/reference, or $FEFFGPU_REFERENCE):
+
+    python tests/golden/make_golden.py [--only NAME ...]
+
+The reference is imported read-only from its source tree and run on the CPU in FP64 (complex128).  Outputs are small
+.npz files; nothing at test time reads the reference itself.
+
+* case_<name>.npz -- for FEFF's seven stored cases (tests/data/W and data/validation/*): the phase tables the path
+  stage reads (first ne1 energies, l up to the largest lmax), FEFF's own path list (paths.dat) and chi (chi.dat),
+  the reference stage's chi on chi.dat's k grid from that path list, and its per-path cchi/reff for a few paths
+  of every leg count (the procedure of the reference's tests/test_xsph.py:85-123).
+* walks_W.npz -- 2- to 8-leg bcc lattice walks with the W phases and the reference stage's cchi (the procedure of
+  tests/test_pathfinder.py:193-230, seed 5).
+* grad_L001.npz, grad_A000.npz -- d(loss)/d(coords) of the reference stage under torch.utils.checkpoint
+  (use_reentrant=False, as src/feffgpu/exafs/forward.py:683 calls it), loss = sum_p deg_p sum_q w_q chi_p(q).
+* L001_phase.pad -- FEFF's phase.pad of the L001 case, copied as written by FEFF, for the reader's test.
+* cfg1_cu.npz -- the Cu fcc cluster (a = 3.61 A, 6 A radius, K edge) through the reference chain
+  (src/feffgpu/chain.py:16-51): phase tables, the path finder's paths (NLEG 4, RPATH 6, default importance cut) and chi on
+  k = 0..20 A^-1 step 0.05.
+* cfg2_phase.npz -- Fe K-edge phase tables (potentials Fe*, Fe, O, Pt, lmax 24) of a cluster cut from the seeded
+  3000-atom Fe/O/Pt packing, on FEFF's own energy grid; cfg2_sample.npz -- the reference stage's cchi on those
+  tables resampled to 401 k points, for a sample of synthetic paths.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+REF = Path(os.environ.get("FEFFGPU_REFERENCE", "/root/reference"))
+sys.path.insert(0, str(REF / "src"))
+sys.path.insert(0, str(REPO))
+
+import torch  # noqa: E402
+
+from feffgpu_b200.pad import phase_to_arrays, phase_from_npz, resample_phase  # noqa: E402
+from feffgpu_b200 import workloads as W  # noqa: E402
+
+CASES = {"W": REF / "tests/data/W", **{c: REF / "data/validation" / c for c in
+                                       ("A000", "A009", "A014", "A018", "L000", "L001")}}
+
+
+def parse_paths(fname):
+    """FEFF's paths.dat: (nleg, deg, coords absorber-first (nleg, 3), ipots (nleg,)) per path."""
+    lines = Path(fname).read_text().splitlines()
+    out, i = [], 2
+    while i < len(lines):
+        if "index, nleg" not in lines[i]:
+            i += 1
+            continue
+        w = lines[i].split()
+        nleg, deg = int(w[1]), float(w[2])
+        rows = [lines[i + 2 + j].split() for j in range(nleg)]
+        pts = np.array([[float(v) for v in r[:3]] for r in rows])
+        ip = [int(r[3]) for r in rows]
+        out.append((nleg, deg, np.concatenate([np.zeros((1, 3)), pts[:-1]]), np.array([0] + ip[:-1])))
+        i += 2 + nleg
+    return out
+
+
+def parse_chi(fname):
+    rows = [l.split() for l in Path(fname).read_text().splitlines() if l.strip() and not l.startswith("#")]
+    tab = np.array([[float(r[0]), float(r[1])] for r in rows if len(r) >= 2 and r[0].replace(".", "", 1).isdigit()])
+    return tab[:, 0], tab[:, 1]
+
+
+def ref_stage(P):
+    from feffgpu.stage import GPUPathStage
+    return GPUPathStage(P, device="cpu", dtype=torch.complex128)
+
+
+def make_case(name):
+    from feffgpu.pad import read_phase_pad
+    from feffgpu.compare import r_factor
+    d = CASES[name]
+    P = read_phase_pad(str(d / "phase.pad"))
+    paths = parse_paths(d / "paths.dat")
+    kf, chi_feff = parse_chi(d / "chi.dat")
+    if name == "W":
+        kf, chi_feff = kf[:601], chi_feff[:601]
+    pos = kf > 1e-9                      # the R-factor grid starts with an added k = 0 (tests/test_validation_cases.py:51)
+    kf, chi_feff = kf[pos], chi_feff[pos]
+    g = ref_stage(P)
+    S = g.linear_matrix(kf)
+    out = phase_to_arrays(P, prefix="ph_")
+    chi = np.zeros(len(kf))
+    with torch.no_grad():
+        for nleg in sorted({p[0] for p in paths}):
+            grp = [p for p in paths if p[0] == nleg]
+            coords = np.stack([p[2] for p in grp])
+            ipots = np.stack([p[3] for p in grp])
+            deg = np.array([p[1] for p in grp])
+            cc, rf = g.cchi(torch.tensor(coords, dtype=torch.float64), torch.tensor(ipots))
+            chi += (torch.tensor(deg)[:, None] * g.chi_fine(cc, rf, kf, S, "feff")).sum(0).numpy()
+            out[f"coords_{nleg}"] = coords
+            out[f"ipots_{nleg}"] = ipots
+            out[f"deg_{nleg}"] = deg
+            keep = min(4, len(grp))
+            out[f"ref_cchi_{nleg}"] = cc[:keep].numpy()
+            out[f"ref_reff_{nleg}"] = rf[:keep].numpy()
+    out["feff_k"], out["feff_chi"], out["ref_chi"] = kf, chi_feff, chi
+    k0 = np.concatenate([[0.0], kf])
+    z0 = lambda c: np.concatenate([[0.0], c])
+    inp = (d / "feff.inp").read_text().split()
+    rmax = 9.3 if name == "W" else float(inp[[w.upper() for w in inp].index("RPATH") + 1]) if "RPATH" in [w.upper() for w in inp] else 6.0
+    out["rmax"] = np.asarray(rmax)
+    out["R_ref_vs_feff"] = np.asarray(r_factor(k0, z0(chi_feff), z0(chi), kmin=3.0, kmax=float(min(23.0, kf.max() - 1.0)),
+                                               rmin=1.0, rmax=rmax))
+    np.savez_compressed(HERE / f"case_{name}.npz", **out)
+    print(name, "paths", len(paths), "R(ref, FEFF) = %.2e" % out["R_ref_vs_feff"])
+
+
+def lattice_walk(rng, nleg, a=3.1652, sd=0.06):
+    """A path of nleg legs over first and second neighbours of a bcc lattice, atoms displaced at random (an atom met
+    twice keeps its displacement; the absorber may be met again and stays at the origin)."""
+    steps = np.vstack([np.array([[i, j, l] for i in (-.5, .5) for j in (-.5, .5) for l in (-.5, .5)]),
+                       np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]])]) * a
+    while True:
+        site, sites = np.zeros(3), []
+        for _ in range(nleg - 1):
+            site = site + steps[rng.integers(len(steps))]
+            sites.append(site.copy())
+        if np.linalg.norm(sites[-1]) > 1e-6:
+            break
+    moved, shift = [np.zeros(3)], {}
+    for s in sites:
+        key = tuple(np.round(s, 3))
+        if np.linalg.norm(s) > 1e-6 and key not in shift:
+            shift[key] = rng.normal(0, sd, 3)
+        moved.append(s + shift.get(key, 0.0))
+    return np.array(moved), np.array([0] + [0 if np.linalg.norm(s) < 1e-6 else 1 for s in sites])
+
+
+def make_walks():
+    from feffgpu.pad import read_phase_pad
+    P = read_phase_pad(str(CASES["W"] / "phase.pad"))
+    g = ref_stage(P)
+    rng = np.random.default_rng(5)
+    out = {}
+    with torch.no_grad():
+        for nleg in range(2, 9):
+            cs, ips = zip(*[lattice_walk(rng, nleg) for _ in range(2)])
+            coords, ipots = np.stack(cs), np.stack(ips)
+            cc, rf = g.cchi(torch.tensor(coords), torch.tensor(ipots))
+            out[f"coords_{nleg}"], out[f"ipots_{nleg}"] = coords, ipots
+            out[f"ref_cchi_{nleg}"], out[f"ref_reff_{nleg}"] = cc.numpy(), rf.numpy()
+    np.savez_compressed(HERE / "walks_W.npz", **out)
+    print("walks_W written")
+
+
+def make_grad(name, nlegs=(2, 3, 4, 5, 6), per=3, seed=11):
+    """Reference gradients: the stage under checkpoint(use_reentrant=False) as the reference's callers use it."""
+    from feffgpu.pad import read_phase_pad
+    from torch.utils.checkpoint import checkpoint
+    P = read_phase_pad(str(CASES[name] / "phase.pad"))
+    g = ref_stage(P)
+    rng = np.random.default_rng(seed)
+    q = np.arange(1, 401) * 0.05
+    S = g.linear_matrix(q)
+    w = torch.tensor(rng.normal(0, 1, len(q)) * q ** 2 / 100.0)
+    out = {"q": q, "w": w.numpy()}
+    src = parse_paths(CASES[name] / "paths.dat")
+    for nleg in nlegs:
+        grp = [p for p in src if p[0] == nleg][:per]
+        if not grp:
+            continue
+        coords = np.stack([p[2] for p in grp]) + rng.normal(0, 0.02, (len(grp), nleg, 3)) * (np.arange(nleg) > 0)[None, :, None]
+        ipots = np.stack([p[3] for p in grp])
+        deg = np.array([p[1] for p in grp])
+        x = torch.tensor(coords, requires_grad=True)
+
+        def f(c):
+            cc, rf = g.cchi(c, torch.tensor(ipots))
+            return g.chi_fine(cc, rf, q, S, "feff")
+
+        chi = checkpoint(f, x, use_reentrant=False)
+        loss = (torch.tensor(deg)[:, None] * chi * w[None]).sum()
+        (gx,) = torch.autograd.grad(loss, x)
+        out[f"coords_{nleg}"], out[f"ipots_{nleg}"], out[f"deg_{nleg}"] = coords, ipots, deg
+        out[f"grad_{nleg}"], out[f"loss_{nleg}"] = gx.numpy(), np.asarray(float(loss.detach()))
+    out.update(phase_to_arrays(P, prefix="ph_"))
+    np.savez_compressed(HERE / f"grad_{name}.npz", **out)
+    print(f"grad_{name} written")
+
+
+def _write_inp(path, title, edge, potentials, atoms, extra=""):
+    lines = [f"TITLE {title}", "CONTROL 1 1 1 1 1 1", "PRINT 0 0 0 0 0 0", f"EDGE {edge}", "S02 1.0", extra, "",
+             "POTENTIALS"]
+    lines += [f"  {ip:4d} {z:4d}  {lab}" for ip, z, lab in potentials]
+    lines += ["", "ATOMS"]
+    lines += [f"  {x:12.6f} {y:12.6f} {z:12.6f}  {ip:d}" for (x, y, z), ip in atoms]
+    lines += ["END", ""]
+    Path(path).write_text("\n".join(lines))
+
+
+def make_cfg1(tmp):
+    """Cu fcc, a = 3.61 A, 6 A cluster, K edge, reference chain with its defaults (NLEG 4)."""
+    from feffgpu.chain import run
+    pts = W.fcc_cluster(3.61, 6.0)
+    inp = Path(tmp) / "cu_feff.inp"
+    _write_inp(inp, "Cu fcc a=3.61 cluster 6 A", "K", [(0, 29, "Cu"), (1, 29, "Cu")],
+               [(p, 0 if i == 0 else 1) for i, p in enumerate(pts)], "NLEG 4\nRPATH 6.0")
+    kf = np.arange(401) * 0.05
+    t = time.time()
+    res = run(str(inp), device="cpu", kgrid=kf)
+    out = phase_to_arrays(res["phase"], prefix="ph_")
+    for nleg, (coords, ipots, deg, xp, atoms) in res["kept"].items():
+        if coords.shape[0] == 0:
+            continue
+        out[f"coords_{nleg}"] = coords.cpu().numpy().astype(np.float64)
+        out[f"ipots_{nleg}"] = ipots.cpu().numpy()
+        out[f"deg_{nleg}"] = deg.cpu().numpy().astype(np.float64)
+    out["k"], out["ref_chi"] = kf, np.asarray(res["chi"])
+    out["natoms"] = np.asarray(len(pts))
+    np.savez_compressed(HERE / "cfg1_cu.npz", **out)
+    print("cfg1_cu: %d atoms, paths %s, %.1f s" % (len(pts), {k: int(v[0].shape[0]) for k, v in res["kept"].items()},
+                                                   time.time() - t))
+
+
+def make_cfg2(tmp):
+    """Fe/O/Pt phases (lmax 24) of a 6 A cluster cut around the central Fe of the seeded packing."""
+    from feffgpu.chain import run
+    pos, lab, box = W.random_packing(3000, 0.08, 1.8, seed=2024)
+    ab = int(W.central_atom(pos, box, lab, "Fe", 1)[0])
+    rel = pos - pos[ab]
+    rel -= box * np.round(rel / box)
+    r = np.linalg.norm(rel, axis=1)
+    sel = np.argsort(r, kind="stable")
+    sel = sel[r[sel] <= 6.0]
+    ipmap = {"Fe": 1, "O": 2, "Pt": 3}
+    atoms = [(rel[i], 0 if i == ab else ipmap[lab[i]]) for i in sel]
+    inp = Path(tmp) / "feopt_feff.inp"
+    _write_inp(inp, "Fe/O/Pt random packing, Fe K edge", "K", [(0, 26, "Fe"), (1, 26, "Fe"), (2, 8, "O"), (3, 78, "Pt")],
+               atoms, "NLEG 2\nRPATH 2.0\nEXAFS 20.5")
+    t = time.time()
+    res = run(str(inp), device="cpu", lmax_override=24)
+    P = res["phase"]
+    np.savez_compressed(HERE / "cfg2_phase.npz", **phase_to_arrays(P, prefix="ph_"))
+    print("cfg2_phase: %d atoms in the cluster, ne1 %d, lmax %d, %.1f s" % (len(sel), P.ne1, P.lmax[:P.ne1].max(),
+                                                                           time.time() - t))
+    # the reference stage on the resampled tables, for a sample of synthetic paths of every leg count
+    Q = resample_phase(phase_from_npz(np.load(HERE / "cfg2_phase.npz"), prefix="ph_"), np.arange(401) * 0.05)
+    g = ref_stage(Q)
+    ipot_of = np.array([ipmap[x] for x in lab])
+    paths = W.random_paths(pos, box, ab, {n: 3 for n in range(2, 9)}, rmax=8.0, seed=7, ipot_of=ipot_of)
+    out = {}
+    with torch.no_grad():
+        for nleg, (coords, ipots, _) in paths.items():
+            cc, rf = g.cchi(torch.tensor(coords), torch.tensor(ipots))
+            out[f"coords_{nleg}"], out[f"ipots_{nleg}"] = coords, ipots
+            out[f"ref_cchi_{nleg}"], out[f"ref_reff_{nleg}"] = cc.numpy(), rf.numpy()
+    np.savez_compressed(HERE / "cfg2_sample.npz", **out)
+    print("cfg2_sample written")
+
+
+def main():
+    import tempfile
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", nargs="*")
+    args = ap.parse_args()
+    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2"])
+    with tempfile.TemporaryDirectory() as tmp:
+        if "cases" in want:
+            import shutil
+            shutil.copyfile(CASES["L001"] / "phase.pad", HERE / "L001_phase.pad")
+            for name in CASES:
+                make_case(name)
+        if "walks" in want:
+            make_walks()
+        if "grad" in want:
+            make_grad("L001")
+            make_grad("A000", nlegs=(2, 3, 4), per=2)
+        if "cfg1" in want:
+            make_cfg1(tmp)
+        if "cfg2" in want:
+            make_cfg2(tmp)
+
+
+if __name__ == "__main__":
+    main()

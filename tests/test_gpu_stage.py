@@ -1,0 +1,191 @@
+"""GPU parity of the path stage against the oracle and the reference's golden outputs (runs on a B200).
+
+Tolerances (written here, checked here):
+  FP64 form (complex128): per-path cchi within 1e-10 of max|cchi| of the reference stage below k = 20 1/A (the
+    reference's own bar against its literal port is 1e-8, tests/test_pathfinder.py:226); chi R < 1e-12.
+  Mixed form (complex64): per-path cchi within 2e-5 of max|cchi|; chi R <= 1e-6 against the reference's FP64 chi
+    (the parity gate of the north-star target).
+  Both: FEFF's chi.dat to the reference's bars (R < 1e-9 for W, tests/test_xsph.py:122; R < 2e-5 otherwise,
+    tests/test_validation_cases.py:50).
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.fixtures import CASES, cfg2_phase, groups, npz, phase, r_window
+
+pytestmark = pytest.mark.gpu
+
+TOL_CCHI = {torch.complex128: 1e-10, torch.complex64: 2e-5}
+TOL_R = {torch.complex128: 1e-12, torch.complex64: 1e-6}
+DTYPES = [torch.complex128, torch.complex64]
+
+
+def _stage(P, dtype):
+    from feffgpu_b200 import GPUPathStage
+    return GPUPathStage(P, device="cuda", dtype=dtype)
+
+
+def _rel(a, b, sel=None):
+    a, b = np.asarray(a), np.asarray(b)
+    if sel is not None:
+        a, b = a[:, sel], b[:, sel]
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def _R(name, k, a, b):
+    k0 = np.concatenate([[0.0], k])
+    z0 = lambda c: np.concatenate([[0.0], c])
+    return O.r_factor(k0, z0(a), z0(b), **r_window(name, k))
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("case", CASES)
+def test_cchi_equals_reference_stage(case, dtype):
+    name = f"case_{case}"
+    P = phase(name)
+    st = _stage(P, dtype)
+    z = npz(name)
+    orc = O.Oracle(P)
+    low = orc.kgrid() < 20.0
+    for nleg, (coords, ipots, deg) in groups(name).items():
+        cc, rf = st.cchi(torch.tensor(coords), torch.tensor(ipots))
+        assert cc.dtype == dtype and rf.dtype == st.rdtype and cc.shape == (len(coords), st.E)
+        cc = cc.cpu().numpy()
+        k = min(4, len(coords))
+        e_ref = _rel(cc[:k], z[f"ref_cchi_{nleg}"], low)
+        oc, orf = orc.cchi(coords, ipots)
+        e_orc = _rel(cc, oc, low)
+        print(f"{case} nleg {nleg} {dtype}: vs reference {e_ref:.2e}, vs oracle {e_orc:.2e}")
+        assert e_ref < TOL_CCHI[dtype] and e_orc < TOL_CCHI[dtype], (nleg, e_ref, e_orc)
+        assert np.allclose(rf.cpu().numpy(), orf, rtol=1e-6 if dtype == torch.complex64 else 1e-12)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("case", CASES)
+def test_chi_equals_reference_and_feff(case, dtype):
+    """FEFF's own path list -> chi through cchi + chi_fine + degeneracy sum, as chain.run does (chain.py:45-49)."""
+    name = f"case_{case}"
+    st = _stage(phase(name), dtype)
+    z = npz(name)
+    kf = z["feff_k"]
+    S = st.linear_matrix(kf)
+    chi = torch.zeros(len(kf), dtype=torch.float64, device="cuda")
+    with torch.no_grad():
+        for nleg, (coords, ipots, deg) in groups(name).items():
+            cc, rf = st.cchi(torch.tensor(coords), torch.tensor(ipots))
+            chi += (torch.tensor(deg, device="cuda")[:, None] * st.chi_fine(cc, rf, kf, S, "feff").double()).sum(0)
+    chi = chi.cpu().numpy()
+    r_ref, r_feff = _R(name, kf, z["ref_chi"], chi), _R(name, kf, z["feff_chi"], chi)
+    print(f"{case} {dtype}: R(ref) {r_ref:.2e}  R(FEFF) {r_feff:.2e}")
+    assert r_ref <= TOL_R[dtype]
+    assert r_feff < (1e-9 if case == "W" else 2e-5)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_walks_two_to_eight_legs(dtype):
+    st = _stage(phase("case_W"), dtype)
+    z = npz("walks_W")
+    low = (st.xk.double().cpu().numpy() / 0.52917721067) < 20.0
+    for nleg in range(2, 9):
+        cc, rf = st.cchi(torch.tensor(z[f"coords_{nleg}"]), torch.tensor(z[f"ipots_{nleg}"]))
+        e = _rel(cc.cpu().numpy(), z[f"ref_cchi_{nleg}"], low)
+        print(f"walk nleg {nleg} {dtype}: {e:.2e}")
+        assert e < TOL_CCHI[dtype], (nleg, e)
+        assert np.allclose(rf.cpu().numpy(), z[f"ref_reff_{nleg}"], rtol=1e-6 if dtype == torch.complex64 else 1e-10)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_resampled_401k_tables(dtype):
+    """The Fe/O/Pt tables (lmax 24) resampled to 401 k points, paths of 2-8 legs, against the reference stage."""
+    st = _stage(cfg2_phase(), dtype)
+    z = npz("cfg2_sample")
+    for nleg in range(2, 9):
+        cc, rf = st.cchi(torch.tensor(z[f"coords_{nleg}"]), torch.tensor(z[f"ipots_{nleg}"]))
+        e = _rel(cc.cpu().numpy(), z[f"ref_cchi_{nleg}"])
+        print(f"cfg2 nleg {nleg} {dtype}: {e:.2e}")
+        assert e < TOL_CCHI[dtype], (nleg, e)
+
+
+def _batch_of(name, rows_of=None):
+    from feffgpu_b200 import PathBatch
+    gs = []
+    for nleg, (coords, ipots, deg) in groups(name).items():
+        row = None if rows_of is None else rows_of(len(coords))
+        gs.append((coords, ipots, deg, row))
+    return PathBatch(gs, device="cuda")
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("case", ["W", "A009", "A014", "L001"])
+def test_fused_chi_reduce(case, dtype):
+    """One persistent launch over all leg counts, fine grid and degeneracy sum: equals the oracle and the reference."""
+    name = f"case_{case}"
+    st = _stage(phase(name), dtype)
+    z = npz(name)
+    kf = z["feff_k"]
+    b = _batch_of(name)
+    rows = st.chi_reduce(b, kf)
+    assert rows.shape == (1, len(kf)) and rows.dtype == torch.float64
+    chi = rows[0].cpu().numpy()
+    r_ref = _R(name, kf, z["ref_chi"], chi)
+    print(f"fused {case} {dtype}: R(ref) {r_ref:.2e}")
+    assert r_ref <= TOL_R[dtype]
+    # deterministic: a second launch gives the same bits
+    assert torch.equal(rows, st.chi_reduce(b, kf))
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_fused_rows_and_sigma2(dtype):
+    """Paths spread over rows, with per-path sigma^2 damping exp(-2 sigma^2 q^2), against the oracle's FP64 sums."""
+    name = "case_A000"
+    P = phase(name)
+    st = _stage(P, dtype)
+    rng = np.random.default_rng(1)
+    b = _batch_of(name, rows_of=lambda n: rng.integers(0, 5, n))
+    s2 = rng.uniform(0, 0.01, b.n)
+    q = np.arange(1, 401) * 0.05
+    rows = st.chi_reduce(b, q, sigma2=torch.tensor(s2)).cpu().numpy()
+    orc = O.Oracle(P)
+    S = orc.linear_matrix(q)
+    coords, ipots, nleg = b.coords.cpu().numpy(), b.ipots.cpu().numpy(), b.nleg.cpu().numpy()
+    chi_p = np.zeros((b.n, len(q)))
+    for n in np.unique(nleg):
+        sel = np.nonzero(nleg == n)[0]
+        cc, rf = orc.cchi(coords[sel, :n], ipots[sel, :n])
+        chi_p[sel] = O.chi_fine(cc, rf, q, S)
+    ref = O.chi_rows(chi_p, b.deg.cpu().numpy(), b.row.cpu().numpy(), b.nrows, q, s2)
+    for r in range(b.nrows):
+        Rr = O.r_factor(np.concatenate([[0.0], q]), np.concatenate([[0.0], ref[r]]), np.concatenate([[0.0], rows[r]]),
+                        kmin=3, kmax=19, rmin=1, rmax=6)
+        assert Rr <= TOL_R[dtype], (r, Rr)
+    if dtype == torch.complex128:
+        assert np.abs(rows - ref).max() < 1e-10 * np.abs(ref).max()
+
+
+def test_edge_cases():
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    P = phase("case_L001")
+    st = GPUPathStage(P, device="cuda", dtype=torch.complex128)
+    cc, rf = st.cchi(torch.zeros(0, 3, 3), torch.zeros(0, 3, dtype=torch.long))
+    assert cc.shape == (0, st.E) and rf.shape == (0,)
+    with pytest.raises(IndexError):
+        st.cchi(torch.tensor([[[0, 0, 0], [1.5, 0, 0.2]]]), torch.tensor([[0, 7]]))
+    with pytest.raises(ValueError):
+        st.cchi(torch.zeros(1, 10, 3), torch.zeros(1, 10, dtype=torch.long))
+    # nine legs (the largest the path finder allows) against the oracle
+    rng = np.random.default_rng(3)
+    coords = np.concatenate([np.zeros((2, 1, 3)), rng.normal(0, 1.5, (2, 8, 3))], 1)
+    ipots = np.ones((2, 9), int)
+    ipots[:, 0] = 0
+    cc, _ = st.cchi(torch.tensor(coords), torch.tensor(ipots))
+    oc, _ = O.Oracle(P).cchi(coords, ipots)
+    assert _rel(cc.cpu().numpy(), oc) < 1e-10
+    # coords on the host and float32 input are accepted, as in the reference
+    cc32, _ = st.cchi(torch.tensor(coords, dtype=torch.float32), torch.tensor(ipots))
+    assert cc32.device.type == "cuda"
+    # an empty batch and an empty row
+    b = PathBatch([(coords, ipots, None, np.array([0, 2]))], nrows=3, device="cuda")
+    rows = st.chi_reduce(b, np.arange(1, 101) * 0.1)
+    assert rows.shape == (3, 100) and torch.all(rows[1] == 0)
