@@ -37,7 +37,7 @@ UNIT = "path·k/s"
 
 
 # ------------------------------------------------------------------------------------------------ workload
-def workload(rank: int, world: int):
+def workload(rank: int, world: int, scale: float = 1.0):
     from feffgpu_b200 import workloads as W
     from feffgpu_b200.pad import phase_from_npz, resample_phase
     z = np.load(ROOT / "tests" / "golden" / "cfg2_phase.npz")
@@ -47,7 +47,8 @@ def workload(rank: int, world: int):
     ipot_of = np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
     groups = []
     for i, ab in enumerate(absorbers):
-        paths = W.random_paths(pos, box, int(ab), W.FEOPT_LEG_COUNTS, rmax=8.0, seed=1000 + int(ab), ipot_of=ipot_of)
+        counts = {n: max(1, int(round(c * scale))) for n, c in W.FEOPT_LEG_COUNTS.items()}
+        paths = W.random_paths(pos, box, int(ab), counts, rmax=8.0, seed=1000 + int(ab), ipot_of=ipot_of)
         for nleg, (c, ip, _atoms) in paths.items():
             groups.append((c, ip, None, np.full(len(c), i)))
     return P, groups
@@ -144,6 +145,51 @@ def cpu_sample(P, groups, budget_s: float, nthreads: int):
                                     f"timed per leg count and extrapolated to the full batch"
 
 
+def extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms):
+    """End-to-end, forward+backward and plain-FP64 measurements beside the headline."""
+    import torch
+    from feffgpu_b200 import GPUPathStage
+    coords_h = batch.coords.cpu().pin_memory()
+    coords_d = torch.empty_like(batch.coords)
+    rows_h = torch.empty(batch.nrows, NK, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        coords_d.copy_(coords_h, non_blocking=True)
+        rows = stage.chi_reduce(batch, Q, S, coords=coords_d)
+        rows_h.copy_(rows, non_blocking=True)
+
+    with torch.no_grad():
+        ms_e2e, _ = timed(e2e_step, args.steps, 1)
+    e2e = {"value": world * n_paths * NK / (ms_e2e * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": int(coords_h.numel() * coords_h.element_size()),
+           "d2h_bytes_per_step": int(rows_h.numel() * rows_h.element_size())}
+
+    # forward + backward (gradients with respect to every path coordinate and per-path sigma^2)
+    fwd_bwd = None
+    try:
+        s2 = torch.zeros(n_paths, dtype=torch.float64, device=dev, requires_grad=True)
+        cg = batch.coords.clone().requires_grad_(True)
+        w = torch.randn(batch.nrows, NK, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
+
+        def fb():
+            rows = stage.chi_reduce(batch, Q, S, coords=cg, sigma2=s2)
+            (rows * w).sum().backward()
+
+        ms_fb, _ = timed(fb, max(2, args.steps // 2), 1)
+        fwd_bwd = {"value": world * n_paths * NK / (ms_fb * 1e-3), "unit": UNIT, "ms_per_step": ms_fb}
+    except NotImplementedError as err:
+        fwd_bwd = {"value": None, "unit": UNIT, "note": f"not available: {err}"}
+
+    # the plain FP64 drop-in (complex128) on the same batch
+    stage64 = GPUPathStage(P, device=dev, dtype=torch.complex128)
+    with torch.no_grad():
+        ms64, _ = timed(lambda: stage64.chi_reduce(batch, Q, S), 2, 1)
+    plain = {"value": world * n_paths * NK / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
+             "speedup_mixed_over_fp64": ms64 / ms}
+
+    return e2e, fwd_bwd, plain
+
+
 # ------------------------------------------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -152,6 +198,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work for the CPU baseline")
+    ap.add_argument("--paths-scale", type=float, default=1.0, help="scale the paths per leg count (profiling runs)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--no-extras", action="store_true", help="only the headline forward (profiling runs)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -161,7 +210,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        P, groups = workload(0, 1)
+        P, groups = workload(0, 1, args.paths_scale)
         vals = []
         for i in range(args.warmup + args.steps):
             v, desc = cpu_sample(P, groups, budget_s=max(2.0, args.cpu_budget / 3), nthreads=nthreads)
@@ -189,7 +238,7 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
-    P, groups = workload(rank, world)
+    P, groups = workload(rank, world, args.paths_scale)
     stage = GPUPathStage(P, device=dev, dtype=torch.complex64)
     batch = PathBatch(groups, nrows=2, device=dev)
     S = stage.linear_matrix(Q)
@@ -238,45 +287,9 @@ def main():
             ms, kern = timed(lambda: stage.chi_reduce(batch, Q, S), args.steps, args.warmup, kernel_time=True)
     value = world * n_paths * NK / (ms * 1e-3)
 
-    # end to end through the public API: coordinates from pinned host memory, rows back to the host, every step
-    coords_h = batch.coords.cpu().pin_memory()
-    coords_d = torch.empty_like(batch.coords)
-    rows_h = torch.empty(batch.nrows, NK, dtype=torch.float64).pin_memory()
-
-    def e2e_step():
-        coords_d.copy_(coords_h, non_blocking=True)
-        rows = stage.chi_reduce(batch, Q, S, coords=coords_d)
-        rows_h.copy_(rows, non_blocking=True)
-
-    with torch.no_grad():
-        ms_e2e, _ = timed(e2e_step, args.steps, 1)
-    e2e = {"value": world * n_paths * NK / (ms_e2e * 1e-3), "unit": UNIT,
-           "h2d_bytes_per_step": int(coords_h.numel() * coords_h.element_size()),
-           "d2h_bytes_per_step": int(rows_h.numel() * rows_h.element_size())}
-
-    # forward + backward (gradients with respect to every path coordinate and per-path sigma^2)
-    fwd_bwd = None
-    try:
-        s2 = torch.zeros(n_paths, dtype=torch.float64, device=dev, requires_grad=True)
-        cg = batch.coords.clone().requires_grad_(True)
-        w = torch.randn(batch.nrows, NK, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
-
-        def fb():
-            rows = stage.chi_reduce(batch, Q, S, coords=cg, sigma2=s2)
-            (rows * w).sum().backward()
-
-        ms_fb, _ = timed(fb, max(2, args.steps // 2), 1)
-        fwd_bwd = {"value": world * n_paths * NK / (ms_fb * 1e-3), "unit": UNIT, "ms_per_step": ms_fb}
-    except NotImplementedError as err:
-        fwd_bwd = {"value": None, "unit": UNIT, "note": f"not available: {err}"}
-
-    # the plain FP64 drop-in (complex128) on the same batch
-    stage64 = GPUPathStage(P, device=dev, dtype=torch.complex128)
-    with torch.no_grad():
-        ms64, _ = timed(lambda: stage64.chi_reduce(batch, Q, S), 2, 1)
-    plain = {"value": world * n_paths * NK / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
-             "speedup_mixed_over_fp64": ms64 / ms}
-
+    e2e = fwd_bwd = plain = None
+    if not args.no_extras:
+        e2e, fwd_bwd, plain = extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms)
     # roofline of the dominant kernel (the fused per-path kernel): algorithmic FLOPs of the reference's loops
     import ctypes
     peak = ctypes.c_double()
@@ -298,7 +311,7 @@ def main():
                            "MEASURED_PEAKS.json holds no FP32 figure"}
 
     cpu = None
-    if rank == 0:
+    if rank == 0 and not args.no_cpu:
         v, desc = cpu_sample(P, groups, budget_s=args.cpu_budget, nthreads=nthreads)
         cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc}
 
