@@ -54,12 +54,12 @@ _SIGS = {
     "fg_cchi_backward": (C.c_int, [_P, C.c_int, C.c_int64, C.c_int32, _P, C.c_int32, _P, _P, _P, _P, _P, C.c_size_t,
                                    _P]),
     "fg_chi_fine": (C.c_int, [_P, C.c_int, C.c_int64, _P, _P, C.c_int32, _P, _P, _P, _P, _P]),
-    "fg_chi_fine_backward": (C.c_int, [_P, C.c_int, C.c_int64, _P, _P, C.c_int32, _P, _P, _P, _P, _P, _P, _P]),
+    "fg_chi_fine_backward": (C.c_int, [_P, C.c_int, C.c_int64, _P, _P, C.c_int32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "fg_chi_reduce_workspace": (C.c_size_t, [_P, C.POINTER(Paths), C.c_int32]),
     "fg_chi_reduce": (C.c_int, [_P, C.c_int, C.POINTER(Paths), C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.c_size_t, _P]),
     "fg_chi_reduce_backward_workspace": (C.c_size_t, [_P, C.POINTER(Paths), C.c_int32]),
     "fg_chi_reduce_backward": (C.c_int, [_P, C.c_int, C.POINTER(Paths), C.c_int32, _P, _P, _P, _P, _P, _P, _P, _P, _P,
-                                         C.c_size_t, _P]),
+                                         _P, C.c_size_t, _P]),
     "fg_set_kernel_timing": (C.c_int, [C.c_int32]),
     "fg_kernel_time_ms": (C.c_int, [C.POINTER(C.c_float)]),
     "fg_fp32_fma_peak": (C.c_int, [C.POINTER(C.c_double), _P]),

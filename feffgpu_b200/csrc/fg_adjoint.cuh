@@ -1,30 +1,1027 @@
-// fg_adjoint.cuh -- adjoint kernels (hand-written reverse mode of the forward path stage).
+// fg_adjoint.cuh -- the hand-written adjoint of the path stage (reverse mode, recomputing the per-leg matrices).
+//
+// Per path (one warp) and energy (one lane), with the upstream gradient gbar = dL/dRe(cchi) + i dL/dIm(cchi):
+//   dL = Re(conj(gbar) dcchi),  cchi = ptrac cfac,  ptrac = Tr(T F_nsc ... F_1).
+// T does not depend on the chain, so it is formed first.  Sweep 1 stores the prefix products P_k = F_k ... F_1
+// (k < nsc) in local memory; sweep 2 runs k = nsc .. 1 with the suffix R_k = T F_nsc ... F_(k+1) in registers,
+// recomputes F_k and, in the same partial-wave loop, contracts dF_k against M_k = P_(k-1) R_k:
+//   d/drho_(k+1), d/drho_k  through tangent recursions of the spherical-wave factors (dz/drho = -i z^2),
+//   d/dbeta_k               through the tangent recursion of d^l(beta) (a second rotation table),
+//   d/deta_(k+1)            from F~_k after the loop (F = e^{-i eta m1} F~).
+// The termination's parameters (rho_1, rho_nleg, beta_nleg, eta_1) are differentiated with P_nsc, and cfac gives
+// d/dri_j = cfac (i (ck - xk) - 1/ri_j).  The per-energy gradients of (ri, beta, eta) are summed over the energies
+// (lane accumulators, then a fixed-order warp reduction) and carried to the coordinates by forward-mode dual numbers
+// through the geometry (one coordinate direction per lane), with the reference's branch choices
+// (stage.py:148-206 under torch autograd).
 #pragma once
 #include "fg_kernels.cuh"
 
 namespace fg {
 
-template <typename R, int EDGE>
-fg_status Launch<R, EDGE>::cchi_bwd(const StageView &, const Tables<R> &, int64_t, int, const void *, int,
-                                    const int64_t *, const void *, const void *, void *, unsigned char *, int,
-                                    cudaStream_t)
+// ------------------------------------------------------------------------------------------------ setup
+// Rotation-table derivatives d/dbeta D^(k) for k = 1..nsc and the termination's d/dbeta d^{l_t}(beta_nleg).
+template <typename R>
+__device__ void adj_setup(const WarpPath<R> &g, R *dhd, R (*dterm_db)[49], const Tables<R> &T, int nleg, int lane,
+                          int MM)
 {
-    return fail(FG_ERR_NOT_IMPLEMENTED, "adjoint not built yet");
+    const int nsc = nleg - 1;
+    const int NC = ncanon(MM), DS = dstride(MM), L1 = T.L1;
+    for (int task = lane; task < nsc * NC; task += 32) {
+        const int k = task / NC + 1, r = task % NC;
+        int m1, m2;
+        canon_mn(MM, r, m1, m2);
+        const double b = g.beta[k];
+        const double c = cos(b), s = sin(b), c2 = cos(0.5 * b), s2 = sin(0.5 * b);
+        R *out = dhd + (size_t)(k - 1) * (L1 + 1) * DS + r;
+        const double *xf = T.xfac + (m1 + 3) * 7 + (m2 + 3);
+        double dm1 = 0.0, d0 = 0.0, em1 = 0.0, e0 = 0.0;   // d and d/dbeta at l-2, l-1
+        for (int l = 0; l < L1; ++l) {
+            double dl, el;
+            if (l <= 3) {
+                dl = wigner_small(l, m1, m2, c2, s2);
+                el = wigner_small_dbeta(l, m1, m2, c2, s2);
+            } else {
+                const double *q = T.rc + (((size_t)(l - 1) * 7 + (m1 + 3)) * 7 + (m2 + 3)) * 3;
+                const double f = fma(q[0], c, -q[1]);
+                dl = fma(f, d0, -q[2] * dm1);
+                el = fma(f, e0, fma(-q[0] * s, d0, -q[2] * em1));
+            }
+            out[(size_t)(l + 1) * DS] = (R)(el * xf[(size_t)(l + 1) * 49]);
+            dm1 = d0; d0 = dl;
+            em1 = e0; e0 = el;
+        }
+    }
+    for (int task = lane; task < T.nterm * 49; task += 32) {
+        const int t = task / 49, m1 = (task % 49) / 7 - 3, m2 = task % 7 - 3;
+        const double b = g.beta[nleg];
+        dterm_db[t][task % 49] = (R)wigner_small_dbeta(T.term_l[t], m1, m2, cos(0.5 * b), sin(0.5 * b));
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ termination
+// c[il][im] and dc/drho of one leg for il <= ITM with the truncation of GPUPathStage._clm (see clm_small)
+template <typename R, int ITM, int NCOL>
+__device__ __forceinline__ void clm_small_t(C2<R> z, int lxp1, C2<R> (&c)[ITM + 1][NCOL + 1],
+                                            C2<R> (&dc)[ITM + 1][NCOL + 1])
+{
+    const C2<R> dz = cmul(C2<R>{R(0), R(-1)}, cmul(z, z));   // dz/drho = -i z^2
+    C2<R> pv[NCOL + 1], cv[NCOL + 1], dpv[NCOL + 1], dcv[NCOL + 1];
+#pragma unroll
+    for (int j = 0; j <= NCOL; ++j) {
+        pv[j] = cv[j] = dpv[j] = dcv[j] = cz<R>();
+        c[0][j] = dc[0][j] = cz<R>();
+    }
+    pv[1] = cv[1] = C2<R>{R(1), R(0)};
+#pragma unroll
+    for (int il = 1; il <= ITM; ++il) {
+#pragma unroll
+        for (int j = 0; j <= NCOL; ++j) {
+            const bool keep = (il <= lxp1) || (j == 1 && il <= 2);
+            c[il][j] = keep ? cv[j] : cz<R>();
+            dc[il][j] = keep ? dcv[j] : cz<R>();
+        }
+        const R w = R(2 * il - 1);
+        const C2<R> wz = cscl(z, w), wdz = cscl(dz, w);
+        C2<R> nv[NCOL + 1], dnv[NCOL + 1];
+        nv[0] = dnv[0] = cz<R>();
+#pragma unroll
+        for (int j = 1; j <= NCOL; ++j) {
+            const C2<R> sv = j > 1 ? cadd(cv[j], cv[j - 1]) : cv[j];
+            const C2<R> dsv = j > 1 ? cadd(dcv[j], dcv[j - 1]) : dcv[j];
+            nv[j] = cfms(wz, sv, pv[j]);
+            dnv[j] = cfms(wdz, sv, cfms(wz, dsv, dpv[j]));
+        }
+#pragma unroll
+        for (int j = 1; j <= NCOL; ++j) {
+            pv[j] = cv[j]; cv[j] = nv[j];
+            dpv[j] = dcv[j]; dcv[j] = dnv[j];
+        }
+    }
+}
+
+// G1_t (gam of leg 1), G2_t ((2l+1) gamtl of leg nleg) for the final-state entries and their rho-derivatives
+template <typename R, int KIND> struct TermLegs {
+    static constexpr LamTab L = lamtab(KIND);
+    C2<R> G1[2][L.N0], G2[2][L.N0], dG1[2][L.N0], dG2[2][L.N0];
+};
+
+template <typename R, int KIND>
+__device__ __forceinline__ void term_legs(const WarpPath<R> &g, const Tables<R> &T, int e, int nleg, C2<R> ck,
+                                          TermLegs<R, KIND> &tl)
+{
+    constexpr LamTab L = lamtab(KIND);
+    constexpr int N0 = L.N0, ITM = 4, NCOL = 6;
+    const int E = T.E;
+    const int la = T.lmax[g.ip[0] * E + e], l1 = T.lmax[g.ip[1] * E + e], ln = T.lmax[g.ip[nleg - 1] * E + e];
+    C2<R> c1[ITM + 1][NCOL + 1], cn[ITM + 1][NCOL + 1], d1[ITM + 1][NCOL + 1], dn[ITM + 1][NCOL + 1];
+    clm_small_t<R, ITM, NCOL>(zfac(cscl(ck, (R)g.ri[1])), max(la, l1) + 1, c1, d1);
+    clm_small_t<R, ITM, NCOL>(zfac(cscl(ck, (R)g.ri[nleg])), max(ln, la) + 1, cn, dn);
+    for (int t = 0; t < T.nterm; ++t) {
+        const int il = T.term_l[t] + 1;
+#pragma unroll
+        for (int i = 0; i < N0; ++i) {
+            const int am = L.m[i] < 0 ? -L.m[i] : L.m[i];
+            const bool ok = am + 1 <= il;
+            const int imn = am + L.n[i] + 1, in = L.n[i] + 1;
+            C2<R> a1 = cz<R>(), an = cz<R>(), b1 = cz<R>(), bn = cz<R>();
+#pragma unroll
+            for (int q = 1; q <= ITM; ++q)
+                if (q == il) {
+                    a1 = c1[q][imn < NCOL ? imn : NCOL]; b1 = d1[q][imn < NCOL ? imn : NCOL];
+                    an = cn[q][in]; bn = dn[q][in];
+                }
+            const R xn = (R)T.xnlm[il * 8 + am + 1];
+            const R f1 = (ok && imn <= il) ? ((am & 1) ? -xn : xn) : R(0);
+            const R f2 = ok ? (R)(2 * il - 1) / xn : R(0);
+            tl.G1[t][i] = cscl(a1, f1); tl.dG1[t][i] = cscl(b1, f1);
+            tl.G2[t][i] = cscl(an, f2); tl.dG2[t][i] = cscl(bn, f2);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ streaming dF
+// Per partial wave: accumulate F~_k (canonical entries) and contract dF_k with the weights Wh (per canonical entry:
+// sum over its flip orbit of sign * e^{-i eta m1} * M[b][a]) for the derivatives along rho_in, rho_out, beta_k.
+template <typename R, int KIND, int NR, int NC>
+__device__ __forceinline__ void accumulate_f_adj(C2<R> (&acc)[RepTab<KIND, NR, NC>().n],
+                                                 const C2<R> (&Wh)[RepTab<KIND, NR, NC>().n], const R *dhk,
+                                                 const R *dhdk, const C2<R> *tlk, int E, int ilx, C2<R> z_in,
+                                                 C2<R> z_out, C2<R> &g_in, C2<R> &g_out, C2<R> &g_beta)
+{
+    constexpr RepTab<KIND, NR, NC> RT{};
+    constexpr LamTab L = lamtab(KIND);
+    constexpr int DS = dstride(L.MM);
+    constexpr int NCAN = ncanon(L.MM);
+    constexpr int CI = L.CI, CO = L.CO;
+#pragma unroll
+    for (int r = 0; r < RT.n; ++r) acc[r] = cz<R>();
+    const C2<R> dz_in = cmul(C2<R>{R(0), R(-1)}, cmul(z_in, z_in));
+    const C2<R> dz_out = cmul(C2<R>{R(0), R(-1)}, cmul(z_out, z_out));
+    C2<R> pi[CI + 1], ci[CI + 1], po[CO + 1], co[CO + 1];
+    C2<R> dpi[CI + 1], dci[CI + 1], dpo[CO + 1], dco[CO + 1];
+#pragma unroll
+    for (int j = 0; j <= CI; ++j) pi[j] = ci[j] = dpi[j] = dci[j] = cz<R>();
+#pragma unroll
+    for (int j = 0; j <= CO; ++j) po[j] = co[j] = dpo[j] = dco[j] = cz<R>();
+    pi[1] = ci[1] = po[1] = co[1] = C2<R>{R(1), R(0)};
+    C2<R> gi = cz<R>(), go = cz<R>(), gb = cz<R>();
+    for (int il = 1; il <= ilx; ++il) {
+        const C2<R> t = tlk[(size_t)il * E];
+        const R *dr = dhk + (size_t)il * DS;
+        const R *ddr = dhdk + (size_t)il * DS;
+        R d[NCAN], dd[NCAN];
+#pragma unroll
+        for (int q = 0; q < NCAN; ++q) { d[q] = dr[q]; dd[q] = ddr[q]; }
+        C2<R> tco[CO + 1], tdco[CO + 1];
+#pragma unroll
+        for (int j = 1; j <= CO; ++j) { tco[j] = cmul(t, co[j]); tdco[j] = cmul(t, dco[j]); }
+        // X[ci][co] = sum Wh D, Y[ci][co] = sum Wh D'
+        C2<R> X[CI + 1][CO + 1], Y[CI + 1][CO + 1];
+#pragma unroll
+        for (int a = 0; a <= CI; ++a)
+#pragma unroll
+            for (int b = 0; b <= CO; ++b) X[a][b] = Y[a][b] = cz<R>();
+#pragma unroll
+        for (int r = 0; r < RT.n; ++r) {
+            acc[r] = cfmr(cmul(ci[RT.ci[r]], tco[RT.co[r]]), d[RT.d[r]], acc[r]);
+            X[RT.ci[r]][RT.co[r]] = cfmr(Wh[r], d[RT.d[r]], X[RT.ci[r]][RT.co[r]]);
+            Y[RT.ci[r]][RT.co[r]] = cfmr(Wh[r], dd[RT.d[r]], Y[RT.ci[r]][RT.co[r]]);
+        }
+#pragma unroll
+        for (int a = 1; a <= CI; ++a) {
+            C2<R> v = cz<R>();
+#pragma unroll
+            for (int b = 1; b <= CO; ++b) {
+                v = cfma(X[a][b], tco[b], v);
+                gb = cfma(Y[a][b], cmul(ci[a], tco[b]), gb);
+            }
+            gi = cfma(dci[a], v, gi);
+        }
+#pragma unroll
+        for (int b = 1; b <= CO; ++b) {
+            C2<R> v = cz<R>();
+#pragma unroll
+            for (int a = 1; a <= CI; ++a) v = cfma(X[a][b], ci[a], v);
+            go = cfma(tdco[b], v, go);
+        }
+        // next partial wave, values and rho-tangents
+        const R w = R(2 * il - 1);
+        const C2<R> wi = cscl(z_in, w), wo = cscl(z_out, w), wdi = cscl(dz_in, w), wdo = cscl(dz_out, w);
+        C2<R> ni[CI + 1], no[CO + 1], dni[CI + 1], dno[CO + 1];
+#pragma unroll
+        for (int j = 1; j <= CI; ++j) {
+            const C2<R> sv = j > 1 ? cadd(ci[j], ci[j - 1]) : ci[j];
+            const C2<R> dsv = j > 1 ? cadd(dci[j], dci[j - 1]) : dci[j];
+            ni[j] = cfms(wi, sv, pi[j]);
+            dni[j] = cfms(wdi, sv, cfms(wi, dsv, dpi[j]));
+        }
+#pragma unroll
+        for (int j = 1; j <= CO; ++j) {
+            const C2<R> sv = j > 1 ? cadd(co[j], co[j - 1]) : co[j];
+            const C2<R> dsv = j > 1 ? cadd(dco[j], dco[j - 1]) : dco[j];
+            no[j] = cfms(wo, sv, po[j]);
+            dno[j] = cfms(wdo, sv, cfms(wo, dsv, dpo[j]));
+        }
+#pragma unroll
+        for (int j = 1; j <= CI; ++j) { pi[j] = ci[j]; ci[j] = ni[j]; dpi[j] = dci[j]; dci[j] = dni[j]; }
+#pragma unroll
+        for (int j = 1; j <= CO; ++j) { po[j] = co[j]; co[j] = no[j]; dpo[j] = dco[j]; dco[j] = dno[j]; }
+    }
+    g_in = gi;
+    g_out = go;
+    g_beta = gb;
+}
+
+// Weights of the contraction: Wh[r] = sum over the orbit of r of sign * ph(m_a) * M(b, a), and the same with an
+// extra -i m_a for the Euler-angle derivative.  M(b, a) is given as a functor.
+template <typename R, int KIND, int NR, int NC, int MM, class MF>
+__device__ __forceinline__ void orbit_weights(const MF &M, const C2<R> (&ph)[2 * MM + 1],
+                                              C2<R> (&Wh)[RepTab<KIND, NR, NC>().n],
+                                              C2<R> (&We)[RepTab<KIND, NR, NC>().n])
+{
+    constexpr RepTab<KIND, NR, NC> RT{};
+    constexpr LamTab L = lamtab(KIND);
+#pragma unroll
+    for (int r = 0; r < RT.n; ++r) Wh[r] = We[r] = cz<R>();
+#pragma unroll
+    for (int a = 0; a < NR; ++a)
+#pragma unroll
+        for (int b = 0; b < NC; ++b) {
+            const C2<R> v = cmul(ph[L.m[a] + MM], M(b, a));
+            const C2<R> sv = RT.sg[a][b] > 0 ? v : cscl(v, R(-1));
+            Wh[RT.rep[a][b]] = cadd(Wh[RT.rep[a][b]], sv);
+            // -i m_a sv
+            We[RT.rep[a][b]] = cadd(We[RT.rep[a][b]], C2<R>{sv.y * R(L.m[a]), -sv.x * R(L.m[a])});
+        }
+}
+
+// Per-lane gradient accumulators of one path: dL/d(ri_j), dL/d(beta_j), dL/d(eta_j), j = 1..nleg (bohr, rad).
+struct ParGrad {
+    double ri[kMaxLeg + 1], beta[kMaxLeg + 1], eta[kMaxLeg + 1];
+};
+
+// Termination contribution with P (the full chain, N0 x N0): ptrac and the gradients along eta_1, beta_nleg,
+// rho_1, rho_nleg (each times s, real part taken by the caller).  Rows a_lo <= a < a_hi only.
+template <typename R, int KIND, class PF>
+__device__ __forceinline__ C2<R> term_adj(const WarpPath<R> &g, const R (*dterm_db)[49], const Tables<R> &T, int e,
+                                          const TermLegs<R, KIND> &tl, const PF &P, C2<R> &g_eta1, C2<R> &g_betan,
+                                          C2<R> &g_rho1, C2<R> &g_rhon, int a_lo = 0, int a_hi = kLamTot)
+{
+    constexpr LamTab L = lamtab(KIND);
+    constexpr int N0 = L.N0, MM = L.MM;
+    C2<R> ph1[2 * MM + 1];
+    phase_powers<R, MM>(g.phs[1], ph1);
+    C2<R> ptrac = cz<R>();
+    for (int t = 0; t < T.nterm; ++t) {
+        const C2<R> W = T.wt[t * T.E + e];
+        C2<R> s = cz<R>(), se = cz<R>(), sb = cz<R>(), s1 = cz<R>(), sn = cz<R>();
+#pragma unroll
+        for (int a = 0; a < N0; ++a) {
+            if (a < a_lo || a >= a_hi) continue;
+            C2<R> x = cz<R>(), xb = cz<R>(), xn = cz<R>();
+#pragma unroll
+            for (int b = 0; b < N0; ++b) {
+                const int di = (L.m[a] + 3) * 7 + L.m[b] + 3;
+                const C2<R> p = P(b, a);
+                x = cfma(cscl(tl.G2[t][b], g.dterm[t][di]), p, x);
+                xb = cfma(cscl(tl.G2[t][b], dterm_db[t][di]), p, xb);
+                xn = cfma(cscl(tl.dG2[t][b], g.dterm[t][di]), p, xn);
+            }
+            const C2<R> f = ph1[L.m[a] + MM];
+            const C2<R> v = cmul(cmul(f, tl.G1[t][a]), x);
+            s = cadd(s, v);
+            se = cadd(se, C2<R>{v.y * R(L.m[a]), -v.x * R(L.m[a])});
+            sb = cfma(cmul(f, tl.G1[t][a]), xb, sb);
+            s1 = cfma(cmul(f, tl.dG1[t][a]), x, s1);
+            sn = cfma(cmul(f, tl.G1[t][a]), xn, sn);
+        }
+        ptrac = cfma(W, s, ptrac);
+        g_eta1 = cfma(W, se, g_eta1);
+        g_betan = cfma(W, sb, g_betan);
+        g_rho1 = cfma(W, s1, g_rho1);
+        g_rhon = cfma(W, sn, g_rhon);
+    }
+    return ptrac;
+}
+
+// Termination matrix rows T[a][b] (a, b < N0), as termination() forms them
+template <typename R, int KIND>
+__device__ __forceinline__ void term_matrix(const WarpPath<R> &g, const Tables<R> &T, int e,
+                                            const TermLegs<R, KIND> &tl, C2<R> (&Tm)[lamtab(KIND).N0][lamtab(KIND).N0])
+{
+    constexpr LamTab L = lamtab(KIND);
+    constexpr int N0 = L.N0, MM = L.MM;
+    C2<R> ph1[2 * MM + 1];
+    phase_powers<R, MM>(g.phs[1], ph1);
+#pragma unroll
+    for (int a = 0; a < N0; ++a)
+#pragma unroll
+        for (int b = 0; b < N0; ++b) Tm[a][b] = cz<R>();
+    for (int t = 0; t < T.nterm; ++t) {
+        const C2<R> W = T.wt[t * T.E + e];
+#pragma unroll
+        for (int a = 0; a < N0; ++a) {
+            const C2<R> f = cmul(W, cmul(ph1[L.m[a] + MM], tl.G1[t][a]));
+#pragma unroll
+            for (int b = 0; b < N0; ++b)
+                Tm[a][b] = cfma(f, cscl(tl.G2[t][b], g.dterm[t][(L.m[a] + 3) * 7 + L.m[b] + 3]), Tm[a][b]);
+        }
+    }
+}
+
+// Adds Re(s * dcfac/dri) = Re(s * cfac... ) terms: dL/dri_j += Re(conj(gbar) cchi (i dk - 1/ri_j)).
+template <typename R>
+__device__ __forceinline__ void cfac_grad(const WarpPath<R> &g, const Tables<R> &T, int e, int nleg, C2<R> gbar,
+                                          C2<R> cchi, ParGrad &pg)
+{
+    const double2 dk = T.dk[e];
+    // conj(gbar) cchi
+    const double ax = (double)gbar.x * cchi.x + (double)gbar.y * cchi.y;
+    const double ay = (double)gbar.x * cchi.y - (double)gbar.y * cchi.x;
+    // times i dk = (-dk.y, dk.x)
+    const double re_idk = ax * (-dk.y) - ay * dk.x;
+    for (int j = 1; j <= nleg; ++j) pg.ri[j] += re_idk - ax / g.ri[j];
+}
+
+// ------------------------------------------------------------------------------------------------ one energy
+// Multiple scattering (nleg >= 3).  Adds this energy's parameter gradients into pg.
+template <typename R, int KIND>
+__device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, const R (*dterm_db)[49],
+                              const Tables<R> &T, int e, int nleg, C2<R> gbar, ParGrad &pg)
+{
+    constexpr LamTab L = lamtab(KIND);
+    constexpr int N = L.N, N0 = L.N0, MM = L.MM, DS = dstride(MM);
+    const int E = T.E, nsc = nleg - 1;
+    const size_t dleg = (size_t)(T.L1 + 1) * DS, tlip = (size_t)(T.L1 + 1) * E;
+    const C2<R> ck = T.ck[e];
+    if (fabs((double)ck.x) + fabs((double)ck.y) <= 1e-16) return;
+    TermLegs<R, KIND> tl;
+    term_legs<R, KIND>(g, T, e, nleg, ck, tl);
+    // sweep 1: prefix products P_k = F_k ... F_1, k = 1..nsc-1 (lamx x laml0x), kept in local memory
+    C2<R> Pst[kMaxLeg - 2][N][N0];
+    {
+        constexpr RepTab<KIND, N, N0> RT{};
+        C2<R> acc[RT.n];
+        const int ip = g.ip[1];
+        accumulate_f<R, KIND, N, N0>(acc, dh, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
+                                     zfac(cscl(ck, (R)g.ri[2])), zfac(cscl(ck, (R)g.ri[1])));
+        C2<R> ph[2 * MM + 1];
+        phase_powers<R, MM>(g.phs[2], ph);
+#pragma unroll
+        for (int a = 0; a < N; ++a)
+#pragma unroll
+            for (int b = 0; b < N0; ++b) {
+                const C2<R> v = RT.sg[a][b] > 0 ? acc[RT.rep[a][b]] : cscl(acc[RT.rep[a][b]], R(-1));
+                Pst[0][a][b] = cmul(ph[L.m[a] + MM], v);
+            }
+    }
+    for (int k = 2; k < nsc; ++k) {
+        constexpr RepTab<KIND, N, N> RT{};
+        C2<R> acc[RT.n];
+        const int ip = g.ip[k];
+        accumulate_f<R, KIND, N, N>(acc, dh + (k - 1) * dleg, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
+                                    zfac(cscl(ck, (R)g.ri[k + 1])), zfac(cscl(ck, (R)g.ri[k])));
+        C2<R> ph[2 * MM + 1];
+        phase_powers<R, MM>(g.phs[k + 1], ph);
+#pragma unroll
+        for (int a = 0; a < N; ++a)
+#pragma unroll
+            for (int b = 0; b < N0; ++b) {
+                C2<R> s = cz<R>();
+#pragma unroll
+                for (int c = 0; c < N; ++c) {
+                    const C2<R> f = acc[RT.rep[a][c]];
+                    s = RT.sg[a][c] > 0 ? cfma(f, Pst[k - 2][c][b], s) : cfms(f, Pst[k - 2][c][b], s);
+                }
+                Pst[k - 1][a][b] = cmul(ph[L.m[a] + MM], s);
+            }
+    }
+    const C2<R> cf = cfac(g, T, e, nleg, ck);
+    const C2<R> sd = cmul(C2<R>{gbar.x, -gbar.y}, cf);      // s = conj(gbar) cfac: dL = Re(s dptrac)
+    const C2<R> sck = cmul(sd, ck);
+    auto add_re = [](double &acc, C2<R> s, C2<R> v) { acc += (double)s.x * v.x - (double)s.y * v.y; };
+    // sweep 2, k = nsc: the last matrix (laml0x x lamx), M = P_(nsc-1) T
+    C2<R> Tm[N0][N0];
+    term_matrix<R, KIND>(g, T, e, tl, Tm);
+    C2<R> Rm[N0][N];    // R_k = T F_nsc ... F_(k+1)
+    {
+        constexpr RepTab<KIND, N0, N> RT{};
+        C2<R> ph[2 * MM + 1];
+        phase_powers<R, MM>(g.phs[nleg], ph);
+        C2<R> Wh[RT.n], We[RT.n];
+        // M(b, a) = sum_c P_(nsc-1)[b][c] T[c][a]: b < N (cols of F), a < N0 (rows of F)
+        orbit_weights<R, KIND, N0, N, MM>(
+            [&](int b, int a) {
+                C2<R> m = cz<R>();
+#pragma unroll
+                for (int c = 0; c < N0; ++c) m = cfma(Pst[nsc - 2][b][c], Tm[c][a], m);
+                return m;
+            },
+            ph, Wh, We);
+        C2<R> acc[RT.n];
+        C2<R> gi, go, gb;
+        const int ip = g.ip[nsc];
+        accumulate_f_adj<R, KIND, N0, N>(acc, Wh, dh + (nsc - 1) * dleg, dhd + (nsc - 1) * dleg,
+                                         T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
+                                         zfac(cscl(ck, (R)g.ri[nleg])), zfac(cscl(ck, (R)g.ri[nsc])), gi, go, gb);
+        C2<R> ge = cz<R>();
+#pragma unroll
+        for (int r = 0; r < RT.n; ++r) ge = cfma(acc[r], We[r], ge);
+        add_re(pg.ri[nleg], sck, gi);
+        add_re(pg.ri[nsc], sck, go);
+        add_re(pg.beta[nsc], sd, gb);
+        add_re(pg.eta[nleg], sd, ge);
+        // F_nsc, P_nsc = F_nsc P_(nsc-1), the termination's own gradients and R_(nsc-1) = T F_nsc
+        C2<R> Fl[N0][N];
+#pragma unroll
+        for (int a = 0; a < N0; ++a)
+#pragma unroll
+            for (int b = 0; b < N; ++b) {
+                const C2<R> v = RT.sg[a][b] > 0 ? acc[RT.rep[a][b]] : cscl(acc[RT.rep[a][b]], R(-1));
+                Fl[a][b] = cmul(ph[L.m[a] + MM], v);
+            }
+        C2<R> ge1 = cz<R>(), gbn = cz<R>(), gr1 = cz<R>(), grn = cz<R>();
+        const C2<R> ptrac = term_adj<R, KIND>(
+            g, dterm_db, T, e, tl,
+            [&](int b, int a) {
+                C2<R> p = cz<R>();
+#pragma unroll
+                for (int c = 0; c < N; ++c) p = cfma(Fl[b][c], Pst[nsc - 2][c][a], p);
+                return p;
+            },
+            ge1, gbn, gr1, grn);
+        add_re(pg.eta[1], sd, ge1);
+        add_re(pg.beta[nleg], sd, gbn);
+        add_re(pg.ri[1], sck, gr1);
+        add_re(pg.ri[nleg], sck, grn);
+        cfac_grad(g, T, e, nleg, gbar, cmul(ptrac, cf), pg);
+#pragma unroll
+        for (int a = 0; a < N0; ++a)
+#pragma unroll
+            for (int b = 0; b < N; ++b) {
+                C2<R> v = cz<R>();
+#pragma unroll
+                for (int c = 0; c < N0; ++c) v = cfma(Tm[a][c], Fl[c][b], v);
+                Rm[a][b] = v;
+            }
+    }
+    // middle matrices k = nsc-1 .. 2 (lamx x lamx): M = P_(k-1) R_k
+    for (int k = nsc - 1; k >= 2; --k) {
+        constexpr RepTab<KIND, N, N> RT{};
+        C2<R> ph[2 * MM + 1];
+        phase_powers<R, MM>(g.phs[k + 1], ph);
+        C2<R> Wh[RT.n], We[RT.n];
+        orbit_weights<R, KIND, N, N, MM>(
+            [&](int b, int a) {
+                C2<R> m = cz<R>();
+#pragma unroll
+                for (int c = 0; c < N0; ++c) m = cfma(Pst[k - 2][b][c], Rm[c][a], m);
+                return m;
+            },
+            ph, Wh, We);
+        C2<R> acc[RT.n];
+        C2<R> gi, go, gb;
+        const int ip = g.ip[k];
+        accumulate_f_adj<R, KIND, N, N>(acc, Wh, dh + (k - 1) * dleg, dhd + (k - 1) * dleg, T.tl + ip * tlip + e, E,
+                                        T.lmax[ip * E + e] + 1, zfac(cscl(ck, (R)g.ri[k + 1])),
+                                        zfac(cscl(ck, (R)g.ri[k])), gi, go, gb);
+        C2<R> ge = cz<R>();
+#pragma unroll
+        for (int r = 0; r < RT.n; ++r) ge = cfma(acc[r], We[r], ge);
+        add_re(pg.ri[k + 1], sck, gi);
+        add_re(pg.ri[k], sck, go);
+        add_re(pg.beta[k], sd, gb);
+        add_re(pg.eta[k + 1], sd, ge);
+        C2<R> Rn[N0][N];
+#pragma unroll
+        for (int a = 0; a < N0; ++a)
+#pragma unroll
+            for (int b = 0; b < N; ++b) {
+                C2<R> v = cz<R>();
+#pragma unroll
+                for (int c = 0; c < N; ++c) {
+                    const C2<R> f = cmul(ph[L.m[c] + MM], acc[RT.rep[c][b]]);
+                    v = RT.sg[c][b] > 0 ? cfma(Rm[a][c], f, v) : cfms(Rm[a][c], f, v);
+                }
+                Rn[a][b] = v;
+            }
+#pragma unroll
+        for (int a = 0; a < N0; ++a)
+#pragma unroll
+            for (int b = 0; b < N; ++b) Rm[a][b] = Rn[a][b];
+    }
+    // first matrix k = 1 (lamx x laml0x): M = R_1 (P_0 = identity)
+    {
+        constexpr RepTab<KIND, N, N0> RT{};
+        C2<R> ph[2 * MM + 1];
+        phase_powers<R, MM>(g.phs[2], ph);
+        C2<R> Wh[RT.n], We[RT.n];
+        orbit_weights<R, KIND, N, N0, MM>([&](int b, int a) { return Rm[b][a]; }, ph, Wh, We);
+        C2<R> acc[RT.n];
+        C2<R> gi, go, gb;
+        const int ip = g.ip[1];
+        accumulate_f_adj<R, KIND, N, N0>(acc, Wh, dh, dhd, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
+                                         zfac(cscl(ck, (R)g.ri[2])), zfac(cscl(ck, (R)g.ri[1])), gi, go, gb);
+        C2<R> ge = cz<R>();
+#pragma unroll
+        for (int r = 0; r < RT.n; ++r) ge = cfma(acc[r], We[r], ge);
+        add_re(pg.ri[2], sck, gi);
+        add_re(pg.ri[1], sck, go);
+        add_re(pg.beta[1], sd, gb);
+        add_re(pg.eta[2], sd, ge);
+    }
+}
+
+// Single scattering, K edge (flip-symmetric six-entry set): T first, then one sweep over F_1 with M = T.
+template <typename R, int KIND>
+__device__ void energy_ss_sym_adj(const WarpPath<R> &g, const R *dh, const R *dhd, const R (*dterm_db)[49],
+                                  const Tables<R> &T, int e, C2<R> gbar, ParGrad &pg)
+{
+    constexpr LamTab L = lamtab(KIND);
+    constexpr int N = L.N, N0 = L.N0, MM = L.MM;
+    const int E = T.E;
+    const size_t tlip = (size_t)(T.L1 + 1) * E;
+    const C2<R> ck = T.ck[e];
+    if (fabs((double)ck.x) + fabs((double)ck.y) <= 1e-16) return;
+    TermLegs<R, KIND> tl;
+    term_legs<R, KIND>(g, T, e, 2, ck, tl);
+    C2<R> Tm[N0][N0];
+    term_matrix<R, KIND>(g, T, e, tl, Tm);
+    const C2<R> cf = cfac(g, T, e, 2, ck);
+    const C2<R> sd = cmul(C2<R>{gbar.x, -gbar.y}, cf);
+    const C2<R> sck = cmul(sd, ck);
+    auto add_re = [](double &acc, C2<R> s, C2<R> v) { acc += (double)s.x * v.x - (double)s.y * v.y; };
+    constexpr RepTab<KIND, N, N0> RT{};
+    C2<R> ph[2 * MM + 1];
+    phase_powers<R, MM>(g.phs[2], ph);
+    C2<R> Wh[RT.n], We[RT.n];
+    orbit_weights<R, KIND, N, N0, MM>([&](int b, int a) { return Tm[b][a]; }, ph, Wh, We);
+    C2<R> acc[RT.n];
+    C2<R> gi, go, gb;
+    const int ip = g.ip[1];
+    accumulate_f_adj<R, KIND, N, N0>(acc, Wh, dh, dhd, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
+                                     zfac(cscl(ck, (R)g.ri[2])), zfac(cscl(ck, (R)g.ri[1])), gi, go, gb);
+    C2<R> ge = cz<R>();
+#pragma unroll
+    for (int r = 0; r < RT.n; ++r) ge = cfma(acc[r], We[r], ge);
+    add_re(pg.ri[2], sck, gi);
+    add_re(pg.ri[1], sck, go);
+    add_re(pg.beta[1], sd, gb);
+    add_re(pg.eta[2], sd, ge);
+    C2<R> ge1 = cz<R>(), gbn = cz<R>(), gr1 = cz<R>(), grn = cz<R>();
+    const C2<R> ptrac = term_adj<R, KIND>(
+        g, dterm_db, T, e, tl,
+        [&](int b, int a) {
+            const C2<R> v = RT.sg[b][a] > 0 ? acc[RT.rep[b][a]] : cscl(acc[RT.rep[b][a]], R(-1));
+            return cmul(ph[L.m[b] + MM], v);
+        },
+        ge1, gbn, gr1, grn);
+    add_re(pg.eta[1], sd, ge1);
+    add_re(pg.beta[2], sd, gbn);
+    add_re(pg.ri[1], sck, gr1);
+    add_re(pg.ri[2], sck, grn);
+    cfac_grad(g, T, e, 2, gbar, cmul(ptrac, cf), pg);
+}
+
+// Single scattering at L and M edges: one column of F at a time (as energy_ss_col), each with its own sweep.
+template <typename R, int KIND>
+__device__ void energy_ss_col_adj(const WarpPath<R> &g, const R *dh, const R *dhd, const R (*dterm_db)[49],
+                                  const Tables<R> &T, int e, C2<R> gbar, ParGrad &pg)
+{
+    constexpr LamTab L = lamtab(KIND);
+    constexpr int N = L.N, MM = L.MM, DS = dstride(MM), CI = L.CI, CO = L.CO;
+    const int E = T.E;
+    const size_t tlip = (size_t)(T.L1 + 1) * E;
+    const C2<R> ck = T.ck[e];
+    if (fabs((double)ck.x) + fabs((double)ck.y) <= 1e-16) return;
+    TermLegs<R, KIND> tl;
+    term_legs<R, KIND>(g, T, e, 2, ck, tl);
+    const C2<R> cf = cfac(g, T, e, 2, ck);
+    const C2<R> sd = cmul(C2<R>{gbar.x, -gbar.y}, cf);
+    const C2<R> sck = cmul(sd, ck);
+    auto add_re = [](double &acc, C2<R> s, C2<R> v) { acc += (double)s.x * v.x - (double)s.y * v.y; };
+    const int ip = g.ip[1];
+    const C2<R> *tlk = T.tl + ip * tlip + e;
+    const int ilx = T.lmax[ip * E + e] + 1;
+    const C2<R> z_in = zfac(cscl(ck, (R)g.ri[2])), z_out = zfac(cscl(ck, (R)g.ri[1]));
+    const C2<R> dz_in = cmul(C2<R>{R(0), R(-1)}, cmul(z_in, z_in));
+    const C2<R> dz_out = cmul(C2<R>{R(0), R(-1)}, cmul(z_out, z_out));
+    C2<R> ph[2 * MM + 1], ph1[2 * MM + 1];
+    phase_powers<R, MM>(g.phs[2], ph);
+    phase_powers<R, MM>(g.phs[1], ph1);
+    C2<R> ptrac = cz<R>();
+#pragma unroll 1
+    for (int col = 0; col < N; ++col) {
+        int m2 = 0, n2 = 0;
+#pragma unroll
+        for (int q = 0; q < N; ++q)
+            if (q == col) { m2 = L.m[q]; n2 = L.n[q]; }
+        // the termination row T[col][a] weights column col of F: W[a] = ph(m_a) T[col][a]
+        C2<R> Trow[N];
+#pragma unroll
+        for (int a = 0; a < N; ++a) Trow[a] = cz<R>();
+        for (int t = 0; t < T.nterm; ++t) {
+            const C2<R> W = T.wt[t * E + e];
+            C2<R> g1 = cz<R>();
+#pragma unroll
+            for (int q = 0; q < N; ++q)
+                if (q == col) g1 = cmul(W, cmul(ph1[L.m[q] + MM], tl.G1[t][q]));
+#pragma unroll
+            for (int a = 0; a < N; ++a)
+                Trow[a] = cfma(g1, cscl(tl.G2[t][a], g.dterm[t][(m2 + 3) * 7 + L.m[a] + 3]), Trow[a]);
+        }
+        C2<R> acc[N];
+#pragma unroll
+        for (int a = 0; a < N; ++a) acc[a] = cz<R>();
+        C2<R> pi[CI + 1], ci[CI + 1], po[CO + 1], co[CO + 1], dpi[CI + 1], dci[CI + 1], dpo[CO + 1], dco[CO + 1];
+#pragma unroll
+        for (int j = 0; j <= CI; ++j) pi[j] = ci[j] = dpi[j] = dci[j] = cz<R>();
+#pragma unroll
+        for (int j = 0; j <= CO; ++j) po[j] = co[j] = dpo[j] = dco[j] = cz<R>();
+        pi[1] = ci[1] = po[1] = co[1] = C2<R>{R(1), R(0)};
+        C2<R> gi = cz<R>(), go = cz<R>(), gb = cz<R>();
+        for (int il = 1; il <= ilx; ++il) {
+            const C2<R> t = tlk[(size_t)il * E];
+            const R *dr = dh + (size_t)il * DS;
+            const R *ddr = dhd + (size_t)il * DS;
+            C2<R> tco = cz<R>(), tdco = cz<R>();
+#pragma unroll
+            for (int j = 1; j <= CO; ++j)
+                if (j == n2 + 1) { tco = cmul(t, co[j]); tdco = cmul(t, dco[j]); }
+#pragma unroll
+            for (int a = 0; a < N; ++a) {
+                const int m1 = L.m[a];
+                const int am = m1 < 0 ? -m1 : m1;
+                const bool can = canonical(m1, m2);
+                const int idx = can ? dcanon(MM, m1, m2) : dcanon(MM, -m1, -m2);
+                R dv = dr[idx], ddv = ddr[idx];
+                if (!can && ((m1 - m2) & 1)) { dv = -dv; ddv = -ddv; }
+                const int cidx = am + L.n[a] + 1;
+                const C2<R> u = cmul(ci[cidx], tco);
+                acc[a] = cfmr(u, dv, acc[a]);
+                const C2<R> w = cmul(ph[m1 + MM], Trow[a]);
+                gi = cfma(cscl(w, dv), cmul(dci[cidx], tco), gi);
+                go = cfma(cscl(w, dv), cmul(ci[cidx], tdco), go);
+                gb = cfma(cscl(w, ddv), u, gb);
+            }
+            const R wt = R(2 * il - 1);
+            const C2<R> wi = cscl(z_in, wt), wo = cscl(z_out, wt), wdi = cscl(dz_in, wt), wdo = cscl(dz_out, wt);
+            C2<R> ni[CI + 1], no[CO + 1], dni[CI + 1], dno[CO + 1];
+#pragma unroll
+            for (int j = 1; j <= CI; ++j) {
+                const C2<R> sv = j > 1 ? cadd(ci[j], ci[j - 1]) : ci[j];
+                const C2<R> dsv = j > 1 ? cadd(dci[j], dci[j - 1]) : dci[j];
+                ni[j] = cfms(wi, sv, pi[j]);
+                dni[j] = cfms(wdi, sv, cfms(wi, dsv, dpi[j]));
+            }
+#pragma unroll
+            for (int j = 1; j <= CO; ++j) {
+                const C2<R> sv = j > 1 ? cadd(co[j], co[j - 1]) : co[j];
+                const C2<R> dsv = j > 1 ? cadd(dco[j], dco[j - 1]) : dco[j];
+                no[j] = cfms(wo, sv, po[j]);
+                dno[j] = cfms(wdo, sv, cfms(wo, dsv, dpo[j]));
+            }
+#pragma unroll
+            for (int j = 1; j <= CI; ++j) { pi[j] = ci[j]; ci[j] = ni[j]; dpi[j] = dci[j]; dci[j] = dni[j]; }
+#pragma unroll
+            for (int j = 1; j <= CO; ++j) { po[j] = co[j]; co[j] = no[j]; dpo[j] = dco[j]; dco[j] = dno[j]; }
+        }
+        C2<R> ge = cz<R>();
+#pragma unroll
+        for (int a = 0; a < N; ++a) {
+            const C2<R> v = cmul(cmul(ph[L.m[a] + MM], Trow[a]), acc[a]);
+            ge = cadd(ge, C2<R>{v.y * R(L.m[a]), -v.x * R(L.m[a])});
+        }
+        add_re(pg.ri[2], sck, gi);
+        add_re(pg.ri[1], sck, go);
+        add_re(pg.beta[1], sd, gb);
+        add_re(pg.eta[2], sd, ge);
+        // the termination row col with column col of F as P(b, col)
+        C2<R> ge1 = cz<R>(), gbn = cz<R>(), gr1 = cz<R>(), grn = cz<R>();
+        ptrac = cadd(ptrac, term_adj<R, KIND>(
+                                g, dterm_db, T, e, tl, [&](int b, int) { return cmul(ph[L.m[b] + MM], acc[b]); }, ge1,
+                                gbn, gr1, grn, col, col + 1));
+        add_re(pg.eta[1], sd, ge1);
+        add_re(pg.beta[2], sd, gbn);
+        add_re(pg.ri[1], sck, gr1);
+        add_re(pg.ri[2], sck, grn);
+    }
+    cfac_grad(g, T, e, 2, gbar, cmul(ptrac, cf), pg);
 }
 
 template <typename R, int EDGE>
-fg_status Launch<R, EDGE>::fused_bwd(const StageView &, const Tables<R> &, const fg_paths *, int, const double *,
-                                     const double *, const int *, const double *, const void *, const double *,
-                                     double *, double *, unsigned char *, int, cudaStream_t)
+__device__ __forceinline__ void path_energy_adj(const WarpPath<R> &g, const R *dh, const R *dhd,
+                                                const R (*dterm_db)[49], const Tables<R> &T, int e, int nleg,
+                                                C2<R> gbar, ParGrad &pg)
 {
-    return fail(FG_ERR_NOT_IMPLEMENTED, "adjoint not built yet");
+    using K = Kinds<EDGE>;
+    if (nleg == 2) {
+        if constexpr (EDGE == 1)
+            energy_ss_sym_adj<R, K::SS>(g, dh, dhd, dterm_db, T, e, gbar, pg);
+        else
+            energy_ss_col_adj<R, K::SS>(g, dh, dhd, dterm_db, T, e, gbar, pg);
+        return;
+    }
+    energy_ms_adj<R, K::MS>(g, dh, dhd, dterm_db, T, e, nleg, gbar, pg);
+}
+
+// ------------------------------------------------------------------------------------------------ kernels
+template <typename R> struct AdjShared {
+    R dterm_db[2][49];
+    double gpar[3 * (kMaxLeg + 1)];
+};
+
+template <typename R> __host__ __device__ constexpr size_t adj_head_bytes()
+{
+    return geo_bytes<R>() + (sizeof(AdjShared<R>) + 15) / 16 * 16;
+}
+
+template <typename R> inline size_t adj_warp_bytes(int L1, int nsc_max, int MM)
+{
+    return adj_head_bytes<R>() + 2 * align_up((size_t)nsc_max * (L1 + 1) * dstride(MM) * sizeof(R), 16);
+}
+
+// Geometry adjoint: dL/dcoords (nleg, 3) of one path from the reduced parameter gradients in gpar (bohr units),
+// one coordinate direction per lane (dual numbers through leg_geometry).
+template <typename R>
+__device__ __forceinline__ double coord_grad(const WarpPath<R> &g, const double *gpar, int nleg, int lane)
+{
+    if (lane >= 3 * nleg) return 0.0;
+    const int atom = lane / 3, comp = lane % 3;
+    const double inv = 1.0 / kBohr;
+    auto rat = [&](int i, Dual *o) {
+        const int a = (i == 0 || i == nleg) ? 0 : i;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o[c] = Dual{g.xyz[a][c], (a == atom && c == comp) ? inv : 0.0};
+    };
+    Dual alpha_prev = Dual{0.0, 0.0};
+    double out = 0.0;
+    // alpha_0 = alpha_nleg: evaluate leg nleg first
+    {
+        const LegGeomT<Dual> lg = leg_geometry<Dual>(rat, nleg, nleg);
+        alpha_prev = lg.alpha;
+    }
+    for (int j = 1; j <= nleg; ++j) {
+        const LegGeomT<Dual> lg = leg_geometry<Dual>(rat, j, nleg);
+        const double deta = alpha_prev.d + lg.gamma.d;
+        out += gpar[j] * lg.ri.d + gpar[(kMaxLeg + 1) + j] * lg.beta.d + gpar[2 * (kMaxLeg + 1) + j] * deta;
+        alpha_prev = lg.alpha;
+    }
+    return out;
+}
+
+// The adjoint over a set of paths: per path the seeds gbar (E, complex) and dL/dreff (A), out dL/dcoords.
+// Paths come from `order` (or are 0..B-1), coordinates/ipots with a row stride of `stride` legs.
+template <typename R, int EDGE, typename CT>
+__global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restrict__ coords,
+                                                  const int64_t *__restrict__ ipots, int stride,
+                                                  const int *__restrict__ nlegs, int nleg_uniform, int64_t B,
+                                                  const int *__restrict__ order, const C2<R> *__restrict__ gbar,
+                                                  const double *__restrict__ greff_d, const R *__restrict__ greff_r,
+                                                  R *__restrict__ gout_r, double *__restrict__ gout_d,
+                                                  unsigned long long *counter, int nsc_max, size_t wbytes)
+{
+    using K = Kinds<EDGE>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int E = T.E, L1 = T.L1;
+    unsigned char *base = smem + (size_t)w * wbytes;
+    WarpPath<R> &g = *reinterpret_cast<WarpPath<R> *>(base);
+    AdjShared<R> &as = *reinterpret_cast<AdjShared<R> *>(base + geo_bytes<R>());
+    const size_t dsz = align_up((size_t)nsc_max * (L1 + 1) * dstride(K::MM) * sizeof(R), 16);
+    R *dh = reinterpret_cast<R *>(base + adj_head_bytes<R>());
+    R *dhd = reinterpret_cast<R *>(base + adj_head_bytes<R>() + dsz);
+    for (;;) {
+        unsigned long long tk = 0;
+        if (lane == 0) tk = atomicAdd(counter, 1ull);
+        tk = __shfl_sync(0xffffffffu, tk, 0);
+        if (tk >= (unsigned long long)B) break;
+        const int64_t p = order ? order[tk] : (int64_t)tk;
+        const int nleg = nlegs ? nlegs[p] : nleg_uniform;
+        const int MM = nleg == 2 ? K::MMSS : K::MMMS;
+        path_setup<R, CT>(g, dh, T, coords + p * stride * 3, ipots + p * stride, nleg, lane, nullptr, MM);
+        adj_setup<R>(g, dhd, as.dterm_db, T, nleg, lane, MM);
+        __syncwarp();
+        ParGrad pg;
+        for (int j = 0; j <= kMaxLeg; ++j) pg.ri[j] = pg.beta[j] = pg.eta[j] = 0.0;
+        for (int e0 = 0; e0 < E; e0 += 32) {
+            const int e = e0 + lane;
+            if (e < E) path_energy_adj<R, EDGE>(g, dh, dhd, as.dterm_db, T, e, nleg, gbar[p * E + e], pg);
+        }
+        // fixed-order warp reduction of the per-lane sums
+        for (int j = 1; j <= nleg; ++j) {
+            double v[3] = {pg.ri[j], pg.beta[j], pg.eta[j]};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+            }
+            if (lane == 0) {
+                as.gpar[j] = v[0];
+                as.gpar[(kMaxLeg + 1) + j] = v[1];
+                as.gpar[2 * (kMaxLeg + 1) + j] = v[2];
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            // reff (A) = BOHR sum ri (bohr) / 2
+            const double gr = greff_d ? greff_d[p] : (greff_r ? (double)greff_r[p] : 0.0);
+            for (int j = 1; j <= nleg; ++j) as.gpar[j] += gr * kBohr * 0.5;
+        }
+        __syncwarp();
+        const double gc = coord_grad<R>(g, as.gpar, nleg, lane);
+        if (lane < 3 * stride) {
+            const int64_t o = p * stride * 3 + lane;
+            const double v = lane < 3 * nleg ? gc : 0.0;
+            if (gout_d) gout_d[o] = v;
+            else gout_r[o] = (R)v;
+        }
+        __syncwarp();
+    }
+}
+
+// Fine-grid adjoint (stage.py:372-388 differentiated): per path, from upstream weights G(q) on the fine grid, the
+// seeds gbar(e) = dL/dRe(cchi) + i dL/dIm(cchi), dL/dreff (A) and, with per-path sigma2, dL/dsigma2.
+// mode 0: G = grad_chi[p][q] (chi_fine's adjoint); mode 1: G = grad_rows[row[p]][q] deg[p] exp(-2 sigma2 q^2)
+// (the fused sum's adjoint).  Interpolation transposed with the column ranges tspan of S.
+template <typename R>
+__global__ void __launch_bounds__(256) k_fine_adjoint(int64_t B, int E, int NK, int mode,
+                                                       const C2<R> *__restrict__ cchi, const R *__restrict__ reff_r,
+                                                       const double *__restrict__ reff_d, const R *__restrict__ q_r,
+                                                       const double *__restrict__ q_d, const R *__restrict__ S_r,
+                                                       const double *__restrict__ S_d, const int *__restrict__ span,
+                                                       const int *__restrict__ tspan, const R *__restrict__ gchi,
+                                                       const double *__restrict__ grows, const int *__restrict__ row,
+                                                       const double *__restrict__ deg, const double *__restrict__ sigma2,
+                                                       C2<R> *__restrict__ gbar, R *__restrict__ greff_r,
+                                                       double *__restrict__ greff_d, double *__restrict__ gsig,
+                                                       size_t wbytes)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    unsigned char *base = smem + (size_t)w * wbytes;
+    R *amp = reinterpret_cast<R *>(base);
+    double *pha = reinterpret_cast<double *>(base + align_up((size_t)E * sizeof(R), 16));
+    double *dA = reinterpret_cast<double *>(base + align_up((size_t)E * sizeof(R), 16) + align_up((size_t)E * 8, 16));
+    double *dP = dA + NK;
+    auto Sv = [&](int k, int j) { return S_d ? S_d[(size_t)k * E + j] : (double)S_r[(size_t)k * E + j]; };
+    for (int64_t p = (int64_t)blockIdx.x * nw + w; p < B; p += (int64_t)gridDim.x * nw) {
+        const C2<R> *c = cchi + p * E;
+        amp_phase<R>(E, lane, [&](int e) { return c[e]; }, amp, pha);
+        __syncwarp();
+        const double rf = reff_d ? reff_d[p] : (double)reff_r[p];
+        const double s2 = (mode == 1 && sigma2) ? sigma2[p] : 0.0;
+        const double wd = mode == 1 ? deg[p] : 1.0;
+        const double *gr = mode == 1 ? grows + (int64_t)row[p] * NK : nullptr;
+        double g_reff = 0.0, g_s2 = 0.0;
+        for (int k0 = 0; k0 < NK; k0 += 32) {
+            const int k = k0 + lane;
+            double da = 0.0, dp = 0.0;
+            if (k < NK) {
+                const int lo = span[2 * k], hi = span[2 * k + 1];
+                double a = 0.0, ph = 0.0;
+                for (int j = lo; j < hi; ++j) {
+                    const double sv = Sv(k, j);
+                    a += sv * (double)amp[j];
+                    ph += sv * pha[j];
+                }
+                const double qk = q_d ? q_d[k] : (double)q_r[k];
+                const double damp = exp(-2.0 * s2 * qk * qk);
+                const double G = (mode == 1 ? gr[k] * wd : (double)gchi[p * NK + k]) * damp;
+                const double arg = ph + 2.0 * qk * rf;
+                const double sn = sin_arg<R>(arg), cs = sin_arg<R>(arg + 1.5707963267948966);
+                da = G * sn;
+                dp = G * a * cs;
+                g_reff += dp * 2.0 * qk;
+                g_s2 += G * a * sn * (-2.0 * qk * qk);
+                dA[k] = da;
+                dP[k] = dp;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            g_reff += __shfl_xor_sync(0xffffffffu, g_reff, o);
+            g_s2 += __shfl_xor_sync(0xffffffffu, g_s2, o);
+        }
+        __syncwarp();
+        for (int e0 = 0; e0 < E; e0 += 32) {
+            const int e = e0 + lane;
+            if (e < E) {
+                const int lo = tspan[2 * e], hi = tspan[2 * e + 1];
+                double ga = 0.0, gp = 0.0;
+                for (int k = lo; k < hi; ++k) {
+                    const double sv = Sv(k, e);
+                    ga += sv * dA[k];
+                    gp += sv * dP[k];
+                }
+                const C2<R> cv = c[e];
+                const double x = (double)cv.x, y = (double)cv.y;
+                const double a = sqrt(x * x + y * y + 1e-30);
+                double gx = ga * x / a, gy = ga * y / a;
+                if (a >= 1e-16) {
+                    const double r2 = x * x + y * y;
+                    gx += gp * (-y) / r2;
+                    gy += gp * x / r2;
+                }
+                gbar[p * E + e] = C2<R>{(R)gx, (R)gy};
+            }
+        }
+        if (lane == 0) {
+            if (greff_d) greff_d[p] = g_reff;
+            if (greff_r) greff_r[p] = (R)g_reff;
+            if (gsig) gsig[p] = g_s2;
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ launches
+template <typename R, int EDGE, typename CT>
+fg_status launch_adjoint(const StageView &sv, const Tables<R> &T, const CT *coords, const int64_t *ipots, int stride,
+                         const int *nlegs, int nleg_uniform, int nsc_max, int64_t B, const int *order,
+                         const C2<R> *gbar, const double *greff_d, const R *greff_r, R *gout_r, double *gout_d,
+                         unsigned long long *counter, int warps, cudaStream_t st)
+{
+    using K = Kinds<EDGE>;
+    const int threads = warps * 32;
+    const size_t wb = adj_warp_bytes<R>(sv.L1, nsc_max, K::MM);
+    auto kern = k_adjoint<R, EDGE, CT>;
+    int blocks = 0;
+    if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;
+    FG_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+    timer_begin(st);
+    kern<<<blocks, threads, wb * warps, st>>>(T, coords, ipots, stride, nlegs, nleg_uniform, B, order, gbar, greff_d,
+                                              greff_r, gout_r, gout_d, counter, nsc_max, wb);
+    timer_end(st);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
 }
 
 template <typename R>
-fg_status LaunchCommon<R>::chi_fine_bwd(const StageView &, int64_t, const void *, const void *, int, const void *,
-                                        const void *, const int *, const void *, void *, void *, cudaStream_t)
+fg_status launch_fine_adjoint(const StageView &sv, int64_t B, int NK, int mode, const void *cchi, const R *reff_r,
+                              const double *reff_d, const R *q_r, const double *q_d, const R *S_r, const double *S_d,
+                              const int *span, const int *tspan, const R *gchi, const double *grows, const int *row,
+                              const double *deg, const double *sigma2, C2<R> *gbar, R *greff_r, double *greff_d,
+                              double *gsig, cudaStream_t st)
 {
-    return fail(FG_ERR_NOT_IMPLEMENTED, "adjoint not built yet");
+    const int warps = 4, threads = warps * 32;
+    const size_t wb = align_up((size_t)sv.E * sizeof(R), 16) + align_up((size_t)sv.E * 8, 16) +
+                      align_up((size_t)NK * 16, 16);
+    auto kern = k_fine_adjoint<R>;
+    int blocks = 0;
+    if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;
+    kern<<<blocks, threads, wb * warps, st>>>(B, sv.E, NK, mode, static_cast<const C2<R> *>(cchi), reff_r, reff_d, q_r,
+                                              q_d, S_r, S_d, span, tspan, gchi, grows, row, deg, sigma2, gbar, greff_r,
+                                              greff_d, gsig, wb);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+template <typename R, int EDGE>
+fg_status Launch<R, EDGE>::cchi_bwd(const StageView &sv, const Tables<R> &T, int64_t B, int nleg, const void *coords,
+                                    int coords_f64, const int64_t *ipots, const void *grad_cchi, const void *grad_reff,
+                                    void *grad_coords, unsigned char *ws, int warps, cudaStream_t st)
+{
+    unsigned long long *counter = reinterpret_cast<unsigned long long *>(ws);
+    const C2<R> *gb = static_cast<const C2<R> *>(grad_cchi);
+    const R *gr = static_cast<const R *>(grad_reff);
+    if (coords_f64)
+        return launch_adjoint<R, EDGE, double>(sv, T, static_cast<const double *>(coords), ipots, nleg, nullptr, nleg,
+                                               nleg - 1, B, nullptr, gb, nullptr, gr, static_cast<R *>(grad_coords),
+                                               nullptr, counter, warps, st);
+    return launch_adjoint<R, EDGE, float>(sv, T, static_cast<const float *>(coords), ipots, nleg, nullptr, nleg,
+                                          nleg - 1, B, nullptr, gb, nullptr, gr, static_cast<R *>(grad_coords),
+                                          nullptr, counter, warps, st);
+}
+
+template <typename R, int EDGE>
+fg_status Launch<R, EDGE>::fused_bwd(const StageView &sv, const Tables<R> &T, const fg_paths *P, int NK,
+                                     const double *q, const double *S, const int *span, const int *tspan,
+                                     const double *grad_rows, const void *cchi_saved, const double *reff_saved,
+                                     double *grad_coords, double *grad_sigma2, unsigned char *ws, int warps,
+                                     cudaStream_t st)
+{
+    unsigned long long *counter = reinterpret_cast<unsigned long long *>(ws);
+    C2<R> *gbar = reinterpret_cast<C2<R> *>(ws + kCounterBytes);
+    double *greff = reinterpret_cast<double *>(ws + kCounterBytes + align_up((size_t)P->n * sv.E * sizeof(C2<double>), 256));
+    if (P->n == 0) return FG_OK;
+    if (fg_status rc = launch_fine_adjoint<R>(sv, P->n, NK, 1, cchi_saved, nullptr, reff_saved, nullptr, q, nullptr, S,
+                                              span, tspan, nullptr, grad_rows, P->row, P->deg, P->sigma2, gbar, nullptr,
+                                              greff, grad_sigma2, st))
+        return rc;
+    return launch_adjoint<R, EDGE, double>(sv, T, P->coords, P->ipots, P->nleg_max, P->nleg, 0, P->nleg_max - 1, P->n,
+                                           P->order, gbar, greff, nullptr, nullptr, grad_coords, counter, warps, st);
+}
+
+template <typename R>
+fg_status LaunchCommon<R>::chi_fine_bwd(const StageView &sv, int64_t B, const void *cchi, const void *reff, int NK,
+                                        const void *q, const void *S, const int *span, const int *tspan,
+                                        const void *grad_chi, void *grad_cchi, void *grad_reff, cudaStream_t st)
+{
+    return launch_fine_adjoint<R>(sv, B, NK, 0, cchi, static_cast<const R *>(reff), nullptr, static_cast<const R *>(q),
+                                  nullptr, static_cast<const R *>(S), nullptr, span, tspan,
+                                  static_cast<const R *>(grad_chi), nullptr, nullptr, nullptr, nullptr,
+                                  static_cast<C2<R> *>(grad_cchi), static_cast<R *>(grad_reff), nullptr, nullptr, st);
 }
 
 }  // namespace fg

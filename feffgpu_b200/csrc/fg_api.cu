@@ -434,23 +434,23 @@ extern "C" fg_status fg_chi_fine(const fg_stage *s, fg_precision prec, int64_t B
 
 extern "C" fg_status fg_chi_fine_backward(const fg_stage *s, fg_precision prec, int64_t B, const void *cchi,
                                           const void *reff, int32_t NK, const void *q, const void *S,
-                                          const int32_t *span, const void *grad_chi, void *grad_cchi,
-                                          void *grad_reff, void *stream)
+                                          const int32_t *span, const int32_t *tspan, const void *grad_chi,
+                                          void *grad_cchi, void *grad_reff, void *stream)
 {
     g_err.clear();
     if (!s) return fail(FG_ERR_VALUE, "null stage");
     if (B < 0 || NK < 0) return fail(FG_ERR_VALUE, "negative size");
     if (B == 0) return FG_OK;
-    if (!cchi || !reff || !q || !S || !span || !grad_chi || !grad_cchi || !grad_reff)
+    if (!cchi || !reff || !q || !S || !span || !tspan || !grad_chi || !grad_cchi || !grad_reff)
         return fail(FG_ERR_VALUE, "null array");
     if (fg_status rc = set_device(s)) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (prec == FG_FP64)
-        return LaunchCommon<double>::chi_fine_bwd(view(s), B, cchi, reff, NK, q, S, span, grad_chi, grad_cchi,
+        return LaunchCommon<double>::chi_fine_bwd(view(s), B, cchi, reff, NK, q, S, span, tspan, grad_chi, grad_cchi,
                                                   grad_reff, st);
     if (prec != FG_MIXED) return fail(FG_ERR_VALUE, "precision must be FG_MIXED or FG_FP64");
-    return LaunchCommon<float>::chi_fine_bwd(view(s), B, cchi, reff, NK, q, S, span, grad_chi, grad_cchi, grad_reff,
-                                             st);
+    return LaunchCommon<float>::chi_fine_bwd(view(s), B, cchi, reff, NK, q, S, span, tspan, grad_chi, grad_cchi,
+                                             grad_reff, st);
 }
 
 extern "C" size_t fg_chi_reduce_workspace(const fg_stage *s, const fg_paths *P, int32_t NK)
@@ -485,12 +485,12 @@ extern "C" fg_status fg_chi_reduce(const fg_stage *s, fg_precision prec, const f
 extern "C" size_t fg_chi_reduce_backward_workspace(const fg_stage *s, const fg_paths *P, int32_t NK)
 {
     if (!s || !P || NK < 0) return 0;
-    return fused_bwd_workspace(P, NK);
+    return fused_bwd_workspace(P, NK, s->E);
 }
 
 extern "C" fg_status fg_chi_reduce_backward(const fg_stage *s, fg_precision prec, const fg_paths *P, int32_t NK,
                                             const double *q, const double *S, const int32_t *span,
-                                            const double *grad_rows, const void *cchi_saved,
+                                            const int32_t *tspan, const double *grad_rows, const void *cchi_saved,
                                             const double *reff_saved, double *grad_coords, double *grad_sigma2,
                                             void *workspace, size_t workspace_bytes, void *stream)
 {
@@ -499,16 +499,17 @@ extern "C" fg_status fg_chi_reduce_backward(const fg_stage *s, fg_precision prec
     if (fg_status rc = check_paths(P)) return rc;
     if (NK < 0) return fail(FG_ERR_VALUE, "negative NK");
     if (P->n == 0) return FG_OK;
-    if (!q || !S || !span || !grad_rows || !cchi_saved || !reff_saved || !grad_coords)
+    if (!q || !S || !span || !tspan || !grad_rows || !cchi_saved || !reff_saved || !grad_coords)
         return fail(FG_ERR_VALUE, "null array");
-    const size_t need = fused_bwd_workspace(P, NK);
+    const size_t need = fused_bwd_workspace(P, NK, s->E);
     if (need && (!workspace || workspace_bytes < need))
         return fail(FG_ERR_WORKSPACE, "workspace needs " + std::to_string(need) + " bytes");
     if (fg_status rc = set_device(s)) return rc;
     const StageView sv = view(s);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return by_kind(s, prec, [&](auto L, const auto &T) {
-        return decltype(L)::fused_bwd(sv, T, P, NK, q, S, span, grad_rows, cchi_saved, reff_saved, grad_coords,
-                                      grad_sigma2, static_cast<unsigned char *>(workspace), g_bwd_warps, st);
+        return decltype(L)::fused_bwd(sv, T, P, NK, q, S, span, tspan, grad_rows, cchi_saved, reff_saved,
+                                      grad_coords, grad_sigma2, static_cast<unsigned char *>(workspace), g_bwd_warps,
+                                      st);
     });
 }

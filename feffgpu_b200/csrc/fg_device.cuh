@@ -165,55 +165,96 @@ template <typename R> struct Tables {
 };
 
 // ------------------------------------------------------------------------------------------------ geometry
-// trig.f, as stage.py:148-157 and genfmt.py:56-69
-__device__ __forceinline__ void trig(double x, double y, double z, double &ct, double &st, double &cp, double &sp)
+// Forward-mode dual number (value, derivative along one direction): the adjoint differentiates the geometry by
+// running it once per coordinate direction, one direction per lane.
+struct Dual {
+    double v, d;
+};
+__device__ __forceinline__ double val(double x) { return x; }
+__device__ __forceinline__ double val(Dual x) { return x.v; }
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return Dual{a.v + b.v, a.d + b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return Dual{a.v - b.v, a.d - b.d}; }
+__device__ __forceinline__ Dual operator-(Dual a) { return Dual{-a.v, -a.d}; }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return Dual{a.v * b.v, a.d * b.v + a.v * b.d}; }
+__device__ __forceinline__ Dual operator/(Dual a, Dual b)
 {
-    const double r = sqrt(x * x + y * y + z * z), rxy = sqrt(x * x + y * y);
-    const bool sr = r < 1e-6, sxy = rxy < 1e-6;
-    ct = sr ? 1.0 : z / r;
-    st = sr ? 0.0 : rxy / r;
-    cp = sxy ? (ct < 0 ? -1.0 : 1.0) : x / rxy;
-    sp = sxy ? 0.0 : y / rxy;
+    const double q = a.v / b.v;
+    return Dual{q, (a.d - q * b.d) / b.v};
+}
+__device__ __forceinline__ Dual operator*(double a, Dual b) { return Dual{a * b.v, a * b.d}; }
+__device__ __forceinline__ Dual operator+(double a, Dual b) { return Dual{a + b.v, b.d}; }
+__device__ __forceinline__ Dual operator-(double a, Dual b) { return Dual{a - b.v, -b.d}; }
+__device__ __forceinline__ Dual sqrt(Dual a)
+{
+    const double r = ::sqrt(a.v);
+    return Dual{r, r > 0.0 ? a.d / (2.0 * r) : 0.0};
+}
+__device__ __forceinline__ Dual atan2(Dual y, Dual x)
+{
+    const double den = x.v * x.v + y.v * y.v;
+    return Dual{::atan2(y.v, x.v), den > 0.0 ? (x.v * y.d - y.v * x.d) / den : 0.0};
+}
+// keep the math library's overloads visible beside the Dual ones
+using ::atan2;
+using ::sqrt;
+
+template <typename S> __device__ __forceinline__ S cst(double v);
+template <> __device__ __forceinline__ double cst<double>(double v) { return v; }
+template <> __device__ __forceinline__ Dual cst<Dual>(double v) { return Dual{v, 0.0}; }
+
+// trig.f, as stage.py:148-157 and genfmt.py:56-69; the small-vector branches are constants (zero derivative)
+template <typename S>
+__device__ __forceinline__ void trig(S x, S y, S z, S &ct, S &st, S &cp, S &sp)
+{
+    const S r = sqrt(x * x + y * y + z * z), rxy = sqrt(x * x + y * y);
+    const bool sr = val(r) < 1e-6, sxy = val(rxy) < 1e-6;
+    ct = sr ? cst<S>(1.0) : z / r;
+    st = sr ? cst<S>(0.0) : rxy / r;
+    cp = sxy ? cst<S>(val(ct) < 0 ? -1.0 : 1.0) : x / rxy;
+    sp = sxy ? cst<S>(0.0) : y / rxy;
 }
 
-// arg with FEFF's 1e-6 thresholds (stage.py:160-168)
-__device__ __forceinline__ double arg_fi(double x, double y, double fi)
+// arg with FEFF's 1e-6 thresholds (stage.py:160-168): a component below the threshold counts as zero (and has
+// no derivative), both zero gives fi
+template <typename S> __device__ __forceinline__ S arg_fi(S x, S y, S fi)
 {
-    x = fabs(x) < 1e-6 ? 0.0 : x;
-    y = fabs(y) < 1e-6 ? 0.0 : y;
-    return (x == 0.0 && y == 0.0) ? fi : atan2(y, x);
+    x = fabs(val(x)) < 1e-6 ? cst<S>(0.0) : x;
+    y = fabs(val(y)) < 1e-6 ? cst<S>(0.0) : y;
+    return (val(x) == 0.0 && val(y) == 0.0) ? fi : atan2(y, x);
 }
 
 // Leg j (1-based) of a path: length (bohr), scattering angle beta and the Euler angles alpha, gamma
-// (pathgeom, stage.py:170-206).  rat(j) returns atom j in bohr; atom 0 and atom nleg are the absorber.
-struct LegGeom { double ri, beta, alpha, gamma; };
+// (pathgeom, stage.py:170-206).  rat(i, o) writes atom i in bohr; atom 0 and atom nleg are the absorber.
+template <typename S> struct LegGeomT { S ri, beta, alpha, gamma; };
+using LegGeom = LegGeomT<double>;
 
-template <class Rat> __device__ __forceinline__ LegGeom leg_geometry(const Rat &rat, int j, int nleg)
+template <typename S, class Rat> __device__ __forceinline__ LegGeomT<S> leg_geometry(const Rat &rat, int j, int nleg)
 {
     const int nsc = nleg - 1;
     int i, ip1, im1;
     if (j == nsc + 1) { i = 0; ip1 = 1; im1 = nsc; } else { i = j; ip1 = j + 1; im1 = j - 1; }
-    double ai[3], bi[3], ci[3];
+    S ai[3], bi[3], ci[3];
     rat(i, ai); rat(ip1, bi); rat(im1, ci);
-    double ctp, stp, cpp, spp, ct, st, cp, sp;
-    trig(bi[0] - ai[0], bi[1] - ai[1], bi[2] - ai[2], ctp, stp, cpp, spp);
-    trig(ai[0] - ci[0], ai[1] - ci[1], ai[2] - ci[2], ct, st, cp, sp);
-    const double cppp = cp * cpp + sp * spp, sppp = spp * cp - cpp * sp;
-    const double phi = atan2(sp, cp), phip = atan2(spp, cpp);
-    const double ax = -(st * ctp - ct * stp * cppp), ay = stp * sppp;
-    double b = ct * ctp + st * stp * cppp;
-    b = fmin(1.0, fmax(-1.0, b));
-    const double u1x = st * cp, u1y = st * sp, u1z = ct, u2x = stp * cpp, u2y = stp * spp, u2z = ctp;
-    const double wx = u1y * u2z - u1z * u2y, wy = u1z * u2x - u1x * u2z, wz = u1x * u2y - u1y * u2x;
-    const double sb2 = wx * wx + wy * wy + wz * wz;
-    const double gx = -(st * ctp * cppp - ct * stp), gy = -st * sppp;
-    const double a_j = arg_fi(ax, ay, phip - phi);
-    const double g_j = arg_fi(gx, gy, 0.0);
-    LegGeom g;
+    S ctp, stp, cpp, spp, ct, st, cp, sp;
+    trig<S>(bi[0] - ai[0], bi[1] - ai[1], bi[2] - ai[2], ctp, stp, cpp, spp);
+    trig<S>(ai[0] - ci[0], ai[1] - ci[1], ai[2] - ci[2], ct, st, cp, sp);
+    const S cppp = cp * cpp + sp * spp, sppp = spp * cp - cpp * sp;
+    const S phi = atan2(sp, cp), phip = atan2(spp, cpp);
+    const S ax = -(st * ctp - ct * stp * cppp), ay = stp * sppp;
+    S b = ct * ctp + st * stp * cppp;
+    if (val(b) > 1.0) b = cst<S>(1.0);          // clamp: no derivative outside [-1, 1]
+    if (val(b) < -1.0) b = cst<S>(-1.0);
+    const S u1x = st * cp, u1y = st * sp, u1z = ct, u2x = stp * cpp, u2y = stp * spp, u2z = ctp;
+    const S wx = u1y * u2z - u1z * u2y, wy = u1z * u2x - u1x * u2z, wz = u1x * u2y - u1y * u2x;
+    const S sb2 = wx * wx + wy * wy + wz * wz;
+    const S gx = -(st * ctp * cppp - ct * stp), gy = -st * sppp;
+    const S a_j = arg_fi<S>(ax, ay, phip - phi);
+    const S g_j = arg_fi<S>(gx, gy, cst<S>(0.0));
+    LegGeomT<S> g;
     g.alpha = M_PI - g_j;
     g.gamma = M_PI - a_j;
-    g.beta = atan2(sqrt(sb2 + 1e-30), b);
-    const double dx = ai[0] - ci[0], dy = ai[1] - ci[1], dz = ai[2] - ci[2];
+    g.beta = atan2(sqrt(sb2 + cst<S>(1e-30)), b);
+    const S dx = ai[0] - ci[0], dy = ai[1] - ci[1], dz = ai[2] - ci[2];
     g.ri = sqrt(dx * dx + dy * dy + dz * dz);
     return g;
 }
@@ -237,6 +278,38 @@ __device__ __forceinline__ double wigner_small(int l, int m, int n, double c2, d
         for (int q = 0; q < pc; ++q) pw *= c2;
         for (int q = 0; q < ps; ++q) pw *= s2;
         out += term * pw;
+    }
+    return out;
+}
+
+// d/dbeta of d^l_{mn}(beta) for l <= 3 (the derivative of the half-angle powers of Wigner's sum)
+__device__ __forceinline__ double wigner_small_dbeta(int l, int m, int n, double c2, double s2)
+{
+    if (abs(m) > l || abs(n) > l) return 0.0;
+    const double f[8] = {1, 1, 2, 6, 24, 120, 720, 5040};
+    const double pref = sqrt(f[l + m] * f[l - m] * f[l + n] * f[l - n]);
+    double out = 0.0;
+    for (int k = 0; k <= 2 * l; ++k) {
+        const int a = l + n - k, b = k, c = m - n + k, d = l - m - k;
+        if (a < 0 || b < 0 || c < 0 || d < 0) continue;
+        double term = pref / (f[a] * f[b] * f[c] * f[d]);
+        if ((m - n + k) & 1) term = -term;
+        const int pc = 2 * l + n - m - 2 * k, ps = m - n + 2 * k;
+        // d/dbeta c2^pc s2^ps = (ps c2^(pc+1) s2^(ps-1) - pc c2^(pc-1) s2^(ps+1)) / 2
+        double t1 = 0.0, t2 = 0.0;
+        if (ps > 0) {
+            double pw = 1.0;
+            for (int q = 0; q < pc + 1; ++q) pw *= c2;
+            for (int q = 0; q < ps - 1; ++q) pw *= s2;
+            t1 = ps * pw;
+        }
+        if (pc > 0) {
+            double pw = 1.0;
+            for (int q = 0; q < pc - 1; ++q) pw *= c2;
+            for (int q = 0; q < ps + 1; ++q) pw *= s2;
+            t2 = pc * pw;
+        }
+        out += term * 0.5 * (t1 - t2);
     }
     return out;
 }

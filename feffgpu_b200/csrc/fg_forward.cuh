@@ -62,7 +62,7 @@ __device__ void path_setup(WarpPath<R> &g, R *dh, const Tables<R> &T, const CT *
             const int a = (i == 0 || i == nleg) ? 0 : i;
             o[0] = g.xyz[a][0]; o[1] = g.xyz[a][1]; o[2] = g.xyz[a][2];
         };
-        LegGeom lg = leg_geometry(rat, lane, nleg);
+        LegGeom lg = leg_geometry<double>(rat, lane, nleg);
         g.ri[lane] = lg.ri; g.beta[lane] = lg.beta; g.alpha[lane] = lg.alpha; g.gamma[lane] = lg.gamma;
     }
     __syncwarp();

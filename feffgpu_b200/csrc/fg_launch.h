@@ -33,7 +33,8 @@ template <typename R, int EDGE> struct Launch {
                               int coords_f64, const int64_t *ipots, const void *grad_cchi, const void *grad_reff,
                               void *grad_coords, unsigned char *ws, int warps, cudaStream_t st);
     static fg_status fused_bwd(const StageView &sv, const Tables<R> &T, const fg_paths *P, int NK, const double *q,
-                               const double *S, const int *span, const double *grad_rows, const void *cchi_saved,
+                               const double *S, const int *span, const int *tspan, const double *grad_rows,
+                               const void *cchi_saved,
                                const double *reff_saved, double *grad_coords, double *grad_sigma2, unsigned char *ws,
                                int warps, cudaStream_t st);
 };
@@ -43,8 +44,8 @@ template <typename R> struct LaunchCommon {
     static fg_status chi_fine(const StageView &sv, int64_t B, const void *cchi, const void *reff, int NK,
                               const void *q, const void *S, const int *span, void *chi, cudaStream_t st);
     static fg_status chi_fine_bwd(const StageView &sv, int64_t B, const void *cchi, const void *reff, int NK,
-                                  const void *q, const void *S, const int *span, const void *grad_chi,
-                                  void *grad_cchi, void *grad_reff, cudaStream_t st);
+                                  const void *q, const void *S, const int *span, const int *tspan,
+                                  const void *grad_chi, void *grad_cchi, void *grad_reff, cudaStream_t st);
 };
 
 // Fused reduction kernels (precision independent, FP64).
@@ -56,7 +57,7 @@ void timer_begin(cudaStream_t st);
 void timer_end(cudaStream_t st);
 
 size_t fused_workspace(const fg_paths *P, int NK);
-size_t fused_bwd_workspace(const fg_paths *P, int NK);
+size_t fused_bwd_workspace(const fg_paths *P, int NK, int E);
 size_t cchi_bwd_workspace(int64_t B, int nleg);
 
 }  // namespace fg

@@ -64,8 +64,12 @@ size_t fused_workspace(const fg_paths *P, int NK)
 }  // namespace fg
 
 namespace fg {
-size_t fused_bwd_workspace(const fg_paths *, int) { return 0; }
-size_t cchi_bwd_workspace(int64_t, int) { return 0; }
+// counter, per-path seeds of the chain adjoint (n x E complex, sized for FP64), per-path dL/dreff
+size_t fused_bwd_workspace(const fg_paths *P, int, int E)
+{
+    return kCounterBytes + align_up((size_t)P->n * E * 2 * sizeof(double), 256) + align_up((size_t)P->n * sizeof(double), 256);
+}
+size_t cchi_bwd_workspace(int64_t, int) { return kCounterBytes; }
 }  // namespace fg
 
 // ------------------------------------------------------------------------------------------------ FP32 FMA peak

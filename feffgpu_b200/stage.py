@@ -36,6 +36,11 @@ def _stream(device: torch.device) -> int:
     return torch.cuda.current_stream(device).cuda_stream
 
 
+def _tspan_of(S: torch.Tensor) -> torch.Tensor:
+    """(E, 2) int32 [lo, hi) of each column's non-zero rows (the transposed interpolation's ranges)."""
+    return _span_of(S.t())
+
+
 def _span_of(S: torch.Tensor) -> torch.Tensor:
     """(NK, 2) int32 [lo, hi) of each row's non-zero columns (rows without any: [0, 0))."""
     nz = S != 0
@@ -177,13 +182,13 @@ class GPUPathStage:
         d = d - 2 * math.pi * torch.round(d / (2 * math.pi))
         return torch.cat([phase[..., :1], phase[..., :1] + torch.cumsum(d, -1)], -1)
 
-    def _span(self, S: torch.Tensor) -> torch.Tensor:
-        key = (S.data_ptr(), tuple(S.shape), S.dtype, S._version)
+    def _span(self, S: torch.Tensor, transposed: bool = False) -> torch.Tensor:
+        key = (S.data_ptr(), tuple(S.shape), S.dtype, S._version, transposed)
         sp = self._span_cache.get(key)
         if sp is None:
-            if len(self._span_cache) > 16:
+            if len(self._span_cache) > 32:
                 self._span_cache.clear()
-            sp = _span_of(S)
+            sp = _tspan_of(S) if transposed else _span_of(S)
             self._span_cache[key] = sp
         return sp
 
@@ -217,8 +222,8 @@ class GPUPathStage:
         g = g.to(reff.dtype).contiguous()
         _lib.check(self._lib.fg_chi_fine_backward(self._h, prec, B, cchi.contiguous().data_ptr(),
                                                   reff.contiguous().data_ptr(), NK, q.data_ptr(), S.data_ptr(),
-                                                  self._span(S).data_ptr(), g.data_ptr(), gc.data_ptr(),
-                                                  gr.data_ptr(), _stream(self.device)))
+                                                  self._span(S).data_ptr(), self._span(S, True).data_ptr(),
+                                                  g.data_ptr(), gc.data_ptr(), gr.data_ptr(), _stream(self.device)))
         return gc, gr
 
     # -- fused stage ----------------------------------------------------------------------------------------
@@ -271,7 +276,8 @@ class GPUPathStage:
         ws_n = int(self._lib.fg_chi_reduce_backward_workspace(self._h, C.byref(ps), NK))
         ws = batch.workspace(ws_n, backward=True)
         _lib.check(self._lib.fg_chi_reduce_backward(self._h, prec, C.byref(ps), NK, q.data_ptr(), S.data_ptr(),
-                                                    self._span(S).data_ptr(), g_rows.contiguous().data_ptr(),
+                                                    self._span(S).data_ptr(), self._span(S, True).data_ptr(),
+                                                    g_rows.contiguous().data_ptr(),
                                                     cchi.data_ptr(), reff.data_ptr(), gc.data_ptr(), _ptr(gs),
                                                     ws.data_ptr(), ws_n, _stream(self.device)))
         return gc, gs

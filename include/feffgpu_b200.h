@@ -107,10 +107,12 @@ FG_API fg_status fg_cchi_backward(const fg_stage *stage, fg_precision prec, int6
  * q (NK) and reff (B) have the precision's real type. */
 FG_API fg_status fg_chi_fine(const fg_stage *stage, fg_precision prec, int64_t B, const void *cchi, const void *reff,
                       int32_t NK, const void *q, const void *S, const int32_t *span, void *chi, void *stream);
-/* Adjoint of fg_chi_fine: grad_cchi (B, E) complex (PyTorch convention) and grad_reff (B) from grad_chi (B, NK). */
+/* Adjoint of fg_chi_fine: grad_cchi (B, E) complex (PyTorch convention) and grad_reff (B) from grad_chi (B, NK).
+ * tspan (E, 2) int32 gives each column's non-zero row range of S (the transposed interpolation). */
 FG_API fg_status fg_chi_fine_backward(const fg_stage *stage, fg_precision prec, int64_t B, const void *cchi,
                                const void *reff, int32_t NK, const void *q, const void *S, const int32_t *span,
-                               const void *grad_chi, void *grad_cchi, void *grad_reff, void *stream);
+                               const int32_t *tspan, const void *grad_chi, void *grad_cchi, void *grad_reff,
+                               void *stream);
 
 /* A batch of paths with mixed leg counts for the fused stage (one persistent launch over every leg count). */
 typedef struct fg_paths {
@@ -143,10 +145,12 @@ FG_API fg_status fg_chi_reduce(const fg_stage *stage, fg_precision prec, const f
                         void *workspace, size_t workspace_bytes, void *stream);
 
 /* Adjoint of fg_chi_reduce: grad_coords (n, nleg_max, 3) FP64 and grad_sigma2 (n) FP64 (may be NULL) from
- * grad_rows (nrows, NK), using the saved cchi and reff.  No reference counterpart for sigma^2 (a new input). */
+ * grad_rows (nrows, NK), using the saved cchi and reff; tspan as in fg_chi_fine_backward.  No reference
+ * counterpart for sigma^2 (a new input). */
 FG_API size_t fg_chi_reduce_backward_workspace(const fg_stage *stage, const fg_paths *paths, int32_t NK);
 FG_API fg_status fg_chi_reduce_backward(const fg_stage *stage, fg_precision prec, const fg_paths *paths, int32_t NK,
-                                 const double *q, const double *S, const int32_t *span, const double *grad_rows,
+                                 const double *q, const double *S, const int32_t *span, const int32_t *tspan,
+                                 const double *grad_rows,
                                  const void *cchi_saved, const double *reff_saved, double *grad_coords,
                                  double *grad_sigma2, void *workspace, size_t workspace_bytes, void *stream);
 

@@ -1,0 +1,214 @@
+"""GPU parity of the hand-written adjoint: d(loss)/d(coords) and d(loss)/d(sigma^2).
+
+Oracles: the reference stage's gradient under torch.utils.checkpoint(use_reentrant=False) (golden fixtures,
+tests/golden/grad_*.npz) and central finite differences (h = 1e-4 A) of the oracle / of the stage itself.
+Tolerances (relative to the largest gradient component): FP64 form 1e-7 against the reference's autograd (its own
+agreement with finite differences is ~1e-6), mixed form 1e-4 (the north-star gradient bar); finite differences 1e-4.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests.fixtures import npz, phase
+
+pytestmark = pytest.mark.gpu
+
+TOL = {torch.complex128: 1e-7, torch.complex64: 1e-4}
+DTYPES = [torch.complex128, torch.complex64]
+
+
+def _rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("name", ["grad_L001", "grad_A000"])
+def test_cchi_chi_fine_gradient_equals_reference_autograd(name, dtype):
+    """The reference callers' pattern: cchi -> chi_fine -> weighted sum, backward through both custom adjoints."""
+    from feffgpu_b200 import GPUPathStage
+    z = npz(name)
+    st = GPUPathStage(phase(name), device="cuda", dtype=dtype)
+    q = z["q"]
+    S = st.linear_matrix(q)
+    w = torch.tensor(z["w"], device="cuda")
+    for nleg in sorted(int(k.split("_")[1]) for k in z if k.startswith("coords_")):
+        x = torch.tensor(z[f"coords_{nleg}"], device="cuda", dtype=st.rdtype, requires_grad=True)
+        cc, rf = st.cchi(x, torch.tensor(z[f"ipots_{nleg}"]))
+        chi = st.chi_fine(cc, rf, q, S)
+        loss = (torch.tensor(z[f"deg_{nleg}"], device="cuda")[:, None] * chi.double() * w[None]).sum()
+        loss.backward()
+        e = _rel(x.grad.double().cpu().numpy(), z[f"grad_{nleg}"])
+        print(f"{name} nleg {nleg} {dtype}: gradient vs reference autograd {e:.2e}")
+        assert e < TOL[dtype], (nleg, e)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_checkpointed_call_as_the_reference_callers_make_it(dtype):
+    """torch.utils.checkpoint(use_reentrant=False) around cchi + chi_fine (exafs/forward.py:158-159) works."""
+    from torch.utils.checkpoint import checkpoint
+    from feffgpu_b200 import GPUPathStage
+    z = npz("grad_L001")
+    st = GPUPathStage(phase("grad_L001"), device="cuda", dtype=dtype)
+    q = z["q"]
+    S = st.linear_matrix(q)
+    x = torch.tensor(z["coords_3"], device="cuda", dtype=st.rdtype, requires_grad=True)
+    ip = torch.tensor(z["ipots_3"])
+
+    def f(c):
+        cc, rf = st.cchi(c, ip)
+        return st.chi_fine(cc, rf, q, S)
+
+    chi = checkpoint(f, x, use_reentrant=False)
+    (torch.tensor(z["deg_3"], device="cuda")[:, None] * chi.double() * torch.tensor(z["w"], device="cuda")).sum().backward()
+    assert _rel(x.grad.double().cpu().numpy(), z["grad_3"]) < TOL[dtype]
+
+
+def test_finite_differences_of_the_stage_two_to_eight_legs():
+    """Central differences of the FP64 stage's own loss (h = 1e-4 A) on 2-8-leg lattice walks (W phases)."""
+    from feffgpu_b200 import GPUPathStage
+    z = npz("walks_W")
+    st = GPUPathStage(phase("case_W"), device="cuda", dtype=torch.complex128)
+    q = np.arange(1, 401) * 0.05
+    S = st.linear_matrix(q)
+    rng = np.random.default_rng(2)
+    w = torch.tensor(rng.normal(size=len(q)) * q ** 2, device="cuda")
+    for nleg in range(2, 9):
+        c0 = torch.tensor(z[f"coords_{nleg}"][:1], device="cuda")
+        ip = torch.tensor(z[f"ipots_{nleg}"][:1])
+
+        def loss(c):
+            cc, rf = st.cchi(c, ip)
+            return (st.chi_fine(cc, rf, q, S) * w[None]).sum()
+
+        x = c0.clone().requires_grad_(True)
+        loss(x).backward()
+        g = x.grad.cpu().numpy()[0]
+        fd = np.zeros_like(g)
+        h = 1e-4
+        with torch.no_grad():
+            for i in range(nleg):
+                for k in range(3):
+                    cp, cm = c0.clone(), c0.clone()
+                    cp[0, i, k] += h
+                    cm[0, i, k] -= h
+                    fd[i, k] = (float(loss(cp)) - float(loss(cm))) / (2 * h)
+        e = _rel(g, fd)
+        print(f"walk nleg {nleg}: adjoint vs central differences {e:.2e}")
+        assert e < 1e-4, (nleg, e)
+
+
+def test_reff_output_gradient():
+    """d(sum reff)/d(coords): reff is half the closed path length, so each atom gets half the sum of the unit vectors
+    from its two neighbours."""
+    from feffgpu_b200 import GPUPathStage
+    st = GPUPathStage(phase("case_L001"), device="cuda", dtype=torch.complex128)
+    rng = np.random.default_rng(4)
+    c0 = torch.tensor(np.concatenate([np.zeros((2, 1, 3)), rng.normal(0, 1.5, (2, 4, 3))], 1), device="cuda")
+    ip = torch.ones(2, 5, dtype=torch.long)
+    ip[:, 0] = 0
+    x = c0.clone().requires_grad_(True)
+    _, rf = st.cchi(x, ip)
+    rf.sum().backward()
+    c = c0.cpu().numpy()
+    fd = np.zeros_like(c)
+    # analytic: reff = sum of leg lengths / 2; each atom's gradient = (unit vector to previous + to next) / 2
+    for b in range(2):
+        ring = list(range(5))
+        for j in ring:
+            prv, nxt = c[b, ring[j - 1]], c[b, ring[(j + 1) % 5]]
+            u1 = (c[b, j] - prv) / np.linalg.norm(c[b, j] - prv)
+            u2 = (c[b, j] - nxt) / np.linalg.norm(c[b, j] - nxt)
+            fd[b, j] = 0.5 * (u1 + u2)
+    assert _rel(x.grad.cpu().numpy(), fd) < 1e-12
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_fused_gradient_coords_and_sigma2(dtype):
+    """chi_reduce's adjoint: coordinates against the reference's autograd, sigma^2 against the analytic factor."""
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    z = npz("grad_L001")
+    st = GPUPathStage(phase("grad_L001"), device="cuda", dtype=dtype)
+    q = z["q"]
+    nlegs = sorted(int(k.split("_")[1]) for k in z if k.startswith("coords_"))
+    b = PathBatch([(z[f"coords_{n}"], z[f"ipots_{n}"], z[f"deg_{n}"]) for n in nlegs], device="cuda")
+    x = b.coords.clone().requires_grad_(True)
+    s2 = torch.zeros(b.n, dtype=torch.float64, device="cuda", requires_grad=True)
+    rows = st.chi_reduce(b, q, coords=x, sigma2=s2)
+    w = torch.tensor(z["w"], device="cuda")
+    (rows[0] * w).sum().backward()
+    g = x.grad.cpu().numpy()
+    off = 0
+    for n in nlegs:
+        m = len(z[f"coords_{n}"])
+        e = _rel(g[off:off + m, :n], z[f"grad_{n}"])
+        print(f"fused nleg {n} {dtype}: gradient vs reference autograd {e:.2e}")
+        assert e < TOL[dtype], (n, e)
+        assert np.all(g[off:off + m, n:] == 0)
+        off += m
+    # sigma^2: d/dsigma2_p of sum_q w_q deg_p chi_p(q) exp(-2 sigma2 q^2) at sigma2 = 0 is -2 sum_q q^2 w_q deg_p chi_p
+    orc = O.Oracle(phase("grad_L001"))
+    S = orc.linear_matrix(q)
+    ref = []
+    for n in nlegs:
+        cc, rf = orc.cchi(z[f"coords_{n}"], z[f"ipots_{n}"])
+        chi = O.chi_fine(cc, rf, q, S)
+        ref.append((-2 * q ** 2 * z["w"] * z[f"deg_{n}"][:, None] * chi).sum(1))
+    e = _rel(s2.grad.cpu().numpy(), np.concatenate(ref))
+    print(f"fused sigma2 {dtype}: {e:.2e}")
+    assert e < TOL[dtype]
+
+
+def test_fused_gradient_mixed_leg_counts_and_rows_by_finite_differences():
+    """Random paths of 2-8 legs over several rows with non-zero sigma^2: adjoint of the FP64 fused stage against
+    central differences of the oracle's FP64 sums."""
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    from tests.fixtures import cfg2_phase
+    z = npz("cfg2_sample")
+    P = cfg2_phase()
+    st = GPUPathStage(P, device="cuda", dtype=torch.complex128)
+    rng = np.random.default_rng(9)
+    groups = [(z[f"coords_{n}"][:1], z[f"ipots_{n}"][:1], np.array([1.0 + n]), np.array([n % 3])) for n in range(2, 9)]
+    b = PathBatch(groups, nrows=3, device="cuda")
+    q = np.arange(1, 401) * 0.05
+    s2 = rng.uniform(0.001, 0.01, b.n)
+    W = rng.normal(size=(3, len(q)))
+    x = b.coords.clone().requires_grad_(True)
+    st_s2 = torch.tensor(s2, device="cuda", requires_grad=True)
+    rows = st.chi_reduce(b, q, coords=x, sigma2=st_s2)
+    (rows * torch.tensor(W, device="cuda")).sum().backward()
+    orc = O.Oracle(P)
+    S = orc.linear_matrix(q)
+    nl = b.nleg.cpu().numpy()
+    deg, row = b.deg.cpu().numpy(), b.row.cpu().numpy()
+
+    def loss(coords, sig):
+        chi = np.zeros((b.n, len(q)))
+        for i in range(b.n):
+            n = nl[i]
+            cc, rf = orc.cchi(coords[i:i + 1, :n], b.ipots.cpu().numpy()[i:i + 1, :n], nthreads=1)
+            chi[i] = O.chi_fine(cc, rf, q, S)[0]
+        return float((O.chi_rows(chi, deg, row, 3, q, sig) * W).sum())
+
+    c0 = b.coords.cpu().numpy()
+    g = x.grad.cpu().numpy()
+    h = 1e-4
+    fd = np.zeros_like(c0)
+    for i in range(b.n):
+        for j in range(nl[i]):
+            for k in range(3):
+                cp, cm = c0.copy(), c0.copy()
+                cp[i, j, k] += h
+                cm[i, j, k] -= h
+                fd[i, j, k] = (loss(cp, s2) - loss(cm, s2)) / (2 * h)
+    e = _rel(g, fd)
+    print(f"fused mixed legs: adjoint vs central differences {e:.2e}")
+    assert e < 1e-4
+    fds = np.zeros(b.n)
+    for i in range(b.n):
+        sp, sm = s2.copy(), s2.copy()
+        sp[i] += 1e-5
+        sm[i] -= 1e-5
+        fds[i] = (loss(c0, sp) - loss(c0, sm)) / 2e-5
+    assert _rel(st_s2.grad.cpu().numpy(), fds) < 1e-5
