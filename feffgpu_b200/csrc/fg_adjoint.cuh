@@ -943,8 +943,9 @@ fg_status launch_adjoint(const StageView &sv, const Tables<R> &T, const CT *coor
                          unsigned long long *counter, int warps, cudaStream_t st)
 {
     using K = Kinds<EDGE>;
-    const int threads = warps * 32;
     const size_t wb = adj_warp_bytes<R>(sv.L1, nsc_max, K::MM);
+    warps = fit_warps(warps, wb, sv.max_smem);
+    const int threads = warps * 32;
     auto kern = k_adjoint<R, EDGE, CT>;
     int blocks = 0;
     if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;
@@ -964,9 +965,9 @@ fg_status launch_fine_adjoint(const StageView &sv, int64_t B, int NK, int mode, 
                               const double *deg, const double *sigma2, C2<R> *gbar, R *greff_r, double *greff_d,
                               double *gsig, cudaStream_t st)
 {
-    const int warps = 4, threads = warps * 32;
     const size_t wb = align_up((size_t)sv.E * sizeof(R), 16) + align_up((size_t)sv.E * 8, 16) +
                       align_up((size_t)NK * 16, 16);
+    const int warps = fit_warps(4, wb, sv.max_smem), threads = warps * 32;
     auto kern = k_fine_adjoint<R>;
     int blocks = 0;
     if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;

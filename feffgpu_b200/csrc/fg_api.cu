@@ -32,6 +32,7 @@ struct fg_stage {
     int device = 0, E = 0, nph = 0, nph1 = 0, ltot = 0, ihole = 0, iorder = 2, kinit = 0, ilinit = 0, L1 = 0;
     int nterm = 0, term_l[2] = {0, 0};
     int num_sms = 148;
+    int max_smem = 227 * 1024;
     std::vector<int> lmax_host;     // (E, nph1)
     std::vector<double> xk_host;    // (E)
     Tables<float> tf{};
@@ -284,6 +285,7 @@ extern "C" fg_status fg_stage_create(const fg_phase_desc *d, int device, fg_stag
     cudaError_t ce = cudaSetDevice(device);
     if (ce != cudaSuccess) { delete s; return fail(FG_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce)); }
     cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device);
+    cudaDeviceGetAttribute(&s->max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     fg_status st = build_tables<float>(s, s->tf, tl, ck, dk, wt, xfac, xn, rc, lmax_t);
     if (!st) st = build_tables<double>(s, s->td, tl, ck, dk, wt, xfac, xn, rc, lmax_t);
     if (st) { fg_stage_destroy(s); return st; }
@@ -336,7 +338,7 @@ fg_status set_device(const fg_stage *s)
     return FG_OK;
 }
 
-StageView view(const fg_stage *s) { return StageView{s->E, s->L1, s->nph1, s->num_sms, s->ilinit}; }
+StageView view(const fg_stage *s) { return StageView{s->E, s->L1, s->nph1, s->num_sms, s->ilinit, s->max_smem}; }
 
 // Calls F::template run<R, EDGE>(tables) for the stage's precision and initial-state class.
 template <class F> fg_status by_kind(const fg_stage *s, fg_precision prec, F &&f)

@@ -233,9 +233,10 @@ fg_status Launch<R, EDGE>::cchi(const StageView &sv, const Tables<R> &T, int64_t
                                 cudaStream_t st)
 {
     using K = Kinds<EDGE>;
-    const int threads = warps * 32;
     const int MM = nleg == 2 ? K::MMSS : K::MMMS;
     const size_t wb = warp_bytes<R>(sv.L1, nleg - 1, MM, sv.E, false);
+    warps = fit_warps(warps, wb, sv.max_smem);
+    const int threads = warps * 32;
     const size_t smem = wb * warps;
     int blocks = 0;
     if (coords_f64) {
@@ -268,9 +269,10 @@ fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const 
     double *partial = reinterpret_cast<double *>(ws + kCounterBytes + align_up((size_t)P->n * NK * sizeof(double), 256));
     FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes, st));
     if (P->n > 0) {
-        const int threads = warps * 32;
         const int nsc_max = P->nleg_max - 1;
         const size_t wb = warp_bytes<R>(sv.L1, nsc_max, K::MM, sv.E, true);
+        warps = fit_warps(warps, wb, sv.max_smem);
+        const int threads = warps * 32;
         auto kern = k_fused<R, EDGE>;
         int blocks = 0;
         if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, P->n, blocks)) return rc;
@@ -288,8 +290,8 @@ template <typename R>
 fg_status LaunchCommon<R>::chi_fine(const StageView &sv, int64_t B, const void *cchi, const void *reff, int NK,
                                     const void *q, const void *S, const int *span, void *chi, cudaStream_t st)
 {
-    const int warps = 8, threads = warps * 32;
     const size_t wb = align_up((size_t)sv.E * sizeof(R), 16) + align_up((size_t)sv.E * sizeof(double), 16);
+    const int warps = fit_warps(8, wb, sv.max_smem), threads = warps * 32;
     auto kern = k_chi_fine<R>;
     int blocks = 0;
     if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;

@@ -19,7 +19,16 @@ constexpr size_t kCounterBytes = 256;   // head of every fused workspace: work-q
 // What the launches need to know about a stage.
 struct StageView {
     int E, L1, nph1, num_sms, ilinit;
+    int max_smem;   // opt-in shared memory per block (bytes)
 };
+
+// Warps per block that fit the per-warp shared memory (at least 1; the launch reports a block that does not fit)
+inline int fit_warps(int want, size_t per_warp, int max_smem)
+{
+    int w = want < 1 ? 1 : want;
+    while (w > 1 && per_warp * (size_t)w > (size_t)max_smem) --w;
+    return w;
+}
 
 // Per precision R and initial-state class EDGE (l_init + 1 = 1, 2, 3: K/L1, L2/L3/M2/M3, M4/M5/N4/N5 edges).
 template <typename R, int EDGE> struct Launch {

@@ -13,6 +13,7 @@ The reference is imported read-only from its source tree and run on the CPU in F
   of every leg count (the procedure of the reference's tests/test_xsph.py:85-123).
 * walks_W.npz -- 2- to 8-leg bcc lattice walks with the W phases and the reference stage's cchi (the procedure of
   tests/test_pathfinder.py:193-230, seed 5).
+* grad_walks_W.npz -- the same for the W walks (loss sum_q w_q chi(q) with seeded w).
 * grad_L001.npz, grad_A000.npz -- d(loss)/d(coords) of the reference stage under torch.utils.checkpoint
   (use_reentrant=False, as src/feffgpu/exafs/forward.py:683 calls it), loss = sum_p deg_p sum_q w_q chi_p(q).
 * L001_phase.pad -- FEFF's phase.pad of the L001 case, copied as written by FEFF, for the reader's test.
@@ -191,6 +192,34 @@ def make_grad(name, nlegs=(2, 3, 4, 5, 6), per=3, seed=11):
     print(f"grad_{name} written")
 
 
+def make_grad_walks():
+    """Reference gradients of the 2-8-leg walks (W phases), loss sum_q w_q chi(q), seeded w: includes paths that
+    revisit an atom (A -> B -> A), where the Euler angles are not differentiable and the reference's branch
+    choices define the gradient."""
+    from feffgpu.pad import read_phase_pad
+    from torch.utils.checkpoint import checkpoint
+    P = read_phase_pad(str(CASES["W"] / "phase.pad"))
+    g = ref_stage(P)
+    z = np.load(HERE / "walks_W.npz")
+    q = np.arange(1, 401) * 0.05
+    S = g.linear_matrix(q)
+    w = torch.tensor(np.random.default_rng(2).normal(size=len(q)) * q ** 2)
+    out = {"q": q, "w": w.numpy()}
+    for nleg in range(2, 9):
+        x = torch.tensor(z[f"coords_{nleg}"], requires_grad=True)
+        ip = torch.tensor(z[f"ipots_{nleg}"])
+
+        def f(c):
+            cc, rf = g.cchi(c, ip)
+            return g.chi_fine(cc, rf, q, S)
+
+        loss = (checkpoint(f, x, use_reentrant=False) * w[None]).sum()
+        (gx,) = torch.autograd.grad(loss, x)
+        out[f"grad_{nleg}"] = gx.numpy()
+    np.savez_compressed(HERE / "grad_walks_W.npz", **out)
+    print("grad_walks_W written")
+
+
 def _write_inp(path, title, edge, potentials, atoms, extra=""):
     lines = [f"TITLE {title}", "CONTROL 1 1 1 1 1 1", "PRINT 0 0 0 0 0 0", f"EDGE {edge}", "S02 1.0", extra, "",
              "POTENTIALS"]
@@ -276,6 +305,7 @@ def main():
         if "walks" in want:
             make_walks()
         if "grad" in want:
+            make_grad_walks()
             make_grad("L001")
             make_grad("A000", nlegs=(2, 3, 4), per=2)
         if "cfg1" in want:

@@ -65,8 +65,40 @@ def test_checkpointed_call_as_the_reference_callers_make_it(dtype):
     assert _rel(x.grad.double().cpu().numpy(), z["grad_3"]) < TOL[dtype]
 
 
+def _distinct_atoms(coords):
+    """True if no two atoms of the path coincide (a path that revisits an atom scatters straight back, where the
+    Euler angles are not differentiable and only the reference's branch choice defines a gradient)."""
+    c = np.asarray(coords)
+    d = np.linalg.norm(c[:, None] - c[None], axis=-1) + np.eye(len(c))
+    return bool(d.min() > 1e-3)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_walk_gradients_equal_reference_autograd(dtype):
+    """2-8-leg lattice walks (W phases, l up to 47), including paths that revisit an atom, against the reference's
+    checkpointed autograd.  A revisit (A -> B -> A) puts B's scattering angle exactly at pi, where the Euler angles
+    are not differentiable: the gradient there is the reference's branch choice, reproduced up to the rounding that
+    decides the branch tests (1e-4 relative for such paths)."""
+    from feffgpu_b200 import GPUPathStage
+    z, zg = npz("walks_W"), npz("grad_walks_W")
+    st = GPUPathStage(phase("case_W"), device="cuda", dtype=dtype)
+    q = zg["q"]
+    S = st.linear_matrix(q)
+    w = torch.tensor(zg["w"], device="cuda")
+    for nleg in range(2, 9):
+        x = torch.tensor(z[f"coords_{nleg}"], device="cuda", dtype=st.rdtype, requires_grad=True)
+        cc, rf = st.cchi(x, torch.tensor(z[f"ipots_{nleg}"]))
+        (st.chi_fine(cc, rf, q, S).double() * w[None]).sum().backward()
+        g = x.grad.double().cpu().numpy()
+        for b in range(len(g)):
+            e = _rel(g[b], zg[f"grad_{nleg}"][b])
+            smooth = _distinct_atoms(z[f"coords_{nleg}"][b])
+            print(f"walk nleg {nleg} path {b} {dtype} {'distinct' if smooth else 'revisit'}: vs reference autograd {e:.2e}")
+            assert e < (TOL[dtype] if smooth else max(TOL[dtype], 1e-4)), (nleg, b, e)
+
+
 def test_finite_differences_of_the_stage_two_to_eight_legs():
-    """Central differences of the FP64 stage's own loss (h = 1e-4 A) on 2-8-leg lattice walks (W phases)."""
+    """Central differences of the FP64 stage's own loss (h = 1e-4 A) on the 2-8-leg walks whose atoms are distinct."""
     from feffgpu_b200 import GPUPathStage
     z = npz("walks_W")
     st = GPUPathStage(phase("case_W"), device="cuda", dtype=torch.complex128)
@@ -74,29 +106,35 @@ def test_finite_differences_of_the_stage_two_to_eight_legs():
     S = st.linear_matrix(q)
     rng = np.random.default_rng(2)
     w = torch.tensor(rng.normal(size=len(q)) * q ** 2, device="cuda")
+    checked = 0
     for nleg in range(2, 9):
-        c0 = torch.tensor(z[f"coords_{nleg}"][:1], device="cuda")
-        ip = torch.tensor(z[f"ipots_{nleg}"][:1])
+        for b in range(len(z[f"coords_{nleg}"])):
+            if not _distinct_atoms(z[f"coords_{nleg}"][b]):
+                continue
+            c0 = torch.tensor(z[f"coords_{nleg}"][b:b + 1], device="cuda")
+            ip = torch.tensor(z[f"ipots_{nleg}"][b:b + 1])
 
-        def loss(c):
-            cc, rf = st.cchi(c, ip)
-            return (st.chi_fine(cc, rf, q, S) * w[None]).sum()
+            def loss(c):
+                cc, rf = st.cchi(c, ip)
+                return (st.chi_fine(cc, rf, q, S) * w[None]).sum()
 
-        x = c0.clone().requires_grad_(True)
-        loss(x).backward()
-        g = x.grad.cpu().numpy()[0]
-        fd = np.zeros_like(g)
-        h = 1e-4
-        with torch.no_grad():
-            for i in range(nleg):
-                for k in range(3):
-                    cp, cm = c0.clone(), c0.clone()
-                    cp[0, i, k] += h
-                    cm[0, i, k] -= h
-                    fd[i, k] = (float(loss(cp)) - float(loss(cm))) / (2 * h)
-        e = _rel(g, fd)
-        print(f"walk nleg {nleg}: adjoint vs central differences {e:.2e}")
-        assert e < 1e-4, (nleg, e)
+            x = c0.clone().requires_grad_(True)
+            loss(x).backward()
+            g = x.grad.cpu().numpy()[0]
+            fd = np.zeros_like(g)
+            h = 1e-4
+            with torch.no_grad():
+                for i in range(nleg):
+                    for k in range(3):
+                        cp, cm = c0.clone(), c0.clone()
+                        cp[0, i, k] += h
+                        cm[0, i, k] -= h
+                        fd[i, k] = (float(loss(cp)) - float(loss(cm))) / (2 * h)
+            e = _rel(g, fd)
+            print(f"walk nleg {nleg} path {b}: adjoint vs central differences {e:.2e}")
+            assert e < 1e-4, (nleg, b, e)
+            checked += 1
+    assert checked >= 7
 
 
 def test_reff_output_gradient():
@@ -161,15 +199,21 @@ def test_fused_gradient_coords_and_sigma2(dtype):
 
 
 def test_fused_gradient_mixed_leg_counts_and_rows_by_finite_differences():
-    """Random paths of 2-8 legs over several rows with non-zero sigma^2: adjoint of the FP64 fused stage against
-    central differences of the oracle's FP64 sums."""
+    """Random paths of 2-8 legs (distinct atoms) over several rows with non-zero sigma^2: adjoint of the FP64 fused
+    stage against central differences of the oracle's FP64 sums."""
     from feffgpu_b200 import GPUPathStage, PathBatch
     from tests.fixtures import cfg2_phase
     z = npz("cfg2_sample")
     P = cfg2_phase()
     st = GPUPathStage(P, device="cuda", dtype=torch.complex128)
     rng = np.random.default_rng(9)
-    groups = [(z[f"coords_{n}"][:1], z[f"ipots_{n}"][:1], np.array([1.0 + n]), np.array([n % 3])) for n in range(2, 9)]
+    groups = []
+    for n in range(2, 9):
+        ok = [i for i in range(len(z[f"coords_{n}"])) if _distinct_atoms(z[f"coords_{n}"][i])]
+        if ok:
+            i = ok[0]
+            groups.append((z[f"coords_{n}"][i:i + 1], z[f"ipots_{n}"][i:i + 1], np.array([1.0 + n]), np.array([n % 3])))
+    assert len(groups) >= 5
     b = PathBatch(groups, nrows=3, device="cuda")
     q = np.arange(1, 401) * 0.05
     s2 = rng.uniform(0.001, 0.01, b.n)
