@@ -14,11 +14,13 @@ LIB_PATH = Path(__file__).resolve().parent / "_build" / "libfeffgpu_b200.so"
 
 FG_OK, FG_ERR_VALUE, FG_ERR_NOT_IMPLEMENTED, FG_ERR_CUDA, FG_ERR_WORKSPACE = range(5)
 FG_MIXED, FG_FP64 = 0, 1
+NOALLOC_SCRATCH_BYTES = 32 << 20    # FG_NOALLOC_SCRATCH_BYTES of include/feffgpu_b200.h
 
 # every entry point of include/feffgpu_b200.h
 EXPORTS = ("fg_stage_create", "fg_stage_destroy", "fg_stage_get_info", "fg_stage_lmax", "fg_stage_xk",
            "fg_last_error", "fg_cchi", "fg_cchi_backward_workspace", "fg_cchi_backward", "fg_chi_fine",
-           "fg_chi_fine_backward", "fg_chi_reduce_workspace", "fg_chi_reduce", "fg_chi_reduce_backward_workspace",
+           "fg_chi_fine_backward", "fg_chi_reduce_workspace", "fg_chi_reduce", "fg_chi_reduce_noalloc",
+           "fg_chi_reduce_backward_workspace",
            "fg_chi_reduce_backward", "fg_set_kernel_timing", "fg_kernel_time_ms", "fg_fp32_fma_peak", "fg_set_launch")
 
 
@@ -57,6 +59,7 @@ _SIGS = {
     "fg_chi_fine_backward": (C.c_int, [_P, C.c_int, C.c_int64, _P, _P, C.c_int32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "fg_chi_reduce_workspace": (C.c_size_t, [_P, C.POINTER(Paths), C.c_int32]),
     "fg_chi_reduce": (C.c_int, [_P, C.c_int, C.POINTER(Paths), C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.c_size_t, _P]),
+    "fg_chi_reduce_noalloc": (C.c_int, [_P, C.c_int, C.POINTER(Paths), C.c_int32, _P, _P, _P, _P, _P]),
     "fg_chi_reduce_backward_workspace": (C.c_size_t, [_P, C.POINTER(Paths), C.c_int32]),
     "fg_chi_reduce_backward": (C.c_int, [_P, C.c_int, C.POINTER(Paths), C.c_int32, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                                          _P, C.c_size_t, _P]),

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -513,5 +514,58 @@ extern "C" fg_status fg_chi_reduce_backward(const fg_stage *s, fg_precision prec
         return decltype(L)::fused_bwd(sv, T, P, NK, q, S, span, tspan, grad_rows, cchi_saved, reff_saved,
                                       grad_coords, grad_sigma2, static_cast<unsigned char *>(workspace), g_bwd_warps,
                                       st);
+    });
+}
+
+// ------------------------------------------------------------------------------------------------ no-allocation variant
+// The scratch of fg_chi_reduce_noalloc: a fixed array in the library's device image (one per GPU that loads it).
+// In host code the name is only a host-side stand-in; the device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[FG_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 128;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `device` (which must be current); looked up once per device.
+fg_status noalloc_scratch(int device, void **out)
+{
+    if (device < 0 || device >= kMaxDevices) return fail(FG_ERR_VALUE, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(FG_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+        g_noalloc_addr[device] = p;
+    }
+    *out = g_noalloc_addr[device];
+    return FG_OK;
+}
+}  // namespace
+
+extern "C" fg_status fg_chi_reduce_noalloc(const fg_stage *s, fg_precision prec, const fg_paths *P, int32_t NK,
+                                           const double *q, const double *S, const int32_t *span, double *rows,
+                                           void *stream)
+{
+    g_err.clear();
+    if (!s) return fail(FG_ERR_VALUE, "null stage");
+    if (fg_status rc = check_paths(P)) return rc;
+    if (NK < 0) return fail(FG_ERR_VALUE, "negative NK");
+    if (NK == 0 || P->nrows == 0) return FG_OK;
+    if (!q || !S || !span || !rows) return fail(FG_ERR_VALUE, "null array");
+    const size_t need = fused_workspace(P, NK);
+    if (need > FG_NOALLOC_SCRATCH_BYTES)
+        return fail(FG_ERR_VALUE, "fg_chi_reduce_noalloc: this batch needs " + std::to_string(need) +
+                                      " bytes of scratch, the library's fixed scratch holds " +
+                                      std::to_string((size_t)FG_NOALLOC_SCRATCH_BYTES) + " bytes; split it by rows");
+    if (fg_status rc = set_device(s)) return rc;
+    void *ws = nullptr;
+    if (fg_status rc = noalloc_scratch(s->device, &ws)) return rc;
+    const StageView sv = view(s);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return by_kind(s, prec, [&](auto L, const auto &T) {
+        return decltype(L)::fused(sv, T, P, NK, q, S, span, rows, nullptr, nullptr, static_cast<unsigned char *>(ws),
+                                  g_fwd_warps, st);
     });
 }

@@ -144,6 +144,22 @@ FG_API fg_status fg_chi_reduce(const fg_stage *stage, fg_precision prec, const f
                         const double *S, const int32_t *span, double *rows, void *cchi_save, double *reff_save,
                         void *workspace, size_t workspace_bytes, void *stream);
 
+/* Scratch-free variant of fg_chi_reduce.  No counterpart in the reference: it exists for callers that must not
+ * allocate device memory -- for example a host program whose GPU memory is handed out by an allocator it does not
+ * control (a simulation code that reserves the whole device for its own pool at start-up) and so cannot provide
+ * the workspace fg_chi_reduce asks for.  Instead of a caller workspace it uses an array compiled into the library,
+ * FG_NOALLOC_SCRATCH_BYTES (32 MiB) on every GPU that loads the library, held until the process exits; a batch
+ * whose fg_chi_reduce_workspace exceeds that is rejected with FG_ERR_VALUE (split it by rows).  It allocates
+ * nothing: no cudaMalloc, no cudaFree, no allocating library call.  The first call on a device looks up the
+ * array's device address with that device current; make that first call before any stream capture.  All calls
+ * share the array and it keeps the last call's contents (each call clears the queue counter it needs): calls whose
+ * work overlaps on the GPU -- other streams, other host threads -- race on it and must be serialised by the caller.
+ * Same inputs and result as fg_chi_reduce; the per-path signals are not kept (no adjoint). */
+#define FG_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+FG_API fg_status fg_chi_reduce_noalloc(const fg_stage *stage, fg_precision prec, const fg_paths *paths, int32_t NK,
+                                       const double *q, const double *S, const int32_t *span, double *rows,
+                                       void *stream);
+
 /* Adjoint of fg_chi_reduce: grad_coords (n, nleg_max, 3) FP64 and grad_sigma2 (n) FP64 (may be NULL) from
  * grad_rows (nrows, NK), using the saved cchi and reff; tspan as in fg_chi_fine_backward.  No reference
  * counterpart for sigma^2 (a new input). */
