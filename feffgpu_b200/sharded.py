@@ -1,0 +1,83 @@
+"""Multi-GPU path stage: one process per GPU, paths sharded across ranks, rows summed with one all-reduce.
+
+The paths of a job are independent; the only exchange is the final sum of every rank's partial rows (rows x NK FP64,
+e.g. 2 x 401 x 8 B per absorber pair).  ``shard`` splits a path list across ranks by cost (longest-processing-time
+first over the ranks, deterministic); ``allreduce_rows`` sums partial rows over the process group (NCCL on GPUs, gloo
+elsewhere) and is differentiable: every rank computes the loss from the same summed rows, so the gradient reaching
+each rank's partial rows is the upstream gradient itself.  Gradients of positions shared by all ranks (an RMC model)
+are then summed with ``allreduce_grad``.
+
+The reference runs multi-GPU jobs as independent processes per MD-frame shard (``src/feffgpu/parallel/__init__.py:
+78-133``); this module adds the path-level split with one collective.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+import torch.distributed as dist
+
+
+def path_cost(nleg: np.ndarray) -> np.ndarray:
+    """Relative cost of a path by its leg count (the scattering-matrix chain grows linearly with the legs)."""
+    nleg = np.asarray(nleg)
+    return np.where(nleg == 2, 0.45, nleg - 1.0)
+
+
+def shard(nleg: np.ndarray, world: int) -> np.ndarray:
+    """Rank of every path: longest-processing-time-first assignment of the path costs to the least-loaded rank.
+    Deterministic for a given input."""
+    nleg = np.asarray(nleg)
+    cost = path_cost(nleg)
+    order = np.argsort(-cost, kind="stable")
+    load = np.zeros(world)
+    owner = np.zeros(len(nleg), np.int64)
+    for i in order:
+        r = int(np.argmin(load))
+        owner[i] = r
+        load[r] += cost[i]
+    return owner
+
+
+def split_groups(groups, world: int, rank: int):
+    """The rank's share of a list of path groups (coords, ipots, deg, row) as returned for PathBatch."""
+    nl = np.concatenate([np.full(len(g[0]), np.asarray(g[0]).shape[1]) for g in groups]) if groups else np.zeros(0)
+    owner = shard(nl, world)
+    out, off = [], 0
+    for g in groups:
+        n = len(g[0])
+        sel = np.nonzero(owner[off:off + n] == rank)[0]
+        off += n
+        if len(sel) == 0:
+            continue
+        gg = [np.asarray(g[0])[sel], np.asarray(g[1])[sel]]
+        gg.append(None if len(g) < 3 or g[2] is None else np.asarray(g[2])[sel])
+        gg.append(None if len(g) < 4 or g[3] is None else np.asarray(g[3])[sel])
+        out.append(tuple(gg))
+    return out
+
+
+class _AllReduceSum(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, group):
+        y = x.detach().clone()
+        dist.all_reduce(y, op=dist.ReduceOp.SUM, group=group)
+        return y
+
+    @staticmethod
+    def backward(ctx, g):
+        # every rank holds the same loss of the summed rows: its partial rows receive the upstream gradient
+        return g, None
+
+
+def allreduce_rows(rows: torch.Tensor, group=None) -> torch.Tensor:
+    """Sum of the ranks' partial rows, differentiable (identity backward)."""
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return rows
+    return _AllReduceSum.apply(rows, group)
+
+
+def allreduce_grad(t: torch.Tensor, group=None) -> torch.Tensor:
+    """In-place sum over ranks of a gradient of parameters that every rank holds (shared positions)."""
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t

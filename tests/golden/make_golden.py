@@ -20,6 +20,8 @@ The reference is imported read-only from its source tree and run on the CPU in F
 * cfg1_cu.npz -- the Cu fcc cluster (a = 3.61 A, 6 A radius, K edge) through the reference chain
   (src/feffgpu/chain.py:16-51): phase tables, the path finder's paths (NLEG 4, RPATH 6, default importance cut) and chi on
   k = 0..20 A^-1 step 0.05.
+* cfg4_fe_phase.npz, cfg5_nik_phase.npz, cfg5_ok_phase.npz -- bcc Fe (K edge) and rock-salt NiO (Ni K and O K
+  edges) phase tables of 6 A clusters through the reference chain, for the MD-batch and two-edge refinement cases.
 * cfg2_phase.npz -- Fe K-edge phase tables (potentials Fe*, Fe, O, Pt, lmax 24) of a cluster cut from the seeded
   3000-atom Fe/O/Pt packing, on FEFF's own energy grid; cfg2_sample.npz -- the reference stage's cchi on those
   tables resampled to 401 k points, for a sample of synthetic paths.
@@ -290,12 +292,44 @@ def make_cfg2(tmp):
     print("cfg2_sample written")
 
 
+def _cluster_phase(name, pts, labels, center, edge_sym, pots, lmax=None):
+    """Phase tables of a cluster cut (6 A) around `center` through the reference chain (NLEG 2, short RPATH)."""
+    from feffgpu.chain import run
+    import tempfile
+    rel = pts - pts[center]
+    r = np.linalg.norm(rel, axis=1)
+    sel = np.argsort(r, kind="stable")
+    sel = sel[r[sel] <= 6.0]
+    ipmap = {lab: i + 1 for i, (_, _, lab) in enumerate(pots[1:])}
+    atoms = [(rel[i], 0 if i == center else ipmap[labels[i]]) for i in sel]
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = Path(tmp) / "feff.inp"
+        _write_inp(inp, name, edge_sym, pots, atoms, "NLEG 2\nRPATH 2.0\nEXAFS 20.5")
+        t = time.time()
+        res = run(str(inp), device="cpu", lmax_override=lmax)
+    P = res["phase"]
+    np.savez_compressed(HERE / f"{name}.npz", **phase_to_arrays(P, prefix="ph_"))
+    print(f"{name}: {len(sel)} atoms, ne1 {P.ne1}, lmax {P.lmax[:P.ne1].max()}, {time.time() - t:.1f} s")
+
+
+def make_cfg45():
+    """bcc Fe (the MD batch) and rock-salt NiO with Ni K and O K edges (the two-edge refinement)."""
+    pts, box = W.bcc_supercell(6, 2.87)
+    c = int(W.central_atom(pts, box, None, None, 1)[0])
+    _cluster_phase("cfg4_fe_phase", pts, np.array(["Fe"] * len(pts)), c, "K", [(0, 26, "Fe"), (1, 26, "Fe")])
+    pts, lab, box = W.rock_salt_supercell(4, 4.177)
+    ni = int(W.central_atom(pts, box, lab, "Ni", 1)[0])
+    o = int(W.central_atom(pts, box, lab, "O", 1)[0])
+    _cluster_phase("cfg5_nik_phase", pts, lab, ni, "K", [(0, 28, "Ni"), (1, 28, "Ni"), (2, 8, "O")])
+    _cluster_phase("cfg5_ok_phase", pts, lab, o, "K", [(0, 8, "O"), (1, 28, "Ni"), (2, 8, "O")])
+
+
 def main():
     import tempfile
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
-    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2"])
+    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45"])
     with tempfile.TemporaryDirectory() as tmp:
         if "cases" in want:
             import shutil
@@ -312,6 +346,8 @@ def main():
             make_cfg1(tmp)
         if "cfg2" in want:
             make_cfg2(tmp)
+        if "cfg45" in want:
+            make_cfg45()
 
 
 if __name__ == "__main__":

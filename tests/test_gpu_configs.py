@@ -1,0 +1,200 @@
+"""The benchmark configurations as parity cases (B200).
+
+1. Cu fcc 6 A cluster, K edge: the reference chain's own phases and path finder output (317 paths), chi on
+   k = 0..20 step 0.05 against the reference's FP64 chi (R <= 1e-6 mixed, 1e-12 FP64).
+3. Adjoint on an 800-atom Fe/O/Pt packing: gradient of an R-space misfit with respect to every position and every
+   per-path sigma^2 against central differences (h = 1e-4 A), FP32-vs-FP64 gradient error stated.
+4. MD batch: frames of a thermally displaced bcc Fe supercell x absorbers in one launch, chi averaged per frame,
+   against the oracle's FP64 sums.
+5. Two-edge refinement (Ni K + O K of a rock-salt NiO model with vacancies): the step captured as a CUDA graph equals
+   the eager step and the misfit falls.
+"""
+import numpy as np
+import pytest
+import torch
+
+from feffgpu_b200 import workloads as W
+from oracle import oracle as O
+from tests.fixtures import groups, npz, phase
+
+pytestmark = pytest.mark.gpu
+
+K401 = np.arange(401) * 0.05
+
+
+def _R(k, ref, x):
+    return O.r_factor(np.asarray(k), ref, x, kmin=3.0, kmax=19.0, rmin=1.0, rmax=6.0)
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.complex64, 1e-6), (torch.complex128, 1e-12)])
+def test_cfg1_cu_cluster(dtype, tol):
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    z = npz("cfg1_cu")
+    st = GPUPathStage(phase("cfg1_cu"), device="cuda", dtype=dtype)
+    gs = groups("cfg1_cu")
+    assert {n: len(v[0]) for n, v in gs.items()} == {2: 5, 3: 234, 4: 78}
+    rows = st.chi_reduce(PathBatch([(c, i, d) for c, i, d in gs.values()], device="cuda"), K401)[0].cpu().numpy()
+    R = _R(K401, z["ref_chi"], rows)
+    print(f"cfg1 fused {dtype}: R {R:.2e}")
+    assert R <= tol
+    # the chain's own loop over leg counts (chain.py:45-49) through the drop-in methods
+    S = st.linear_matrix(K401)
+    chi = torch.zeros(len(K401), dtype=torch.float64, device="cuda")
+    with torch.no_grad():
+        for c, i, d in gs.values():
+            cc, rf = st.cchi(torch.tensor(c), torch.tensor(i))
+            chi += (torch.tensor(d, device="cuda")[:, None] * st.chi_fine(cc, rf, K401, S, "feff").double()).sum(0)
+    assert _R(K401, z["ref_chi"], chi.cpu().numpy()) <= tol
+
+
+def _distinct(atoms):
+    a = np.asarray(atoms)
+    return np.array([len(set(r.tolist())) == len(r) for r in a])
+
+
+def _feopt_model(dtype, n_atoms=800, seed=31):
+    from feffgpu_b200 import GPUPathStage
+    from feffgpu_b200.model import PathModel
+    from tests.fixtures import cfg2_phase
+    pos, lab, box = W.random_packing(n_atoms, 0.08, 1.8, seed=seed)
+    ab = int(W.central_atom(pos, box, lab, "Fe", 1)[0])
+    ipot_of = np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
+    paths = W.random_paths(pos, box, ab, {2: 40, 3: 300, 4: 400, 5: 300}, rmax=6.0, seed=5, ipot_of=ipot_of)
+    gs = []
+    for nleg, (c, ip, atoms) in paths.items():
+        full = np.concatenate([np.full((len(atoms), 1), ab), atoms], 1)
+        keep = _distinct(full)            # revisiting paths are not differentiable at the revisit
+        gs.append((full[keep], ip[keep], np.ones(int(keep.sum())), np.zeros(int(keep.sum()), int)))
+    st = GPUPathStage(cfg2_phase(), device="cuda", dtype=dtype)
+    return st, PathModel(st, gs, pos, nrows=1, box=box), pos, box
+
+
+def test_cfg3_adjoint_800_atoms():
+    from feffgpu_b200.rspace import FitWindow, RSpaceMisfit
+    q = torch.tensor(K401, device="cuda")
+    grads = {}
+    for dtype in (torch.complex128, torch.complex64):
+        st, model, pos, box = _feopt_model(dtype)
+        S = st.linear_matrix(K401).double()
+        target_pos = W.thermal(pos, 0.05, seed=77)
+        with torch.no_grad():
+            target = model.rows(torch.tensor(target_pos, device="cuda"), q, S)[0]
+        mis = RSpaceMisfit(len(K401), target, FitWindow(kmin=3.0, kmax=16.0, rmin=1.0, rmax=6.0))
+        x = torch.tensor(pos, device="cuda", requires_grad=True)
+        s2 = torch.full((model.batch.n,), 0.003, dtype=torch.float64, device="cuda", requires_grad=True)
+        loss = mis(model.rows(x, q, S, sigma2=s2))[0]
+        loss.backward()
+        grads[dtype] = (x.grad.cpu().numpy(), s2.grad.cpu().numpy(), float(loss))
+        if dtype != torch.complex128:
+            continue
+        # central differences on the atoms with the largest gradients and on a few sigma^2
+        gx = grads[dtype][0]
+        top = np.argsort(-np.abs(gx).ravel())[:6]
+        with torch.no_grad():
+            for idx in top:
+                i, k = divmod(int(idx), 3)
+                xp, xm = pos.copy(), pos.copy()
+                xp[i, k] += 1e-4
+                xm[i, k] -= 1e-4
+                lp = float(mis(model.rows(torch.tensor(xp, device="cuda"), q, S, sigma2=s2.detach()))[0])
+                lm = float(mis(model.rows(torch.tensor(xm, device="cuda"), q, S, sigma2=s2.detach()))[0])
+                fd = (lp - lm) / 2e-4
+                assert abs(gx[i, k] - fd) <= 1e-4 * abs(gx).max(), (i, k, gx[i, k], fd)
+            gs = grads[dtype][1]
+            for p in np.argsort(-np.abs(gs))[:4]:
+                sp, sm = s2.detach().clone(), s2.detach().clone()
+                sp[p] += 1e-6
+                sm[p] -= 1e-6
+                fd = (float(mis(model.rows(x.detach(), q, S, sigma2=sp))[0]) -
+                      float(mis(model.rows(x.detach(), q, S, sigma2=sm))[0])) / 2e-6
+                assert abs(gs[p] - fd) <= 1e-4 * abs(gs).max(), (p, gs[p], fd)
+    e_x = np.abs(grads[torch.complex64][0] - grads[torch.complex128][0]).max() / np.abs(grads[torch.complex128][0]).max()
+    e_s = np.abs(grads[torch.complex64][1] - grads[torch.complex128][1]).max() / np.abs(grads[torch.complex128][1]).max()
+    print(f"cfg3: FP32 vs FP64 gradient error: positions {e_x:.2e}, sigma2 {e_s:.2e}")
+    assert e_x < 1e-4 and e_s < 1e-4
+
+
+def test_cfg4_md_frames_times_absorbers():
+    from feffgpu_b200 import GPUPathStage
+    from feffgpu_b200.model import PathModel
+    P = phase("cfg4_fe_phase")
+    st = GPUPathStage(P, device="cuda", dtype=torch.complex64)
+    base, box = W.bcc_supercell(6, 2.87)
+    frames, A = 3, 4
+    rng = np.random.default_rng(12)
+    gs, allpos = [], []
+    N = len(base)
+    for f in range(frames):
+        pos = W.thermal(base, 0.08, seed=100 + f)
+        allpos.append(pos)
+        for a in rng.choice(N, size=A, replace=False):
+            paths = W.random_paths(pos, box, int(a), {2: 14, 3: 60}, rmax=5.5, leg_max=5.5, seed=int(a) + 7 * f)
+            for nleg, (c, ip, atoms) in paths.items():
+                full = np.concatenate([np.full((len(atoms), 1), a), atoms], 1) + f * N
+                gs.append((full, ip, np.full(len(atoms), 1.0 / A), np.full(len(atoms), f)))
+    allpos = np.concatenate(allpos)
+    model = PathModel(st, gs, allpos, nrows=frames, box=box)      # every path stays within its own frame
+    q = torch.tensor(K401, device="cuda")
+    S = st.linear_matrix(K401).double()
+    with torch.no_grad():
+        rows = model.rows(torch.tensor(allpos, device="cuda"), q, S).cpu().numpy()
+    orc = O.Oracle(P)
+    So = orc.linear_matrix(K401)
+    coords = model.coords(torch.tensor(allpos, device="cuda")).cpu().numpy()
+    nl, deg, row = model.batch.nleg.cpu().numpy(), model.batch.deg.cpu().numpy(), model.batch.row.cpu().numpy()
+    ip = model.batch.ipots.cpu().numpy()
+    chi = np.zeros((len(nl), len(K401)))
+    for n in np.unique(nl):
+        sel = np.nonzero(nl == n)[0]
+        cc, rf = orc.cchi(coords[sel, :n], ip[sel, :n])
+        chi[sel] = O.chi_fine(cc, rf, K401, So)
+    ref = O.chi_rows(chi, deg, row, frames, K401)
+    for f in range(frames):
+        R = _R(K401, ref[f], rows[f])
+        print(f"cfg4 frame {f}: R {R:.2e}")
+        assert R <= 1e-6
+
+
+def test_cfg5_two_edge_refinement_graph():
+    from feffgpu_b200 import GPUPathStage
+    from feffgpu_b200.model import GraphedRefinement, PathModel
+    from feffgpu_b200.rspace import FitWindow, RSpaceMisfit
+    pos0, lab, box = W.rock_salt_supercell(3, 4.177)
+    rng = np.random.default_rng(5)
+    keep = rng.random(len(pos0)) >= 0.05
+    pos0, lab = pos0[keep], lab[keep]
+    pos = W.thermal(pos0, 0.1, seed=6)
+    hidden = W.thermal(pos, 0.03, seed=7)
+    q = torch.tensor(K401, device="cuda")
+    models = []
+    for edge, fname, ipmap in (("Ni", "cfg5_nik_phase", {"Ni": 1, "O": 2}), ("O", "cfg5_ok_phase", {"Ni": 1, "O": 2})):
+        st = GPUPathStage(phase(fname), device="cuda", dtype=torch.complex64)
+        ipot_of = np.array([ipmap[x] for x in lab])
+        gs = []
+        for a in W.central_atom(pos, box, lab, edge, 2):
+            paths = W.random_paths(pos, box, int(a), {2: 12, 3: 60, 4: 60}, rmax=5.0, leg_max=5.0, seed=int(a),
+                                   ipot_of=ipot_of)
+            for nleg, (c, ip, atoms) in paths.items():
+                gs.append((np.concatenate([np.full((len(atoms), 1), a), atoms], 1), ip, np.ones(len(atoms)),
+                           np.zeros(len(atoms), int)))
+        model = PathModel(st, gs, pos, nrows=1, box=box)
+        S = st.linear_matrix(K401).double().contiguous()
+        with torch.no_grad():
+            target = model.rows(torch.tensor(hidden, device="cuda"), q, S)[0]
+        models.append((model, q, S, RSpaceMisfit(len(K401), target, FitWindow(kmin=3.0, kmax=14.0, rmin=1.0, rmax=5.0))))
+    g = GraphedRefinement(models, pos, lr=0.002)
+    eager_pos = torch.tensor(pos, device="cuda", requires_grad=True)        # the same steps without the graph
+    opt = torch.optim.Adam([eager_pos], lr=0.002, capturable=True)
+    losses = []
+    for it in range(15):
+        g.step()
+        opt.zero_grad()
+        loss = sum(mis(m.rows(eager_pos, qq, SS).mean(0, keepdim=True))[0] for m, qq, SS, mis in models)
+        loss.backward()
+        opt.step()
+        torch.cuda.synchronize()
+        losses.append(float(g.loss))
+        assert abs(float(g.loss) - float(loss)) <= 1e-9 * abs(float(loss)), (it, float(g.loss), float(loss))
+    assert torch.allclose(g.pos.detach(), eager_pos.detach(), rtol=0, atol=1e-9)
+    print(f"cfg5: misfit {losses[0]:.4e} -> {losses[-1]:.4e}")
+    assert losses[-1] < 0.8 * losses[0]
