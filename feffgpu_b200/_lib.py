@@ -7,10 +7,14 @@ same condition (ValueError, NotImplementedError) or RuntimeError for CUDA errors
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "_build" / "libfeffgpu_b200.so"
+# a different build of the same library (e.g. one compiled with other launch bounds) may be named here
+if os.environ.get("FEFFGPU_B200_LIB"):
+    LIB_PATH = Path(os.environ["FEFFGPU_B200_LIB"]).resolve()
 
 FG_OK, FG_ERR_VALUE, FG_ERR_NOT_IMPLEMENTED, FG_ERR_CUDA, FG_ERR_WORKSPACE = range(5)
 FG_MIXED, FG_FP64 = 0, 1

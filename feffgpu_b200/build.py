@@ -35,16 +35,21 @@ def _headers_mtime() -> float:
     return max(f.stat().st_mtime for f in files)
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> Path:
-    """Compile (if stale) and return the library path."""
-    OUT.mkdir(exist_ok=True)
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False, out: Path | None = None,
+          defines: dict | None = None) -> Path:
+    """Compile (if stale) and return the library path.  out/defines build a variant elsewhere (preprocessor
+    definitions such as FG_FUSED_MIN_BLOCKS) for the autotuner's offline comparisons."""
+    out_dir = OUT if out is None else Path(out)
+    lib = out_dir / LIB.name
+    out_dir.mkdir(parents=True, exist_ok=True)
+    extra = [f"-D{k}={v}" for k, v in (defines or {}).items()]
     sources = sorted(CSRC.glob("*.cu"))
     hdr = _headers_mtime()
     jobs = []
     for src in sources:
-        obj = OUT / (src.stem + ".o")
+        obj = out_dir / (src.stem + ".o")
         if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, hdr):
-            cmd = [nvcc(), *ARCH, *FLAGS, "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-c", str(src), "-o", str(obj)]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
             jobs.append((src, cmd))
@@ -62,16 +67,16 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
                     sys.stderr.write(r.stdout + r.stderr)
                 if r.returncode:
                     raise RuntimeError(f"nvcc failed on {src.name}")
-    objs = [str(OUT / (s.stem + ".o")) for s in sources]
-    if jobs or not LIB.exists() or LIB.stat().st_mtime < max(Path(o).stat().st_mtime for o in objs):
-        tmp = LIB.with_suffix(".so.tmp")
+    objs = [str(out_dir / (s.stem + ".o")) for s in sources]
+    if jobs or not lib.exists() or lib.stat().st_mtime < max(Path(o).stat().st_mtime for o in objs):
+        tmp = lib.with_suffix(".so.tmp")
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("nvcc link failed")
-        os.replace(tmp, LIB)
-    return LIB
+        os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":

@@ -344,13 +344,17 @@ __device__ __forceinline__ void cfac_grad(const WarpPath<R> &g, const Tables<R> 
 }
 
 // ------------------------------------------------------------------------------------------------ one energy
-// Multiple scattering (nleg >= 3).  Adds this energy's parameter gradients into pg.
+// Multiple scattering (nleg >= 3).  Adds this energy's parameter gradients into pg.  Every scattering matrix is
+// handled as a full lamx x lamx matrix (one code path for the first, middle and last matrices, so that the large
+// unrolled loops fit the instruction cache): the first matrix's columns beyond laml0x and the last matrix's rows
+// beyond laml0x get zero weight.
 template <typename R, int KIND>
 __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, const R (*dterm_db)[49],
                               const Tables<R> &T, int e, int nleg, C2<R> gbar, ParGrad &pg)
 {
     constexpr LamTab L = lamtab(KIND);
     constexpr int N = L.N, N0 = L.N0, MM = L.MM, DS = dstride(MM);
+    constexpr RepTab<KIND, N, N> RT{};
     const int E = T.E, nsc = nleg - 1;
     const size_t dleg = (size_t)(T.L1 + 1) * DS, tlip = (size_t)(T.L1 + 1) * E;
     const C2<R> ck = T.ck[e];
@@ -359,24 +363,7 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     term_legs<R, KIND>(g, T, e, nleg, ck, tl);
     // sweep 1: prefix products P_k = F_k ... F_1, k = 1..nsc-1 (lamx x laml0x), kept in local memory
     C2<R> Pst[kMaxLeg - 2][N][N0];
-    {
-        constexpr RepTab<KIND, N, N0> RT{};
-        C2<R> acc[RT.n];
-        const int ip = g.ip[1];
-        accumulate_f<R, KIND, N, N0>(acc, dh, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
-                                     zfac(cscl(ck, (R)g.ri[2])), zfac(cscl(ck, (R)g.ri[1])));
-        C2<R> ph[2 * MM + 1];
-        phase_powers<R, MM>(g.phs[2], ph);
-#pragma unroll
-        for (int a = 0; a < N; ++a)
-#pragma unroll
-            for (int b = 0; b < N0; ++b) {
-                const C2<R> v = RT.sg[a][b] > 0 ? acc[RT.rep[a][b]] : cscl(acc[RT.rep[a][b]], R(-1));
-                Pst[0][a][b] = cmul(ph[L.m[a] + MM], v);
-            }
-    }
-    for (int k = 2; k < nsc; ++k) {
-        constexpr RepTab<KIND, N, N> RT{};
+    for (int k = 1; k < nsc; ++k) {
         C2<R> acc[RT.n];
         const int ip = g.ip[k];
         accumulate_f<R, KIND, N, N>(acc, dh + (k - 1) * dleg, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
@@ -388,10 +375,14 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
 #pragma unroll
             for (int b = 0; b < N0; ++b) {
                 C2<R> s = cz<R>();
+                if (k == 1) {
+                    s = RT.sg[a][b] > 0 ? acc[RT.rep[a][b]] : cscl(acc[RT.rep[a][b]], R(-1));
+                } else {
 #pragma unroll
-                for (int c = 0; c < N; ++c) {
-                    const C2<R> f = acc[RT.rep[a][c]];
-                    s = RT.sg[a][c] > 0 ? cfma(f, Pst[k - 2][c][b], s) : cfms(f, Pst[k - 2][c][b], s);
+                    for (int c = 0; c < N; ++c) {
+                        const C2<R> f = acc[RT.rep[a][c]];
+                        s = RT.sg[a][c] > 0 ? cfma(f, Pst[k - 2][c][b], s) : cfms(f, Pst[k - 2][c][b], s);
+                    }
                 }
                 Pst[k - 1][a][b] = cmul(ph[L.m[a] + MM], s);
             }
@@ -400,80 +391,25 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     const C2<R> sd = cmul(C2<R>{gbar.x, -gbar.y}, cf);      // s = conj(gbar) cfac: dL = Re(s dptrac)
     const C2<R> sck = cmul(sd, ck);
     auto add_re = [](double &acc, C2<R> s, C2<R> v) { acc += (double)s.x * v.x - (double)s.y * v.y; };
-    // sweep 2, k = nsc: the last matrix (laml0x x lamx), M = P_(nsc-1) T
     C2<R> Tm[N0][N0];
     term_matrix<R, KIND>(g, T, e, tl, Tm);
-    C2<R> Rm[N0][N];    // R_k = T F_nsc ... F_(k+1)
-    {
-        constexpr RepTab<KIND, N0, N> RT{};
-        C2<R> ph[2 * MM + 1];
-        phase_powers<R, MM>(g.phs[nleg], ph);
-        C2<R> Wh[RT.n], We[RT.n];
-        // M(b, a) = sum_c P_(nsc-1)[b][c] T[c][a]: b < N (cols of F), a < N0 (rows of F)
-        orbit_weights<R, KIND, N0, N, MM>(
-            [&](int b, int a) {
-                C2<R> m = cz<R>();
+    // sweep 2, k = nsc .. 1 with R_k = T F_nsc ... F_(k+1) (laml0x x lamx; for k = nsc only its first laml0x
+    // columns are T itself) and M_k = P_(k-1) R_k
+    C2<R> Rm[N0][N];
 #pragma unroll
-                for (int c = 0; c < N0; ++c) m = cfma(Pst[nsc - 2][b][c], Tm[c][a], m);
-                return m;
-            },
-            ph, Wh, We);
-        C2<R> acc[RT.n];
-        C2<R> gi, go, gb;
-        const int ip = g.ip[nsc];
-        accumulate_f_adj<R, KIND, N0, N>(acc, Wh, dh + (nsc - 1) * dleg, dhd + (nsc - 1) * dleg,
-                                         T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
-                                         zfac(cscl(ck, (R)g.ri[nleg])), zfac(cscl(ck, (R)g.ri[nsc])), gi, go, gb);
-        C2<R> ge = cz<R>();
+    for (int a = 0; a < N0; ++a)
 #pragma unroll
-        for (int r = 0; r < RT.n; ++r) ge = cfma(acc[r], We[r], ge);
-        add_re(pg.ri[nleg], sck, gi);
-        add_re(pg.ri[nsc], sck, go);
-        add_re(pg.beta[nsc], sd, gb);
-        add_re(pg.eta[nleg], sd, ge);
-        // F_nsc, P_nsc = F_nsc P_(nsc-1), the termination's own gradients and R_(nsc-1) = T F_nsc
-        C2<R> Fl[N0][N];
-#pragma unroll
-        for (int a = 0; a < N0; ++a)
-#pragma unroll
-            for (int b = 0; b < N; ++b) {
-                const C2<R> v = RT.sg[a][b] > 0 ? acc[RT.rep[a][b]] : cscl(acc[RT.rep[a][b]], R(-1));
-                Fl[a][b] = cmul(ph[L.m[a] + MM], v);
-            }
-        C2<R> ge1 = cz<R>(), gbn = cz<R>(), gr1 = cz<R>(), grn = cz<R>();
-        const C2<R> ptrac = term_adj<R, KIND>(
-            g, dterm_db, T, e, tl,
-            [&](int b, int a) {
-                C2<R> p = cz<R>();
-#pragma unroll
-                for (int c = 0; c < N; ++c) p = cfma(Fl[b][c], Pst[nsc - 2][c][a], p);
-                return p;
-            },
-            ge1, gbn, gr1, grn);
-        add_re(pg.eta[1], sd, ge1);
-        add_re(pg.beta[nleg], sd, gbn);
-        add_re(pg.ri[1], sck, gr1);
-        add_re(pg.ri[nleg], sck, grn);
-        cfac_grad(g, T, e, nleg, gbar, cmul(ptrac, cf), pg);
-#pragma unroll
-        for (int a = 0; a < N0; ++a)
-#pragma unroll
-            for (int b = 0; b < N; ++b) {
-                C2<R> v = cz<R>();
-#pragma unroll
-                for (int c = 0; c < N0; ++c) v = cfma(Tm[a][c], Fl[c][b], v);
-                Rm[a][b] = v;
-            }
-    }
-    // middle matrices k = nsc-1 .. 2 (lamx x lamx): M = P_(k-1) R_k
-    for (int k = nsc - 1; k >= 2; --k) {
-        constexpr RepTab<KIND, N, N> RT{};
+        for (int b = 0; b < N; ++b) Rm[a][b] = b < N0 ? Tm[a][b] : cz<R>();
+    for (int k = nsc; k >= 1; --k) {
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
         C2<R> Wh[RT.n], We[RT.n];
         orbit_weights<R, KIND, N, N, MM>(
             [&](int b, int a) {
+                // M(b, a) for F rows a, columns b: the last matrix has laml0x live rows, the first laml0x columns
                 C2<R> m = cz<R>();
+                if (k == nsc && a >= N0) return m;
+                if (k == 1) return b < N0 ? Rm[b][a] : m;
 #pragma unroll
                 for (int c = 0; c < N0; ++c) m = cfma(Pst[k - 2][b][c], Rm[c][a], m);
                 return m;
@@ -492,43 +428,48 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
         add_re(pg.ri[k], sck, go);
         add_re(pg.beta[k], sd, gb);
         add_re(pg.eta[k + 1], sd, ge);
-        C2<R> Rn[N0][N];
+        if (k == nsc) {
+            // P_nsc = F_nsc P_(nsc-1) (laml0x x laml0x): the termination's own gradients and ptrac
+            C2<R> ge1 = cz<R>(), gbn = cz<R>(), gr1 = cz<R>(), grn = cz<R>();
+            const C2<R> ptrac = term_adj<R, KIND>(
+                g, dterm_db, T, e, tl,
+                [&](int b, int a) {
+                    C2<R> p = cz<R>();
 #pragma unroll
-        for (int a = 0; a < N0; ++a)
+                    for (int c = 0; c < N; ++c) {
+                        const C2<R> f = cmul(ph[L.m[b] + MM], acc[RT.rep[b][c]]);
+                        p = RT.sg[b][c] > 0 ? cfma(f, Pst[nsc - 2][c][a], p) : cfms(f, Pst[nsc - 2][c][a], p);
+                    }
+                    return p;
+                },
+                ge1, gbn, gr1, grn);
+            add_re(pg.eta[1], sd, ge1);
+            add_re(pg.beta[nleg], sd, gbn);
+            add_re(pg.ri[1], sck, gr1);
+            add_re(pg.ri[nleg], sck, grn);
+            cfac_grad(g, T, e, nleg, gbar, cmul(ptrac, cf), pg);
+        }
+        if (k > 1) {
+            // R_(k-1) = R_k F_k over the live rows of F_k
+            C2<R> Rn[N0][N];
 #pragma unroll
-            for (int b = 0; b < N; ++b) {
-                C2<R> v = cz<R>();
+            for (int a = 0; a < N0; ++a)
 #pragma unroll
-                for (int c = 0; c < N; ++c) {
-                    const C2<R> f = cmul(ph[L.m[c] + MM], acc[RT.rep[c][b]]);
-                    v = RT.sg[c][b] > 0 ? cfma(Rm[a][c], f, v) : cfms(Rm[a][c], f, v);
+                for (int b = 0; b < N; ++b) {
+                    C2<R> v = cz<R>();
+#pragma unroll
+                    for (int c = 0; c < N; ++c) {
+                        if (k == nsc && c >= N0) continue;
+                        const C2<R> f = cmul(ph[L.m[c] + MM], acc[RT.rep[c][b]]);
+                        v = RT.sg[c][b] > 0 ? cfma(Rm[a][c], f, v) : cfms(Rm[a][c], f, v);
+                    }
+                    Rn[a][b] = v;
                 }
-                Rn[a][b] = v;
-            }
 #pragma unroll
-        for (int a = 0; a < N0; ++a)
+            for (int a = 0; a < N0; ++a)
 #pragma unroll
-            for (int b = 0; b < N; ++b) Rm[a][b] = Rn[a][b];
-    }
-    // first matrix k = 1 (lamx x laml0x): M = R_1 (P_0 = identity)
-    {
-        constexpr RepTab<KIND, N, N0> RT{};
-        C2<R> ph[2 * MM + 1];
-        phase_powers<R, MM>(g.phs[2], ph);
-        C2<R> Wh[RT.n], We[RT.n];
-        orbit_weights<R, KIND, N, N0, MM>([&](int b, int a) { return Rm[b][a]; }, ph, Wh, We);
-        C2<R> acc[RT.n];
-        C2<R> gi, go, gb;
-        const int ip = g.ip[1];
-        accumulate_f_adj<R, KIND, N, N0>(acc, Wh, dh, dhd, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
-                                         zfac(cscl(ck, (R)g.ri[2])), zfac(cscl(ck, (R)g.ri[1])), gi, go, gb);
-        C2<R> ge = cz<R>();
-#pragma unroll
-        for (int r = 0; r < RT.n; ++r) ge = cfma(acc[r], We[r], ge);
-        add_re(pg.ri[2], sck, gi);
-        add_re(pg.ri[1], sck, go);
-        add_re(pg.beta[1], sd, gb);
-        add_re(pg.eta[2], sd, ge);
+                for (int b = 0; b < N; ++b) Rm[a][b] = Rn[a][b];
+        }
     }
 }
 

@@ -110,6 +110,30 @@ __device__ void path_setup(WarpPath<R> &g, R *dh, const Tables<R> &T, const CT *
     __syncwarp();
 }
 
+// A rotation-table row (NCAN entries of a 16-byte aligned row) with vector loads
+template <typename R, int NCAN> __device__ __forceinline__ void load_row(const R *row, R (&d)[NCAN])
+{
+    if constexpr (sizeof(R) == 4) {
+        const float4 *v = reinterpret_cast<const float4 *>(row);
+#pragma unroll
+        for (int i = 0; i < (NCAN + 3) / 4; ++i) {
+            const float4 x = v[i];
+            if (4 * i + 0 < NCAN) d[4 * i + 0] = x.x;
+            if (4 * i + 1 < NCAN) d[4 * i + 1] = x.y;
+            if (4 * i + 2 < NCAN) d[4 * i + 2] = x.z;
+            if (4 * i + 3 < NCAN) d[4 * i + 3] = x.w;
+        }
+    } else {
+        const double2 *v = reinterpret_cast<const double2 *>(row);
+#pragma unroll
+        for (int i = 0; i < (NCAN + 1) / 2; ++i) {
+            const double2 x = v[i];
+            if (2 * i + 0 < NCAN) d[2 * i + 0] = x.x;
+            if (2 * i + 1 < NCAN) d[2 * i + 1] = x.y;
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------------------------ streaming F
 // Accumulates the canonical entries of F~_k (before the Euler phase) for rows lam1 < NR, columns lam2 < NC.
 // Scatterer k, gam leg k+1 (rho_in), gamtl leg k (rho_out), partial waves il = 1..ilx.
@@ -135,14 +159,15 @@ __device__ __forceinline__ void accumulate_f(C2<R> (&acc)[RepTab<KIND, NR, NC>()
     ci[1] = C2<R>{R(1), R(0)};
     po[1] = C2<R>{R(1), R(0)};
     co[1] = C2<R>{R(1), R(0)};
-    C2<R> tnext = tlk[E];
+    // t-matrix of the next two partial waves in flight (the table is read from L2)
+    C2<R> t1 = tlk[E], t2 = ilx >= 2 ? tlk[(size_t)2 * E] : cz<R>();
     for (int il = 1; il <= ilx; ++il) {
-        const C2<R> t = tnext;
-        if (il < ilx) tnext = tlk[(size_t)(il + 1) * E];
+        const C2<R> t = t1;
+        t1 = t2;
+        if (il + 2 <= ilx) t2 = tlk[(size_t)(il + 2) * E];
         const R *dr = dhk + (size_t)il * DS;
         R d[NCAN];
-#pragma unroll
-        for (int q = 0; q < NCAN; ++q) d[q] = dr[q];
+        load_row<R, NCAN>(dr, d);
         C2<R> tco[CO + 1];
 #pragma unroll
         for (int j = 1; j <= CO; ++j) tco[j] = cmul(t, co[j]);
@@ -290,37 +315,22 @@ __device__ __forceinline__ C2<R> cfac(const WarpPath<R> &g, const Tables<R> &T, 
 }
 
 // ------------------------------------------------------------------------------------------------ one energy
-// Paths with two or more scatterers (nleg >= 3).
+// Paths with two or more scatterers (nleg >= 3).  Every scattering matrix is accumulated as a full lamx x lamx
+// matrix -- the first matrix's columns beyond laml0x and the last one's rows beyond laml0x are computed and not
+// used -- so that one unrolled loop serves the whole chain: measured on B200 the smaller instruction footprint
+// outweighs the extra entries (57.4 vs 62.4 ms for the 2e5-path benchmark launch).
 template <typename R, int KIND>
 __device__ C2<R> energy_ms(const WarpPath<R> &g, const R *dh, const Tables<R> &T, int e, int nleg)
 {
     constexpr LamTab L = lamtab(KIND);
     constexpr int N = L.N, N0 = L.N0, MM = L.MM, DS = dstride(MM);
+    constexpr RepTab<KIND, N, N> RT{};
     const int E = T.E, nsc = nleg - 1;
     const size_t dleg = (size_t)(T.L1 + 1) * DS, tlip = (size_t)(T.L1 + 1) * E;
     const C2<R> ck = T.ck[e];
     if (fabs((double)ck.x) + fabs((double)ck.y) <= 1e-16) return cz<R>();
     C2<R> P[N][N0];
-    // F_1 = f(2,1): scatterer 1, gam leg 2, gamtl leg 1
-    {
-        constexpr RepTab<KIND, N, N0> RT{};
-        C2<R> acc[RT.n];
-        const int ip = g.ip[1];
-        accumulate_f<R, KIND, N, N0>(acc, dh, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
-                                     zfac(cscl(ck, (R)g.ri[2])), zfac(cscl(ck, (R)g.ri[1])));
-        C2<R> ph[2 * MM + 1];
-        phase_powers<R, MM>(g.phs[2], ph);
-#pragma unroll
-        for (int a = 0; a < N; ++a)
-#pragma unroll
-            for (int b = 0; b < N0; ++b) {
-                const C2<R> v = RT.sg[a][b] > 0 ? acc[RT.rep[a][b]] : cscl(acc[RT.rep[a][b]], R(-1));
-                P[a][b] = cmul(ph[L.m[a] + MM], v);
-            }
-    }
-    // F_k, k = 2..nsc-1 (lamx x lamx)
-    for (int k = 2; k < nsc; ++k) {
-        constexpr RepTab<KIND, N, N> RT{};
+    for (int k = 1; k <= nsc; ++k) {
         C2<R> acc[RT.n];
         const int ip = g.ip[k];
         accumulate_f<R, KIND, N, N>(acc, dh + (k - 1) * dleg, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
@@ -333,10 +343,14 @@ __device__ C2<R> energy_ms(const WarpPath<R> &g, const R *dh, const Tables<R> &T
 #pragma unroll
             for (int b = 0; b < N0; ++b) {
                 C2<R> s = cz<R>();
+                if (k == 1) {
+                    s = RT.sg[a][b] > 0 ? acc[RT.rep[a][b]] : cscl(acc[RT.rep[a][b]], R(-1));
+                } else {
 #pragma unroll
-                for (int c = 0; c < N; ++c) {
-                    const C2<R> f = acc[RT.rep[a][c]];
-                    s = RT.sg[a][c] > 0 ? cfma(f, P[c][b], s) : cfms(f, P[c][b], s);
+                    for (int c = 0; c < N; ++c) {
+                        const C2<R> f = acc[RT.rep[a][c]];
+                        s = RT.sg[a][c] > 0 ? cfma(f, P[c][b], s) : cfms(f, P[c][b], s);
+                    }
                 }
                 Pn[a][b] = cmul(ph[L.m[a] + MM], s);
             }
@@ -345,33 +359,9 @@ __device__ C2<R> energy_ms(const WarpPath<R> &g, const R *dh, const Tables<R> &T
 #pragma unroll
             for (int b = 0; b < N0; ++b) P[a][b] = Pn[a][b];
     }
-    // F_nsc = f(nleg, nleg-1): laml0x x lamx
-    C2<R> Q[N0][N0];
-    {
-        constexpr RepTab<KIND, N0, N> RT{};
-        C2<R> acc[RT.n];
-        const int ip = g.ip[nsc];
-        accumulate_f<R, KIND, N0, N>(acc, dh + (nsc - 1) * dleg, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
-                                     zfac(cscl(ck, (R)g.ri[nleg])), zfac(cscl(ck, (R)g.ri[nsc])));
-        C2<R> ph[2 * MM + 1];
-        phase_powers<R, MM>(g.phs[nleg], ph);
-#pragma unroll
-        for (int a = 0; a < N0; ++a)
-#pragma unroll
-            for (int b = 0; b < N0; ++b) {
-                C2<R> s = cz<R>();
-#pragma unroll
-                for (int c = 0; c < N; ++c) {
-                    const C2<R> f = acc[RT.rep[a][c]];
-                    s = RT.sg[a][c] > 0 ? cfma(f, P[c][b], s) : cfms(f, P[c][b], s);
-                }
-                Q[a][b] = cmul(ph[L.m[a] + MM], s);
-            }
-    }
-    const C2<R> ptrac = termination<R, KIND>(g, T, e, nleg, ck, [&](int b, int a) { return Q[b][a]; });
+    const C2<R> ptrac = termination<R, KIND>(g, T, e, nleg, ck, [&](int b, int a) { return P[b][a]; });
     return cmul(ptrac, cfac(g, T, e, nleg, ck));
 }
-
 // Single scattering (nleg = 2), K edge: the six-entry set, flip-symmetric accumulation.
 template <typename R, int KIND>
 __device__ C2<R> energy_ss_sym(const WarpPath<R> &g, const R *dh, const Tables<R> &T, int e)

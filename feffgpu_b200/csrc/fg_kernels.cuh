@@ -12,10 +12,17 @@ template <typename R> __host__ __device__ constexpr size_t geo_bytes() { return 
 
 // Per-warp shared memory: the path state, the rotation tables of nsc legs and (fused kernels) the path's signal
 // and unwrapped phase.
+// The unwrapped phase of the fused kernel reuses the rotation tables' space once the energies are done.
+template <typename R> __host__ __device__ inline size_t table_bytes(int L1, int nsc_max, int MM, int E, bool with_signal)
+{
+    const size_t d = align_up((size_t)nsc_max * (L1 + 1) * dstride(MM) * sizeof(R), 16);
+    const size_t p = with_signal ? align_up((size_t)E * sizeof(double), 16) : 0;
+    return d > p ? d : p;
+}
 template <typename R> inline size_t warp_bytes(int L1, int nsc_max, int MM, int E, bool with_signal)
 {
-    size_t b = geo_bytes<R>() + align_up((size_t)nsc_max * (L1 + 1) * dstride(MM) * sizeof(R), 16);
-    if (with_signal) b += align_up((size_t)E * sizeof(C2<R>), 16) + align_up((size_t)E * sizeof(double), 16);
+    size_t b = geo_bytes<R>() + table_bytes<R>(L1, nsc_max, MM, E, with_signal);
+    if (with_signal) b += align_up((size_t)E * sizeof(C2<R>), 16);
     return b;
 }
 
@@ -157,8 +164,12 @@ struct PathsDev {
 // Fused forward: every path of the batch, all leg counts, from one work queue (costliest first); per path the
 // signal at all E, its amplitude and unwrapped phase, and the weighted fine-grid terms
 // deg exp(-2 sigma2 q^2) a(q) sin(phi(q) + 2 q reff) for the deterministic reduction that follows.
+#ifndef FG_FUSED_MIN_BLOCKS
+#define FG_FUSED_MIN_BLOCKS 2
+#endif
 template <typename R, int EDGE>
-__global__ void __launch_bounds__(256) k_fused(Tables<R> T, PathsDev P, int NK, const double *__restrict__ q,
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
+    k_fused(Tables<R> T, PathsDev P, int NK, const double *__restrict__ q,
                                                 const double *__restrict__ S, const int *__restrict__ span,
                                                 double *__restrict__ terms, C2<R> *__restrict__ cchi_save,
                                                 double *__restrict__ reff_save, unsigned long long *counter, int *bad,
@@ -171,9 +182,8 @@ __global__ void __launch_bounds__(256) k_fused(Tables<R> T, PathsDev P, int NK, 
     unsigned char *base = smem + (size_t)w * wbytes;
     WarpPath<R> &g = *reinterpret_cast<WarpPath<R> *>(base);
     R *dh = reinterpret_cast<R *>(base + geo_bytes<R>());
-    unsigned char *sig = base + geo_bytes<R>() + align_up((size_t)nsc_max * (L1 + 1) * dstride(K::MM) * sizeof(R), 16);
-    C2<R> *cbuf = reinterpret_cast<C2<R> *>(sig);
-    double *pha = reinterpret_cast<double *>(sig + align_up((size_t)E * sizeof(C2<R>), 16));
+    C2<R> *cbuf = reinterpret_cast<C2<R> *>(base + geo_bytes<R>() + table_bytes<R>(L1, nsc_max, K::MM, E, true));
+    double *pha = reinterpret_cast<double *>(dh);   // the tables are dead once the path's energies are done
     for (;;) {
         unsigned long long t = 0;
         if (lane == 0) t = atomicAdd(counter, 1ull);
@@ -271,7 +281,7 @@ fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const 
     if (P->n > 0) {
         const int nsc_max = P->nleg_max - 1;
         const size_t wb = warp_bytes<R>(sv.L1, nsc_max, K::MM, sv.E, true);
-        warps = fit_warps(warps, wb, sv.max_smem);
+        warps = fit_warps(warps > 4 ? 4 : warps, wb, sv.max_smem);
         const int threads = warps * 32;
         auto kern = k_fused<R, EDGE>;
         int blocks = 0;
