@@ -232,6 +232,94 @@ __device__ __forceinline__ void accumulate_f_adj(C2<R> (&acc)[RepTab<KIND, NR, N
     g_beta = gb;
 }
 
+// The contraction part of accumulate_f_adj alone (F~_k itself is known from the first sweep): per partial wave the
+// weighted sums along rho_in, rho_out and beta_k, with the spherical-wave values and tangents streamed.
+template <typename R, int KIND, int NR, int NC>
+__device__ __forceinline__ void contract_f_adj(const C2<R> (&Wh)[RepTab<KIND, NR, NC>().n], const R *dhk,
+                                               const R *dhdk, const C2<R> *tlk, int E, int ilx, C2<R> z_in,
+                                               C2<R> z_out, C2<R> &g_in, C2<R> &g_out, C2<R> &g_beta)
+{
+    constexpr RepTab<KIND, NR, NC> RT{};
+    constexpr LamTab L = lamtab(KIND);
+    constexpr int DS = dstride(L.MM);
+    constexpr int NCAN = ncanon(L.MM);
+    constexpr int CI = L.CI, CO = L.CO;
+    const C2<R> dz_in = cmul(C2<R>{R(0), R(-1)}, cmul(z_in, z_in));
+    const C2<R> dz_out = cmul(C2<R>{R(0), R(-1)}, cmul(z_out, z_out));
+    C2<R> pi[CI + 1], ci[CI + 1], po[CO + 1], co[CO + 1];
+    C2<R> dpi[CI + 1], dci[CI + 1], dpo[CO + 1], dco[CO + 1];
+#pragma unroll
+    for (int j = 0; j <= CI; ++j) pi[j] = ci[j] = dpi[j] = dci[j] = cz<R>();
+#pragma unroll
+    for (int j = 0; j <= CO; ++j) po[j] = co[j] = dpo[j] = dco[j] = cz<R>();
+    pi[1] = ci[1] = po[1] = co[1] = C2<R>{R(1), R(0)};
+    C2<R> gi = cz<R>(), go = cz<R>(), gb = cz<R>();
+    C2<R> t1 = tlk[E], t2 = ilx >= 2 ? tlk[(size_t)2 * E] : cz<R>();
+    for (int il = 1; il <= ilx; ++il) {
+        const C2<R> t = t1;
+        t1 = t2;
+        if (il + 2 <= ilx) t2 = tlk[(size_t)(il + 2) * E];
+        R d[NCAN], dd[NCAN];
+        load_row<R, NCAN>(dhk + (size_t)il * DS, d);
+        load_row<R, NCAN>(dhdk + (size_t)il * DS, dd);
+        C2<R> tco[CO + 1], tdco[CO + 1];
+#pragma unroll
+        for (int j = 1; j <= CO; ++j) { tco[j] = cmul(t, co[j]); tdco[j] = cmul(t, dco[j]); }
+        C2<R> X[CI + 1][CO + 1], Y[CI + 1][CO + 1];
+#pragma unroll
+        for (int a = 0; a <= CI; ++a)
+#pragma unroll
+            for (int b = 0; b <= CO; ++b) X[a][b] = Y[a][b] = cz<R>();
+#pragma unroll
+        for (int r = 0; r < RT.n; ++r) {
+            X[RT.ci[r]][RT.co[r]] = cfmr(Wh[r], d[RT.d[r]], X[RT.ci[r]][RT.co[r]]);
+            Y[RT.ci[r]][RT.co[r]] = cfmr(Wh[r], dd[RT.d[r]], Y[RT.ci[r]][RT.co[r]]);
+        }
+#pragma unroll
+        for (int a = 1; a <= CI; ++a) {
+            C2<R> v = cz<R>(), y = cz<R>();
+#pragma unroll
+            for (int b = 1; b <= CO; ++b) {
+                v = cfma(X[a][b], tco[b], v);
+                y = cfma(Y[a][b], tco[b], y);
+            }
+            gi = cfma(dci[a], v, gi);
+            gb = cfma(ci[a], y, gb);
+        }
+#pragma unroll
+        for (int b = 1; b <= CO; ++b) {
+            C2<R> v = cz<R>();
+#pragma unroll
+            for (int a = 1; a <= CI; ++a) v = cfma(X[a][b], ci[a], v);
+            go = cfma(tdco[b], v, go);
+        }
+        const R w = R(2 * il - 1);
+        const C2<R> wi = cscl(z_in, w), wo = cscl(z_out, w), wdi = cscl(dz_in, w), wdo = cscl(dz_out, w);
+        C2<R> ni[CI + 1], no[CO + 1], dni[CI + 1], dno[CO + 1];
+#pragma unroll
+        for (int j = 1; j <= CI; ++j) {
+            const C2<R> sv = j > 1 ? cadd(ci[j], ci[j - 1]) : ci[j];
+            const C2<R> dsv = j > 1 ? cadd(dci[j], dci[j - 1]) : dci[j];
+            ni[j] = cfms(wi, sv, pi[j]);
+            dni[j] = cfms(wdi, sv, cfms(wi, dsv, dpi[j]));
+        }
+#pragma unroll
+        for (int j = 1; j <= CO; ++j) {
+            const C2<R> sv = j > 1 ? cadd(co[j], co[j - 1]) : co[j];
+            const C2<R> dsv = j > 1 ? cadd(dco[j], dco[j - 1]) : dco[j];
+            no[j] = cfms(wo, sv, po[j]);
+            dno[j] = cfms(wdo, sv, cfms(wo, dsv, dpo[j]));
+        }
+#pragma unroll
+        for (int j = 1; j <= CI; ++j) { pi[j] = ci[j]; ci[j] = ni[j]; dpi[j] = dci[j]; dci[j] = dni[j]; }
+#pragma unroll
+        for (int j = 1; j <= CO; ++j) { po[j] = co[j]; co[j] = no[j]; dpo[j] = dco[j]; dco[j] = dno[j]; }
+    }
+    g_in = gi;
+    g_out = go;
+    g_beta = gb;
+}
+
 // Weights of the contraction: Wh[r] = sum over the orbit of r of sign * ph(m_a) * M(b, a), and the same with an
 // extra -i m_a for the Euler-angle derivative.  M(b, a) is given as a functor.
 template <typename R, int KIND, int NR, int NC, int MM, class MF>
@@ -347,7 +435,8 @@ __device__ __forceinline__ void cfac_grad(const WarpPath<R> &g, const Tables<R> 
 // Multiple scattering (nleg >= 3).  Adds this energy's parameter gradients into pg.  Every scattering matrix is
 // handled as a full lamx x lamx matrix (one code path for the first, middle and last matrices, so that the large
 // unrolled loops fit the instruction cache): the first matrix's columns beyond laml0x and the last matrix's rows
-// beyond laml0x get zero weight.
+// beyond laml0x get zero weight.  Sweep 1 keeps every F~_k and P_k in local memory, so that sweep 2's partial-wave
+// loop carries only the contraction.
 template <typename R, int KIND>
 __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, const R (*dterm_db)[49],
                               const Tables<R> &T, int e, int nleg, C2<R> gbar, ParGrad &pg)
@@ -359,15 +448,21 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     const size_t dleg = (size_t)(T.L1 + 1) * DS, tlip = (size_t)(T.L1 + 1) * E;
     const C2<R> ck = T.ck[e];
     if (fabs((double)ck.x) + fabs((double)ck.y) <= 1e-16) return;
-    TermLegs<R, KIND> tl;
-    term_legs<R, KIND>(g, T, e, nleg, ck, tl);
-    // sweep 1: prefix products P_k = F_k ... F_1, k = 1..nsc-1 (lamx x laml0x), kept in local memory
+    auto add_re = [](double &acc, C2<R> s, C2<R> v) { acc += (double)s.x * v.x - (double)s.y * v.y; };
+    const C2<R> cf = cfac(g, T, e, nleg, ck);
+    const C2<R> sd = cmul(C2<R>{gbar.x, -gbar.y}, cf);      // s = conj(gbar) cfac: dL = Re(s dptrac)
+    const C2<R> sck = cmul(sd, ck);
+    // sweep 1: F~_k for k = 1..nsc and the prefix products P_k = F_k ... F_1 (k < nsc), in local memory
+    C2<R> Fst[kMaxLeg - 1][RT.n];
     C2<R> Pst[kMaxLeg - 2][N][N0];
-    for (int k = 1; k < nsc; ++k) {
+    for (int k = 1; k <= nsc; ++k) {
         C2<R> acc[RT.n];
         const int ip = g.ip[k];
         accumulate_f<R, KIND, N, N>(acc, dh + (k - 1) * dleg, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
                                     zfac(cscl(ck, (R)g.ri[k + 1])), zfac(cscl(ck, (R)g.ri[k])));
+#pragma unroll
+        for (int r = 0; r < RT.n; ++r) Fst[k - 1][r] = acc[r];
+        if (k == nsc) break;
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
 #pragma unroll
@@ -387,67 +482,65 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
                 Pst[k - 1][a][b] = cmul(ph[L.m[a] + MM], s);
             }
     }
-    const C2<R> cf = cfac(g, T, e, nleg, ck);
-    const C2<R> sd = cmul(C2<R>{gbar.x, -gbar.y}, cf);      // s = conj(gbar) cfac: dL = Re(s dptrac)
-    const C2<R> sck = cmul(sd, ck);
-    auto add_re = [](double &acc, C2<R> s, C2<R> v) { acc += (double)s.x * v.x - (double)s.y * v.y; };
-    C2<R> Tm[N0][N0];
-    term_matrix<R, KIND>(g, T, e, tl, Tm);
+    // the termination with P_nsc = F_nsc P_(nsc-1): its own gradients, ptrac and cfac's gradient
+    TermLegs<R, KIND> tl;
+    term_legs<R, KIND>(g, T, e, nleg, ck, tl);
+    {
+        C2<R> phl[2 * MM + 1];
+        phase_powers<R, MM>(g.phs[nleg], phl);
+        C2<R> Pn[N0][N0];
+#pragma unroll
+        for (int b = 0; b < N0; ++b)
+#pragma unroll
+            for (int a = 0; a < N0; ++a) {
+                C2<R> p = cz<R>();
+#pragma unroll
+                for (int c = 0; c < N; ++c) {
+                    const C2<R> f = Fst[nsc - 1][RT.rep[b][c]];
+                    p = RT.sg[b][c] > 0 ? cfma(f, Pst[nsc - 2][c][a], p) : cfms(f, Pst[nsc - 2][c][a], p);
+                }
+                Pn[b][a] = cmul(phl[L.m[b] + MM], p);
+            }
+        C2<R> ge1 = cz<R>(), gbn = cz<R>(), gr1 = cz<R>(), grn = cz<R>();
+        const C2<R> ptrac = term_adj<R, KIND>(g, dterm_db, T, e, tl, [&](int b, int a) { return Pn[b][a]; }, ge1, gbn,
+                                              gr1, grn);
+        add_re(pg.eta[1], sd, ge1);
+        add_re(pg.beta[nleg], sd, gbn);
+        add_re(pg.ri[1], sck, gr1);
+        add_re(pg.ri[nleg], sck, grn);
+        cfac_grad(g, T, e, nleg, gbar, cmul(ptrac, cf), pg);
+    }
     // sweep 2, k = nsc .. 1 with R_k = T F_nsc ... F_(k+1) (laml0x x lamx; for k = nsc only its first laml0x
     // columns are T itself) and M_k = P_(k-1) R_k
     C2<R> Rm[N0][N];
+    {
+        C2<R> Tm[N0][N0];
+        term_matrix<R, KIND>(g, T, e, tl, Tm);
 #pragma unroll
-    for (int a = 0; a < N0; ++a)
+        for (int a = 0; a < N0; ++a)
 #pragma unroll
-        for (int b = 0; b < N; ++b) Rm[a][b] = b < N0 ? Tm[a][b] : cz<R>();
+            for (int b = 0; b < N; ++b) Rm[a][b] = b < N0 ? Tm[a][b] : cz<R>();
+    }
     for (int k = nsc; k >= 1; --k) {
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
-        C2<R> Wh[RT.n], We[RT.n];
-        orbit_weights<R, KIND, N, N, MM>(
-            [&](int b, int a) {
-                // M(b, a) for F rows a, columns b: the last matrix has laml0x live rows, the first laml0x columns
-                C2<R> m = cz<R>();
-                if (k == nsc && a >= N0) return m;
-                if (k == 1) return b < N0 ? Rm[b][a] : m;
-#pragma unroll
-                for (int c = 0; c < N0; ++c) m = cfma(Pst[k - 2][b][c], Rm[c][a], m);
-                return m;
-            },
-            ph, Wh, We);
-        C2<R> acc[RT.n];
-        C2<R> gi, go, gb;
-        const int ip = g.ip[k];
-        accumulate_f_adj<R, KIND, N, N>(acc, Wh, dh + (k - 1) * dleg, dhd + (k - 1) * dleg, T.tl + ip * tlip + e, E,
-                                        T.lmax[ip * E + e] + 1, zfac(cscl(ck, (R)g.ri[k + 1])),
-                                        zfac(cscl(ck, (R)g.ri[k])), gi, go, gb);
-        C2<R> ge = cz<R>();
-#pragma unroll
-        for (int r = 0; r < RT.n; ++r) ge = cfma(acc[r], We[r], ge);
-        add_re(pg.ri[k + 1], sck, gi);
-        add_re(pg.ri[k], sck, go);
-        add_re(pg.beta[k], sd, gb);
-        add_re(pg.eta[k + 1], sd, ge);
-        if (k == nsc) {
-            // P_nsc = F_nsc P_(nsc-1) (laml0x x laml0x): the termination's own gradients and ptrac
-            C2<R> ge1 = cz<R>(), gbn = cz<R>(), gr1 = cz<R>(), grn = cz<R>();
-            const C2<R> ptrac = term_adj<R, KIND>(
-                g, dterm_db, T, e, tl,
+        C2<R> Wh[RT.n];
+        {
+            C2<R> We[RT.n];
+            orbit_weights<R, KIND, N, N, MM>(
                 [&](int b, int a) {
-                    C2<R> p = cz<R>();
+                    C2<R> m = cz<R>();
+                    if (k == nsc && a >= N0) return m;
+                    if (k == 1) return b < N0 ? Rm[b][a] : m;
 #pragma unroll
-                    for (int c = 0; c < N; ++c) {
-                        const C2<R> f = cmul(ph[L.m[b] + MM], acc[RT.rep[b][c]]);
-                        p = RT.sg[b][c] > 0 ? cfma(f, Pst[nsc - 2][c][a], p) : cfms(f, Pst[nsc - 2][c][a], p);
-                    }
-                    return p;
+                    for (int c = 0; c < N0; ++c) m = cfma(Pst[k - 2][b][c], Rm[c][a], m);
+                    return m;
                 },
-                ge1, gbn, gr1, grn);
-            add_re(pg.eta[1], sd, ge1);
-            add_re(pg.beta[nleg], sd, gbn);
-            add_re(pg.ri[1], sck, gr1);
-            add_re(pg.ri[nleg], sck, grn);
-            cfac_grad(g, T, e, nleg, gbar, cmul(ptrac, cf), pg);
+                ph, Wh, We);
+            C2<R> ge = cz<R>();
+#pragma unroll
+            for (int r = 0; r < RT.n; ++r) ge = cfma(Fst[k - 1][r], We[r], ge);
+            add_re(pg.eta[k + 1], sd, ge);
         }
         if (k > 1) {
             // R_(k-1) = R_k F_k over the live rows of F_k
@@ -460,7 +553,7 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
 #pragma unroll
                     for (int c = 0; c < N; ++c) {
                         if (k == nsc && c >= N0) continue;
-                        const C2<R> f = cmul(ph[L.m[c] + MM], acc[RT.rep[c][b]]);
+                        const C2<R> f = cmul(ph[L.m[c] + MM], Fst[k - 1][RT.rep[c][b]]);
                         v = RT.sg[c][b] > 0 ? cfma(Rm[a][c], f, v) : cfms(Rm[a][c], f, v);
                     }
                     Rn[a][b] = v;
@@ -470,6 +563,14 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
 #pragma unroll
                 for (int b = 0; b < N; ++b) Rm[a][b] = Rn[a][b];
         }
+        C2<R> gi, go, gb;
+        const int ip = g.ip[k];
+        contract_f_adj<R, KIND, N, N>(Wh, dh + (k - 1) * dleg, dhd + (k - 1) * dleg, T.tl + ip * tlip + e, E,
+                                      T.lmax[ip * E + e] + 1, zfac(cscl(ck, (R)g.ri[k + 1])),
+                                      zfac(cscl(ck, (R)g.ri[k])), gi, go, gb);
+        add_re(pg.ri[k + 1], sck, gi);
+        add_re(pg.ri[k], sck, go);
+        add_re(pg.beta[k], sd, gb);
     }
 }
 
