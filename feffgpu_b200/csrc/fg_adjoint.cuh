@@ -110,12 +110,13 @@ __device__ __forceinline__ void term_legs(const WarpPath<R> &g, const Tables<R> 
                                           TermLegs<R, KIND> &tl)
 {
     constexpr LamTab L = lamtab(KIND);
-    constexpr int N0 = L.N0, ITM = 4, NCOL = 6;
+    // columns up to |m| + n + 1 of leg 1 (CI) and n + 1 of leg nleg (CO) enter
+    constexpr int N0 = L.N0, ITM = 4, CI = L.CI, CO = L.CO;
     const int E = T.E;
     const int la = T.lmax[g.ip[0] * E + e], l1 = T.lmax[g.ip[1] * E + e], ln = T.lmax[g.ip[nleg - 1] * E + e];
-    C2<R> c1[ITM + 1][NCOL + 1], cn[ITM + 1][NCOL + 1], d1[ITM + 1][NCOL + 1], dn[ITM + 1][NCOL + 1];
-    clm_small_t<R, ITM, NCOL>(zfac(cscl(ck, (R)g.ri[1])), max(la, l1) + 1, c1, d1);
-    clm_small_t<R, ITM, NCOL>(zfac(cscl(ck, (R)g.ri[nleg])), max(ln, la) + 1, cn, dn);
+    C2<R> c1[ITM + 1][CI + 1], cn[ITM + 1][CO + 1], d1[ITM + 1][CI + 1], dn[ITM + 1][CO + 1];
+    clm_small_t<R, ITM, CI>(zfac(cscl(ck, (R)g.ri[1])), max(la, l1) + 1, c1, d1);
+    clm_small_t<R, ITM, CO>(zfac(cscl(ck, (R)g.ri[nleg])), max(ln, la) + 1, cn, dn);
     for (int t = 0; t < T.nterm; ++t) {
         const int il = T.term_l[t] + 1;
 #pragma unroll
@@ -127,7 +128,7 @@ __device__ __forceinline__ void term_legs(const WarpPath<R> &g, const Tables<R> 
 #pragma unroll
             for (int q = 1; q <= ITM; ++q)
                 if (q == il) {
-                    a1 = c1[q][imn < NCOL ? imn : NCOL]; b1 = d1[q][imn < NCOL ? imn : NCOL];
+                    a1 = c1[q][imn]; b1 = d1[q][imn];
                     an = cn[q][in]; bn = dn[q][in];
                 }
             const R xn = (R)T.xnlm[il * 8 + am + 1];
@@ -433,10 +434,12 @@ __device__ __forceinline__ void cfac_grad(const WarpPath<R> &g, const Tables<R> 
 
 // ------------------------------------------------------------------------------------------------ one energy
 // Multiple scattering (nleg >= 3).  Adds this energy's parameter gradients into pg.  Every scattering matrix is
-// handled as a full lamx x lamx matrix (one code path for the first, middle and last matrices, so that the large
-// unrolled loops fit the instruction cache): the first matrix's columns beyond laml0x and the last matrix's rows
-// beyond laml0x get zero weight.  Sweep 1 keeps every F~_k and P_k in local memory, so that sweep 2's partial-wave
-// loop carries only the contraction.
+// handled as a full lamx x lamx matrix (one code path for the first, middle and last matrices): the first matrix's
+// columns beyond laml0x meet the zero rows of P_0 (the lamx x laml0x identity) and the last matrix's rows beyond
+// laml0x meet the zero columns of R_nsc = [T 0].  Sweep 1 keeps every F~_k and P_k in per-lane local memory, so that
+// sweep 2's partial-wave loop carries only the contraction.  The small matrix products between the partial-wave
+// loops run as rolled loops over one index of the local-memory operand: the per-energy code then stays within the
+// instruction cache (the unrolled products made the kernel several times larger than its two hot loops).
 template <typename R, int KIND>
 __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, const R (*dterm_db)[49],
                               const Tables<R> &T, int e, int nleg, C2<R> gbar, ParGrad &pg)
@@ -452,9 +455,15 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     const C2<R> cf = cfac(g, T, e, nleg, ck);
     const C2<R> sd = cmul(C2<R>{gbar.x, -gbar.y}, cf);      // s = conj(gbar) cfac: dL = Re(s dptrac)
     const C2<R> sck = cmul(sd, ck);
-    // sweep 1: F~_k for k = 1..nsc and the prefix products P_k = F_k ... F_1 (k < nsc), in local memory
+    // per-lane local memory: F~_k (k = 1..nsc), P_k = F_k ... F_1 P_0 (k = 0..nsc), R_k
     C2<R> Fst[kMaxLeg - 1][RT.n];
-    C2<R> Pst[kMaxLeg - 2][N][N0];
+    C2<R> Pst[kMaxLeg][N][N0];
+    C2<R> Rst[N0][N];
+#pragma unroll
+    for (int a = 0; a < N; ++a)
+#pragma unroll
+        for (int b = 0; b < N0; ++b) Pst[0][a][b] = a == b ? C2<R>{R(1), R(0)} : cz<R>();
+    // sweep 1
     for (int k = 1; k <= nsc; ++k) {
         C2<R> acc[RT.n];
         const int ip = g.ip[k];
@@ -462,106 +471,106 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
                                     zfac(cscl(ck, (R)g.ri[k + 1])), zfac(cscl(ck, (R)g.ri[k])));
 #pragma unroll
         for (int r = 0; r < RT.n; ++r) Fst[k - 1][r] = acc[r];
-        if (k == nsc) break;
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
+        // P_k = e^{-i eta_(k+1) m} F~_k P_(k-1), one column of P at a time
+#pragma unroll 1
+        for (int b = 0; b < N0; ++b) {
+            C2<R> col[N];
 #pragma unroll
-        for (int a = 0; a < N; ++a)
+            for (int c = 0; c < N; ++c) col[c] = Pst[k - 1][c][b];
 #pragma unroll
-            for (int b = 0; b < N0; ++b) {
+            for (int a = 0; a < N; ++a) {
                 C2<R> s = cz<R>();
-                if (k == 1) {
-                    s = RT.sg[a][b] > 0 ? acc[RT.rep[a][b]] : cscl(acc[RT.rep[a][b]], R(-1));
-                } else {
 #pragma unroll
-                    for (int c = 0; c < N; ++c) {
-                        const C2<R> f = acc[RT.rep[a][c]];
-                        s = RT.sg[a][c] > 0 ? cfma(f, Pst[k - 2][c][b], s) : cfms(f, Pst[k - 2][c][b], s);
-                    }
+                for (int c = 0; c < N; ++c) {
+                    const C2<R> f = acc[RT.rep[a][c]];
+                    s = RT.sg[a][c] > 0 ? cfma(f, col[c], s) : cfms(f, col[c], s);
                 }
-                Pst[k - 1][a][b] = cmul(ph[L.m[a] + MM], s);
+                Pst[k][a][b] = cmul(ph[L.m[a] + MM], s);
             }
+        }
     }
-    // the termination with P_nsc = F_nsc P_(nsc-1): its own gradients, ptrac and cfac's gradient
+    // the termination with P_nsc: its own gradients, ptrac and cfac's gradient
     TermLegs<R, KIND> tl;
     term_legs<R, KIND>(g, T, e, nleg, ck, tl);
     {
-        C2<R> phl[2 * MM + 1];
-        phase_powers<R, MM>(g.phs[nleg], phl);
-        C2<R> Pn[N0][N0];
-#pragma unroll
-        for (int b = 0; b < N0; ++b)
-#pragma unroll
-            for (int a = 0; a < N0; ++a) {
-                C2<R> p = cz<R>();
-#pragma unroll
-                for (int c = 0; c < N; ++c) {
-                    const C2<R> f = Fst[nsc - 1][RT.rep[b][c]];
-                    p = RT.sg[b][c] > 0 ? cfma(f, Pst[nsc - 2][c][a], p) : cfms(f, Pst[nsc - 2][c][a], p);
-                }
-                Pn[b][a] = cmul(phl[L.m[b] + MM], p);
-            }
         C2<R> ge1 = cz<R>(), gbn = cz<R>(), gr1 = cz<R>(), grn = cz<R>();
-        const C2<R> ptrac = term_adj<R, KIND>(g, dterm_db, T, e, tl, [&](int b, int a) { return Pn[b][a]; }, ge1, gbn,
-                                              gr1, grn);
+        const C2<R> ptrac = term_adj<R, KIND>(g, dterm_db, T, e, tl, [&](int b, int a) { return Pst[nsc][b][a]; },
+                                              ge1, gbn, gr1, grn);
         add_re(pg.eta[1], sd, ge1);
         add_re(pg.beta[nleg], sd, gbn);
         add_re(pg.ri[1], sck, gr1);
         add_re(pg.ri[nleg], sck, grn);
         cfac_grad(g, T, e, nleg, gbar, cmul(ptrac, cf), pg);
     }
-    // sweep 2, k = nsc .. 1 with R_k = T F_nsc ... F_(k+1) (laml0x x lamx; for k = nsc only its first laml0x
-    // columns are T itself) and M_k = P_(k-1) R_k
-    C2<R> Rm[N0][N];
+    // sweep 2, k = nsc .. 1 with R_k = T F_nsc ... F_(k+1) (laml0x x lamx, R_nsc = [T 0]) and M_k = P_(k-1) R_k
     {
         C2<R> Tm[N0][N0];
         term_matrix<R, KIND>(g, T, e, tl, Tm);
 #pragma unroll
         for (int a = 0; a < N0; ++a)
 #pragma unroll
-            for (int b = 0; b < N; ++b) Rm[a][b] = b < N0 ? Tm[a][b] : cz<R>();
+            for (int b = 0; b < N; ++b) Rst[a][b] = b < N0 ? Tm[a][b] : cz<R>();
     }
     for (int k = nsc; k >= 1; --k) {
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
+        // Wh[r] = sum over the flip orbit of r of sign * e^{-i eta m_a} M(b, a), We the same times -i m_a;
+        // M(b, a) = sum_c P_(k-1)(b, c) R_k(c, a), one c at a time
         C2<R> Wh[RT.n];
         {
             C2<R> We[RT.n];
-            orbit_weights<R, KIND, N, N, MM>(
-                [&](int b, int a) {
-                    C2<R> m = cz<R>();
-                    if (k == nsc && a >= N0) return m;
-                    if (k == 1) return b < N0 ? Rm[b][a] : m;
 #pragma unroll
-                    for (int c = 0; c < N0; ++c) m = cfma(Pst[k - 2][b][c], Rm[c][a], m);
-                    return m;
-                },
-                ph, Wh, We);
+            for (int r = 0; r < RT.n; ++r) Wh[r] = We[r] = cz<R>();
+#pragma unroll 1
+            for (int c = 0; c < N0; ++c) {
+                C2<R> pc[N], rr[N], re[N];
+#pragma unroll
+                for (int b = 0; b < N; ++b) pc[b] = Pst[k - 1][b][c];
+#pragma unroll
+                for (int a = 0; a < N; ++a) {
+                    rr[a] = cmul(ph[L.m[a] + MM], Rst[c][a]);
+                    re[a] = C2<R>{rr[a].y * R(L.m[a]), -rr[a].x * R(L.m[a])};     // -i m_a rr
+                }
+#pragma unroll
+                for (int a = 0; a < N; ++a)
+#pragma unroll
+                    for (int b = 0; b < N; ++b) {
+                        const int r = RT.rep[a][b];
+                        if (RT.sg[a][b] > 0) {
+                            Wh[r] = cfma(pc[b], rr[a], Wh[r]);
+                            if (L.m[a] != 0) We[r] = cfma(pc[b], re[a], We[r]);
+                        } else {
+                            Wh[r] = cfms(pc[b], rr[a], Wh[r]);
+                            if (L.m[a] != 0) We[r] = cfms(pc[b], re[a], We[r]);
+                        }
+                    }
+            }
             C2<R> ge = cz<R>();
 #pragma unroll
             for (int r = 0; r < RT.n; ++r) ge = cfma(Fst[k - 1][r], We[r], ge);
             add_re(pg.eta[k + 1], sd, ge);
         }
         if (k > 1) {
-            // R_(k-1) = R_k F_k over the live rows of F_k
-            C2<R> Rn[N0][N];
+            // R_(k-1) = R_k F_k with F_k(c, b) = e^{-i eta m_c} sign F~_k[rep(c, b)], one row of R at a time
+            C2<R> f[RT.n];
 #pragma unroll
-            for (int a = 0; a < N0; ++a)
+            for (int r = 0; r < RT.n; ++r) f[r] = Fst[k - 1][r];
+#pragma unroll 1
+            for (int a = 0; a < N0; ++a) {
+                C2<R> row[N];
+#pragma unroll
+                for (int c = 0; c < N; ++c) row[c] = cmul(Rst[a][c], ph[L.m[c] + MM]);
 #pragma unroll
                 for (int b = 0; b < N; ++b) {
                     C2<R> v = cz<R>();
 #pragma unroll
-                    for (int c = 0; c < N; ++c) {
-                        if (k == nsc && c >= N0) continue;
-                        const C2<R> f = cmul(ph[L.m[c] + MM], Fst[k - 1][RT.rep[c][b]]);
-                        v = RT.sg[c][b] > 0 ? cfma(Rm[a][c], f, v) : cfms(Rm[a][c], f, v);
-                    }
-                    Rn[a][b] = v;
+                    for (int c = 0; c < N; ++c)
+                        v = RT.sg[c][b] > 0 ? cfma(row[c], f[RT.rep[c][b]], v) : cfms(row[c], f[RT.rep[c][b]], v);
+                    Rst[a][b] = v;
                 }
-#pragma unroll
-            for (int a = 0; a < N0; ++a)
-#pragma unroll
-                for (int b = 0; b < N; ++b) Rm[a][b] = Rn[a][b];
+            }
         }
         C2<R> gi, go, gb;
         const int ip = g.ip[k];

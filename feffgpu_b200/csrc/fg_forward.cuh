@@ -243,16 +243,15 @@ __device__ __forceinline__ C2<R> termination(const WarpPath<R> &g, const Tables<
 {
     constexpr LamTab L = lamtab(KIND);
     constexpr int N0 = L.N0, MM = L.MM;
-    constexpr int ITM = 4, NCOL = 6;
-    const int nph1 = T.nph1;
-    (void)nph1;
+    // columns up to |m| + n + 1 of leg 1 (CI) and n + 1 of leg nleg (CO) enter
+    constexpr int ITM = 4, CI = L.CI, CO = L.CO;
     const int E = T.E;
     const int la = T.lmax[g.ip[0] * E + e], l1 = T.lmax[g.ip[1] * E + e], ln = T.lmax[g.ip[nleg - 1] * E + e];
     const int lx1 = max(la, l1) + 1, lxn = max(ln, la) + 1;
     const C2<R> r1 = cscl(ck, (R)g.ri[1]), rn = cscl(ck, (R)g.ri[nleg]);
-    C2<R> c1[ITM + 1][NCOL + 1], cn[ITM + 1][NCOL + 1];
-    clm_small<R, ITM, NCOL>(zfac(r1), lx1, c1);
-    clm_small<R, ITM, NCOL>(zfac(rn), lxn, cn);
+    C2<R> c1[ITM + 1][CI + 1], cn[ITM + 1][CO + 1];
+    clm_small<R, ITM, CI>(zfac(r1), lx1, c1);
+    clm_small<R, ITM, CO>(zfac(rn), lxn, cn);
     C2<R> ph1[2 * MM + 1];
     phase_powers<R, MM>(g.phs[1], ph1);
     C2<R> ptrac = cz<R>();
@@ -268,7 +267,7 @@ __device__ __forceinline__ C2<R> termination(const WarpPath<R> &g, const Tables<
             C2<R> cv1 = cz<R>(), cvn = cz<R>();
 #pragma unroll
             for (int q = 1; q <= ITM; ++q)
-                if (q == il) { cv1 = c1[q][imn < NCOL ? imn : NCOL]; cvn = cn[q][in]; }
+                if (q == il) { cv1 = c1[q][imn]; cvn = cn[q][in]; }
             const R xn = (R)T.xnlm[il * 8 + am + 1];
             const R f1 = (am & 1) ? -xn : xn;
             const R f2 = ok ? (R)(2 * il - 1) / xn : R(0);
