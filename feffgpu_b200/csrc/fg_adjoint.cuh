@@ -111,13 +111,13 @@ __device__ __forceinline__ void term_legs(const WarpPath<R> &g, const Tables<R> 
 {
     constexpr LamTab L = lamtab(KIND);
     // columns up to |m| + n + 1 of leg 1 (CI) and n + 1 of leg nleg (CO) enter
-    constexpr int N0 = L.N0, ITM = 4, CI = L.CI, CO = L.CO;
+    constexpr int N0 = L.N0, ITM = L.IT, CI = L.CI, CO = L.CO;
     const int E = T.E;
     const int la = T.lmax[g.ip[0] * E + e], l1 = T.lmax[g.ip[1] * E + e], ln = T.lmax[g.ip[nleg - 1] * E + e];
     C2<R> c1[ITM + 1][CI + 1], cn[ITM + 1][CO + 1], d1[ITM + 1][CI + 1], dn[ITM + 1][CO + 1];
     clm_small_t<R, ITM, CI>(zfac(cscl(ck, (R)g.ri[1])), max(la, l1) + 1, c1, d1);
     clm_small_t<R, ITM, CO>(zfac(cscl(ck, (R)g.ri[nleg])), max(ln, la) + 1, cn, dn);
-    for (int t = 0; t < T.nterm; ++t) {
+    for (int t = 0; t < lamtab(KIND).NT && t < T.nterm; ++t) {
         const int il = T.term_l[t] + 1;
 #pragma unroll
         for (int i = 0; i < N0; ++i) {
@@ -350,11 +350,13 @@ struct ParGrad {
 };
 
 // Termination contribution with P (the full chain, N0 x N0): ptrac and the gradients along eta_1, beta_nleg,
-// rho_1, rho_nleg (each times s, real part taken by the caller).  Rows a_lo <= a < a_hi only.
+// rho_1, rho_nleg (each times s, real part taken by the caller).  Rows a_lo <= a < a_hi only.  With Tm (row
+// stride ldt; in local memory) non-null it also receives the termination matrix itself, as term_matrix forms it.
 template <typename R, int KIND, class PF>
 __device__ __forceinline__ C2<R> term_adj(const WarpPath<R> &g, const R (*dterm_db)[49], const Tables<R> &T, int e,
                                           const TermLegs<R, KIND> &tl, const PF &P, C2<R> &g_eta1, C2<R> &g_betan,
-                                          C2<R> &g_rho1, C2<R> &g_rhon, int a_lo = 0, int a_hi = kLamTot)
+                                          C2<R> &g_rho1, C2<R> &g_rhon, C2<R> *Tm = nullptr, int ldt = 0,
+                                          int a_lo = 0, int a_hi = kLamTot)
 {
     constexpr LamTab L = lamtab(KIND);
     constexpr int N0 = L.N0, MM = L.MM;
@@ -367,14 +369,17 @@ __device__ __forceinline__ C2<R> term_adj(const WarpPath<R> &g, const R (*dterm_
 #pragma unroll
         for (int a = 0; a < N0; ++a) {
             if (a < a_lo || a >= a_hi) continue;
+            const C2<R> wf = cmul(W, cmul(ph1[L.m[a] + MM], tl.G1[t][a]));
             C2<R> x = cz<R>(), xb = cz<R>(), xn = cz<R>();
 #pragma unroll
             for (int b = 0; b < N0; ++b) {
                 const int di = (L.m[a] + 3) * 7 + L.m[b] + 3;
                 const C2<R> p = P(b, a);
-                x = cfma(cscl(tl.G2[t][b], g.dterm[t][di]), p, x);
+                const C2<R> gd = cscl(tl.G2[t][b], g.dterm[t][di]);
+                x = cfma(gd, p, x);
                 xb = cfma(cscl(tl.G2[t][b], dterm_db[t][di]), p, xb);
                 xn = cfma(cscl(tl.dG2[t][b], g.dterm[t][di]), p, xn);
+                if (Tm) Tm[a * ldt + b] = t == 0 ? cmul(wf, gd) : cfma(wf, gd, Tm[a * ldt + b]);
             }
             const C2<R> f = ph1[L.m[a] + MM];
             const C2<R> v = cmul(cmul(f, tl.G1[t][a]), x);
@@ -455,7 +460,8 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     const C2<R> cf = cfac(g, T, e, nleg, ck);
     const C2<R> sd = cmul(C2<R>{gbar.x, -gbar.y}, cf);      // s = conj(gbar) cfac: dL = Re(s dptrac)
     const C2<R> sck = cmul(sd, ck);
-    // per-lane local memory: F~_k (k = 1..nsc), P_k = F_k ... F_1 P_0 (k = 0..nsc), R_k
+    // per-lane local memory: F~_k (k = 1..nsc), P_k = F_k ... F_1 P_0 (k = 0..nsc), R_k.  (Measured on B200: loading
+    // the next column while the current one is in use, or forming P_0 on the fly instead of storing it, is slower.)
     C2<R> Fst[kMaxLeg - 1][RT.n];
     C2<R> Pst[kMaxLeg][N][N0];
     C2<R> Rst[N0][N];
@@ -496,23 +502,20 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     term_legs<R, KIND>(g, T, e, nleg, ck, tl);
     {
         C2<R> ge1 = cz<R>(), gbn = cz<R>(), gr1 = cz<R>(), grn = cz<R>();
+        // sweep 2 starts from R_nsc = [T 0] (laml0x x lamx): term_adj writes T into the first columns
+#pragma unroll
+        for (int a = 0; a < N0; ++a)
+#pragma unroll
+            for (int b = N0; b < N; ++b) Rst[a][b] = cz<R>();
         const C2<R> ptrac = term_adj<R, KIND>(g, dterm_db, T, e, tl, [&](int b, int a) { return Pst[nsc][b][a]; },
-                                              ge1, gbn, gr1, grn);
+                                              ge1, gbn, gr1, grn, &Rst[0][0], N);
         add_re(pg.eta[1], sd, ge1);
         add_re(pg.beta[nleg], sd, gbn);
         add_re(pg.ri[1], sck, gr1);
         add_re(pg.ri[nleg], sck, grn);
         cfac_grad(g, T, e, nleg, gbar, cmul(ptrac, cf), pg);
     }
-    // sweep 2, k = nsc .. 1 with R_k = T F_nsc ... F_(k+1) (laml0x x lamx, R_nsc = [T 0]) and M_k = P_(k-1) R_k
-    {
-        C2<R> Tm[N0][N0];
-        term_matrix<R, KIND>(g, T, e, tl, Tm);
-#pragma unroll
-        for (int a = 0; a < N0; ++a)
-#pragma unroll
-            for (int b = 0; b < N; ++b) Rst[a][b] = b < N0 ? Tm[a][b] : cz<R>();
-    }
+    // sweep 2, k = nsc .. 1 with R_k = T F_nsc ... F_(k+1) and M_k = P_(k-1) R_k
     for (int k = nsc; k >= 1; --k) {
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
@@ -751,7 +754,7 @@ __device__ void energy_ss_col_adj(const WarpPath<R> &g, const R *dh, const R *dh
         C2<R> ge1 = cz<R>(), gbn = cz<R>(), gr1 = cz<R>(), grn = cz<R>();
         ptrac = cadd(ptrac, term_adj<R, KIND>(
                                 g, dterm_db, T, e, tl, [&](int b, int) { return cmul(ph[L.m[b] + MM], acc[b]); }, ge1,
-                                gbn, gr1, grn, col, col + 1));
+                                gbn, gr1, grn, nullptr, 0, col, col + 1));
         add_re(pg.eta[1], sd, ge1);
         add_re(pg.beta[2], sd, gbn);
         add_re(pg.ri[1], sck, gr1);

@@ -252,6 +252,14 @@ extern "C" fg_status fg_stage_create(const fg_phase_desc *d, int device, fg_stag
             wt[(size_t)t * E + ie] += bdiag[k] * r * r;
         }
     }
+    // the kernels unroll the termination's partial waves up to il = l_init + 2 (LamTab::IT) and its terms up to one
+    // from an s level, two otherwise (LamTab::NT)
+    bool terms_ok = s->nterm <= (s->ilinit == 1 ? 1 : 2);
+    for (int t = 0; t < s->nterm; ++t) terms_ok = terms_ok && s->term_l[t] + 1 <= s->ilinit + 1;
+    if (!terms_ok) {
+        delete s;
+        return fail(FG_ERR_VALUE, "final-state terms outside l_init +- 1");
+    }
     // xnlm, xfac (folded Legendre factors), recursion coefficients of d^l
     const int XR = std::max(L1 + 2, 6);
     std::vector<double> xn((size_t)XR * 8, 0.0), xfac((size_t)XR * 49, 0.0), rc((size_t)(L1 + 1) * 49 * 3, 0.0);

@@ -67,6 +67,8 @@ template <typename R> __device__ __forceinline__ C2<R> zfac(C2<R> rho)
 // edges (mmax = nmax = l_init + 1, FEFF's LAMTOT = 15 truncates the M set).
 struct LamTab {
     int N, N0, MM, CI, CO;
+    int IT;                     // largest il = l + 1 of a final-state term: l_init + 2 (K and L1: 2, L2/L3: 3, M: 4)
+    int NT;                     // distinct final-state l: 1 from an s level (K, L1), 2 otherwise (l_init +- 1)
     int m[kLamTot], n[kLamTot];
 };
 
@@ -96,6 +98,8 @@ __host__ __device__ constexpr LamTab lamtab(int kind)
         t.N = c;
         t.N0 = c;
     }
+    t.IT = (kind == 0 || kind == 2) ? 2 : (kind == 3 ? 3 : 4);
+    t.NT = (kind == 0 || kind == 2) ? 1 : 2;
     t.MM = 0; t.CI = 0; t.CO = 0;
     for (int i = 0; i < t.N; ++i) {
         int am = t.m[i] < 0 ? -t.m[i] : t.m[i];

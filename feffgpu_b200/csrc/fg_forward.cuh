@@ -244,7 +244,7 @@ __device__ __forceinline__ C2<R> termination(const WarpPath<R> &g, const Tables<
     constexpr LamTab L = lamtab(KIND);
     constexpr int N0 = L.N0, MM = L.MM;
     // columns up to |m| + n + 1 of leg 1 (CI) and n + 1 of leg nleg (CO) enter
-    constexpr int ITM = 4, CI = L.CI, CO = L.CO;
+    constexpr int ITM = L.IT, CI = L.CI, CO = L.CO;
     const int E = T.E;
     const int la = T.lmax[g.ip[0] * E + e], l1 = T.lmax[g.ip[1] * E + e], ln = T.lmax[g.ip[nleg - 1] * E + e];
     const int lx1 = max(la, l1) + 1, lxn = max(ln, la) + 1;
@@ -255,7 +255,7 @@ __device__ __forceinline__ C2<R> termination(const WarpPath<R> &g, const Tables<
     C2<R> ph1[2 * MM + 1];
     phase_powers<R, MM>(g.phs[1], ph1);
     C2<R> ptrac = cz<R>();
-    for (int t = 0; t < T.nterm; ++t) {
+    for (int t = 0; t < lamtab(KIND).NT && t < T.nterm; ++t) {
         const int il = T.term_l[t] + 1;
         const C2<R> W = T.wt[t * E + e];
         C2<R> G1[N0], G2[N0];
