@@ -181,11 +181,11 @@ def extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms):
         fwd_bwd = {"value": None, "unit": UNIT, "note": f"not available: {err}"}
 
     # the plain FP64 drop-in (complex128) on the same batch
-    stage64 = GPUPathStage(P, device=dev, dtype=torch.complex128)
+    stage64 = GPUPathStage(P, device=dev, dtype=torch.complex128, autotune=True)
     with torch.no_grad():
         ms64, _ = timed(lambda: stage64.chi_reduce(batch, Q, S), 2, 1)
     plain = {"value": world * n_paths * NK / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
-             "speedup_mixed_over_fp64": ms64 / ms}
+             "speedup_mixed_over_fp64": ms64 / ms, "launch_warps": list(stage64._launch)}
 
     return e2e, fwd_bwd, plain
 
@@ -232,6 +232,8 @@ def main():
     import torch.distributed as dist
     from feffgpu_b200 import GPUPathStage, PathBatch, _lib
     from feffgpu_b200.roofline import batch_flops
+    from feffgpu_b200.autotune import default_tuner
+    tuner = default_tuner()
 
     if world > 1:
         torch.cuda.set_device(local)
@@ -239,7 +241,7 @@ def main():
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
     P, groups = workload(rank, world, args.paths_scale)
-    stage = GPUPathStage(P, device=dev, dtype=torch.complex64)
+    stage = GPUPathStage(P, device=dev, dtype=torch.complex64, autotune=True)
     batch = PathBatch(groups, nrows=2, device=dev)
     S = stage.linear_matrix(Q)
     lib = _lib.load()
@@ -324,6 +326,9 @@ def main():
                    "paths_per_gpu": n_paths, "legs": batch.counts, "energies": stage.E, "nk": NK,
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"dp{world} (absorbers per rank)"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "fwd_bwd": fwd_bwd, "plain_fp64": plain,
+        "autotune": {"fwd_warps": stage._launch[0], "bwd_warps": stage._launch[1],
+                     "timed": [{"kind": k, "warps": w_, "ms": round(t_, 3)} for sig, k, w_, t_ in tuner.log
+                               if sig.split("|")[1] == "p0"]},
         "gpu_launches": 3 * args.steps, "clocks": clk.summary(),
     }
     if rank == 0:

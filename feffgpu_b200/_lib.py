@@ -25,7 +25,8 @@ EXPORTS = ("fg_stage_create", "fg_stage_destroy", "fg_stage_get_info", "fg_stage
            "fg_last_error", "fg_cchi", "fg_cchi_backward_workspace", "fg_cchi_backward", "fg_chi_fine",
            "fg_chi_fine_backward", "fg_chi_reduce_workspace", "fg_chi_reduce", "fg_chi_reduce_noalloc",
            "fg_chi_reduce_backward_workspace",
-           "fg_chi_reduce_backward", "fg_set_kernel_timing", "fg_kernel_time_ms", "fg_fp32_fma_peak", "fg_set_launch")
+           "fg_chi_reduce_backward", "fg_set_kernel_timing", "fg_kernel_time_ms", "fg_fp32_fma_peak", "fg_set_launch",
+           "fg_stage_set_launch")
 
 
 class PhaseDesc(C.Structure):
@@ -71,6 +72,7 @@ _SIGS = {
     "fg_kernel_time_ms": (C.c_int, [C.POINTER(C.c_float)]),
     "fg_fp32_fma_peak": (C.c_int, [C.POINTER(C.c_double), _P]),
     "fg_set_launch": (C.c_int, [C.c_int32, C.c_int32]),
+    "fg_stage_set_launch": (C.c_int, [_P, C.c_int32, C.c_int32]),
 }
 
 _lock = threading.Lock()

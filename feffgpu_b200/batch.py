@@ -28,6 +28,7 @@ class PathBatch:
 
     def __init__(self, groups, nrows: int | None = None, device="cuda", chunk: int = 256):
         self.device = torch.device(device)
+        self.chunk = chunk
         cs, ips, nl, dg, rw = [], [], [], [], []
         nleg_max = 2
         groups = [tuple(g) + (None,) * (4 - len(g)) for g in groups]
@@ -95,6 +96,22 @@ class PathBatch:
         self.row_chunks = torch.as_tensor(np.asarray(row_chunks, np.int64)).to(d)
         self.counts = {int(k): int(v) for k, v in zip(*np.unique(nl_np, return_counts=True))}
         self._ws = {}
+        self._tuned = {}             # launch shapes chosen for this batch, per (stage, precision, k points)
+
+    def sample(self, max_paths: int) -> "PathBatch":
+        """A batch of at most max_paths of these paths: every k-th path in launch order, so every leg count keeps
+        its share (the autotuner's timing sample).  The batch itself when it is small enough."""
+        if self.n <= max_paths:
+            return self
+        step = -(-self.n // max_paths)
+        idx = self.order[::step].long()
+        nl = self.nleg[idx]
+        groups = []
+        for n in sorted(set(nl.tolist())):
+            sel = idx[nl == n]
+            groups.append((self.coords[sel, :n].cpu(), self.ipots[sel, :n].cpu(), self.deg[sel].cpu(),
+                           self.row[sel].cpu()))
+        return PathBatch(groups, nrows=self.nrows, device=self.device, chunk=self.chunk)
 
     def workspace(self, nbytes: int, backward: bool = False) -> torch.Tensor:
         """A cached device scratch buffer of at least nbytes (one per direction)."""

@@ -34,6 +34,7 @@ struct fg_stage {
     int nterm = 0, term_l[2] = {0, 0};
     int num_sms = 148;
     int max_smem = 227 * 1024;
+    int fwd_warps = 0, bwd_warps = 0;   // launch shape of this stage's calls, 0 = the process default
     std::vector<int> lmax_host;     // (E, nph1)
     std::vector<double> xk_host;    // (E)
     Tables<float> tf{};
@@ -169,6 +170,15 @@ extern "C" fg_status fg_set_launch(int32_t fwd_warps, int32_t bwd_warps)
     if (fwd_warps < 0 || fwd_warps > 8 || bwd_warps < 0 || bwd_warps > 8) return fail(FG_ERR_VALUE, "warps must be 0..8");
     g_fwd_warps = fwd_warps ? fwd_warps : 4;
     g_bwd_warps = bwd_warps ? bwd_warps : 4;
+    return FG_OK;
+}
+
+extern "C" fg_status fg_stage_set_launch(fg_stage *s, int32_t fwd_warps, int32_t bwd_warps)
+{
+    if (!s) return fail(FG_ERR_VALUE, "null stage");
+    if (fwd_warps < 0 || fwd_warps > 8 || bwd_warps < 0 || bwd_warps > 8) return fail(FG_ERR_VALUE, "warps must be 0..8");
+    s->fwd_warps = fwd_warps;
+    s->bwd_warps = bwd_warps;
     return FG_OK;
 }
 
@@ -347,6 +357,9 @@ fg_status set_device(const fg_stage *s)
     return FG_OK;
 }
 
+int fwd_warps(const fg_stage *s) { return s->fwd_warps ? s->fwd_warps : g_fwd_warps; }
+int bwd_warps(const fg_stage *s) { return s->bwd_warps ? s->bwd_warps : g_bwd_warps; }
+
 StageView view(const fg_stage *s) { return StageView{s->E, s->L1, s->nph1, s->num_sms, s->ilinit, s->max_smem}; }
 
 // Calls F::template run<R, EDGE>(tables) for the stage's precision and initial-state class.
@@ -395,7 +408,7 @@ extern "C" fg_status fg_cchi(const fg_stage *s, fg_precision prec, int64_t B, in
     const StageView sv = view(s);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return by_kind(s, prec, [&](auto L, const auto &T) {
-        return decltype(L)::cchi(sv, T, B, nleg, coords, coords_f64, ipots, cchi, reff, bad_ipot, g_fwd_warps, st);
+        return decltype(L)::cchi(sv, T, B, nleg, coords, coords_f64, ipots, cchi, reff, bad_ipot, fwd_warps(s), st);
     });
 }
 
@@ -424,7 +437,7 @@ extern "C" fg_status fg_cchi_backward(const fg_stage *s, fg_precision prec, int6
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return by_kind(s, prec, [&](auto L, const auto &T) {
         return decltype(L)::cchi_bwd(sv, T, B, nleg, coords, coords_f64, ipots, grad_cchi, grad_reff, grad_coords,
-                                     static_cast<unsigned char *>(workspace), g_bwd_warps, st);
+                                     static_cast<unsigned char *>(workspace), bwd_warps(s), st);
     });
 }
 
@@ -489,7 +502,7 @@ extern "C" fg_status fg_chi_reduce(const fg_stage *s, fg_precision prec, const f
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return by_kind(s, prec, [&](auto L, const auto &T) {
         return decltype(L)::fused(sv, T, P, NK, q, S, span, rows, cchi_save, reff_save,
-                                  static_cast<unsigned char *>(workspace), g_fwd_warps, st);
+                                  static_cast<unsigned char *>(workspace), fwd_warps(s), st);
     });
 }
 
@@ -520,7 +533,7 @@ extern "C" fg_status fg_chi_reduce_backward(const fg_stage *s, fg_precision prec
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return by_kind(s, prec, [&](auto L, const auto &T) {
         return decltype(L)::fused_bwd(sv, T, P, NK, q, S, span, tspan, grad_rows, cchi_saved, reff_saved,
-                                      grad_coords, grad_sigma2, static_cast<unsigned char *>(workspace), g_bwd_warps,
+                                      grad_coords, grad_sigma2, static_cast<unsigned char *>(workspace), bwd_warps(s),
                                       st);
     });
 }
@@ -574,6 +587,6 @@ extern "C" fg_status fg_chi_reduce_noalloc(const fg_stage *s, fg_precision prec,
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return by_kind(s, prec, [&](auto L, const auto &T) {
         return decltype(L)::fused(sv, T, P, NK, q, S, span, rows, nullptr, nullptr, static_cast<unsigned char *>(ws),
-                                  g_fwd_warps, st);
+                                  fwd_warps(s), st);
     });
 }

@@ -56,7 +56,7 @@ def _span_of(S: torch.Tensor) -> torch.Tensor:
 class GPUPathStage:
     """FEFF's path stage for one phase file on a B200 (see the module docstring)."""
 
-    def __init__(self, phase, device="cuda", dtype=torch.complex64, iorder=2):
+    def __init__(self, phase, device="cuda", dtype=torch.complex64, iorder=2, autotune=False):
         P = read_phase_pad(phase) if isinstance(phase, str) else load_phase(phase)
         if P.nsp != 1:
             raise NotImplementedError("spin-dependent phase files are not ported")
@@ -96,6 +96,10 @@ class GPUPathStage:
         self.xk = torch.tensor(xk, device=self.device, dtype=self.rdtype)
         self.ck = torch.tensor(np.sqrt(2 * (em - eref)), device=self.device, dtype=dtype)
         self._span_cache: dict = {}
+        # launch shape (warps per CTA of the forward and adjoint kernels; 0 = the library default), per workload
+        # when autotuning (feffgpu_b200.autotune)
+        self.autotune = bool(autotune)
+        self._launch = (0, 0)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -226,6 +230,42 @@ class GPUPathStage:
                                                   g.data_ptr(), gc.data_ptr(), gr.data_ptr(), _stream(self.device)))
         return gc, gr
 
+    # -- launch shape ---------------------------------------------------------------------------------------
+    def set_launch(self, fwd_warps: int = 0, bwd_warps: int = 0) -> None:
+        """Warps per CTA of this stage's forward and adjoint kernels (0 = the library default)."""
+        if (fwd_warps, bwd_warps) != self._launch:
+            _lib.check(self._lib.fg_stage_set_launch(self._h, int(fwd_warps), int(bwd_warps)))
+            self._launch = (int(fwd_warps), int(bwd_warps))
+
+    def tune(self, batch: "PathBatch", q, S=None, backward: bool = True, dtype=None, tuner=None):
+        """Times the launch shapes on (a sample of) batch, applies and returns the fastest (fwd, bwd) warps."""
+        from .autotune import default_tuner
+        if S is None:
+            S = self.linear_matrix(q)
+        Sd = torch.as_tensor(S).to(self.device, torch.float64).contiguous()
+        qt = torch.as_tensor(q, device=self.device, dtype=torch.float64).contiguous()
+        prec = self.prec if dtype is None else (_lib.FG_FP64 if dtype == torch.complex128 else _lib.FG_MIXED)
+        choice = (tuner or default_tuner()).tune(self, batch, qt, Sd, prec, backward)
+        batch._tuned[(id(self), prec, int(qt.shape[0]))] = choice
+        self.set_launch(*choice)
+        return choice
+
+    def _pick_launch(self, batch, qt, Sd, prec, backward: bool) -> None:
+        if not self.autotune:
+            return
+        from .autotune import default_tuner, signature
+        key = (id(self), prec, int(qt.shape[0]))
+        choice = batch._tuned.get(key)
+        if choice is None or (backward and choice[1] == 0):
+            tuner = default_tuner()
+            choice = tuner.lookup(signature(self, batch, int(qt.shape[0]), prec), backward)
+            if choice is None and not torch.cuda.is_current_stream_capturing():
+                choice = tuner.tune(self, batch, qt, Sd, prec, backward)
+            if choice is None:
+                return
+            batch._tuned[key] = choice
+        self.set_launch(*choice)
+
     # -- fused stage ----------------------------------------------------------------------------------------
     def chi_reduce(self, batch: "PathBatch", q, S=None, coords=None, sigma2=None, dtype=None):
         """rows (nrows, len(q)) FP64: sum over the batch's paths of deg exp(-2 sigma2 q^2) chi_path(q) into each
@@ -240,6 +280,8 @@ class GPUPathStage:
         crd = crd.to(self.device, torch.float64)
         s2 = None if sigma2 is None else torch.as_tensor(sigma2).to(self.device, torch.float64)
         prec = self.prec if dtype is None else (_lib.FG_FP64 if dtype == torch.complex128 else _lib.FG_MIXED)
+        grad = torch.is_grad_enabled() and (crd.requires_grad or (s2 is not None and s2.requires_grad))
+        self._pick_launch(batch, qt, Sd, prec, backward=grad)
         if s2 is None:
             return _ChiReduce.apply(crd, qt, Sd, self, batch, prec)
         return _ChiReduceS2.apply(crd, s2, qt, Sd, self, batch, prec)
@@ -268,6 +310,9 @@ class GPUPathStage:
         return rows, cchi, reff
 
     def _chi_reduce_backward(self, batch, coords, sigma2, q, S, prec, g_rows, cchi, reff, want_s2: bool):
+        choice = batch._tuned.get((id(self), prec, int(q.shape[0]))) if self.autotune else None
+        if choice is not None:
+            self.set_launch(*choice)
         coords = coords.contiguous()
         NK = q.shape[0]
         ps = self._paths_struct(batch, coords, sigma2)

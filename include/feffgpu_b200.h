@@ -180,9 +180,12 @@ FG_API fg_status fg_kernel_time_ms(float *ms);
  * timed with CUDA events on `stream` (the roofline denominator of the FP32 CUDA-core kernels). */
 FG_API fg_status fg_fp32_fma_peak(double *tflops, void *stream);
 
-/* Launch tuning (set by the autotuner): warps per block for the forward and the adjoint kernels (1..8),
- * 0 = the built-in default. */
+/* Launch tuning: warps per block (paths per CTA) of the persistent per-path kernels, forward and adjoint (1..8),
+ * 0 = the built-in default.  fg_set_launch sets the process-wide default; fg_stage_set_launch overrides it for the
+ * calls on one stage (what the autotuner sets per workload).  Shapes whose shared memory does not fit are
+ * narrowed to the largest that fits.  No reference counterpart (the reference has no launch shapes to tune). */
 FG_API fg_status fg_set_launch(int32_t fwd_warps, int32_t bwd_warps);
+FG_API fg_status fg_stage_set_launch(fg_stage *stage, int32_t fwd_warps, int32_t bwd_warps);
 
 #ifdef __cplusplus
 }
