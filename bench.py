@@ -9,6 +9,10 @@ cfac, fine-grid signal and the deterministic degeneracy-weighted sum into the tw
 mixed precision form (FP32 complex chain, FP64 phase argument and sums).  Under torchrun every rank evaluates its
 own two absorbers (weak scaling, no collective on the data path).
 
+Beside the headline line's value: the end-to-end form (host buffers, copies timed), forward+backward, the plain FP64
+form, the MD-EXAFS batch (bcc Fe, 500 frames x 32 absorbers in one launch) and the RMC refinement (NiO, two edges,
+each step one CUDA graph replay), each in its own key of the JSON line.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl reference times the reference's path stage on the CPU (the FP64 oracle port of its algorithm with all host
@@ -190,6 +194,98 @@ def extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms):
     return e2e, fwd_bwd, plain
 
 
+def md_extra(args, dev, timed, world, rank):
+    """MD-EXAFS batch: bcc Fe 16^3 cells (8192 atoms, a = 2.87 A), 500 seeded thermal frames (sigma 0.08 A), 32
+    absorbers per frame, every 2- and 3-leg path within 5.5 A (442 per absorber): all frames x absorbers in one fused
+    launch, chi averaged per frame.  Error: R-factor of each frame's mixed-precision chi against the FP64 form of the
+    same batch (the FP64 form itself matches the oracle to R < 1e-12 in the parity tests)."""
+    import torch
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    from feffgpu_b200 import workloads as W
+    from feffgpu_b200.compare import r_factor
+    from feffgpu_b200.pad import phase_from_npz
+    P = phase_from_npz(np.load(ROOT / "tests" / "golden" / "cfg4_fe_phase.npz"), prefix="ph_")
+    frames, absorbers = args.md_frames, 32
+    groups, per = W.md_batch(frames=frames, absorbers=absorbers, seed=rank)
+    batch = PathBatch(groups, nrows=frames, device=dev)
+    st = GPUPathStage(P, device=dev, dtype=torch.complex64, autotune=True)
+    S = st.linear_matrix(Q)
+    with torch.no_grad():
+        ms, _ = timed(lambda: st.chi_reduce(batch, Q, S), max(2, args.steps // 2), 1)
+        rows = st.chi_reduce(batch, Q, S).cpu().numpy()
+        st64 = GPUPathStage(P, device=dev, dtype=torch.complex128, autotune=True)
+        ms64, _ = timed(lambda: st64.chi_reduce(batch, Q, S), 2, 1)
+        ref = st64.chi_reduce(batch, Q, S).cpu().numpy()
+    R = [r_factor(Q, ref[f], rows[f], kmin=3.0, kmax=19.0, rmin=1.0, rmax=5.5) for f in range(frames)]
+    out = {"value": world * batch.n * NK / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "paths_per_gpu": batch.n,
+           "frames": frames, "absorbers_per_frame": absorbers, "paths_per_absorber": per, "legs": batch.counts,
+           "fp64_ms_per_step": ms64, "r_factor_vs_fp64_max": max(R), "r_factor_vs_fp64_median": float(np.median(R)),
+           "launch_warps": list(st._launch)}
+    del batch
+    torch.cuda.empty_cache()
+    return out
+
+
+def rmc_extra(args, dev, world, rank):
+    """RMC refinement: rock-salt NiO 8^3 cells (4096 sites, a = 4.177 A) with 5 % vacancies and 0.1 A disorder; Ni K
+    and O K edges, 32 absorbers each (seeded paths of 2-4 legs, rmax 5 A); targets from a hidden 0.03 A perturbation;
+    each step (both edges' rows, R-space misfits, backward, Adam on all positions) one CUDA graph replay with the
+    autotuned launch shapes; `rmc_steps` steps timed with CUDA events and the host clock."""
+    import time as _time
+    import torch
+    from feffgpu_b200 import GPUPathStage
+    from feffgpu_b200 import workloads as W
+    from feffgpu_b200.model import GraphedRefinement, PathModel
+    from feffgpu_b200.pad import phase_from_npz
+    from feffgpu_b200.rspace import FitWindow, RSpaceMisfit
+    pos0, lab, box = W.rock_salt_supercell(8, 4.177)
+    rng = np.random.default_rng(5 + rank)
+    keep = rng.random(len(pos0)) >= 0.05
+    pos0, lab = pos0[keep], lab[keep]
+    pos = W.thermal(pos0, 0.1, seed=6 + rank)
+    hidden = W.thermal(pos, 0.03, seed=7 + rank)
+    q = torch.tensor(Q, device=dev)
+    models, npaths = [], 0
+    for edge, fname in (("Ni", "cfg5_nik_phase"), ("O", "cfg5_ok_phase")):
+        st = GPUPathStage(phase_from_npz(np.load(ROOT / "tests" / "golden" / f"{fname}.npz"), prefix="ph_"),
+                          device=dev, dtype=torch.complex64, autotune=True)
+        ipot_of = np.array([{"Ni": 1, "O": 2}[x] for x in lab])
+        gs = []
+        for a in W.central_atom(pos, box, lab, edge, 32):
+            paths = W.random_paths(pos, box, int(a), {2: 24, 3: 120, 4: 200}, rmax=5.0, leg_max=5.0,
+                                   seed=int(a) + 17 * rank, ipot_of=ipot_of)
+            for nleg, (c, ip, atoms) in paths.items():
+                # deg 1/32: the row is the absorbers' average spectrum
+                gs.append((np.concatenate([np.full((len(atoms), 1), a), atoms], 1), ip, np.full(len(atoms), 1 / 32),
+                           np.zeros(len(atoms), int)))
+        model = PathModel(st, gs, pos, nrows=1, box=box)
+        npaths += model.batch.n
+        S = st.linear_matrix(Q).double().contiguous()
+        with torch.no_grad():
+            target = model.rows(torch.tensor(hidden, device=dev), q, S)[0]
+        models.append((model, q, S, RSpaceMisfit(NK, target, FitWindow(kmin=3.0, kmax=14.0, rmin=1.0, rmax=5.0),
+                                                 device=dev)))
+    g = GraphedRefinement(models, pos, lr=0.002)
+    torch.cuda.synchronize(dev)
+    g.step()
+    torch.cuda.synchronize(dev)
+    first = float(g.loss)
+    g.reset()
+    n = args.rmc_steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    t0 = _time.perf_counter()
+    e0.record()
+    for _ in range(n):
+        g.step()
+    e1.record()
+    e1.synchronize()
+    wall = (_time.perf_counter() - t0) * 1e3 / n
+    return {"steps": n, "ms_per_step": e0.elapsed_time(e1) / n, "wall_ms_per_step": wall, "atoms": len(pos),
+            "paths_per_gpu": npaths, "misfit_first_step": first, "misfit_final": float(g.loss),
+            "launch_warps": [list(m[0].stage._launch) for m in models], "graph": "one CUDA graph replay per step"}
+
+
 # ------------------------------------------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -201,6 +297,8 @@ def main():
     ap.add_argument("--paths-scale", type=float, default=1.0, help="scale the paths per leg count (profiling runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-extras", action="store_true", help="only the headline forward (profiling runs)")
+    ap.add_argument("--md-frames", type=int, default=500, help="frames of the MD-batch leg (0: skip it)")
+    ap.add_argument("--rmc-steps", type=int, default=200, help="steps of the RMC leg (0: skip it)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -289,9 +387,13 @@ def main():
             ms, kern = timed(lambda: stage.chi_reduce(batch, Q, S), args.steps, args.warmup, kernel_time=True)
     value = world * n_paths * NK / (ms * 1e-3)
 
-    e2e = fwd_bwd = plain = None
+    e2e = fwd_bwd = plain = md = rmc = None
     if not args.no_extras:
         e2e, fwd_bwd, plain = extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms)
+        if args.md_frames > 0:
+            md = md_extra(args, dev, timed, world, rank)
+        if args.rmc_steps > 0:
+            rmc = rmc_extra(args, dev, world, rank)
     # roofline of the dominant kernel (the fused per-path kernel): algorithmic FLOPs of the reference's loops
     import ctypes
     peak = ctypes.c_double()
@@ -326,6 +428,7 @@ def main():
                    "paths_per_gpu": n_paths, "legs": batch.counts, "energies": stage.E, "nk": NK,
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"dp{world} (absorbers per rank)"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "fwd_bwd": fwd_bwd, "plain_fp64": plain,
+        "md_batch": md, "rmc_refinement": rmc,
         "autotune": {"fwd_warps": stage._launch[0], "bwd_warps": stage._launch[1],
                      "timed": [{"kind": k, "warps": w_, "ms": round(t_, 3)} for sig, k, w_, t_ in tuner.log
                                if sig.split("|")[1] == "p0"]},

@@ -186,3 +186,59 @@ def central_atom(pos, box, labels=None, species=None, k=1):
     if labels is not None and species is not None:
         d = np.where(np.asarray(labels) == species, d, np.inf)
     return np.argsort(d, kind="stable")[:k]
+
+
+def bcc_site_paths(n, a, rmax=5.5):
+    """Every 2- and 3-leg path of an ideal bcc lattice (n^3 conventional cells of bcc_supercell) with half path
+    length <= rmax, as site offsets: {2: (P2, 1, 3) int, 3: (P3, 2, 3) int} scatterer offsets in units of a/2 (bcc
+    sites: all-even or all-odd half-lattice coordinates), i.e. the path finder's output for one absorber before
+    degeneracy merging (MD frames break the symmetry, so every path is kept)."""
+    m = int(np.ceil(2 * rmax / a)) + 1
+    g = np.arange(-m, m + 1)
+    v = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    v = v[((v[:, 0] % 2) == (v[:, 1] % 2)) & ((v[:, 1] % 2) == (v[:, 2] % 2)) & (np.abs(v).sum(1) > 0)]
+    r = np.linalg.norm(v * a / 2, axis=1)
+    v, r = v[r <= rmax + 1e-9], r[r <= rmax + 1e-9]
+    v = v[np.lexsort((v[:, 2], v[:, 1], v[:, 0], np.round(r, 9)))]
+    r = np.linalg.norm(v * a / 2, axis=1)
+    d = np.linalg.norm((v[:, None] - v[None]) * a / 2, axis=2)
+    i, j = np.nonzero((r[:, None] + d + r[None, :] <= 2 * rmax + 1e-9) & (d > 1e-9))
+    return {2: v[:, None, :], 3: np.stack([v[i], v[j]], 1)}
+
+
+def bcc_site_index(n, half):
+    """Atom index in bcc_supercell(n) of half-lattice coordinates (..., 3) (wrapped periodically)."""
+    h = np.mod(half, 2 * n)
+    body = h[..., 0] % 2
+    c = h // 2
+    return body * n ** 3 + (c[..., 0] * n + c[..., 1]) * n + c[..., 2]
+
+
+def md_batch(frames=500, absorbers=32, n=16, a=2.87, sigma=0.08, rmax=5.5, seed=0):
+    """MD-EXAFS batch of bcc Fe: `frames` seeded thermal snapshots (Gaussian displacements sigma) of the n^3-cell
+    supercell, `absorbers` random absorbers per frame, every 2- and 3-leg path within rmax of each (minimum-image
+    coordinates relative to the absorber).  Returns groups for PathBatch with deg = 1/absorbers and row = frame (the
+    frame's absorber average), and the number of paths per absorber."""
+    base, box = bcc_supercell(n, a)
+    half0 = np.rint(base / (a / 2)).astype(np.int64)
+    sites = bcc_site_paths(n, a, rmax)
+    rng = np.random.default_rng(seed)
+    groups = {}
+    for f in range(frames):
+        pos = thermal(base, sigma, seed=seed * 100003 + f + 1)
+        ab = rng.choice(len(base), size=absorbers, replace=False)
+        for nleg, off in sites.items():
+            idx = bcc_site_index(n, half0[ab][:, None, None, :] + off[None])          # (A, P, nleg-1)
+            rel = pos[idx] - pos[ab][:, None, None, :]
+            rel -= box * np.round(rel / box)
+            B = idx.shape[0] * idx.shape[1]
+            c = np.concatenate([np.zeros((B, 1, 3)), rel.reshape(B, nleg - 1, 3)], 1)
+            groups.setdefault(nleg, []).append((c, np.full(B, f, np.int32)))
+    out = []
+    for nleg, parts in sorted(groups.items()):
+        c = np.concatenate([p[0] for p in parts])
+        row = np.concatenate([p[1] for p in parts])
+        ip = np.ones((len(c), nleg), np.int64)
+        ip[:, 0] = 0
+        out.append((c, ip, np.full(len(c), 1.0 / absorbers), row))
+    return out, sum(len(s) for s in sites.values())

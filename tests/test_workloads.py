@@ -29,3 +29,21 @@ def test_lattices():
     assert len(p) == 128 and box == 4 * 2.87
     p, lab, box = W.rock_salt_supercell(2, 4.177)
     assert len(p) == 64 and (lab == "Ni").sum() == 32
+
+
+def test_md_batch_paths_of_bcc():
+    """Every 2- and 3-leg bcc path within 5.5 A (58 + 384 per absorber), exact lattice offsets without disorder,
+    deg = 1 / absorbers and one row per frame."""
+    s = W.bcc_site_paths(16, 2.87, 5.5)
+    assert len(s[2]) == 58 and len(s[3]) == 384
+    a = 2.87 / 2
+    r = np.linalg.norm(s[3] * a, axis=2)
+    d = np.linalg.norm((s[3][:, 1] - s[3][:, 0]) * a, axis=1)
+    assert np.all(r.sum(1) + d <= 11.0 + 1e-9) and np.all(d > 0)
+    groups, per = W.md_batch(frames=3, absorbers=4, sigma=0.0, seed=1)
+    assert per == 442
+    for (c, ip, deg, row), nleg in zip(groups, (2, 3)):
+        assert c.shape == (3 * 4 * len(s[nleg]), nleg, 3)
+        assert np.allclose(c[: 4 * len(s[nleg]), 1:].reshape(4, -1, nleg - 1, 3), s[nleg][None] * a, atol=1e-12)
+        assert np.all(ip[:, 0] == 0) and np.all(ip[:, 1:] == 1)
+        assert np.allclose(deg, 0.25) and sorted(set(row.tolist())) == [0, 1, 2]
