@@ -185,7 +185,7 @@ def extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms):
         fwd_bwd = {"value": None, "unit": UNIT, "note": f"not available: {err}"}
 
     # the plain FP64 drop-in (complex128) on the same batch
-    stage64 = GPUPathStage(P, device=dev, dtype=torch.complex128, autotune=True)
+    stage64 = GPUPathStage(P, device=dev, dtype=torch.complex128, autotune=not args.no_autotune)
     with torch.no_grad():
         ms64, _ = timed(lambda: stage64.chi_reduce(batch, Q, S), 2, 1)
     plain = {"value": world * n_paths * NK / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
@@ -208,12 +208,12 @@ def md_extra(args, dev, timed, world, rank):
     frames, absorbers = args.md_frames, 32
     groups, per = W.md_batch(frames=frames, absorbers=absorbers, seed=rank)
     batch = PathBatch(groups, nrows=frames, device=dev)
-    st = GPUPathStage(P, device=dev, dtype=torch.complex64, autotune=True)
+    st = GPUPathStage(P, device=dev, dtype=torch.complex64, autotune=not args.no_autotune)
     S = st.linear_matrix(Q)
     with torch.no_grad():
         ms, _ = timed(lambda: st.chi_reduce(batch, Q, S), max(2, args.steps // 2), 1)
         rows = st.chi_reduce(batch, Q, S).cpu().numpy()
-        st64 = GPUPathStage(P, device=dev, dtype=torch.complex128, autotune=True)
+        st64 = GPUPathStage(P, device=dev, dtype=torch.complex128, autotune=not args.no_autotune)
         ms64, _ = timed(lambda: st64.chi_reduce(batch, Q, S), 2, 1)
         ref = st64.chi_reduce(batch, Q, S).cpu().numpy()
     R = [r_factor(Q, ref[f], rows[f], kmin=3.0, kmax=19.0, rmin=1.0, rmax=5.5) for f in range(frames)]
@@ -248,7 +248,7 @@ def rmc_extra(args, dev, world, rank):
     models, npaths = [], 0
     for edge, fname in (("Ni", "cfg5_nik_phase"), ("O", "cfg5_ok_phase")):
         st = GPUPathStage(phase_from_npz(np.load(ROOT / "tests" / "golden" / f"{fname}.npz"), prefix="ph_"),
-                          device=dev, dtype=torch.complex64, autotune=True)
+                          device=dev, dtype=torch.complex64, autotune=not args.no_autotune)
         ipot_of = np.array([{"Ni": 1, "O": 2}[x] for x in lab])
         gs = []
         for a in W.central_atom(pos, box, lab, edge, 32):
@@ -298,6 +298,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-extras", action="store_true", help="only the headline forward (profiling runs)")
     ap.add_argument("--md-frames", type=int, default=500, help="frames of the MD-batch leg (0: skip it)")
+    ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (profiling runs)")
     ap.add_argument("--rmc-steps", type=int, default=200, help="steps of the RMC leg (0: skip it)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -339,7 +340,7 @@ def main():
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
     P, groups = workload(rank, world, args.paths_scale)
-    stage = GPUPathStage(P, device=dev, dtype=torch.complex64, autotune=True)
+    stage = GPUPathStage(P, device=dev, dtype=torch.complex64, autotune=not args.no_autotune)
     batch = PathBatch(groups, nrows=2, device=dev)
     S = stage.linear_matrix(Q)
     lib = _lib.load()
