@@ -53,6 +53,53 @@ template <typename R> __device__ __forceinline__ C2<R> cinv(C2<R> a)
     R d = R(1) / fma(a.x, a.x, a.y * a.y);
     return C2<R>{a.x * d, -a.y * d};
 }
+// Packed forms for the partial-wave loops: in FP32 each complex operation is issued as FP32-pair instructions
+// (sm_100 FFMA2 / FMUL2 / FADD2, both components in one instruction); the broadcast and rotated operand pairs
+// (a.x a.x), (a.y a.y), (-b.y b.x) are shared by the loops' repeated operands.  FP64 keeps the scalar forms.
+__device__ __forceinline__ float2 pk(C2<float> a) { return make_float2(a.x, a.y); }
+__device__ __forceinline__ C2<float> upk(float2 a) { return C2<float>{a.x, a.y}; }
+__device__ __forceinline__ float2 bcast(float r) { return make_float2(r, r); }
+__device__ __forceinline__ float2 rot(C2<float> b) { return make_float2(-b.y, b.x); }   // i b
+// a b
+template <typename R> __device__ __forceinline__ C2<R> pmul(C2<R> a, C2<R> b)
+{
+    if constexpr (sizeof(R) == 4)
+        return upk(__ffma2_rn(bcast(a.y), rot(b), __fmul2_rn(bcast(a.x), pk(b))));
+    else
+        return cmul(a, b);
+}
+// acc + a r
+template <typename R> __device__ __forceinline__ C2<R> pfmr(C2<R> a, R r, C2<R> acc)
+{
+    if constexpr (sizeof(R) == 4)
+        return upk(__ffma2_rn(pk(a), bcast(r), pk(acc)));
+    else
+        return cfmr(a, r, acc);
+}
+// acc + a b
+template <typename R> __device__ __forceinline__ C2<R> pfma(C2<R> a, C2<R> b, C2<R> acc)
+{
+    if constexpr (sizeof(R) == 4)
+        return upk(__ffma2_rn(bcast(a.y), rot(b), __ffma2_rn(bcast(a.x), pk(b), pk(acc))));
+    else
+        return cfma(a, b, acc);
+}
+// acc - a b
+template <typename R> __device__ __forceinline__ C2<R> pfms(C2<R> a, C2<R> b, C2<R> acc)
+{
+    if constexpr (sizeof(R) == 4)
+        return upk(__ffma2_rn(bcast(-a.y), rot(b), __ffma2_rn(bcast(-a.x), pk(b), pk(acc))));
+    else
+        return cfms(a, b, acc);
+}
+template <typename R> __device__ __forceinline__ C2<R> padd(C2<R> a, C2<R> b)
+{
+    if constexpr (sizeof(R) == 4)
+        return upk(__fadd2_rn(pk(a), pk(b)));
+    else
+        return cadd(a, b);
+}
+
 // -i / rho, the argument of FEFF's spherical-wave factors (genfmt.py:210)
 template <typename R> __device__ __forceinline__ C2<R> zfac(C2<R> rho)
 {

@@ -138,7 +138,9 @@ template <typename R, int NCAN> __device__ __forceinline__ void load_row(const R
 // Accumulates the canonical entries of F~_k (before the Euler phase) for rows lam1 < NR, columns lam2 < NC.
 // Scatterer k, gam leg k+1 (rho_in), gamtl leg k (rho_out), partial waves il = 1..ilx.  UNR unrolls the partial-wave
 // loop (two steps per trip rotate the recursion's registers instead of copying them: 6 % faster for the forward
-// kernel on B200; the adjoint's first sweep, under its higher register pressure, is faster rolled).
+// kernel on B200; the adjoint's first sweep, under its higher register pressure, is faster rolled).  The products
+// and the accumulation run as FP32-pair instructions (4.6 % faster on B200); the recursion stays scalar (pairing it
+// measured slower).
 template <typename R, int KIND, int NR, int NC, int UNR = 1>
 __device__ __forceinline__ void accumulate_f(C2<R> (&acc)[RepTab<KIND, NR, NC>().n], const R *dhk,
                                              const C2<R> *tlk, int E, int ilx, C2<R> z_in, C2<R> z_out)
@@ -173,9 +175,9 @@ __device__ __forceinline__ void accumulate_f(C2<R> (&acc)[RepTab<KIND, NR, NC>()
         load_row<R, NCAN>(dr, d);
         C2<R> tco[CO + 1];
 #pragma unroll
-        for (int j = 1; j <= CO; ++j) tco[j] = cmul(t, co[j]);
+        for (int j = 1; j <= CO; ++j) tco[j] = pmul(t, co[j]);
 #pragma unroll
-        for (int r = 0; r < RT.n; ++r) acc[r] = cfmr(cmul(ci[RT.ci[r]], tco[RT.co[r]]), d[RT.d[r]], acc[r]);
+        for (int r = 0; r < RT.n; ++r) acc[r] = pfmr(pmul(ci[RT.ci[r]], tco[RT.co[r]]), d[RT.d[r]], acc[r]);
         // next partial wave
         const R w = R(2 * il - 1);
         const C2<R> wi = cscl(z_in, w), wo = cscl(z_out, w);
