@@ -445,7 +445,9 @@ __device__ __forceinline__ void cfac_grad(const WarpPath<R> &g, const Tables<R> 
 // laml0x meet the zero columns of R_nsc = [T 0].  Sweep 1 keeps every F~_k and P_k in per-lane local memory, so that
 // sweep 2's partial-wave loop carries only the contraction.  The small matrix products between the partial-wave
 // loops run as rolled loops over one index of the local-memory operand: the per-energy code then stays within the
-// instruction cache (the unrolled products made the kernel several times larger than its two hot loops).
+// instruction cache (the unrolled products made the kernel several times larger than its two hot loops); their
+// complex multiply-adds are FP32-pair instructions (3 % faster; in the forward's register-resident chain product the
+// pairing measured slower and is not used).
 template <typename R, int KIND>
 __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, const R (*dterm_db)[49],
                               const Tables<R> &T, int e, int nleg, C2<R> gbar, ParGrad &pg)
@@ -492,7 +494,7 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
 #pragma unroll
                 for (int c = 0; c < N; ++c) {
                     const C2<R> f = acc[RT.rep[a][c]];
-                    s = RT.sg[a][c] > 0 ? cfma(f, col[c], s) : cfms(f, col[c], s);
+                    s = RT.sg[a][c] > 0 ? pfma(f, col[c], s) : pfms(f, col[c], s);
                 }
                 Pst[k][a][b] = cmul(ph[L.m[a] + MM], s);
             }
@@ -543,11 +545,11 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
                     for (int b = 0; b < N; ++b) {
                         const int r = RT.rep[a][b];
                         if (RT.sg[a][b] > 0) {
-                            Wh[r] = cfma(pc[b], rr[a], Wh[r]);
-                            if (L.m[a] != 0) We[r] = cfma(pc[b], re[a], We[r]);
+                            Wh[r] = pfma(pc[b], rr[a], Wh[r]);
+                            if (L.m[a] != 0) We[r] = pfma(pc[b], re[a], We[r]);
                         } else {
-                            Wh[r] = cfms(pc[b], rr[a], Wh[r]);
-                            if (L.m[a] != 0) We[r] = cfms(pc[b], re[a], We[r]);
+                            Wh[r] = pfms(pc[b], rr[a], Wh[r]);
+                            if (L.m[a] != 0) We[r] = pfms(pc[b], re[a], We[r]);
                         }
                     }
             }
@@ -571,7 +573,7 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
                     C2<R> v = cz<R>();
 #pragma unroll
                     for (int c = 0; c < N; ++c)
-                        v = RT.sg[c][b] > 0 ? cfma(row[c], f[RT.rep[c][b]], v) : cfms(row[c], f[RT.rep[c][b]], v);
+                        v = RT.sg[c][b] > 0 ? pfma(row[c], f[RT.rep[c][b]], v) : pfms(row[c], f[RT.rep[c][b]], v);
                     Rst[a][b] = v;
                 }
             }
