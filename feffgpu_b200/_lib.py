@@ -26,7 +26,8 @@ EXPORTS = ("fg_stage_create", "fg_stage_destroy", "fg_stage_get_info", "fg_stage
            "fg_chi_fine_backward", "fg_chi_reduce_workspace", "fg_chi_reduce", "fg_chi_reduce_noalloc",
            "fg_chi_reduce_backward_workspace",
            "fg_chi_reduce_backward", "fg_set_kernel_timing", "fg_kernel_time_ms", "fg_fp32_fma_peak", "fg_set_launch",
-           "fg_stage_set_launch")
+           "fg_stage_set_launch", "fg_pf_candidates", "fg_pf_extend", "fg_pf_terminal", "fg_pf_describe",
+           "fg_pf_windows")
 
 
 class PhaseDesc(C.Structure):
@@ -46,6 +47,11 @@ class Paths(C.Structure):
                 ("ipots", C.c_void_p), ("nleg", C.c_void_p), ("deg", C.c_void_p), ("sigma2", C.c_void_p),
                 ("row", C.c_void_p), ("order", C.c_void_p), ("sorted", C.c_void_p), ("chunk_bounds", C.c_void_p),
                 ("row_chunks", C.c_void_p), ("nchunks", C.c_int64)]
+
+
+class PfTables(C.Structure):
+    _fields_ = [("E", C.c_int32), ("nph1", C.c_int32), ("ik0", C.c_int32), ("fbeta", C.c_void_p),
+                ("cksp", C.c_void_p), ("xlam", C.c_void_p), ("trap", C.c_void_p)]
 
 
 _P = C.c_void_p
@@ -73,6 +79,12 @@ _SIGS = {
     "fg_fp32_fma_peak": (C.c_int, [C.POINTER(C.c_double), _P]),
     "fg_set_launch": (C.c_int, [C.c_int32, C.c_int32]),
     "fg_stage_set_launch": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "fg_pf_candidates": (C.c_int, [_P, C.c_int64, C.c_float, _P, C.c_int32, C.c_float, _P, _P, _P, _P, _P]),
+    "fg_pf_extend": (C.c_int, [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.c_float, _P, _P, _P, _P, _P, _P]),
+    "fg_pf_terminal": (C.c_int, [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, _P]),
+    "fg_pf_describe": (C.c_int, [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.POINTER(PfTables), _P, _P, _P,
+                                 _P, _P, _P, _P]),
+    "fg_pf_windows": (C.c_int, [_P, _P, C.c_int64, C.c_float, _P]),
 }
 
 _lock = threading.Lock()

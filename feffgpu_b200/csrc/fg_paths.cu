@@ -1,0 +1,358 @@
+// fg_paths.cu -- the path finder on the device (the reference's GPUPathFinder, src/feffgpu/pathfinder.py:159-279,
+// itself FEFF's paths.f / pathsd.f / prcrit.f), batched over absorbers.
+//
+// A path of nleg legs is a sequence of nleg - 1 "intermediates" of its absorber: the candidates (atoms within rmax of
+// the absorber, minimum image, the absorber excluded, in atom order) followed by the absorber itself.  Sequences grow
+// one atom per level from the candidates: a child appends any intermediate other than its parent's last atom whose
+// closed length (absorber -> sequence -> absorber) fits 2 rmax.  A sequence whose last atom is a candidate is a path;
+// of a path and its reverse the lexicographically smaller is kept, with degeneracy 2, or 1 for a palindrome
+// (pathfinder.py:233-271).  Children are written in parent order and, within a parent, in intermediate order, so the
+// output order is the reference's (its enumeration is the same breadth-first order).
+//
+// Every length is FP32 and formed as the reference's FP32 arithmetic forms it: differences, squares and sums
+// without contraction, correctly rounded square roots, lengths accumulated left to right.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "fg_launch.h"
+
+namespace fg {
+namespace {
+
+constexpr int kNBeta = 40;   // cos(beta) grid of the importance table: 0.025 steps (pathfinder.py:23, 49-50)
+
+__device__ __forceinline__ float len3(float x, float y, float z)
+{
+    return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
+}
+
+// minimum image in a cubic box of length b (b <= 0: none), as rel - b * round(rel / b) without contraction
+__device__ __forceinline__ float wrap1(float r, float b)
+{
+    return b > 0.f ? __fsub_rn(r, __fmul_rn(b, rintf(__fdiv_rn(r, b)))) : r;
+}
+
+// ------------------------------------------------------------------------------------------------ candidates
+// One block per absorber slot.  count: number of candidates; with out != null the candidates are written in atom
+// order at off[a] (ordered compaction: warp ballots, then the warps' counts in order).
+template <bool WRITE>
+__global__ void k_candidates(const float *__restrict__ pos, int64_t n, float box, const int64_t *__restrict__ absorbers,
+                             float rmax, int32_t *__restrict__ count, const int64_t *__restrict__ off,
+                             int64_t *__restrict__ cand_atom, float *__restrict__ cand_rel)
+{
+    __shared__ int warp_n[32];
+    __shared__ int64_t base_s;
+    const int a = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int64_t ab = absorbers[a];
+    const float ax = pos[3 * ab], ay = pos[3 * ab + 1], az = pos[3 * ab + 2];
+    if (threadIdx.x == 0) base_s = WRITE ? off[a] : 0;
+    __syncthreads();
+    int64_t total = 0;
+    for (int64_t i0 = 0; i0 < n; i0 += blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        float rx = 0.f, ry = 0.f, rz = 0.f;
+        bool c = false;
+        if (i < n) {
+            rx = wrap1(__fsub_rn(pos[3 * i], ax), box);
+            ry = wrap1(__fsub_rn(pos[3 * i + 1], ay), box);
+            rz = wrap1(__fsub_rn(pos[3 * i + 2], az), box);
+            c = i != ab && len3(rx, ry, rz) <= rmax;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, c);
+        if (lane == 0) warp_n[w] = __popc(m);
+        __syncthreads();
+        int before = 0, chunk = 0;
+        for (int q = 0; q < nw; ++q) {
+            if (q < w) before += warp_n[q];
+            chunk += warp_n[q];
+        }
+        if (WRITE && c) {
+            const int64_t o = base_s + total + before + __popc(m & ((1u << lane) - 1u));
+            cand_atom[o] = i;
+            cand_rel[3 * o] = rx;
+            cand_rel[3 * o + 1] = ry;
+            cand_rel[3 * o + 2] = rz;
+        }
+        total += chunk;
+        __syncthreads();
+    }
+    if (!WRITE && threadIdx.x == 0) count[a] = (int32_t)total;
+}
+
+// ------------------------------------------------------------------------------------------------ extension
+struct Cands {
+    const int64_t *off;     // (A + 1) candidate offsets per absorber slot
+    const float *rel;       // (total, 3) relative positions
+};
+
+__device__ __forceinline__ void cand_xyz(const Cands &C, int64_t base, int nc, int j, float &x, float &y, float &z)
+{
+    if (j == nc) { x = y = z = 0.f; return; }   // the absorber
+    const float *p = C.rel + 3 * (base + j);
+    x = p[0]; y = p[1]; z = p[2];
+}
+
+// One warp per partial path; lanes walk the intermediates.  WRITE = false: count[p] children; true: write them at
+// child_off[p] in intermediate order.
+template <bool WRITE>
+__global__ void k_extend(int64_t P, int m, const int32_t *__restrict__ seq, const float *__restrict__ len,
+                         const int32_t *__restrict__ slot, Cands C, float two_r, int32_t *__restrict__ count,
+                         const int64_t *__restrict__ child_off, int32_t *__restrict__ cseq, float *__restrict__ clen,
+                         int32_t *__restrict__ cslot)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwg = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t p = wg; p < P; p += nwg) {
+        const int a = slot[p];
+        const int64_t base = C.off[a];
+        const int nc = (int)(C.off[a + 1] - base);
+        const int last = seq[p * m + m - 1];
+        float lx, ly, lz;
+        cand_xyz(C, base, nc, last, lx, ly, lz);
+        const float l0 = len[p];
+        int64_t o = WRITE ? child_off[p] : 0;
+        int cnt = 0;
+        for (int j0 = 0; j0 <= nc; j0 += 32) {
+            const int j = j0 + lane;
+            bool ok = false;
+            float tot = 0.f;
+            if (j <= nc && j != last) {
+                float x, y, z;
+                cand_xyz(C, base, nc, j, x, y, z);
+                tot = __fadd_rn(l0, len3(__fsub_rn(lx, x), __fsub_rn(ly, y), __fsub_rn(lz, z)));
+                ok = __fadd_rn(tot, len3(x, y, z)) <= two_r;
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, ok);
+            if (WRITE && ok) {
+                const int64_t c = o + __popc(mask & ((1u << lane) - 1u));
+                for (int q = 0; q < m; ++q) cseq[c * (m + 1) + q] = seq[p * m + q];
+                cseq[c * (m + 1) + m] = j;
+                clen[c] = tot;
+                cslot[c] = a;
+            }
+            o += __popc(mask);
+            cnt += __popc(mask);
+        }
+        if (!WRITE && lane == 0) count[p] = cnt;
+    }
+}
+
+// Paths among the sequences: last atom a candidate, not after its reverse; deg 1 for a palindrome, else 2.
+__global__ void k_terminal(int64_t Cn, int m, const int32_t *__restrict__ seq, const int32_t *__restrict__ slot,
+                           const int64_t *__restrict__ off, uint8_t *__restrict__ keep, float *__restrict__ deg)
+{
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < Cn; c += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t *s = seq + c * m;
+        const int nc = (int)(off[slot[c] + 1] - off[slot[c]]);
+        bool k = s[m - 1] != nc;
+        int cmp = 0;
+        for (int i = 0; i < m && cmp == 0; ++i) cmp = s[i] < s[m - 1 - i] ? -1 : (s[i] > s[m - 1 - i] ? 1 : 0);
+        keep[c] = (k && cmp <= 0) ? 1 : 0;
+        deg[c] = cmp == 0 ? 1.f : 2.f;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ description
+// One thread per path: coordinates (absorber at the origin), potentials, atom indices, closed length, the plane-wave
+// importance (pathfinder.py:75-100) and, for nleg > 2, the degeneracy key (pathfinder.py:134-157).
+__device__ __forceinline__ int indbet(float c)
+{
+    const float a = fabsf(c);
+    float n = floorf(__fdiv_rn(a, 0.025f));
+    if (__fsub_rn(a, __fmul_rn(n, 0.025f)) > 0.0125f) n = __fadd_rn(n, 1.f);
+    if (c < 0.f) n = -n;
+    int i = (int)n + kNBeta;
+    return i < 0 ? 0 : (i > 2 * kNBeta ? 2 * kNBeta : i);
+}
+
+__global__ void k_describe(int64_t B, int nleg, const int32_t *__restrict__ seq, const int32_t *__restrict__ slot,
+                           Cands C, const int64_t *__restrict__ cand_atom, const int64_t *__restrict__ ipot_of,
+                           const int64_t *__restrict__ absorbers, fg_pf_tables T, float *__restrict__ coords,
+                           int64_t *__restrict__ ipots, int64_t *__restrict__ atoms, float *__restrict__ rtot_out,
+                           float *__restrict__ xport, int64_t *__restrict__ key)
+{
+    const int m = nleg - 1;
+    for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < B; b += (int64_t)gridDim.x * blockDim.x) {
+        const int a = slot[b];
+        const int64_t base = C.off[a];
+        const int nc = (int)(C.off[a + 1] - base);
+        float px[kMaxLeg + 1], py[kMaxLeg + 1], pz[kMaxLeg + 1];
+        int ip[kMaxLeg + 1];
+        px[0] = py[0] = pz[0] = 0.f;
+        ip[0] = 0;
+        coords[b * nleg * 3 + 0] = coords[b * nleg * 3 + 1] = coords[b * nleg * 3 + 2] = 0.f;
+        ipots[b * nleg] = 0;
+        for (int q = 0; q < m; ++q) {
+            const int j = seq[b * m + q];
+            cand_xyz(C, base, nc, j, px[q + 1], py[q + 1], pz[q + 1]);
+            const int64_t atom = j == nc ? absorbers[a] : cand_atom[base + j];
+            ip[q + 1] = j == nc ? 0 : (int)ipot_of[atom];
+            atoms[b * m + q] = atom;
+            ipots[b * nleg + q + 1] = ip[q + 1];
+            coords[(b * nleg + q + 1) * 3 + 0] = px[q + 1];
+            coords[(b * nleg + q + 1) * 3 + 1] = py[q + 1];
+            coords[(b * nleg + q + 1) * 3 + 2] = pz[q + 1];
+        }
+        // legs j = 0..nleg-1: atom j -> atom j+1 (atom nleg = the absorber)
+        float ri[kMaxLeg], ux[kMaxLeg], uy[kMaxLeg], uz[kMaxLeg];
+        float rt = 0.f;
+        for (int j = 0; j < nleg; ++j) {
+            const int k = j + 1 < nleg ? j + 1 : 0;
+            const float dx = __fsub_rn(px[k], px[j]), dy = __fsub_rn(py[k], py[j]), dz = __fsub_rn(pz[k], pz[j]);
+            ri[j] = len3(dx, dy, dz);
+            rt = __fadd_rn(rt, ri[j]);
+            const float r = fmaxf(ri[j], 1e-12f);
+            ux[j] = __fdiv_rn(dx, r); uy[j] = __fdiv_rn(dy, r); uz[j] = __fdiv_rn(dz, r);
+        }
+        rtot_out[b] = rt;
+        // cos(beta) at atom j+1 between leg j and leg j+1 (j = nleg - 1: at the absorber, last leg -> first leg)
+        float cb[kMaxLeg];
+        for (int j = 0; j < nleg; ++j) {
+            const int k = j + 1 < nleg ? j + 1 : 0;
+            cb[j] = __fadd_rn(__fadd_rn(__fmul_rn(ux[j], ux[k]), __fmul_rn(uy[j], uy[k])), __fmul_rn(uz[j], uz[k]));
+        }
+        if (xport) {
+            int ib[kMaxLeg];
+            for (int j = 0; j < m; ++j) ib[j] = indbet(cb[j]);
+            const float cabs = fmaxf(fabsf(cb[nleg - 1]), 0.3f);
+            float s = 0.f;
+            for (int e = T.ik0; e < T.E; ++e) {
+                const float k = T.cksp[e];
+                float crit = __fdiv_rn(cabs, __fmul_rn(ri[nleg - 1], k));
+                for (int j = 0; j < m; ++j) {
+                    const float f = T.fbeta[((int64_t)e * T.nph1 + ip[j + 1]) * (2 * kNBeta + 1) + ib[j]];
+                    crit = __fdiv_rn(__fmul_rn(crit, f), __fmul_rn(ri[j], k));
+                }
+                crit = __fmul_rn(crit, expf(-__fdiv_rn(rt, T.xlam[e])));
+                s = __fadd_rn(s, __fmul_rn(fabsf(crit), T.trap[e - T.ik0]));
+            }
+            xport[b] = s;
+        }
+        if (key && nleg > 2) {
+            // forward key (ri..., cos...) and its reverse (ri reversed, cos of the scatterers reversed, the absorber's
+            // cos last), each rounded to 1e-3; the lexicographically smaller one
+            int64_t kf[2 * kMaxLeg], kr[2 * kMaxLeg];
+            for (int j = 0; j < nleg; ++j) {
+                kf[j] = (int64_t)rintf(__fmul_rn(ri[j], 1000.f));
+                kf[nleg + j] = (int64_t)rintf(__fmul_rn(cb[j], 1000.f));
+                kr[j] = (int64_t)rintf(__fmul_rn(ri[nleg - 1 - j], 1000.f));
+            }
+            for (int j = 0; j < nleg - 1; ++j) kr[nleg + j] = (int64_t)rintf(__fmul_rn(cb[nleg - 2 - j], 1000.f));
+            kr[2 * nleg - 1] = kf[2 * nleg - 1];
+            int cmp = 0;
+            for (int j = 0; j < 2 * nleg && cmp == 0; ++j) cmp = kr[j] < kf[j] ? -1 : (kr[j] > kf[j] ? 1 : 0);
+            for (int j = 0; j < 2 * nleg; ++j) key[b * 2 * nleg + j] = cmp < 0 ? kr[j] : kf[j];
+        }
+    }
+}
+
+int grid_of(int64_t work, int per_block)
+{
+    const int64_t g = (work + per_block - 1) / per_block;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
+}
+
+}  // namespace
+}  // namespace fg
+
+using namespace fg;
+
+extern "C" fg_status fg_pf_candidates(const float *pos, int64_t n, float box, const int64_t *absorbers, int32_t A,
+                                      float rmax, int32_t *count, const int64_t *offset, int64_t *cand_atom,
+                                      float *cand_rel, void *stream)
+{
+    if (n < 0 || A < 0) return fail(FG_ERR_VALUE, "negative size");
+    if (A == 0) return FG_OK;
+    if (!pos || !absorbers) return fail(FG_ERR_VALUE, "null argument");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!offset) {
+        if (!count) return fail(FG_ERR_VALUE, "null count");
+        k_candidates<false><<<A, 256, 0, st>>>(pos, n, box, absorbers, rmax, count, nullptr, nullptr, nullptr);
+    } else {
+        if (!cand_atom || !cand_rel) return fail(FG_ERR_VALUE, "null output");
+        k_candidates<true><<<A, 256, 0, st>>>(pos, n, box, absorbers, rmax, nullptr, offset, cand_atom, cand_rel);
+    }
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+extern "C" fg_status fg_pf_extend(int64_t P, int32_t m, const int32_t *seq, const float *len, const int32_t *slot,
+                                  const int64_t *cand_off, const float *cand_rel, float two_r, int32_t *count,
+                                  const int64_t *child_off, int32_t *child_seq, float *child_len, int32_t *child_slot,
+                                  void *stream)
+{
+    if (P < 0 || m < 1 || m + 1 > kMaxLeg - 1) return fail(FG_ERR_VALUE, "bad partial-path shape");
+    if (P == 0) return FG_OK;
+    if (!seq || !len || !slot || !cand_off || !cand_rel) return fail(FG_ERR_VALUE, "null argument");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const Cands C{cand_off, cand_rel};
+    const int blocks = grid_of(P * 32, 256);
+    if (!child_off) {
+        if (!count) return fail(FG_ERR_VALUE, "null count");
+        k_extend<false><<<blocks, 256, 0, st>>>(P, m, seq, len, slot, C, two_r, count, nullptr, nullptr, nullptr,
+                                                nullptr);
+    } else {
+        if (!child_seq || !child_len || !child_slot) return fail(FG_ERR_VALUE, "null output");
+        k_extend<true><<<blocks, 256, 0, st>>>(P, m, seq, len, slot, C, two_r, nullptr, child_off, child_seq, child_len,
+                                               child_slot);
+    }
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+extern "C" fg_status fg_pf_terminal(int64_t C, int32_t m, const int32_t *seq, const int32_t *slot,
+                                    const int64_t *cand_off, uint8_t *keep, float *deg, void *stream)
+{
+    if (C < 0 || m < 1) return fail(FG_ERR_VALUE, "bad shape");
+    if (C == 0) return FG_OK;
+    if (!seq || !slot || !cand_off || !keep || !deg) return fail(FG_ERR_VALUE, "null argument");
+    k_terminal<<<grid_of(C, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(C, m, seq, slot, cand_off, keep, deg);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+extern "C" fg_status fg_pf_describe(int64_t B, int32_t nleg, const int32_t *seq, const int32_t *slot,
+                                    const int64_t *cand_off, const float *cand_rel, const int64_t *cand_atom,
+                                    const int64_t *ipot_of, const int64_t *absorbers, const fg_pf_tables *T,
+                                    float *coords, int64_t *ipots, int64_t *atoms, float *rtot, float *xport,
+                                    int64_t *key, void *stream)
+{
+    if (B < 0 || nleg < 2 || nleg > kMaxLeg) return fail(FG_ERR_VALUE, "bad path shape");
+    if (B == 0) return FG_OK;
+    if (!seq || !slot || !cand_off || !cand_rel || !cand_atom || !ipot_of || !absorbers || !coords || !ipots ||
+        !atoms || !rtot || (xport && !T))
+        return fail(FG_ERR_VALUE, "null argument");
+    fg_pf_tables t{};
+    if (T) {
+        t = *T;
+        if (t.E < 1 || t.nph1 < 1 || t.ik0 < 0 || t.ik0 >= t.E || !t.fbeta || !t.cksp || !t.xlam || !t.trap)
+            return fail(FG_ERR_VALUE, "incomplete importance tables");
+    }
+    k_describe<<<grid_of(B, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        B, nleg, seq, slot, Cands{cand_off, cand_rel}, cand_atom, ipot_of, absorbers, t, coords, ipots, atoms, rtot,
+        xport, key);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+extern "C" fg_status fg_pf_windows(const float *sorted_len, const int64_t *seg_off, int64_t nseg, float eps,
+                                   int64_t *window)
+{
+    if (nseg < 0 || !seg_off || (nseg > 0 && (!sorted_len || !window))) return fail(FG_ERR_VALUE, "null argument");
+    // greedy windows of width eps over each segment's ascending lengths (pathfinder.py:110-119)
+    for (int64_t s = 0; s < nseg; ++s) {
+        const int64_t lo = seg_off[s], hi = seg_off[s + 1];
+        int64_t i = lo, w = 0;
+        while (i < hi) {
+            const float edge = sorted_len[i] + eps;
+            const int64_t j = std::max<int64_t>(std::lower_bound(sorted_len + i, sorted_len + hi, edge) - sorted_len,
+                                                i + 1);
+            for (int64_t q = i; q < j; ++q) window[q] = w;
+            ++w;
+            i = j;
+        }
+    }
+    return FG_OK;
+}

@@ -187,6 +187,56 @@ FG_API fg_status fg_fp32_fma_peak(double *tflops, void *stream);
 FG_API fg_status fg_set_launch(int32_t fwd_warps, int32_t bwd_warps);
 FG_API fg_status fg_stage_set_launch(fg_stage *stage, int32_t fwd_warps, int32_t bwd_warps);
 
+/* ---------------------------------------------------------------------------------------------- path finder
+ * The enumeration of the reference's GPUPathFinder.enumerate (src/feffgpu/pathfinder.py:213-271; its _longer_paths,
+ * :159-211, for five and more legs), batched over absorber slots; the host driver (feffgpu_b200/pathfinder.py)
+ * strings the calls together and does the merges and the importance cut (pathfinder.py:102-157, 271-279).
+ * Positions are FP32 Angstrom, as in the reference.  A path's atoms are stored as candidate-local indices of its
+ * absorber slot (0..nc-1, nc = that slot's candidate count = the absorber itself). */
+
+/* |f(beta)|, momentum and mean-free-path tables of the importance (pathfinder.py:43-65), device arrays. */
+typedef struct fg_pf_tables {
+    int32_t E;               /* energies of the tables (ne1) */
+    int32_t nph1;            /* potentials */
+    int32_t ik0;             /* first energy of the importance integral (0-based) */
+    const float *fbeta;      /* (E, nph1, 81) |f(beta)| on cos(beta) = -1, -0.975, ..., 1 */
+    const float *cksp;       /* (E) Re p, 1/A */
+    const float *xlam;       /* (E) mean free path, A */
+    const float *trap;       /* (E - ik0) trapezoid weights */
+} fg_pf_tables;
+
+/* Candidates (atoms within rmax of each absorber, minimum image in a cubic box of length box, box <= 0: a cluster,
+ * the absorber excluded), in atom order.  offset == NULL: count (A) = candidates per slot.  Else offset (A + 1) is
+ * the exclusive scan of count and cand_atom (total), cand_rel (total, 3) are written.  pathfinder.py:219-224. */
+FG_API fg_status fg_pf_candidates(const float *pos, int64_t n, float box, const int64_t *absorbers, int32_t A,
+                                  float rmax, int32_t *count, const int64_t *offset, int64_t *cand_atom,
+                                  float *cand_rel, void *stream);
+/* One level of growth: P partial paths of m atoms (seq (P, m), closed-so-far lengths len (P), slots (P)) get every
+ * intermediate other than their last atom whose closed length fits two_r.  child_off == NULL: count (P) children
+ * per partial path.  Else child_off (P) is the exclusive scan of count and the children (seq (C, m + 1), len, slot)
+ * are written in parent order and intermediate order.  pathfinder.py:180-196. */
+FG_API fg_status fg_pf_extend(int64_t P, int32_t m, const int32_t *seq, const float *len, const int32_t *slot,
+                              const int64_t *cand_off, const float *cand_rel, float two_r, int32_t *count,
+                              const int64_t *child_off, int32_t *child_seq, float *child_len, int32_t *child_slot,
+                              void *stream);
+/* keep (C) = 1 for the paths among C sequences of m atoms (last atom a candidate, not after its reverse), deg (C) =
+ * 1 for a palindrome, else 2.  pathfinder.py:199-211. */
+FG_API fg_status fg_pf_terminal(int64_t C, int32_t m, const int32_t *seq, const int32_t *slot, const int64_t *cand_off,
+                                uint8_t *keep, float *deg, void *stream);
+/* Per path of nleg legs (seq (B, nleg - 1)): coords (B, nleg, 3) relative to the absorber, ipots (B, nleg) (the
+ * absorber 0, else ipot_of[atom]), atoms (B, nleg - 1) atom indices, closed length rtot (B); with T, the importance
+ * xport (B) (pathfinder.py:75-100); with key and nleg > 2, the degeneracy key (B, 2 nleg): leg lengths and
+ * cos(beta) rounded to 1e-3 in the lexicographically smaller direction (pathfinder.py:134-157). */
+FG_API fg_status fg_pf_describe(int64_t B, int32_t nleg, const int32_t *seq, const int32_t *slot,
+                                const int64_t *cand_off, const float *cand_rel, const int64_t *cand_atom,
+                                const int64_t *ipot_of, const int64_t *absorbers, const fg_pf_tables *T,
+                                float *coords, int64_t *ipots, int64_t *atoms, float *rtot, float *xport,
+                                int64_t *key, void *stream);
+/* Host: greedy windows of width eps over each segment [seg_off[s], seg_off[s+1]) of ascending lengths (the window
+ * of FEFF's accidental-degeneracy merge, pathfinder.py:110-119); window ids restart at 0 per segment. */
+FG_API fg_status fg_pf_windows(const float *sorted_len, const int64_t *seg_off, int64_t nseg, float eps,
+                               int64_t *window);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,6 +22,10 @@ The reference is imported read-only from its source tree and run on the CPU in F
   k = 0..20 A^-1 step 0.05.
 * cfg4_fe_phase.npz, cfg5_nik_phase.npz, cfg5_ok_phase.npz -- bcc Fe (K edge) and rock-salt NiO (Ni K and O K
   edges) phase tables of 6 A clusters through the reference chain, for the MD-batch and two-edge refinement cases.
+* finder_cu.npz, finder_pack.npz, finder_bcc.npz -- the reference's path finder on the Cu cluster (rmax 6, 4 legs),
+  a 400-atom periodic Fe/O/Pt packing (rmax 6.5, 7 legs) and a thermal bcc Fe frame (rmax 5.5, 3 legs), each without
+  and with an importance cut; finder_feopt.npz -- the reference finder's paths on the benchmark packing (counts,
+  hashes and ends of the atom sequences per leg count, two absorbers, rmax 8 A, 8 legs).
 * cfg2_phase.npz -- Fe K-edge phase tables (potentials Fe*, Fe, O, Pt, lmax 24) of a cluster cut from the seeded
   3000-atom Fe/O/Pt packing, on FEFF's own energy grid; cfg2_sample.npz -- the reference stage's cchi on those
   tables resampled to 401 k points, for a sample of synthetic paths.
@@ -324,12 +328,86 @@ def make_cfg45():
     _cluster_phase("cfg5_ok_phase", pts, lab, o, "K", [(0, 8, "O"), (1, 28, "Ni"), (2, 8, "O")])
 
 
+FINDER_CASES = {
+    # name: (structure, phase fixture, absorber species, rmax, nlegmax, critpw list)
+    "cu": ("fcc", "cfg1_cu", None, 6.0, 4, (0.0, 2.5)),
+    "pack": ("pack", "cfg2_phase", "Fe", 6.5, 7, (0.0, 1.0)),
+    "bcc": ("bcc", "cfg4_fe_phase", None, 5.5, 3, (0.0, 2.0)),
+}
+
+
+def finder_structure(kind):
+    """Positions (n, 3) A, cubic box or None, absorber index, potential index per atom of a finder fixture."""
+    if kind == "fcc":
+        pts = W.fcc_cluster(3.61, 6.0)
+        return pts, None, 0, np.ones(len(pts), int)
+    if kind == "pack":
+        pos, lab, box = W.random_packing(400, 0.08, 1.8, seed=77)
+        ab = int(W.central_atom(pos, box, lab, "Fe", 1)[0])
+        return pos, box, ab, np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
+    base, box = W.bcc_supercell(6, 2.87)
+    pos = W.thermal(base, 0.08, seed=3)
+    return pos, box, int(W.central_atom(pos, box, None, None, 1)[0]), np.ones(len(pos), int)
+
+
+def make_finder():
+    """finder_<name>.npz -- the reference's GPUPathFinder (src/feffgpu/pathfinder.py) run on the CPU: the structure,
+    parameters, and per importance cut the kept paths' atoms, degeneracies and importances, and the reference
+    importance.  The phase tables are those of the named fixture."""
+    from feffgpu.pathfinder import GPUPathFinder
+    for name, (kind, phase_name, _sp, rmax, nlegmax, crits) in FINDER_CASES.items():
+        P = phase_from_npz(np.load(HERE / f"{phase_name}.npz"), prefix="ph_")
+        pos, box, ab, ipot = finder_structure(kind)
+        out = {"pos": pos, "box": np.asarray(-1.0 if box is None else box), "absorber": np.asarray(ab),
+               "ipot": ipot, "rmax": np.asarray(rmax), "nlegmax": np.asarray(nlegmax), "crit": np.asarray(crits)}
+        t = time.time()
+        for ci, crit in enumerate(crits):
+            f = GPUPathFinder(P, device="cpu", rmax=rmax, nlegmax=nlegmax, critpw=crit)
+            kept, ref = f.enumerate(pos, box, ab, ipot)
+            out[f"ref_{ci}"] = np.asarray(ref)
+            for nleg, (coords, ipots, deg, xp, atoms) in kept.items():
+                out[f"atoms_{ci}_{nleg}"] = atoms.cpu().numpy()
+                out[f"deg_{ci}_{nleg}"] = deg.cpu().numpy()
+                out[f"xport_{ci}_{nleg}"] = xp.cpu().numpy()
+            print(f"finder_{name} critpw {crit}: " + str({k: int(v[0].shape[0]) for k, v in kept.items()}))
+        np.savez_compressed(HERE / f"finder_{name}.npz", **out)
+        print(f"finder_{name}: {time.time() - t:.1f} s")
+
+
+def make_finder_feopt():
+    """finder_feopt.npz -- the reference's path finder on the benchmark structure (the seeded 3000-atom Fe/O/Pt
+    packing of feffgpu_b200.workloads, its two most central Fe absorbers, rmax 8 A, 8 legs, no importance cut): per
+    absorber and leg count the number of paths, the SHA-256 of the atom sequences (int64, in the finder's order),
+    the degeneracy sum and the first and last 16 sequences."""
+    import hashlib
+    from feffgpu.pathfinder import GPUPathFinder
+    P = phase_from_npz(np.load(HERE / "cfg2_phase.npz"), prefix="ph_")
+    pos, lab, box = W.random_packing(3000, 0.08, 1.8, seed=2024)
+    ipot = np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
+    abs2 = W.central_atom(pos, box, lab, "Fe", 2)
+    out = {"absorbers": np.asarray(abs2)}
+    t = time.time()
+    f = GPUPathFinder(P, device="cpu", rmax=8.0, nlegmax=8, critpw=0.0)
+    for s, ab in enumerate(abs2):
+        kept, ref = f.enumerate(pos, box, int(ab), ipot)
+        out[f"ref_{s}"] = np.asarray(ref)
+        for nleg, (coords, ipots, deg, xp, atoms) in kept.items():
+            a = np.ascontiguousarray(atoms.cpu().numpy().astype(np.int64))
+            out[f"count_{s}_{nleg}"] = np.asarray(len(a))
+            out[f"sha_{s}_{nleg}"] = np.frombuffer(hashlib.sha256(a.tobytes()).digest(), np.uint8)
+            out[f"degsum_{s}_{nleg}"] = np.asarray(float(deg.sum()))
+            out[f"head_{s}_{nleg}"], out[f"tail_{s}_{nleg}"] = a[:16], a[-16:]
+        print(f"finder_feopt absorber {int(ab)}: " + str({n: int(v[0].shape[0]) for n, v in kept.items()}))
+    np.savez_compressed(HERE / "finder_feopt.npz", **out)
+    print(f"finder_feopt: {time.time() - t:.1f} s")
+
+
 def main():
     import tempfile
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
-    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45"])
+    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder"])
     with tempfile.TemporaryDirectory() as tmp:
         if "cases" in want:
             import shutil
@@ -348,6 +426,9 @@ def main():
             make_cfg2(tmp)
         if "cfg45" in want:
             make_cfg45()
+        if "finder" in want:
+            make_finder()
+            make_finder_feopt()
 
 
 if __name__ == "__main__":

@@ -1,0 +1,107 @@
+"""The CUDA path finder against the reference's finder (golden fixtures) and the oracle (B200).
+
+* finder_{cu,pack,bcc}: the same kept paths in the same order (atom sequences), the same degeneracies, importances
+  within 2e-5 relative (FP32 sums in another order), the same reference importance;
+* batched absorbers equal one call per absorber;
+* the benchmark's 3000-atom Fe/O/Pt packing (two absorbers, rmax 8 A, 8 legs, no importance cut, 1.9e5 paths) gives
+  the reference finder's paths exactly;
+* importance(pts, ipots) and degenerate_total against the oracle.
+"""
+import numpy as np
+import pytest
+import torch
+
+from feffgpu_b200 import workloads as W
+from oracle import pathfinder as OF
+from tests.fixtures import npz, phase
+from tests.test_oracle_pathfinder import CASES, finder_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _finder(name, crit):
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    z, box = finder_case(name)
+    return GPUPathFinder(phase(CASES[name]), device="cuda", rmax=float(z["rmax"]), nlegmax=int(z["nlegmax"]),
+                         critpw=float(crit)), z, box
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_finder_equals_reference(name):
+    z, _ = finder_case(name)
+    for ci, crit in enumerate(z["crit"]):
+        f, z, box = _finder(name, crit)
+        kept, ref = f.enumerate(z["pos"], box, int(z["absorber"]), z["ipot"])
+        assert abs(ref - float(z[f"ref_{ci}"])) <= 2e-5 * abs(float(z[f"ref_{ci}"]))
+        legs = sorted(int(k.split("_")[2]) for k in z if k.startswith(f"atoms_{ci}_"))
+        got = {n: v for n, v in kept.items() if v[0].shape[0] > 0}
+        assert set(got) == {n for n in legs if len(z[f"atoms_{ci}_{n}"])}, (name, crit, set(got))
+        for nleg in legs:
+            ra = z[f"atoms_{ci}_{nleg}"]
+            if len(ra) == 0:
+                continue
+            coords, ip, deg, xp, atoms = (t.cpu().numpy() for t in kept[nleg])
+            assert np.array_equal(atoms, ra), (name, crit, nleg, atoms.shape, ra.shape)
+            assert np.array_equal(deg, z[f"deg_{ci}_{nleg}"])
+            assert np.allclose(xp, z[f"xport_{ci}_{nleg}"], rtol=2e-5, atol=0)
+            assert coords.shape == (len(ra), nleg, 3) and np.all(coords[:, 0] == 0)
+            print(f"finder_{name} critpw {crit} nleg {nleg}: {len(ra)} paths equal")
+
+
+def test_batched_absorbers_equal_single_calls():
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    z, box = finder_case("pack")
+    pos, ipot = z["pos"], z["ipot"]
+    abs_ = [int(a) for a in np.nonzero(ipot == 1)[0][:6]]
+    f = GPUPathFinder(phase("cfg2_phase"), device="cuda", rmax=5.5, nlegmax=5, critpw=0.5)
+    many = f.enumerate_many(pos, box, abs_, ipot)
+    for s, a in enumerate(abs_):
+        kept, ref = f.enumerate(pos, box, a, ipot)
+        assert abs(float(many["ref"][s]) - ref) <= 1e-7 * abs(ref)
+        for nleg, v in kept.items():
+            sel = many["paths"][nleg][5] == s
+            for x, y in zip(v, many["paths"][nleg][:5]):
+                assert torch.equal(x, y[sel]), (a, nleg)
+
+
+def test_feopt_paths_equal_reference():
+    """The benchmark packing (3000 atoms, two most central Fe absorbers, rmax 8 A, 8 legs, no importance cut) in one
+    batched call: per absorber and leg count the reference finder's count, atom sequences (SHA-256, first and last
+    16), degeneracy sum (tests/golden/finder_feopt.npz)."""
+    import hashlib
+    from feffgpu_b200.pad import phase_from_npz
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    z = npz("finder_feopt")
+    pos, lab, box = W.random_packing(3000, 0.08, 1.8, seed=2024)
+    ipot = np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
+    f = GPUPathFinder(phase_from_npz(npz("cfg2_phase"), prefix="ph_"), device="cuda", rmax=8.0, nlegmax=8, critpw=0.0)
+    res = f.enumerate_many(pos, box, z["absorbers"], ipot)
+    for s in range(len(z["absorbers"])):
+        assert abs(float(res["ref"][s]) - float(z[f"ref_{s}"])) <= 2e-5 * abs(float(z[f"ref_{s}"]))
+        counts = {}
+        for nleg, v in res["paths"].items():
+            sel = (v[5] == s).cpu().numpy()
+            atoms = np.ascontiguousarray(v[4].cpu().numpy()[sel].astype(np.int64))
+            counts[nleg] = len(atoms)
+            assert len(atoms) == int(z[f"count_{s}_{nleg}"])
+            assert hashlib.sha256(atoms.tobytes()).digest() == bytes(z[f"sha_{s}_{nleg}"])
+            assert np.array_equal(atoms[:16], z[f"head_{s}_{nleg}"]) and np.array_equal(atoms[-16:], z[f"tail_{s}_{nleg}"])
+            assert float(v[2].cpu().numpy()[sel].sum()) == float(z[f"degsum_{s}_{nleg}"])
+        print(f"feopt absorber {int(z['absorbers'][s])}: {counts} equal to the reference finder")
+
+
+def test_importance_and_degeneracy_against_oracle():
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    P = phase("cfg1_cu")
+    f = GPUPathFinder(P, device="cuda", rmax=6.0, nlegmax=4, critpw=0.0)
+    o = OF.Finder(P, rmax=6.0, nlegmax=4, critpw=0.0)
+    z = npz("cfg1_cu")
+    for nleg in (2, 3, 4):
+        c, ip = z[f"coords_{nleg}"].astype(np.float32), z[f"ipots_{nleg}"]
+        a = f.importance(torch.tensor(c), torch.tensor(ip)).cpu().numpy()
+        b = o.importance(c, ip)
+        assert np.allclose(a, b, rtol=2e-5, atol=0)
+        if nleg > 2:
+            deg = np.full(len(c), 2.0, np.float32)
+            dt = GPUPathFinder.degenerate_total(torch.tensor(c), torch.tensor(deg)).numpy()
+            assert np.array_equal(dt, OF.Finder.degenerate_total(c, deg))
