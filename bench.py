@@ -1,8 +1,9 @@
 """bench.py -- throughput of the batched path stage on B200 in path·k-points/s.
 
 Workload (one GPU): the Fe K-edge stage of a seeded random packing of 3000 atoms (Fe/O/Pt, minimum separation
-1.8 A, 0.08 atoms/A^3), the two most central Fe absorbers, paths of 2-8 legs to 8 A with the reference path
-finder's leg-count histogram for that structure (2.02e5 paths, drawn synthetically), phase tables lmax 24 of the
+1.8 A, 0.08 atoms/A^3), the two most central Fe absorbers, every path of 2-8 legs within 8 A that the path finder
+returns (no importance cut; 1.89e5 paths, found by this package's CUDA path finder, identical to the reference
+finder's on this structure), degeneracies included, phase tables lmax 24 of the
 reference's own phase-shift stage resampled to 401 k points (0-20 1/A), output chi(k) on the same 401 points.
 One step = the whole stage over that batch: geometry, rotation matrices, scattering-matrix chain, termination,
 cfac, fine-grid signal and the deterministic degeneracy-weighted sum into the two absorbers' rows, in the
@@ -11,7 +12,7 @@ own two absorbers (weak scaling, no collective on the data path).
 
 Beside the headline line's value: the end-to-end form (host buffers, copies timed), forward+backward, the plain FP64
 form, the MD-EXAFS batch (bcc Fe, 500 frames x 32 absorbers in one launch) and the RMC refinement (NiO, two edges,
-each step one CUDA graph replay), each in its own key of the JSON line.
+each step one CUDA graph replay) and the path finder itself, each in its own key of the JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -41,21 +42,81 @@ UNIT = "path·k/s"
 
 
 # ------------------------------------------------------------------------------------------------ workload
-def workload(rank: int, world: int, scale: float = 1.0):
+def packing():
+    from feffgpu_b200 import workloads as W
+    pos, lab, box = W.random_packing(3000, 0.08, 1.8, seed=2024)
+    ipot_of = np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
+    return pos, lab, box, ipot_of
+
+
+def workload(rank: int, world: int, scale: float = 1.0, finder: str = "gpu"):
+    """Phase tables (resampled to 401 k) and the path groups of this rank's two absorbers: every path of 2-8 legs
+    within 8 A that the path finder returns (no importance cut), degeneracies included, row = absorber.  finder
+    "gpu": this package's CUDA path finder (the paths are the reference finder's, bit for bit); "oracle": the CPU
+    restatement (the reference arm, which runs nothing of this package).  scale < 1 keeps every k-th path per leg
+    count (profiling runs)."""
     from feffgpu_b200 import workloads as W
     from feffgpu_b200.pad import phase_from_npz, resample_phase
     z = np.load(ROOT / "tests" / "golden" / "cfg2_phase.npz")
-    P = resample_phase(phase_from_npz(z, prefix="ph_"), Q)
-    pos, lab, box = W.random_packing(3000, 0.08, 1.8, seed=2024)
+    P0 = phase_from_npz(z, prefix="ph_")
+    P = resample_phase(P0, Q)
+    pos, lab, box, ipot_of = packing()
     absorbers = W.central_atom(pos, box, lab, "Fe", 2 * world)[2 * rank:2 * rank + 2]
-    ipot_of = np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
     groups = []
     for i, ab in enumerate(absorbers):
-        counts = {n: max(1, int(round(c * scale))) for n, c in W.FEOPT_LEG_COUNTS.items()}
-        paths = W.random_paths(pos, box, int(ab), counts, rmax=8.0, seed=1000 + int(ab), ipot_of=ipot_of)
-        for nleg, (c, ip, _atoms) in paths.items():
-            groups.append((c, ip, None, np.full(len(c), i)))
+        if finder == "gpu":
+            from feffgpu_b200.pathfinder import GPUPathFinder
+            kept, _ = GPUPathFinder(P0, device="cuda", rmax=8.0, nlegmax=8, critpw=0.0).enumerate(pos, box, int(ab),
+                                                                                                  ipot_of)
+            kept = {n: tuple(t.cpu().numpy() for t in v) for n, v in kept.items()}
+        else:
+            from oracle.pathfinder import Finder
+            kept, _ = Finder(P0, rmax=8.0, nlegmax=8, critpw=0.0).enumerate(pos, box, int(ab), ipot_of)
+        for nleg, (coords, ip, deg, _xp, _atoms) in sorted(kept.items()):
+            if len(coords) == 0:
+                continue
+            step = max(1, int(round(1.0 / scale)))
+            sel = np.arange(0, len(coords), step)
+            groups.append((coords[sel].astype(np.float64), ip[sel], deg[sel].astype(np.float64), np.full(len(sel), i)))
     return P, groups
+
+
+def finder_leg(args, dev, world, rank):
+    """The path finder itself: every path of 2-8 legs within 8 A of this rank's two absorbers (no importance cut),
+    both absorbers in one batched call, timed with CUDA events after one warm-up call."""
+    import torch
+    from feffgpu_b200 import workloads as W
+    from feffgpu_b200.pad import phase_from_npz
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    P0 = phase_from_npz(np.load(ROOT / "tests" / "golden" / "cfg2_phase.npz"), prefix="ph_")
+    pos, lab, box, ipot_of = packing()
+    absorbers = W.central_atom(pos, box, lab, "Fe", 2 * world)[2 * rank:2 * rank + 2]
+    f = GPUPathFinder(P0, device=dev, rmax=8.0, nlegmax=8, critpw=0.0)
+    res = f.enumerate_many(pos, box, absorbers, ipot_of)
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = f.enumerate_many(pos, box, absorbers, ipot_of)
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    n = sum(int(v[0].shape[0]) for v in res["paths"].values())
+    t = float(np.median(ms))
+    out = {"ms": t, "paths": n, "paths_per_s": n / (t * 1e-3), "absorbers": len(absorbers),
+           "legs": {int(k): int(v[0].shape[0]) for k, v in sorted(res["paths"].items())},
+           "note": "enumeration, geometry, importance, merges; identical paths to the reference finder"}
+    if rank == 0 and not args.no_cpu:
+        # the CPU restatement of the reference finder (numpy, one host thread) on the same absorbers
+        import time as _time
+        from oracle.pathfinder import Finder
+        t0 = _time.perf_counter()
+        fo = Finder(P0, rmax=8.0, nlegmax=8, critpw=0.0)
+        for a in absorbers:
+            fo.enumerate(pos, box, int(a), ipot_of)
+        out["cpu_oracle_ms"] = (_time.perf_counter() - t0) * 1e3
+    return out
 
 
 # ------------------------------------------------------------------------------------------------ clocks
@@ -309,7 +370,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        P, groups = workload(0, 1, args.paths_scale)
+        P, groups = workload(0, 1, args.paths_scale, finder="oracle")
         vals = []
         for i in range(args.warmup + args.steps):
             v, desc = cpu_sample(P, groups, budget_s=max(2.0, args.cpu_budget / 3), nthreads=nthreads)
@@ -321,7 +382,7 @@ def main():
             "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": n_paths * NK / v * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
-            "config": {"workload": f"Fe/O/Pt packing 3000 atoms, 2 Fe K absorbers, rmax 8 A, 2-8 legs, {n_paths} paths, "
+            "config": {"workload": f"Fe/O/Pt packing 3000 atoms, 2 Fe K absorbers, every path finder path of 2-8 legs to 8 A, {n_paths} paths, "
                                    f"lmax 24 x {NK} k", "impl": "FP64 C port of the reference's path stage (oracle)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
@@ -388,8 +449,9 @@ def main():
             ms, kern = timed(lambda: stage.chi_reduce(batch, Q, S), args.steps, args.warmup, kernel_time=True)
     value = world * n_paths * NK / (ms * 1e-3)
 
-    e2e = fwd_bwd = plain = md = rmc = None
+    e2e = fwd_bwd = plain = md = rmc = pf = None
     if not args.no_extras:
+        pf = finder_leg(args, dev, world, rank)
         e2e, fwd_bwd, plain = extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms)
         if args.md_frames > 0:
             md = md_extra(args, dev, timed, world, rank)
@@ -424,12 +486,12 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32 (complex chain) + fp64 (phase argument, sums)", "data": "synthetic",
-        "config": {"workload": f"Fe/O/Pt packing 3000 atoms, 2 Fe K absorbers per GPU, rmax 8 A, 2-8 legs, "
+        "config": {"workload": f"Fe/O/Pt packing 3000 atoms, 2 Fe K absorbers per GPU, every path finder path of 2-8 legs to 8 A, "
                                f"{n_paths} paths per GPU, lmax 24 x {NK} k, chi on {NK} k",
                    "paths_per_gpu": n_paths, "legs": batch.counts, "energies": stage.E, "nk": NK,
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"dp{world} (absorbers per rank)"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "fwd_bwd": fwd_bwd, "plain_fp64": plain,
-        "md_batch": md, "rmc_refinement": rmc,
+        "md_batch": md, "rmc_refinement": rmc, "path_finder": pf,
         "autotune": {"fwd_warps": stage._launch[0], "bwd_warps": stage._launch[1],
                      "timed": [{"kind": k, "warps": w_, "ms": round(t_, 3)} for sig, k, w_, t_ in tuner.log
                                if sig.split("|")[1] == "p0"]},

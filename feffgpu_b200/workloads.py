@@ -1,17 +1,16 @@
 """Seeded synthetic structures and path lists with the shapes of the stage's benchmark configurations.
 
-The reference's path finder (``src/feffgpu/pathfinder.py``) is not part of this package; where a benchmark needs a
-large path list, ``random_paths`` draws closed scattering paths over a structure's atoms with a prescribed number
-of paths per leg count, legs no longer than a cutoff and the half path length below ``rmax`` -- the input layout
-of ``GPUPathStage.cchi`` (coordinates relative to the absorber, absorber first; potential indices absorber 0).
+Path lists come from the path finder (``feffgpu_b200.pathfinder``) where a workload names one; ``random_paths``
+draws closed scattering paths over a structure's atoms with a prescribed number of paths per leg count, legs no
+longer than a cutoff and the half path length below ``rmax`` (test workloads of a chosen size), and
+``bcc_site_paths`` / ``md_batch`` enumerate the 2- and 3-leg paths of a bcc lattice for the MD batch -- all in the
+input layout of ``GPUPathStage.cchi`` (coordinates relative to the absorber, absorber first; potential indices
+absorber 0).
 """
 from __future__ import annotations
 
 import numpy as np
 
-# Leg-count histogram of one Fe absorber of the 3000-atom Fe/O/Pt packing (rmax 8 A, 2-8 legs, no importance cut),
-# as the reference's path finder returns it for seed 2024; two absorbers make the 2e5-path workload.
-FEOPT_LEG_COUNTS = {2: 165, 3: 2136, 4: 15727, 5: 38240, 6: 35172, 7: 9138, 8: 548}
 
 
 def random_packing(n=3000, density=0.08, dmin=1.8, species=("Fe", "O", "Pt"), seed=2024, fractions=None):
