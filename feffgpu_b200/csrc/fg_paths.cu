@@ -38,13 +38,15 @@ __device__ __forceinline__ float wrap1(float r, float b)
 // One block per absorber slot.  count: number of candidates; with out != null the candidates are written in atom
 // order at off[a] (ordered compaction: warp ballots, then the warps' counts in order).
 template <bool WRITE>
-__global__ void k_candidates(const float *__restrict__ pos, int64_t n, float box, const int64_t *__restrict__ absorbers,
-                             float rmax, int32_t *__restrict__ count, const int64_t *__restrict__ off,
+__global__ void k_candidates(const float *__restrict__ pos_all, int64_t n, float box,
+                             const int64_t *__restrict__ absorbers, int32_t per_frame, float rmax,
+                             int32_t *__restrict__ count, const int64_t *__restrict__ off,
                              int64_t *__restrict__ cand_atom, float *__restrict__ cand_rel)
 {
     __shared__ int warp_n[32];
     __shared__ int64_t base_s;
     const int a = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const float *pos = pos_all + (int64_t)(a / per_frame) * n * 3;   // the slot's frame
     const int64_t ab = absorbers[a];
     const float ax = pos[3 * ab], ay = pos[3 * ab + 1], az = pos[3 * ab + 2];
     if (threadIdx.x == 0) base_s = WRITE ? off[a] : 0;
@@ -260,19 +262,21 @@ int grid_of(int64_t work, int per_block)
 using namespace fg;
 
 extern "C" fg_status fg_pf_candidates(const float *pos, int64_t n, float box, const int64_t *absorbers, int32_t A,
-                                      float rmax, int32_t *count, const int64_t *offset, int64_t *cand_atom,
-                                      float *cand_rel, void *stream)
+                                      int32_t per_frame, float rmax, int32_t *count, const int64_t *offset,
+                                      int64_t *cand_atom, float *cand_rel, void *stream)
 {
-    if (n < 0 || A < 0) return fail(FG_ERR_VALUE, "negative size");
+    if (n < 0 || A < 0 || per_frame < 1) return fail(FG_ERR_VALUE, "negative size");
     if (A == 0) return FG_OK;
     if (!pos || !absorbers) return fail(FG_ERR_VALUE, "null argument");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (!offset) {
         if (!count) return fail(FG_ERR_VALUE, "null count");
-        k_candidates<false><<<A, 256, 0, st>>>(pos, n, box, absorbers, rmax, count, nullptr, nullptr, nullptr);
+        k_candidates<false><<<A, 256, 0, st>>>(pos, n, box, absorbers, per_frame, rmax, count, nullptr, nullptr,
+                                               nullptr);
     } else {
         if (!cand_atom || !cand_rel) return fail(FG_ERR_VALUE, "null output");
-        k_candidates<true><<<A, 256, 0, st>>>(pos, n, box, absorbers, rmax, nullptr, offset, cand_atom, cand_rel);
+        k_candidates<true><<<A, 256, 0, st>>>(pos, n, box, absorbers, per_frame, rmax, nullptr, offset, cand_atom,
+                                              cand_rel);
     }
     FG_CUDA(cudaGetLastError());
     return FG_OK;

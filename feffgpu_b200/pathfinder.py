@@ -151,32 +151,42 @@ class GPUPathFinder:
         return kept, float(res["ref"][0])
 
     def enumerate_many(self, pos, box, absorbers, ipot):
-        """Every path of every absorber in one set of launches.  pos (n, 3) A (several frames: concatenate them and
-        give each frame's absorbers as global indices; all atoms of pos are candidates of every absorber, so give
-        frames as separate position blocks only with a box that keeps them apart, or one call per frame), box a
-        cubic length or None, absorbers (A,) atom indices, ipot (n,) potential per atom.  Returns {"paths": {nleg:
-        (coords, ipots, deg, xport, atoms, slot)}, "ref": (A,) reference importance per absorber}, paths grouped by
-        absorber slot in the reference's order."""
+        """Every path of every absorber of every frame in one set of launches.  pos (n, 3) A, or (F, n, 3) for F
+        frames of the same atoms (an MD trajectory); box a cubic length or None; absorbers (A,) atom indices, or
+        (F, A) per frame; ipot (n,) potential per atom.  Returns {"paths": {nleg: (coords, ipots, deg, xport, atoms,
+        slot)}, "ref": (slots,) reference importance}, slot = frame * A + absorber, paths grouped by slot in the
+        reference's order, atoms as indices within the frame."""
         dev, lib, st = self.device, self._lib, self._stream()
-        posd = torch.as_tensor(pos, device=dev, dtype=torch.float32).contiguous()
-        n = posd.shape[0]
+        posd = torch.as_tensor(np.asarray(pos) if not torch.is_tensor(pos) else pos, device=dev,
+                               dtype=torch.float32).contiguous()
+        if posd.dim() == 2:
+            posd = posd[None]
+        F, n = int(posd.shape[0]), int(posd.shape[1])
+        ab_np = np.asarray(absorbers.cpu() if torch.is_tensor(absorbers) else absorbers, np.int64)
+        if ab_np.ndim == 1:
+            ab_np = np.broadcast_to(ab_np, (F, ab_np.shape[0]))      # the same atoms in every frame
+        if ab_np.shape[0] != F:
+            raise ValueError("absorbers must be (A,) or (frames, A)")
+        per_frame = max(int(ab_np.shape[1]), 1)
         if box is not None and not np.isscalar(box) and not (torch.is_tensor(box) and box.dim() == 0):
             raise NotImplementedError("only cubic boxes (a length) or clusters (None) are supported")
         boxf = float(box) if box is not None else -1.0
-        ab = torch.as_tensor(np.asarray(absorbers, np.int64), device=dev).contiguous()
+        ab = torch.as_tensor(ab_np.reshape(-1), device=dev).contiguous()
         A = int(ab.shape[0])
         ipot_of = torch.as_tensor(np.asarray(ipot), device=dev, dtype=torch.int64).contiguous()
         # candidates
         cnt = torch.zeros(A, device=dev, dtype=torch.int32)
-        _lib.check(lib.fg_pf_candidates(posd.data_ptr(), n, boxf, ab.data_ptr(), A, self.rmax, cnt.data_ptr(), None,
-                                        None, None, st))
+        if A == 0:
+            return {"paths": {}, "ref": torch.ones(0, device=dev)}
+        _lib.check(lib.fg_pf_candidates(posd.data_ptr(), n, boxf, ab.data_ptr(), A, per_frame, self.rmax,
+                                        cnt.data_ptr(), None, None, None, st))
         off = torch.zeros(A + 1, device=dev, dtype=torch.int64)
         off[1:] = torch.cumsum(cnt.long(), 0)
         total = int(off[-1])
         cand_atom = torch.empty(max(total, 1), device=dev, dtype=torch.int64)
         cand_rel = torch.empty(max(total, 1), 3, device=dev, dtype=torch.float32)
-        _lib.check(lib.fg_pf_candidates(posd.data_ptr(), n, boxf, ab.data_ptr(), A, self.rmax, None, off.data_ptr(),
-                                        cand_atom.data_ptr(), cand_rel.data_ptr(), st))
+        _lib.check(lib.fg_pf_candidates(posd.data_ptr(), n, boxf, ab.data_ptr(), A, per_frame, self.rmax, None,
+                                        off.data_ptr(), cand_atom.data_ptr(), cand_rel.data_ptr(), st))
         slot = torch.repeat_interleave(torch.arange(A, device=dev, dtype=torch.int32), cnt.long())
         seq = (torch.arange(total, device=dev) - off[slot.long()]).to(torch.int32)[:, None].contiguous()
         cr = cand_rel[:total]

@@ -206,11 +206,13 @@ typedef struct fg_pf_tables {
 } fg_pf_tables;
 
 /* Candidates (atoms within rmax of each absorber, minimum image in a cubic box of length box, box <= 0: a cluster,
- * the absorber excluded), in atom order.  offset == NULL: count (A) = candidates per slot.  Else offset (A + 1) is
- * the exclusive scan of count and cand_atom (total), cand_rel (total, 3) are written.  pathfinder.py:219-224. */
+ * the absorber excluded), in atom order.  pos holds F frames of n atoms (F n, 3); slot a belongs to frame
+ * a / per_frame and absorbers[a] is an atom index within that frame.  offset == NULL: count (A) = candidates per
+ * slot.  Else offset (A + 1) is the exclusive scan of count and cand_atom (total, frame-local atom indices),
+ * cand_rel (total, 3) are written.  pathfinder.py:219-224. */
 FG_API fg_status fg_pf_candidates(const float *pos, int64_t n, float box, const int64_t *absorbers, int32_t A,
-                                  float rmax, int32_t *count, const int64_t *offset, int64_t *cand_atom,
-                                  float *cand_rel, void *stream);
+                                  int32_t per_frame, float rmax, int32_t *count, const int64_t *offset,
+                                  int64_t *cand_atom, float *cand_rel, void *stream);
 /* One level of growth: P partial paths of m atoms (seq (P, m), closed-so-far lengths len (P), slots (P)) get every
  * intermediate other than their last atom whose closed length fits two_r.  child_off == NULL: count (P) children
  * per partial path.  Else child_off (P) is the exclusive scan of count and the children (seq (C, m + 1), len, slot)

@@ -105,3 +105,24 @@ def test_importance_and_degeneracy_against_oracle():
             deg = np.full(len(c), 2.0, np.float32)
             dt = GPUPathFinder.degenerate_total(torch.tensor(c), torch.tensor(deg)).numpy()
             assert np.array_equal(dt, OF.Finder.degenerate_total(c, deg))
+
+
+def test_frames_batched_equal_per_frame():
+    """Frames of an MD trajectory in one call: (F, n, 3) positions, (F, A) absorbers; slot = frame * A + absorber."""
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    base, box = W.bcc_supercell(6, 2.87)
+    F, A = 3, 4
+    pos = np.stack([W.thermal(base, 0.08, seed=40 + f) for f in range(F)])
+    rng = np.random.default_rng(1)
+    abs_ = np.stack([rng.choice(len(base), A, replace=False) for _ in range(F)])
+    f = GPUPathFinder(phase("cfg4_fe_phase"), device="cuda", rmax=5.5, nlegmax=4, critpw=1.0)
+    many = f.enumerate_many(pos, box, abs_, np.ones(len(base), int))
+    for fr in range(F):
+        one = f.enumerate_many(pos[fr], box, abs_[fr], np.ones(len(base), int))
+        assert torch.equal(many["ref"][fr * A:(fr + 1) * A], one["ref"])
+        for nleg, v in one["paths"].items():
+            w = many["paths"][nleg]
+            sel = (w[5] >= fr * A) & (w[5] < (fr + 1) * A)
+            for x, y in zip(v[:5], w[:5]):
+                assert torch.equal(x, y[sel]), (fr, nleg)
+            assert torch.equal(v[5] + fr * A, w[5][sel])
