@@ -164,7 +164,7 @@ class GPUPathFinder:
         F, n = int(posd.shape[0]), int(posd.shape[1])
         ab_np = np.asarray(absorbers.cpu() if torch.is_tensor(absorbers) else absorbers, np.int64)
         if ab_np.ndim == 1:
-            ab_np = np.broadcast_to(ab_np, (F, ab_np.shape[0]))      # the same atoms in every frame
+            ab_np = np.tile(ab_np, (F, 1))      # the same atoms in every frame
         if ab_np.shape[0] != F:
             raise ValueError("absorbers must be (A,) or (frames, A)")
         per_frame = max(int(ab_np.shape[1]), 1)
