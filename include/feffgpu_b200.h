@@ -239,6 +239,26 @@ FG_API fg_status fg_pf_describe(int64_t B, int32_t nleg, const int32_t *seq, con
 FG_API fg_status fg_pf_windows(const float *sorted_len, const int64_t *seg_off, int64_t nseg, float eps,
                                int64_t *window);
 
+/* ---------------------------------------------------------------------------------------------- pair tables
+ * Single scattering of whole configurations from tabulated two-leg signals (the reference's PairTables,
+ * src/feffgpu/exafs/forward.py:178-320); the tables themselves are rows of fg_chi_reduce.  pos (C, n, 3) FP64
+ * angstrom, C copies of n atoms; box: cubic length, <= 0 for a cluster; ipot (n) int32 scatterer potential 0..nph
+ * (0: never a neighbour in the spectrum); the distance grid r_min + dr i, i < nr. */
+
+/* Histogram of absorber-neighbour distances (forward.py:248-289): every pair with 1e-6 < r^2 <= rmax^2 adds its
+ * linear-interpolation weights to row ipot[j] of hist (nph + 1, nr) FP64; absorbers (A) atom indices, the same in
+ * every copy, or NULL for every atom; n_short (device, 1) = pairs closer than r_min.  Deterministic: the weights are
+ * summed in 2^-32 fixed point (exact, order-free), each pair adding exactly one. */
+FG_API fg_status fg_pair_histogram(const double *pos, int32_t C, int64_t n, double box, const int64_t *absorbers,
+                                   int32_t A, const int32_t *ipot, int32_t nph, double r_min, double dr, int32_t nr,
+                                   double rmax, double *hist, uint64_t *n_short, void *stream);
+/* Gradient (C, n, 3) of sum_k g_k chi_k with respect to pos, chi = scale * sum over every ordered pair of every
+ * copy of the interpolated table row (PairTables.single_scattering, forward.py:303-319, with scale = 1 / (C n)),
+ * given D = T g (nph, nr) FP64 (T the tables of potentials 1..nph).  One atom per block, fixed-order sums. */
+FG_API fg_status fg_pair_ss_grad(const double *pos, int32_t C, int64_t n, double box, const int32_t *ipot, int32_t nph,
+                                 const double *D, double r_min, double dr, int32_t nr, double rmax, double scale,
+                                 double *grad, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,6 +26,8 @@ The reference is imported read-only from its source tree and run on the CPU in F
   a 400-atom periodic Fe/O/Pt packing (rmax 6.5, 7 legs) and a thermal bcc Fe frame (rmax 5.5, 3 legs), each without
   and with an importance cut; finder_feopt.npz -- the reference finder's paths on the benchmark packing (counts,
   hashes and ends of the atom sequences per leg count, two absorbers, rmax 8 A, 8 legs).
+* pairs_nio.npz -- the reference's single-scattering pair tables, histogram, all-pairs spectrum and its position
+  gradient on a thermal rock-salt NiO supercell (Ni K edge).
 * cfg2_phase.npz -- Fe K-edge phase tables (potentials Fe*, Fe, O, Pt, lmax 24) of a cluster cut from the seeded
   3000-atom Fe/O/Pt packing, on FEFF's own energy grid; cfg2_sample.npz -- the reference stage's cchi on those
   tables resampled to 401 k points, for a sample of synthetic paths.
@@ -402,12 +404,44 @@ def make_finder_feopt():
     print(f"finder_feopt: {time.time() - t:.1f} s")
 
 
+def make_pairs():
+    """pairs_nio.npz -- the reference's single-scattering pair tables (src/feffgpu/exafs/forward.py:178-320) on the
+    CPU in FP64: a thermally displaced rock-salt NiO supercell (3^3 cells, 216 sites, sigma 0.1 A, periodic), Ni K
+    edge tables on r = 1.5..5 A step 0.02 for k = 0..20 step 0.05, every 25th table row, the histogram of four
+    absorbers, the all-pairs single-scattering spectrum of two copies and the gradient of sum_k w_k chi_k with
+    respect to the positions (seeded w)."""
+    from feffgpu.exafs.forward import PairTables
+    P = phase_from_npz(np.load(HERE / "cfg5_nik_phase.npz"), prefix="ph_")
+    pos0, lab, box = W.rock_salt_supercell(3, 4.177)
+    pos = np.stack([W.thermal(pos0, 0.1, seed=21), W.thermal(pos0, 0.1, seed=22)])
+    ipot = np.array([{"Ni": 1, "O": 2}[x] for x in lab])
+    k = np.arange(401) * 0.05
+    t = time.time()
+    pt = PairTables(P, k, np.zeros(len(k)), 0.0, box=box, rmax=5.0, r_min=1.5, dr=0.02, ms=False, device="cpu",
+                    dtype=torch.complex128)
+    pt.ipot = torch.tensor(ipot)
+    out = {"pos": pos, "box": np.asarray(box), "ipot": ipot, "k": k, "rmax": np.asarray(5.0), "r_min": np.asarray(1.5),
+           "dr": np.asarray(0.02), "nr": np.asarray(pt.nr)}
+    for ip, tab in pt.tables.items():
+        out[f"table_{ip}"] = tab.double().numpy()[::25]
+    absorbers = np.array([0, 7, 100, 150])
+    hist, short = pt.histogram(torch.tensor(pos[0]), torch.tensor(absorbers), torch.tensor(ipot), box=float(box))
+    out["absorbers"], out["hist"], out["short"] = absorbers, hist.numpy(), np.asarray(short)
+    x = torch.tensor(pos, dtype=torch.float32, requires_grad=True)        # the tables are FP32 (forward.py:237)
+    chi = pt.single_scattering(x)
+    w = torch.tensor(np.random.default_rng(3).normal(size=len(k)))
+    (chi.double() * w).sum().backward()
+    out["chi"], out["w"], out["grad"] = chi.detach().double().numpy(), w.numpy(), x.grad.numpy()
+    np.savez_compressed(HERE / "pairs_nio.npz", **out)
+    print(f"pairs_nio: nr {pt.nr}, {time.time() - t:.1f} s")
+
+
 def main():
     import tempfile
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
-    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder"])
+    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder", "pairs"])
     with tempfile.TemporaryDirectory() as tmp:
         if "cases" in want:
             import shutil
@@ -429,6 +463,8 @@ def main():
         if "finder" in want:
             make_finder()
             make_finder_feopt()
+        if "pairs" in want:
+            make_pairs()
 
 
 if __name__ == "__main__":

@@ -1,0 +1,30 @@
+"""The pair-table oracle (oracle/pairs.py) against the reference's PairTables (tests/golden/pairs_nio.npz)."""
+import numpy as np
+
+from oracle import pairs as OP
+from tests.fixtures import npz, phase
+
+
+def _case():
+    z = npz("pairs_nio")
+    return z, float(z["box"]), float(z["r_min"]), float(z["dr"]), float(z["rmax"])
+
+
+def test_tables_histogram_spectrum_gradient():
+    z, box, r0, dr, rmax = _case()
+    P = phase("cfg5_nik_phase")
+    T = OP.tables(P, z["k"], r0, rmax, dr)
+    nr = int(z["nr"])
+    assert T.shape == (P.nph, nr, len(z["k"]))
+    for p in range(1, P.nph + 1):
+        ref = z[f"table_{p}"]
+        # the reference's tables are FP32 copies of its FP64 stage
+        assert np.abs(T[p - 1, ::25] - ref).max() <= 1e-6 * np.abs(ref).max()
+    h, short = OP.histogram(z["pos"][0], z["absorbers"], z["ipot"], box, r0, dr, nr, rmax, P.nph)
+    assert short == int(z["short"])
+    assert np.abs(h - z["hist"]).max() <= 1e-9
+    # the reference's spectrum and gradient come from FP32 positions and tables
+    chi, grad = OP.single_scattering(z["pos"].astype(np.float32).astype(float), box, z["ipot"],
+                                     T.astype(np.float32).astype(float), r0, dr, rmax, w=z["w"])
+    assert np.abs(chi - z["chi"]).max() <= 1e-5 * np.abs(z["chi"]).max()
+    assert np.abs(grad - z["grad"]).max() <= 1e-4 * np.abs(z["grad"]).max()
