@@ -12,7 +12,8 @@ own two absorbers (weak scaling, no collective on the data path).
 
 Beside the headline line's value: the end-to-end form (host buffers, copies timed), forward+backward, the plain FP64
 form, the MD-EXAFS batch (bcc Fe, 500 frames x 32 absorbers in one launch) and the RMC refinement (NiO, two edges,
-each step one CUDA graph replay) and the path finder itself, each in its own key of the JSON line.
+each step one CUDA graph replay), the path finder itself and the single-scattering pair tables, each in its own key
+of the JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -306,6 +307,47 @@ def md_extra(args, dev, timed, world, rank):
     return out
 
 
+def pairs_leg(args, dev, world, rank):
+    """Single scattering from pair tables: rock-salt NiO 8^3 cells (5 % vacancies, 0.1 A disorder, 3,891 atoms), Ni K
+    tables on r = 1.5..6 A step 0.002 (2,251 points x 401 k, one fused-stage call), then the all-pairs
+    single-scattering spectrum (every atom an absorber) and its gradient with respect to every position, timed with
+    CUDA events (median of 5 after a warm-up)."""
+    import time as _time
+    import torch
+    from feffgpu_b200 import workloads as W
+    from feffgpu_b200.pad import phase_from_npz
+    from feffgpu_b200.pairs import PairTables
+    pos0, lab, box = W.rock_salt_supercell(8, 4.177)
+    rng = np.random.default_rng(5 + rank)
+    keep = rng.random(len(pos0)) >= 0.05
+    pos = W.thermal(pos0[keep], 0.1, seed=6 + rank)
+    ipot = np.array([{"Ni": 1, "O": 2}[x] for x in lab[keep]])
+    P = phase_from_npz(np.load(ROOT / "tests" / "golden" / "cfg5_nik_phase.npz"), prefix="ph_")
+    torch.cuda.synchronize(dev)
+    t0 = _time.perf_counter()
+    pt = PairTables(P, Q, box=box, rmax=6.0, r_min=1.5, dr=0.002, device=dev, dtype=torch.complex64)
+    torch.cuda.synchronize(dev)
+    t_tables = (_time.perf_counter() - t0) * 1e3
+    pt.ipot = torch.tensor(ipot)
+    w = torch.randn(NK, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
+
+    def step():
+        x = torch.tensor(pos, device=dev, requires_grad=True)
+        (pt.single_scattering(x) * w).sum().backward()
+
+    step()
+    ms = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return {"atoms": len(pos), "grid_points": pt.nr, "tables_ms": t_tables, "spectrum_and_gradient_ms": float(np.median(ms)),
+            "pairs_per_s": len(pos) * (len(pos) - 1) / (float(np.median(ms)) * 1e-3)}
+
+
 def rmc_extra(args, dev, world, rank):
     """RMC refinement: rock-salt NiO 8^3 cells (4096 sites, a = 4.177 A) with 5 % vacancies and 0.1 A disorder; Ni K
     and O K edges, 32 absorbers each (seeded paths of 2-4 legs, rmax 5 A); targets from a hidden 0.03 A perturbation;
@@ -468,9 +510,10 @@ def main():
             ms, kern = timed(lambda: stage.chi_reduce(batch, Q, S), args.steps, args.warmup, kernel_time=True)
     value = world * n_paths * NK / (ms * 1e-3)
 
-    e2e = fwd_bwd = plain = md = rmc = pf = None
+    e2e = fwd_bwd = plain = md = rmc = pf = pairs = None
     if not args.no_extras:
         pf = finder_leg(args, dev, world, rank)
+        pairs = pairs_leg(args, dev, world, rank)
         e2e, fwd_bwd, plain = extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms)
         if args.md_frames > 0:
             md = md_extra(args, dev, timed, world, rank)
@@ -511,6 +554,7 @@ def main():
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"dp{world} (absorbers per rank)"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "fwd_bwd": fwd_bwd, "plain_fp64": plain,
         "md_batch": md, "rmc_refinement": rmc, "path_finder": pf,
+        "pair_tables": pairs,
         "autotune": {"fwd_warps": stage._launch[0], "bwd_warps": stage._launch[1],
                      "timed": [{"kind": k, "warps": w_, "ms": round(t_, 3)} for sig, k, w_, t_ in tuner.log
                                if sig.split("|")[1] == "p0"]},

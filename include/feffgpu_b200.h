@@ -259,6 +259,14 @@ FG_API fg_status fg_pair_ss_grad(const double *pos, int32_t C, int64_t n, double
                                  const double *D, double r_min, double dr, int32_t nr, double rmax, double scale,
                                  double *grad, void *stream);
 
+/* ---------------------------------------------------------------------------------------------- R-space misfit
+ * The loss of the refinement (src/feffgpu/exafs/transform.py:104-145): per row b of rows (B, NK) FP64,
+ * R[b] = inv_norm * sum_m |(F x_b)_m - target_m|^2 with F (NR, NK) the windowed, k-weighted FFT restricted to the R
+ * window (complex128, interleaved) and target (NR) complex128; with grad non-NULL also grad (B, NK) = dR[b]/dx_b.
+ * One block per row, fixed-order FP64 sums. */
+FG_API fg_status fg_rspace_misfit(int64_t B, int32_t NK, int32_t NR, const double *rows, const double *F,
+                                  const double *target, double inv_norm, double *R, double *grad, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

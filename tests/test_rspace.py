@@ -1,29 +1,58 @@
-"""The R-space misfit equals the reference's conventions (padded FFT, compare.py's R-factor) and is differentiable."""
+"""The R-space transform matrix reproduces the reference's conventions (padded FFT, compare.py's R-factor), and the
+misfit kernel matches it with its gradient (the kernel part on a B200)."""
 import numpy as np
+import pytest
 import torch
 
-from feffgpu_b200.rspace import FitWindow, RSpaceMisfit
+from feffgpu_b200.rspace import FitWindow, RSpaceMisfit, transform_matrix
 from oracle import oracle as O
 
+K = 0.05 * np.arange(401)
+WIN = FitWindow(kmin=3.0, kmax=19.0, dk=1.0, kweight=2, rmin=1.0, rmax=6.0)
 
-def test_misfit_equals_r_factor_and_gradient():
-    k = 0.05 * np.arange(401)
+
+def _signals():
     rng = np.random.default_rng(0)
-    target = np.sin(2 * 2.4 * k) * np.exp(-0.01 * k ** 2) * k / 10
-    model = target + 0.01 * rng.normal(size=k.size)
-    win = FitWindow(kmin=3.0, kmax=19.0, dk=1.0, kweight=2, rmin=1.0, rmax=6.0)
-    mis = RSpaceMisfit(len(k), target, win, device="cpu")
-    x = torch.tensor(model[None], requires_grad=True)
-    v = mis(x)
-    ref = O.r_factor(k, target, model, kmin=3.0, kmax=19.0, rmin=1.0, rmax=6.0, kweight=2, dk=1.0)
-    assert abs(float(v[0]) - ref) < 1e-12 * max(ref, 1e-30) + 1e-15
-    v.sum().backward()
-    # central differences on a few entries
+    target = np.sin(2 * 2.4 * K) * np.exp(-0.01 * K ** 2) * K / 10
+    model = target + 0.01 * rng.normal(size=K.size)
+    return target, model
+
+
+def _misfit_np(F, target, x):
+    tr = F @ target
+    d = F @ x - tr
+    norm = float((np.abs(tr) ** 2).sum())
+    return float((np.abs(d) ** 2).sum() / norm), 2.0 / norm * (np.conj(d)[:, None] * F).real.sum(0)
+
+
+def test_matrix_equals_r_factor_and_gradient():
+    F, r = transform_matrix(len(K), WIN)
+    target, model = _signals()
+    v, g = _misfit_np(F, target, model)
+    ref = O.r_factor(K, target, model, kmin=3.0, kmax=19.0, rmin=1.0, rmax=6.0, kweight=2, dk=1.0)
+    assert abs(v - ref) < 1e-12 * ref
     for i in (100, 200, 300):
         h = 1e-6
         xp, xm = model.copy(), model.copy()
         xp[i] += h
         xm[i] -= h
-        fd = (O.r_factor(k, target, xp, kmin=3, kmax=19, rmin=1, rmax=6) -
-              O.r_factor(k, target, xm, kmin=3, kmax=19, rmin=1, rmax=6)) / (2 * h)
-        assert abs(float(x.grad[0, i]) - fd) < 1e-6 * abs(fd) + 1e-12
+        fd = (O.r_factor(K, target, xp, kmin=3, kmax=19, rmin=1, rmax=6) -
+              O.r_factor(K, target, xm, kmin=3, kmax=19, rmin=1, rmax=6)) / (2 * h)
+        assert abs(g[i] - fd) < 1e-6 * abs(fd) + 1e-12
+
+
+@pytest.mark.gpu
+def test_misfit_kernel_and_gradient():
+    target, model = _signals()
+    mis = RSpaceMisfit(len(K), target, WIN, device="cuda")
+    F, _ = transform_matrix(len(K), WIN)
+    rows = np.stack([model, target, 2 * model])
+    x = torch.tensor(rows, device="cuda", requires_grad=True)
+    v = mis(x)
+    w = torch.tensor([1.0, -0.5, 0.25], device="cuda", dtype=torch.float64)
+    (v * w).sum().backward()
+    for b in range(3):
+        val, g = _misfit_np(F, target, rows[b])
+        assert abs(float(v[b]) - val) <= 1e-12 * max(val, 1e-30) + 1e-15
+        assert np.abs(x.grad[b].cpu().numpy() - float(w[b]) * g).max() <= 1e-10 * np.abs(g).max() + 1e-15
+    assert float(v[1]) < 1e-28
