@@ -14,7 +14,7 @@ The reference is imported read-only from its source tree and run on the CPU in F
 * walks_W.npz -- 2- to 8-leg bcc lattice walks with the W phases and the reference stage's cchi (the procedure of
   tests/test_pathfinder.py:193-230, seed 5).
 * grad_walks_W.npz -- the same for the W walks (loss sum_q w_q chi(q) with seeded w).
-* grad_L001.npz, grad_A000.npz -- d(loss)/d(coords) of the reference stage under torch.utils.checkpoint
+* grad_L001.npz, grad_A000.npz, grad_A014.npz (L3), grad_A009.npz (M5) -- d(loss)/d(coords) of the reference stage under torch.utils.checkpoint
   (use_reentrant=False, as src/feffgpu/exafs/forward.py:683 calls it), loss = sum_p deg_p sum_q w_q chi_p(q).
 * L001_phase.pad -- FEFF's phase.pad of the L001 case, copied as written by FEFF, for the reader's test.
 * cfg1_cu.npz -- the Cu fcc cluster (a = 3.61 A, 6 A radius, K edge) through the reference chain
@@ -454,6 +454,8 @@ def main():
             make_grad_walks()
             make_grad("L001")
             make_grad("A000", nlegs=(2, 3, 4), per=2)
+            make_grad("A014", nlegs=(2, 3, 4, 5), per=2)     # L3 edge: the adjoint's second initial-state class
+            make_grad("A009", nlegs=(2, 3, 4, 5), per=2)     # M5 edge: the third
         if "cfg1" in want:
             make_cfg1(tmp)
         if "cfg2" in want:

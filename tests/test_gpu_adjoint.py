@@ -23,8 +23,11 @@ def _rel(a, b):
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
+GRAD_CASES = ["grad_L001", "grad_A000", "grad_A014", "grad_A009"]     # K, K, L3, M5 edges
+
+
 @pytest.mark.parametrize("dtype", DTYPES)
-@pytest.mark.parametrize("name", ["grad_L001", "grad_A000"])
+@pytest.mark.parametrize("name", GRAD_CASES)
 def test_cchi_chi_fine_gradient_equals_reference_autograd(name, dtype):
     """The reference callers' pattern: cchi -> chi_fine -> weighted sum, backward through both custom adjoints."""
     from feffgpu_b200 import GPUPathStage
@@ -42,6 +45,30 @@ def test_cchi_chi_fine_gradient_equals_reference_autograd(name, dtype):
         e = _rel(x.grad.double().cpu().numpy(), z[f"grad_{nleg}"])
         print(f"{name} nleg {nleg} {dtype}: gradient vs reference autograd {e:.2e}")
         assert e < TOL[dtype], (nleg, e)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("name", GRAD_CASES)
+def test_fused_gradient_equals_reference_autograd(name, dtype):
+    """The same loss through the fused stage (one persistent launch over every leg count, its adjoint): rows =
+    sum_p deg_p chi_p, loss = sum_q w_q rows_q."""
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    z = npz(name)
+    st = GPUPathStage(phase(name), device="cuda", dtype=dtype)
+    legs = sorted(int(k.split("_")[1]) for k in z if k.startswith("coords_"))
+    b = PathBatch([(z[f"coords_{n}"], z[f"ipots_{n}"], z[f"deg_{n}"]) for n in legs], nrows=1, device="cuda")
+    x = b.coords.clone().requires_grad_(True)
+    rows = st.chi_reduce(b, z["q"], coords=x)
+    (rows[0] * torch.tensor(z["w"], device="cuda")).sum().backward()
+    g = x.grad.cpu().numpy()
+    s = 0
+    for n in legs:
+        m = len(z[f"coords_{n}"])
+        e = _rel(g[s:s + m, :n], z[f"grad_{n}"])
+        print(f"{name} fused nleg {n} {dtype}: gradient vs reference autograd {e:.2e}")
+        assert e < TOL[dtype], (n, e)
+        assert np.all(g[s:s + m, n:] == 0)
+        s += m
 
 
 @pytest.mark.parametrize("dtype", DTYPES)
