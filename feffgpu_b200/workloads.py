@@ -134,6 +134,8 @@ def random_paths(pos, box, absorber, counts, rmax=8.0, leg_max=6.0, seed=0, ipot
         # hops no longer than about the mean leg that fits the length budget, so that long paths close often
         hop = min(leg_max, max(2.4, 2.0 * rmax / nleg + 0.8 - 0.3 * max(0, nleg - 6)))
         keep = r0 <= hop
+        if not keep.any():
+            raise ValueError(f"no scatterer-to-scatterer hop within {hop:.2f} A for {nleg}-leg paths: raise rmax")
         nbr, vec = nbr0[keep], vec0[keep]
         offs = np.concatenate([[0], np.cumsum(np.bincount(owner[keep], minlength=n))])
         deg = np.diff(offs)

@@ -283,3 +283,48 @@ def test_fused_gradient_mixed_leg_counts_and_rows_by_finite_differences():
         sm[i] -= 1e-5
         fds[i] = (loss(c0, sp) - loss(c0, sm)) / 2e-5
     assert _rel(st_s2.grad.cpu().numpy(), fds) < 1e-5
+
+
+def test_nine_legs_forward_and_gradient():
+    """Paths of nine legs (eight scatterers, FEFF's own limit): the stage against the oracle (FP64 to 1e-10, mixed to
+    2e-5 of max|cchi|) and the FP64 adjoint against central differences of the stage (h = 1e-4 A), with distinct
+    atoms (W phases, bcc walks of the Fe/O/Pt packing's kind drawn by workloads.random_paths)."""
+    from feffgpu_b200 import GPUPathStage
+    from feffgpu_b200 import workloads as W
+    P = phase("case_W")
+    base, box = W.bcc_supercell(6, 3.1652)
+    pos = W.thermal(base, 0.05, seed=9)
+    ab = int(W.central_atom(pos, box, None, None, 1)[0])
+    paths = W.random_paths(pos, box, ab, {9: 80}, rmax=13.5, leg_max=4.0, seed=4)
+    coords, ip, atoms = paths[9]
+    keep = [b for b in range(len(atoms)) if len(set(atoms[b].tolist()) | {ab}) == 9][:4]
+    coords, ip = coords[keep], ip[keep]
+    assert len(coords) >= 2
+    orc = O.Oracle(P)
+    oc, _ = orc.cchi(coords, ip)
+    for dtype, tol in ((torch.complex128, 1e-10), (torch.complex64, 2e-5)):
+        st = GPUPathStage(P, device="cuda", dtype=dtype)
+        cc, _ = st.cchi(torch.tensor(coords), torch.tensor(ip))
+        e = _rel(cc.cpu().numpy(), oc)
+        print(f"nine legs {dtype}: cchi vs oracle {e:.2e}")
+        assert e < tol
+    st = GPUPathStage(P, device="cuda", dtype=torch.complex128)
+    q = np.arange(1, 401) * 0.05
+    S = st.linear_matrix(q)
+    w = torch.tensor(np.random.default_rng(8).normal(size=len(q)) * q ** 2, device="cuda")
+
+    def loss(c):
+        cc, rf = st.cchi(c, torch.tensor(ip))
+        return (st.chi_fine(cc, rf, q, S) * w[None]).sum()
+
+    x = torch.tensor(coords, device="cuda", requires_grad=True)
+    loss(x).backward()
+    g = x.grad.cpu().numpy()
+    h = 1e-4
+    with torch.no_grad():
+        for b, j, k in [(0, 3, 0), (0, 8, 2), (1, 5, 1), (1, 1, 2)]:
+            cp, cm = coords.copy(), coords.copy()
+            cp[b, j, k] += h
+            cm[b, j, k] -= h
+            fd = (float(loss(torch.tensor(cp, device="cuda"))) - float(loss(torch.tensor(cm, device="cuda")))) / (2 * h)
+            assert abs(fd - g[b, j, k]) <= 1e-4 * np.abs(g).max(), (b, j, k, fd, g[b, j, k])
