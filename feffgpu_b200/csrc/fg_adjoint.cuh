@@ -917,9 +917,9 @@ __global__ void __launch_bounds__(256) k_fine_adjoint(int64_t B, int E, int NK, 
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     unsigned char *base = smem + (size_t)w * wbytes;
-    R *amp = reinterpret_cast<R *>(base);
-    double *pha = reinterpret_cast<double *>(base + align_up((size_t)E * sizeof(R), 16));
-    double *dA = reinterpret_cast<double *>(base + align_up((size_t)E * sizeof(R), 16) + align_up((size_t)E * 8, 16));
+    double *amp = reinterpret_cast<double *>(base);        // FP64, as the forward forms it
+    double *pha = reinterpret_cast<double *>(base + align_up((size_t)E * 8, 16));
+    double *dA = reinterpret_cast<double *>(base + 2 * align_up((size_t)E * 8, 16));
     double *dP = dA + NK;
     auto Sv = [&](int k, int j) { return S_d ? S_d[(size_t)k * E + j] : (double)S_r[(size_t)k * E + j]; };
     for (int64_t p = (int64_t)blockIdx.x * nw + w; p < B; p += (int64_t)gridDim.x * nw) {
@@ -943,7 +943,7 @@ __global__ void __launch_bounds__(256) k_fine_adjoint(int64_t B, int E, int NK, 
                     ph += sv * pha[j];
                 }
                 const double qk = q_d ? q_d[k] : (double)q_r[k];
-                const double damp = exp(-2.0 * s2 * qk * qk);
+                const double damp = s2 != 0.0 ? exp(-2.0 * s2 * qk * qk) : 1.0;
                 const double G = (mode == 1 ? gr[k] * wd : (double)gchi[p * NK + k]) * damp;
                 const double arg = ph + 2.0 * qk * rf;
                 const double sn = sin_arg<R>(arg), cs = sin_arg<R>(arg + 1.5707963267948966);
@@ -1022,8 +1022,7 @@ fg_status launch_fine_adjoint(const StageView &sv, int64_t B, int NK, int mode, 
                               const double *deg, const double *sigma2, C2<R> *gbar, R *greff_r, double *greff_d,
                               double *gsig, cudaStream_t st)
 {
-    const size_t wb = align_up((size_t)sv.E * sizeof(R), 16) + align_up((size_t)sv.E * 8, 16) +
-                      align_up((size_t)NK * 16, 16);
+    const size_t wb = 2 * align_up((size_t)sv.E * 8, 16) + align_up((size_t)NK * 16, 16);
     const int warps = fit_warps(4, wb, sv.max_smem), threads = warps * 32;
     auto kern = k_fine_adjoint<R>;
     int blocks = 0;

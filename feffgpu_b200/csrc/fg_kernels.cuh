@@ -16,7 +16,8 @@ template <typename R> __host__ __device__ constexpr size_t geo_bytes() { return 
 template <typename R> __host__ __device__ inline size_t table_bytes(int L1, int nsc_max, int MM, int E, bool with_signal)
 {
     const size_t d = align_up((size_t)nsc_max * (L1 + 1) * dstride(MM) * sizeof(R), 16);
-    const size_t p = with_signal ? align_up((size_t)E * sizeof(double), 16) : 0;
+    // with the signal: its unwrapped phase and amplitude (FP64) reuse the tables' space once the energies are done
+    const size_t p = with_signal ? 2 * align_up((size_t)E * sizeof(double), 16) : 0;
     return d > p ? d : p;
 }
 template <typename R> inline size_t warp_bytes(int L1, int nsc_max, int MM, int E, bool with_signal)
@@ -74,8 +75,8 @@ __global__ void __launch_bounds__(256) k_cchi(Tables<R> T, const CT *__restrict_
 
 // Amplitude and unwrapped phase of one path's signal (stage.py:366-370, 380-384), one warp: differences brought
 // into (-pi, pi] with round-half-even (torch.round) and summed in FP64.  amp may be null.
-template <typename R, class Load>
-__device__ __forceinline__ void amp_phase(int E, int lane, const Load &load, R *amp, double *pha)
+template <typename R, class Load, typename A = R>
+__device__ __forceinline__ void amp_phase(int E, int lane, const Load &load, A *amp, double *pha)
 {
     double carry = 0.0, prev_raw = 0.0;
     for (int e0 = 0; e0 < E; e0 += 32) {
@@ -99,7 +100,7 @@ __device__ __forceinline__ void amp_phase(int E, int lane, const Load &load, R *
         const double base = e0 == 0 ? __shfl_sync(0xffffffffu, ang, 0) : carry;
         const double u = base + dlt;
         if (e < E) {
-            if (amp) amp[e] = (R)a;
+            if (amp) amp[e] = (A)a;
             pha[e] = u;
         }
         carry = __shfl_sync(0xffffffffu, u, 31);
@@ -184,6 +185,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
     R *dh = reinterpret_cast<R *>(base + geo_bytes<R>());
     C2<R> *cbuf = reinterpret_cast<C2<R> *>(base + geo_bytes<R>() + table_bytes<R>(L1, nsc_max, K::MM, E, true));
     double *pha = reinterpret_cast<double *>(dh);   // the tables are dead once the path's energies are done
+    double *amp = pha + align_up((size_t)E, 2);
     for (;;) {
         unsigned long long t = 0;
         if (lane == 0) t = atomicAdd(counter, 1ull);
@@ -202,7 +204,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
             }
         }
         __syncwarp();
-        amp_phase<R>(E, lane, [&](int e) { return cbuf[e]; }, static_cast<R *>(nullptr), pha);
+        amp_phase<R>(E, lane, [&](int e) { return cbuf[e]; }, amp, pha);
         __syncwarp();
         const double rf = g.reff * kBohr, wdeg = P.deg[p], s2 = P.sigma2 ? P.sigma2[p] : 0.0;
         for (int k0 = 0; k0 < NK; k0 += 32) {
@@ -212,12 +214,12 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
                 double a = 0.0, ph = 0.0;
                 for (int j = lo; j < hi; ++j) {
                     const double sv = S[(size_t)k * E + j];
-                    const C2<R> c = cbuf[j];
-                    a += sv * sqrt((double)c.x * c.x + (double)c.y * c.y + 1e-30);
+                    a += sv * amp[j];
                     ph += sv * pha[j];
                 }
                 const double qk = q[k];
-                terms[p * NK + k] = wdeg * a * sin_arg<R>(ph + 2.0 * qk * rf) * exp(-2.0 * s2 * qk * qk);
+                const double damp = s2 != 0.0 ? exp(-2.0 * s2 * qk * qk) : 1.0;   // exact 1 without sigma^2
+                terms[p * NK + k] = wdeg * a * sin_arg<R>(ph + 2.0 * qk * rf) * damp;
             }
         }
         if (lane == 0 && reff_save) reff_save[p] = rf;
