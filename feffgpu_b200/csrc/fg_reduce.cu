@@ -122,3 +122,4 @@ extern "C" fg_status fg_fp32_fma_peak(double *tflops, void *stream)
     *tflops = 2.0 * 16.0 * iters * (double)blocks * 256 / (ms * 1e-3) / 1e12;
     return FG_OK;
 }
+

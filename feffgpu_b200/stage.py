@@ -230,6 +230,50 @@ class GPUPathStage:
                                                   g.data_ptr(), gc.data_ptr(), gr.data_ptr(), _stream(self.device)))
         return gc, gr
 
+    # -- feffNNNN.dat columns ------------------------------------------------------------------------------
+    def _energy_columns(self):
+        """Per energy: k, real[2 phc], red factor, lambda, real[p] (FEFF's units) and the (E, 4) device table of
+        fg_path_columns.  phc is the absorber's phase shift in the channel l = l_init + 1 (kappa > 0: l = l_init,
+        as FEFF's fdtarr.f picks it); its doubled real part is unwrapped along the energies."""
+        if getattr(self, "_ecols", None) is None:
+            P, E = self.P, self.E
+            ll = self.ilinit if self.kinit > 0 else -self.ilinit
+            caps = np.asarray(P.ph)[:E, ll + P.ltot, 0, 0]
+            ck = np.sqrt(2 * (np.asarray(P.em)[:E] - np.asarray(P.eref)[:E, 0]))
+            red = np.exp(-2 * caps.imag)
+            raw = 2 * caps.real
+            cdelt = raw.copy()
+            for i in range(1, E):                      # sequential unwrap of 2 pi jumps (FEFF's pijump)
+                d = raw[i] - cdelt[i - 1]
+                cdelt[i] = cdelt[i - 1] + d - 2 * np.pi * np.round(d / (2 * np.pi))
+            lam = np.where(np.abs(ck.imag) > 1e-16, 1 / np.where(np.abs(ck.imag) > 1e-16, ck.imag, 1.0), 1e10)
+            shift = cdelt + self.ilinit * np.pi
+            table = np.stack([np.abs(self._xk), 2 / lam, 1 / red, shift], 1)
+            self._ecols = ({"k": self._xk / BOHR, "real_phc": shift, "red_fact": red, "lam": lam * BOHR,
+                            "rep": ck.real / BOHR}, torch.tensor(table, device=self.device, dtype=torch.float64))
+        return self._ecols
+
+    def columns(self, cchi, reff) -> dict:
+        """FEFF's feffNNNN.dat columns of paths from their signals (the reference's PathStage._columns,
+        genfmt.py:449-461): cchi (B, E) and reff (B,) A as cchi() returns them.  Per path mag (B, E) (A) and phase
+        (B, E) on the device; per energy k, real_phc, red_fact, lam, rep (numpy)."""
+        shared, table = self._energy_columns()
+        cc = torch.as_tensor(cchi, device=self.device)
+        if cc.dim() == 1:
+            cc = cc[None]
+        prec = _lib.FG_FP64 if cc.dtype == torch.complex128 else _lib.FG_MIXED
+        cc = cc.to(torch.complex128 if prec == _lib.FG_FP64 else torch.complex64).contiguous()
+        rf = torch.as_tensor(reff, device=self.device).reshape(-1).to(
+            torch.float64 if prec == _lib.FG_FP64 else torch.float32).contiguous()
+        B = int(cc.shape[0])
+        if cc.shape[1] != self.E or rf.shape[0] != B:
+            raise ValueError("cchi must be (B, E) and reff (B,)")
+        mag = torch.empty(B, self.E, device=self.device, dtype=torch.float64)
+        phase = torch.empty_like(mag)
+        _lib.check(self._lib.fg_path_columns(B, self.E, prec, cc.data_ptr(), rf.data_ptr(), table.data_ptr(),
+                                             mag.data_ptr(), phase.data_ptr(), _stream(self.device)))
+        return dict(shared, mag=mag, phase=phase)
+
     # -- launch shape ---------------------------------------------------------------------------------------
     def set_launch(self, fwd_warps: int = 0, bwd_warps: int = 0) -> None:
         """Warps per CTA of this stage's forward and adjoint kernels (0 = the library default)."""

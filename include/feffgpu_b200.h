@@ -259,6 +259,15 @@ FG_API fg_status fg_pair_ss_grad(const double *pos, int32_t C, int64_t n, double
                                  const double *D, double r_min, double dr, int32_t nr, double rmax, double scale,
                                  double *grad, void *stream);
 
+/* ---------------------------------------------------------------------------------------------- path columns
+ * FEFF's feffNNNN.dat columns of B paths from their signals (replaces the reference's PathStage._columns,
+ * genfmt.py:449-461, FEFF's fdtarr.f): mag (B, E) = |cchi| |xk| reff^2 exp(2 reff / lambda) / red factor in
+ * angstrom, phase (B, E) = the unwrapped phase of cchi minus (2 Re phc unwrapped + l pi).  cchi (B, E) and reff (B,
+ * angstrom) in the precision's types (as fg_cchi writes them); cols (E, 4) FP64 per energy: |xk| (1/bohr),
+ * 2 / lambda (1/bohr), 1 / red factor, 2 Re phc unwrapped + l pi (GPUPathStage.columns builds it). */
+FG_API fg_status fg_path_columns(int64_t B, int32_t E, fg_precision prec, const void *cchi, const void *reff,
+                                 const double *cols, double *mag, double *phase, void *stream);
+
 /* ---------------------------------------------------------------------------------------------- R-space misfit
  * The loss of the refinement (src/feffgpu/exafs/transform.py:104-145): per row b of rows (B, NK) FP64,
  * R[b] = inv_norm * sum_m |(F x_b)_m - target_m|^2 with F (NR, NK) the windowed, k-weighted FFT restricted to the R

@@ -26,6 +26,7 @@ The reference is imported read-only from its source tree and run on the CPU in F
   a 400-atom periodic Fe/O/Pt packing (rmax 6.5, 7 legs) and a thermal bcc Fe frame (rmax 5.5, 3 legs), each without
   and with an importance cut; finder_feopt.npz -- the reference finder's paths on the benchmark packing (counts,
   hashes and ends of the atom sequences per leg count, two absorbers, rmax 8 A, 8 legs).
+* feffdat_W.npz -- FEFF's own feff0001..0008.dat of the W case: path geometry and the seven columns.
 * pairs_nio.npz -- the reference's single-scattering pair tables, histogram, all-pairs spectrum and its position
   gradient on a thermal rock-salt NiO supercell (Ni K edge).
 * cfg2_phase.npz -- Fe K-edge phase tables (potentials Fe*, Fe, O, Pt, lmax 24) of a cluster cut from the seeded
@@ -436,12 +437,33 @@ def make_pairs():
     print(f"pairs_nio: nr {pt.nr}, {time.time() - t:.1f} s")
 
 
+def make_feffdat():
+    """feffdat_W.npz -- FEFF's own per-path column files feff0001..0008.dat of the W case (tests/data/W): each path's
+    geometry (absorber first), potentials, degeneracy and reff from the file header, and its seven columns (k,
+    real[2*phc], mag[feff], phase[feff], red factor, lambda, real[p]) as FEFF printed them."""
+    out = {}
+    for i in range(1, 9):
+        lines = (CASES["W"] / f"feff{i:04d}.dat").read_text().splitlines()
+        h = next(j for j, l in enumerate(lines) if "nleg, deg, reff" in l)
+        nleg, deg, reff = (float(v) for v in lines[h].split()[:3])
+        nleg = int(nleg)
+        atoms = [lines[h + 2 + a].split() for a in range(nleg)]
+        coords = np.array([[float(v) for v in a[:3]] for a in atoms])
+        ipots = np.array([int(a[3]) for a in atoms])
+        t = next(j for j, l in enumerate(lines) if l.strip().startswith("k ") and "real[2*phc]" in l)
+        cols = np.array([[float(v) for v in l.split()] for l in lines[t + 1:] if l.strip()])
+        out[f"coords_{i}"], out[f"ipots_{i}"] = coords, ipots
+        out[f"deg_{i}"], out[f"reff_{i}"], out[f"cols_{i}"] = np.asarray(deg), np.asarray(reff), cols
+    np.savez_compressed(HERE / "feffdat_W.npz", **out)
+    print("feffdat_W: 8 paths")
+
+
 def main():
     import tempfile
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
-    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder", "pairs"])
+    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder", "pairs", "feffdat"])
     with tempfile.TemporaryDirectory() as tmp:
         if "cases" in want:
             import shutil
@@ -467,6 +489,8 @@ def main():
             make_finder_feopt()
         if "pairs" in want:
             make_pairs()
+        if "feffdat" in want:
+            make_feffdat()
 
 
 if __name__ == "__main__":
