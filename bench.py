@@ -82,6 +82,13 @@ def workload(rank: int, world: int, scale: float = 1.0, finder: str = "gpu"):
     return P, groups
 
 
+def workload_config(n_paths: int, world: int) -> dict:
+    """The workload's description, the same on both arms of the benchmark."""
+    return {"workload": f"Fe/O/Pt packing 3000 atoms, 2 Fe K absorbers per GPU, every path finder path of 2-8 legs "
+                        f"to 8 A, {n_paths} paths per GPU, lmax 24 x {NK} k, chi on {NK} k",
+            "paths_per_gpu": n_paths, "nk": NK, "parallelism": f"dp{world} (absorbers per rank)"}
+
+
 def finder_leg(args, dev, world, rank):
     """The path finder itself: every path of 2-8 legs within 8 A of this rank's two absorbers (no importance cut),
     both absorbers in one batched call, timed with CUDA events after one warm-up call."""
@@ -443,8 +450,8 @@ def main():
             "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": n_paths * NK / v * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
-            "config": {"workload": f"Fe/O/Pt packing 3000 atoms, 2 Fe K absorbers, every path finder path of 2-8 legs to 8 A, {n_paths} paths, "
-                                   f"lmax 24 x {NK} k", "impl": "FP64 C port of the reference's path stage (oracle)"},
+            "config": dict(workload_config(n_paths, world=args.gpus),
+                           impl="FP64 C port of the reference's path stage (oracle), host cores"),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
@@ -548,10 +555,8 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32 (complex chain) + fp64 (phase argument, sums)", "data": "synthetic",
-        "config": {"workload": f"Fe/O/Pt packing 3000 atoms, 2 Fe K absorbers per GPU, every path finder path of 2-8 legs to 8 A, "
-                               f"{n_paths} paths per GPU, lmax 24 x {NK} k, chi on {NK} k",
-                   "paths_per_gpu": n_paths, "legs": batch.counts, "energies": stage.E, "nk": NK,
-                   "l2": "flushed between steps (256 MB write)", "parallelism": f"dp{world} (absorbers per rank)"},
+        "config": dict(workload_config(n_paths, world), legs=batch.counts, energies=stage.E,
+                       l2="flushed between steps (256 MB write)"),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "fwd_bwd": fwd_bwd, "plain_fp64": plain,
         "md_batch": md, "rmc_refinement": rmc, "path_finder": pf,
         "pair_tables": pairs,
