@@ -44,3 +44,27 @@ def test_stage_create_rejects_spin_and_iorder():
     assert rc == _lib.FG_ERR_NOT_IMPLEMENTED
     d.nsp, d.iorder = 1, 12
     assert lib.fg_stage_create(C.byref(d), 0, C.byref(h)) == _lib.FG_ERR_NOT_IMPLEMENTED
+
+
+def test_new_entry_points_refuse_bad_arguments_on_the_host():
+    """The path finder, pair-table, misfit and column entry points check sizes and pointers before any launch."""
+    lib = _lib.load()
+    V = _lib.FG_ERR_VALUE
+    assert lib.fg_pf_candidates(None, 10, 1.0, None, 1, 1, 5.0, None, None, None, None, None) == V       # null pos
+    assert lib.fg_pf_candidates(None, 10, 1.0, None, 1, 0, 5.0, None, None, None, None, None) == V       # per_frame 0
+    assert lib.fg_pf_extend(1, 0, None, None, None, None, None, 10.0, None, None, None, None, None, None) == V
+    assert lib.fg_pf_extend(1, 9, None, None, None, None, None, 10.0, None, None, None, None, None, None) == V
+    assert lib.fg_pf_terminal(-1, 2, None, None, None, None, None, None) == V
+    assert lib.fg_pf_describe(1, 10, None, None, None, None, None, None, None, None, None, None, None, None, None, None,
+                              None) == V
+    assert lib.fg_pair_histogram(None, 1, 4, 0.0, None, 0, None, 1, 1.5, 0.01, 1, 5.0, None, None, None) == V   # nr 1
+    assert lib.fg_pair_ss_grad(None, 1, 4, 0.0, None, 1, None, 1.5, 0.0, 10, 5.0, 1.0, None, None) == V        # dr 0
+    assert lib.fg_rspace_misfit(-1, 401, 100, None, None, None, 1.0, None, None, None) == V
+    assert lib.fg_rspace_misfit(1, 401, 100, None, None, None, 1.0, None, None, None) == V                  # nulls
+    assert lib.fg_path_columns(1, 0, 0, None, None, None, None, None, None) == V                            # E 0
+    assert lib.fg_path_columns(1, 60, 7, None, None, None, None, None, None) == V
+    w = (C.c_int64 * 3)()
+    sl = (C.c_float * 3)(1.0, 1.0005, 1.5)
+    off = (C.c_int64 * 2)(0, 3)
+    assert lib.fg_pf_windows(sl, off, 1, C.c_float(1e-3), w) == _lib.FG_OK
+    assert list(w) == [0, 0, 1]
