@@ -198,3 +198,27 @@ def test_cfg5_two_edge_refinement_graph():
     assert torch.allclose(g.pos.detach(), eager_pos.detach(), rtol=0, atol=1e-9)
     print(f"cfg5: misfit {losses[0]:.4e} -> {losses[-1]:.4e}")
     assert losses[-1] < 0.8 * losses[0]
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.complex64, 1e-6), (torch.complex128, 1e-12)])
+def test_cfg1_end_to_end_from_the_path_finder(dtype, tol):
+    """The whole configuration on the device: the path finder on the Cu cluster (rmax 6 A, 4 legs, importance cut
+    2.5 %) gives the reference chain's path list (coordinates and degeneracies), the fused stage its chi."""
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    z = npz("cfg1_cu")
+    P = phase("cfg1_cu")
+    pts = W.fcc_cluster(3.61, 6.0)
+    kept, _ = GPUPathFinder(P, device="cuda", rmax=6.0, nlegmax=4, critpw=2.5).enumerate(
+        pts, None, 0, np.ones(len(pts), int))
+    gs = []
+    for nleg, (c, ip, deg, _xp, _atoms) in sorted(kept.items()):
+        c, ip, deg = c.cpu().numpy(), ip.cpu().numpy(), deg.cpu().numpy()
+        assert np.array_equal(c.astype(np.float64), z[f"coords_{nleg}"]), nleg
+        assert np.array_equal(ip, z[f"ipots_{nleg}"]) and np.array_equal(deg.astype(np.float64), z[f"deg_{nleg}"])
+        gs.append((c.astype(np.float64), ip, deg.astype(np.float64)))
+    st = GPUPathStage(P, device="cuda", dtype=dtype)
+    rows = st.chi_reduce(PathBatch(gs, device="cuda"), K401)[0].cpu().numpy()
+    R = _R(K401, z["ref_chi"], rows)
+    print(f"cfg1 from the path finder {dtype}: R {R:.2e}")
+    assert R <= tol
