@@ -35,6 +35,22 @@ def flops_per_energy(nleg: int, L: float) -> float:
     return OFFSET[nleg] + SLOPE[nleg] * L
 
 
+def path_flops(nleg, ipots, lmax_e_ip) -> np.ndarray:
+    """Algorithmic FLOPs of every path over all energies (n,): the per-path cost the multi-GPU split balances."""
+    nleg = np.asarray(nleg, int)
+    ipots = np.asarray(ipots, int)
+    L = np.asarray(lmax_e_ip, float) + 1.0
+    out = np.zeros(len(nleg))
+    for n in np.unique(nleg):
+        sel = np.nonzero(nleg == n)[0]
+        sc = ipots[sel, 1:n]
+        counts = np.zeros((len(sc), L.shape[1]))
+        np.add.at(counts, (np.repeat(np.arange(len(sc)), n - 1), sc.ravel()), 1.0)
+        mean_L = counts @ L.T / (n - 1)
+        out[sel] = np.sum(OFFSET[int(n)] + SLOPE[int(n)] * mean_L, axis=1)
+    return out
+
+
 def batch_flops(nleg, ipots, lmax_e_ip) -> float:
     """Total algorithmic FLOPs of a batch over all energies.  nleg (n,), ipots (n, nleg_max) absorber first,
     lmax_e_ip (E, nph+1) the stage's lmax table."""

@@ -23,11 +23,12 @@ def path_cost(nleg: np.ndarray) -> np.ndarray:
     return np.where(nleg == 2, 0.45, nleg - 1.0)
 
 
-def shard(nleg: np.ndarray, world: int) -> np.ndarray:
-    """Rank of every path: longest-processing-time-first assignment of the path costs to the least-loaded rank.
-    Deterministic for a given input."""
+def shard(nleg: np.ndarray, world: int, cost=None) -> np.ndarray:
+    """Rank of every path: longest-processing-time-first assignment of the path costs (default: by leg count; pass
+    roofline.path_flops for the FLOP cost over all energies) to the least-loaded rank.  Deterministic for a given
+    input."""
     nleg = np.asarray(nleg)
-    cost = path_cost(nleg)
+    cost = path_cost(nleg) if cost is None else np.asarray(cost, float)
     order = np.argsort(-cost, kind="stable")
     load = np.zeros(world)
     owner = np.zeros(len(nleg), np.int64)
@@ -38,10 +39,17 @@ def shard(nleg: np.ndarray, world: int) -> np.ndarray:
     return owner
 
 
-def split_groups(groups, world: int, rank: int):
-    """The rank's share of a list of path groups (coords, ipots, deg, row) as returned for PathBatch."""
+def split_groups(groups, world: int, rank: int, lmax=None):
+    """The rank's share of a list of path groups (coords, ipots, deg, row) as returned for PathBatch; with the
+    stage's lmax table (E, nph+1) the split balances algorithmic FLOPs over all energies."""
     nl = np.concatenate([np.full(len(g[0]), np.asarray(g[0]).shape[1]) for g in groups]) if groups else np.zeros(0)
-    owner = shard(nl, world)
+    cost = None
+    if lmax is not None and len(nl):
+        from .roofline import path_flops
+        nmax = int(nl.max())
+        ip = np.concatenate([np.pad(np.asarray(g[1]), ((0, 0), (0, nmax - np.asarray(g[1]).shape[1]))) for g in groups])
+        cost = path_flops(nl, ip, lmax)
+    owner = shard(nl, world, cost)
     out, off = [], 0
     for g in groups:
         n = len(g[0])

@@ -92,3 +92,24 @@ def test_two_ranks_equal_one_process():
     # d loss / d a with a scaling every rank's part: sum over ranks of 2 total . part = 2 total . total
     np.testing.assert_allclose(out[0][1], 2 * (ref ** 2).sum(), rtol=1e-10)
     np.testing.assert_allclose(out[0][1], out[0][2] + out[1][2], rtol=1e-10)
+
+
+def test_flop_balanced_split():
+    """With the FLOP cost (roofline.path_flops over all energies) every rank gets a near-equal share of the work."""
+    from feffgpu_b200.roofline import path_flops
+    from feffgpu_b200.sharded import shard, split_groups
+    rng = np.random.default_rng(3)
+    lmax = rng.integers(5, 24, size=(60, 4))
+    groups = []
+    for n, m in ((2, 40), (3, 300), (5, 500), (8, 60)):
+        ip = rng.integers(1, 4, size=(m, n))
+        ip[:, 0] = 0
+        groups.append((rng.normal(size=(m, n, 3)), ip, None, None))
+    nl = np.concatenate([np.full(len(g[0]), g[0].shape[1]) for g in groups])
+    ipp = np.concatenate([np.pad(g[1], ((0, 0), (0, 8 - g[1].shape[1]))) for g in groups])
+    cost = path_flops(nl, ipp, lmax)
+    owner = shard(nl, 4, cost)
+    load = np.bincount(owner, weights=cost, minlength=4)
+    assert load.max() / load.min() < 1.01
+    parts = [split_groups(groups, 4, r, lmax=lmax) for r in range(4)]
+    assert sum(len(g[0]) for p in parts for g in p) == len(nl)
