@@ -12,8 +12,8 @@ own two absorbers (weak scaling, no collective on the data path).
 
 Beside the headline line's value: the end-to-end form (host buffers, copies timed), forward+backward, the plain FP64
 form, the MD-EXAFS batch (bcc Fe, 500 frames x 32 absorbers in one launch) and the RMC refinement (NiO, two edges,
-each step one CUDA graph replay), the path finder itself and the single-scattering pair tables, each in its own key
-of the JSON line.
+each step one CUDA graph replay), the path finder itself, the single-scattering pair tables and the reference's own
+GPUPathStage on this GPU (when it is installed under baseline/_ref), each in its own key of the JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -314,6 +314,92 @@ def md_extra(args, dev, timed, world, rank):
     return out
 
 
+def reference_gpu_leg(args, P, groups, dev, ours: dict):
+    """The reference's own GPUPathStage (installed unmodified under baseline/_ref) on this GPU, on a sample of the
+    same batch: per leg count one chunk of up to 4096 paths, the chunk size of its callers (src/feffgpu/chain.py:47),
+    cchi -> chi_fine -> degeneracy-weighted sum into the absorber rows, timed with CUDA events after a warm-up chunk
+    and extrapolated by paths per leg count.  complex64 (its production default) and complex128 forward; complex64
+    forward+backward through non-reentrant checkpointing (src/feffgpu/exafs/forward.py:158-159) in chunks of up to
+    2048 paths, its PathSpectra's default chunk (forward.py:69).  ``ours`` holds this package's ms per step of the
+    same batch to put beside them."""
+    import dataclasses
+    import torch
+    ref = ROOT / "baseline" / "_ref"
+    if not (ref / "feffgpu" / "stage.py").exists():
+        return {"unavailable": "reference not installed under baseline/_ref"}
+    sys.path.insert(0, str(ref))
+    try:
+        from feffgpu.pad import PhaseData as RefPhase
+        from feffgpu.stage import GPUPathStage as RefStage
+    except Exception as err:                                   # noqa: BLE001 - report, do not fail the bench
+        return {"unavailable": f"reference import failed: {err!r}"[:200]}
+    finally:
+        sys.path.remove(str(ref))
+    from torch.utils.checkpoint import checkpoint
+    refP = RefPhase(**{f.name: getattr(P, f.name) for f in dataclasses.fields(RefPhase)})
+    by_leg: dict = {}
+    for c, ip, deg, row in groups:
+        by_leg.setdefault(c.shape[1], []).append((c, ip, deg, row))
+    by_leg = {n: tuple(np.concatenate([x[i] for x in v]) for i in range(4)) for n, v in sorted(by_leg.items())}
+    n_paths = sum(len(v[0]) for v in by_leg.values())
+
+    def ev_time(fn):
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    def arm(dtype, chunk, grad):
+        stage = RefStage(refP, device=dev, dtype=dtype)
+        S = stage.linear_matrix(Q)
+        total, sampled = 0.0, 0
+        for n, (c, ip, deg, row) in by_leg.items():
+            m = min(len(c), chunk)
+            coords = torch.as_tensor(c[:m], device=dev).to(stage.rdtype)
+            ipots = torch.as_tensor(ip[:m], device=dev, dtype=torch.long)
+            w = torch.as_tensor(deg[:m], device=dev, dtype=torch.float64)[:, None]
+            rows = torch.as_tensor(row[:m], device=dev, dtype=torch.long)
+
+            def fwd(x):
+                return stage.chi_fine(*stage.cchi(x, ipots), Q, S, "feff")
+
+            def step():
+                out = torch.zeros(2, NK, device=dev, dtype=torch.float64)
+                if grad:
+                    x = coords.clone().requires_grad_(True)
+                    chi = checkpoint(fwd, x, use_reentrant=False)
+                    out = out.index_add(0, rows, w * chi.to(torch.float64))
+                    out.sum().backward()
+                else:
+                    with torch.no_grad():
+                        out = out.index_add(0, rows, w * fwd(coords).to(torch.float64))
+                return out.cpu()
+
+            step()                                              # warm-up: allocator, kernels, caches
+            total += ev_time(step) * len(c) / m
+            sampled += m
+            torch.cuda.empty_cache()
+        return total, sampled
+
+    out = {"source": "the reference's GPUPathStage, pip-installed unmodified into baseline/_ref, on this GPU"}
+    for key, dtype, chunk, grad, mine in (("fwd_c64", torch.complex64, 4096, False, ours.get("fwd")),
+                                          ("fwd_c128", torch.complex128, 4096, False, ours.get("fwd64")),
+                                          ("fwd_bwd_c64", torch.complex64, 2048, True, ours.get("fwd_bwd"))):
+        try:
+            ms, sampled = arm(dtype, chunk, grad)
+        except torch.cuda.OutOfMemoryError as err:
+            out[key] = {"unavailable": f"out of memory: {err}"[:200]}
+            torch.cuda.empty_cache()
+            continue
+        out[key] = {"value": n_paths * NK / (ms * 1e-3), "unit": UNIT, "ms_full_batch": ms,
+                    "sample": f"{sampled} of {n_paths} paths (one chunk per leg count), extrapolated per leg count",
+                    "ours_over_reference": (ms / mine) if mine else None}
+    return out
+
+
 def pairs_leg(args, dev, world, rank):
     """Single scattering from pair tables: rock-salt NiO 8^3 cells (5 % vacancies, 0.1 A disorder, 3,891 atoms), Ni K
     tables on r = 1.5..6 A step 0.002 (2,251 points x 401 k, one fused-stage call), then the all-pairs
@@ -429,6 +515,7 @@ def main():
     ap.add_argument("--md-frames", type=int, default=500, help="frames of the MD-batch leg (0: skip it)")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (profiling runs)")
     ap.add_argument("--rmc-steps", type=int, default=200, help="steps of the RMC leg (0: skip it)")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's own stage on this GPU")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -517,11 +604,15 @@ def main():
             ms, kern = timed(lambda: stage.chi_reduce(batch, Q, S), args.steps, args.warmup, kernel_time=True)
     value = world * n_paths * NK / (ms * 1e-3)
 
-    e2e = fwd_bwd = plain = md = rmc = pf = pairs = None
+    e2e = fwd_bwd = plain = md = rmc = pf = pairs = ref_gpu = None
     if not args.no_extras:
         pf = finder_leg(args, dev, world, rank)
         pairs = pairs_leg(args, dev, world, rank)
         e2e, fwd_bwd, plain = extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms)
+        if not args.no_ref_gpu:
+            ref_gpu = reference_gpu_leg(args, P, groups, dev, {
+                "fwd": ms, "fwd64": plain["ms_per_step"],
+                "fwd_bwd": (fwd_bwd or {}).get("ms_per_step")})
         if args.md_frames > 0:
             md = md_extra(args, dev, timed, world, rank)
         if args.rmc_steps > 0:
@@ -559,7 +650,7 @@ def main():
                        l2="flushed between steps (256 MB write)"),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "fwd_bwd": fwd_bwd, "plain_fp64": plain,
         "md_batch": md, "rmc_refinement": rmc, "path_finder": pf,
-        "pair_tables": pairs,
+        "pair_tables": pairs, "reference_gpu": ref_gpu,
         "autotune": {"fwd_warps": stage._launch[0], "bwd_warps": stage._launch[1],
                      "timed": [{"kind": k, "warps": w_, "ms": round(t_, 3)} for sig, k, w_, t_ in tuner.log
                                if sig.split("|")[1] == "p0"]},
