@@ -798,6 +798,115 @@ template <typename R> inline size_t adj_warp_bytes(int L1, int nsc_max, int MM)
     return adj_head_bytes<R>() + 2 * align_up((size_t)nsc_max * (L1 + 1) * dstride(MM) * sizeof(R), 16);
 }
 
+// ------------------------------------------------------------------------------------------------ frames
+// FEFF's Euler angles of a leg along z are undefined: trig's small-vector branch (stage.py:148-157) makes them
+// constants, so their derivatives there are not those of the path signal, and near the axis they are large terms
+// that cancel.  The signal is invariant under a rotation of the whole path, so a path with a leg within
+// asin(kAxialSin) of the z axis is differentiated in a rotated frame whose z axis is the candidate axis farthest
+// from every leg (for any nine legs some candidate keeps at least about 18 degrees from all of them), and its
+// coordinate gradient is rotated back.  Every other path keeps the identity frame and its results are unchanged.
+// The candidates: a golden-angle spiral over the upper hemisphere, away from low-index lattice directions.
+constexpr double kAxialSin = 0.1;
+constexpr int kFrames = 8;
+
+__device__ __forceinline__ void frame_axis(int c, double &ux, double &uy, double &uz)
+{
+    constexpr double U[kFrames][3] = {
+        {0.39843402527945515, 0.1600486234699024, 0.903125},   {-0.54971449428963837, 0.2067028885692874, 0.809375},
+        {0.31602489695350588, -0.62290378380655709, 0.715625}, {0.21048585883560078, 0.75429913668599635, 0.621875},
+        {-0.72079234200148334, -0.44893472140949026, 0.528125}, {0.88543036946101195, -0.16532217096063032, 0.434375},
+        {-0.56492954713603705, 0.75155120660382946, 0.340625}, {-0.093899422019386392, -0.96448723833932881, 0.246875}};
+    ux = U[c][0]; uy = U[c][1]; uz = U[c][2];
+}
+
+// Rotation Q of frame f (1..kFrames) taking its axis u to z (Rodrigues about u x z): x' = Q x.
+__device__ __forceinline__ void frame_matrix(int f, double (&Q)[3][3])
+{
+    double ux, uy, uz;
+    frame_axis(f - 1, ux, uy, uz);
+    const double s = sqrt(ux * ux + uy * uy), c = uz, kx = uy / s, ky = -ux / s, t = 1.0 - c;
+    Q[0][0] = c + t * kx * kx; Q[0][1] = t * kx * ky;     Q[0][2] = s * ky;
+    Q[1][0] = t * kx * ky;     Q[1][1] = c + t * ky * ky; Q[1][2] = -s * kx;
+    Q[2][0] = -s * ky;         Q[2][1] = s * kx;          Q[2][2] = c;
+}
+
+// Warp-uniform frame of a path: 0 (identity) unless a leg lies within asin(kAxialSin) of z, else the candidate whose
+// smallest sin(angle to a leg) is largest.  Lane j (1..nleg) holds leg j, x_j - x_(j-1) (x_nleg = x_0).
+template <typename R> __device__ int choose_frame(const WarpPath<R> &g, int nleg, int lane)
+{
+    double vx = 0.0, vy = 0.0, vz = 0.0, r2 = 0.0;
+    if (lane >= 1 && lane <= nleg) {
+        const int a = lane == nleg ? 0 : lane, b = lane - 1;
+        vx = g.xyz[a][0] - g.xyz[b][0]; vy = g.xyz[a][1] - g.xyz[b][1]; vz = g.xyz[a][2] - g.xyz[b][2];
+        r2 = vx * vx + vy * vy + vz * vz;
+    }
+    auto warp_min = [](double v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        return v;
+    };
+    // sin^2 of the angle between the leg and axis u; lanes without a leg, and legs of zero length, do not constrain
+    auto sin2 = [&](double ux, double uy, double uz) {
+        if (r2 <= 0.0) return 1.0;
+        const double d = ux * vx + uy * vy + uz * vz;
+        return 1.0 - d * d / r2;
+    };
+    if (warp_min(sin2(0.0, 0.0, 1.0)) >= kAxialSin * kAxialSin) return 0;
+    int best = 1;
+    double best_s = -1.0;
+    for (int c = 0; c < kFrames; ++c) {
+        double ux, uy, uz;
+        frame_axis(c, ux, uy, uz);
+        const double s = warp_min(sin2(ux, uy, uz));
+        if (s > best_s) { best_s = s; best = c + 1; }
+    }
+    return best;
+}
+
+// Rotates the path's atoms into frame f and recomputes the Euler angles and phases (leg lengths, scattering angles
+// and so the rotation tables are invariant and kept).
+template <typename R> __device__ void reframe_path(WarpPath<R> &g, int nleg, int lane, int f)
+{
+    double Q[3][3];
+    frame_matrix(f, Q);
+    if (lane < nleg) {
+        const double x = g.xyz[lane][0], y = g.xyz[lane][1], z = g.xyz[lane][2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) g.xyz[lane][i] = Q[i][0] * x + Q[i][1] * y + Q[i][2] * z;
+    }
+    __syncwarp();
+    if (lane >= 1 && lane <= nleg) {
+        auto rat = [&](int i, double *o) {
+            const int a = (i == 0 || i == nleg) ? 0 : i;
+            o[0] = g.xyz[a][0]; o[1] = g.xyz[a][1]; o[2] = g.xyz[a][2];
+        };
+        const LegGeom lg = leg_geometry<double>(rat, lane, nleg);
+        g.alpha[lane] = lg.alpha;
+        g.gamma[lane] = lg.gamma;
+    }
+    __syncwarp();
+    if (lane >= 1 && lane <= nleg) {
+        const double eta = g.alpha[lane == 1 ? nleg : lane - 1] + g.gamma[lane];
+        double s, c;
+        sincos(eta, &s, &c);
+        g.phs[lane] = C2<R>{(R)c, (R)(-s)};
+    }
+    __syncwarp();
+}
+
+// The coordinate gradient held one component per lane (lane = 3 atom + component) rotated from frame f back to the
+// original frame: g = Q^T g'.
+__device__ __forceinline__ double unframe_grad(double gc, int lane, int f)
+{
+    double Q[3][3];
+    frame_matrix(f, Q);
+    const int a = lane / 3, c = lane % 3;
+    const double g0 = __shfl_sync(0xffffffffu, gc, min(3 * a, 31));
+    const double g1 = __shfl_sync(0xffffffffu, gc, min(3 * a + 1, 31));
+    const double g2 = __shfl_sync(0xffffffffu, gc, min(3 * a + 2, 31));
+    return Q[0][c] * g0 + Q[1][c] * g1 + Q[2][c] * g2;
+}
+
 // Geometry adjoint: dL/dcoords (nleg, 3) of one path from the reduced parameter gradients in gpar (bohr units),
 // one coordinate direction per lane (dual numbers through leg_geometry).
 template <typename R>
@@ -859,6 +968,8 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
         path_setup<R, CT>(g, dh, T, coords + p * stride * 3, ipots + p * stride, nleg, lane, nullptr, MM);
         adj_setup<R>(g, dhd, as.dterm_db, T, nleg, lane, MM);
         __syncwarp();
+        const int frame = choose_frame<R>(g, nleg, lane);
+        if (frame) reframe_path<R>(g, nleg, lane, frame);
         ParGrad pg;
         for (int j = 0; j <= kMaxLeg; ++j) pg.ri[j] = pg.beta[j] = pg.eta[j] = 0.0;
         for (int e0 = 0; e0 < E; e0 += 32) {
@@ -886,7 +997,8 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
             for (int j = 1; j <= nleg; ++j) as.gpar[j] += gr * kBohr * 0.5;
         }
         __syncwarp();
-        const double gc = coord_grad<R>(g, as.gpar, nleg, lane);
+        double gc = coord_grad<R>(g, as.gpar, nleg, lane);
+        if (frame) gc = unframe_grad(gc, lane, frame);
         if (lane < 3 * stride) {
             const int64_t o = p * stride * 3 + lane;
             const double v = lane < 3 * nleg ? gc : 0.0;

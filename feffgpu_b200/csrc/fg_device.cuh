@@ -164,7 +164,10 @@ __host__ __device__ constexpr int dcanon(int MM, int m1, int m2)
     return m1 == 0 ? m2 : (MM + 1) + (m1 - 1) * (2 * MM + 1) + (m2 + MM);
 }
 __host__ __device__ constexpr int ncanon(int MM) { return (MM + 1) + MM * (2 * MM + 1); }
-__host__ __device__ constexpr int dstride(int MM) { return MM <= 2 ? 16 : 32; }
+// Row stride of the rotation tables: the canonical entries rounded up to a 16-byte multiple of FP32 (and of FP64)
+// so rows load as float4 / double2 (28 for MM = 3 instead of a 32-entry row: less shared memory per warp, more of
+// the unified L1 left as cache for the t-matrix tables, whose hit rate the forward kernel is sensitive to).
+__host__ __device__ constexpr int dstride(int MM) { return (ncanon(MM) + 3) & ~3; }
 
 // Representatives of the scattering-matrix entries (lam1 < NR, lam2 < NC) under the flip (m1, m2) -> (-m1, -m2):
 // the pre-phase matrix obeys F~[flip] = (-1)^(m1-m2) F~ because the spherical-wave factors depend on |m| only and
