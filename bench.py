@@ -609,7 +609,7 @@ def main():
         pf = finder_leg(args, dev, world, rank)
         pairs = pairs_leg(args, dev, world, rank)
         e2e, fwd_bwd, plain = extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms)
-        if not args.no_ref_gpu:
+        if not args.no_ref_gpu and rank == 0:
             ref_gpu = reference_gpu_leg(args, P, groups, dev, {
                 "fwd": ms, "fwd64": plain["ms_per_step"],
                 "fwd_bwd": (fwd_bwd or {}).get("ms_per_step")})
