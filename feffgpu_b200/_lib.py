@@ -80,17 +80,17 @@ _SIGS = {
     "fg_fp32_fma_peak": (C.c_int, [C.POINTER(C.c_double), _P]),
     "fg_set_launch": (C.c_int, [C.c_int32, C.c_int32]),
     "fg_stage_set_launch": (C.c_int, [_P, C.c_int32, C.c_int32]),
-    "fg_pf_candidates": (C.c_int, [_P, C.c_int64, C.c_float, _P, C.c_int32, C.c_int32, C.c_float, _P, _P, _P, _P,
-                                   _P]),
+    "fg_pf_candidates": (C.c_int, [_P, C.c_int64, C.c_float, _P, _P, C.c_int32, C.c_int32, C.c_float, _P, _P, _P,
+                                   _P, _P]),
     "fg_pf_extend": (C.c_int, [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.c_float, _P, _P, _P, _P, _P, _P]),
     "fg_pf_terminal": (C.c_int, [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, _P]),
     "fg_pf_describe": (C.c_int, [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, _P, _P, C.POINTER(PfTables), _P, _P, _P,
                                  _P, _P, _P, _P]),
     "fg_pf_windows": (C.c_int, [_P, _P, C.c_int64, C.c_float, _P]),
-    "fg_pair_histogram": (C.c_int, [_P, C.c_int32, C.c_int64, C.c_double, _P, C.c_int32, _P, C.c_int32, C.c_double,
-                                    C.c_double, C.c_int32, C.c_double, _P, _P, _P]),
-    "fg_pair_ss_grad": (C.c_int, [_P, C.c_int32, C.c_int64, C.c_double, _P, C.c_int32, _P, C.c_double, C.c_double,
-                                  C.c_int32, C.c_double, C.c_double, _P, _P]),
+    "fg_pair_histogram": (C.c_int, [_P, C.c_int32, C.c_int64, C.c_double, _P, _P, C.c_int32, _P, C.c_int32,
+                                    C.c_double, C.c_double, C.c_int32, C.c_double, _P, _P, _P]),
+    "fg_pair_ss_grad": (C.c_int, [_P, C.c_int32, C.c_int64, C.c_double, _P, _P, C.c_int32, _P, C.c_double,
+                                  C.c_double, C.c_int32, C.c_double, C.c_double, _P, _P]),
     "fg_rspace_misfit": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, _P, _P, _P, C.c_double, _P, _P, _P]),
     "fg_path_columns": (C.c_int, [C.c_int64, C.c_int32, C.c_int, _P, _P, _P, _P, _P, _P]),
 }

@@ -34,11 +34,27 @@ __device__ __forceinline__ float wrap1(float r, float b)
     return b > 0.f ? __fsub_rn(r, __fmul_rn(b, rintf(__fdiv_rn(r, b)))) : r;
 }
 
+// minimum image in a general periodic cell (cell.py:26-35 of the reference): f = rel inv(cell), rel = (f - round(f))
+// cell, lattice vectors as the rows of cell; c holds the cell (row-major 3 x 3) and then its inverse
+__device__ __forceinline__ void wrap_cell(const float *__restrict__ c, float &x, float &y, float &z)
+{
+    const float *inv = c + 9;
+    float f[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        f[j] = fmaf(z, inv[6 + j], fmaf(y, inv[3 + j], x * inv[j]));
+        f[j] -= rintf(f[j]);
+    }
+    x = fmaf(f[2], c[6], fmaf(f[1], c[3], f[0] * c[0]));
+    y = fmaf(f[2], c[7], fmaf(f[1], c[4], f[0] * c[1]));
+    z = fmaf(f[2], c[8], fmaf(f[1], c[5], f[0] * c[2]));
+}
+
 // ------------------------------------------------------------------------------------------------ candidates
 // One block per absorber slot.  count: number of candidates; with out != null the candidates are written in atom
 // order at off[a] (ordered compaction: warp ballots, then the warps' counts in order).
 template <bool WRITE>
-__global__ void k_candidates(const float *__restrict__ pos_all, int64_t n, float box,
+__global__ void k_candidates(const float *__restrict__ pos_all, int64_t n, float box, const float *__restrict__ cell,
                              const int64_t *__restrict__ absorbers, int32_t per_frame, float rmax,
                              int32_t *__restrict__ count, const int64_t *__restrict__ off,
                              int64_t *__restrict__ cand_atom, float *__restrict__ cand_rel)
@@ -57,9 +73,16 @@ __global__ void k_candidates(const float *__restrict__ pos_all, int64_t n, float
         float rx = 0.f, ry = 0.f, rz = 0.f;
         bool c = false;
         if (i < n) {
-            rx = wrap1(__fsub_rn(pos[3 * i], ax), box);
-            ry = wrap1(__fsub_rn(pos[3 * i + 1], ay), box);
-            rz = wrap1(__fsub_rn(pos[3 * i + 2], az), box);
+            if (cell) {
+                rx = __fsub_rn(pos[3 * i], ax);
+                ry = __fsub_rn(pos[3 * i + 1], ay);
+                rz = __fsub_rn(pos[3 * i + 2], az);
+                wrap_cell(cell, rx, ry, rz);
+            } else {
+                rx = wrap1(__fsub_rn(pos[3 * i], ax), box);
+                ry = wrap1(__fsub_rn(pos[3 * i + 1], ay), box);
+                rz = wrap1(__fsub_rn(pos[3 * i + 2], az), box);
+            }
             c = i != ab && len3(rx, ry, rz) <= rmax;
         }
         const unsigned m = __ballot_sync(0xffffffffu, c);
@@ -261,7 +284,8 @@ int grid_of(int64_t work, int per_block)
 
 using namespace fg;
 
-extern "C" fg_status fg_pf_candidates(const float *pos, int64_t n, float box, const int64_t *absorbers, int32_t A,
+extern "C" fg_status fg_pf_candidates(const float *pos, int64_t n, float box, const float *cell,
+                                      const int64_t *absorbers, int32_t A,
                                       int32_t per_frame, float rmax, int32_t *count, const int64_t *offset,
                                       int64_t *cand_atom, float *cand_rel, void *stream)
 {
@@ -271,11 +295,11 @@ extern "C" fg_status fg_pf_candidates(const float *pos, int64_t n, float box, co
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (!offset) {
         if (!count) return fail(FG_ERR_VALUE, "null count");
-        k_candidates<false><<<A, 256, 0, st>>>(pos, n, box, absorbers, per_frame, rmax, count, nullptr, nullptr,
+        k_candidates<false><<<A, 256, 0, st>>>(pos, n, box, cell, absorbers, per_frame, rmax, count, nullptr, nullptr,
                                                nullptr);
     } else {
         if (!cand_atom || !cand_rel) return fail(FG_ERR_VALUE, "null output");
-        k_candidates<true><<<A, 256, 0, st>>>(pos, n, box, absorbers, per_frame, rmax, nullptr, offset, cand_atom,
+        k_candidates<true><<<A, 256, 0, st>>>(pos, n, box, cell, absorbers, per_frame, rmax, nullptr, offset, cand_atom,
                                               cand_rel);
     }
     FG_CUDA(cudaGetLastError());

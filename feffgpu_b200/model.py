@@ -15,13 +15,29 @@ import numpy as np
 import torch
 
 from .batch import PathBatch
+from .cell import as_cell, cell_words
 
 
-def min_image(rel: torch.Tensor, box) -> torch.Tensor:
-    """Minimum-image vectors for a cubic box length (float) or None (cluster)."""
-    if box is None:
-        return rel
-    return rel - box * torch.round(rel / box)
+class MinImage:
+    """The minimum image of a box in any of the reference's forms (None, a cubic length, (3,) edges, a 3 x 3 cell),
+    with the cell and its inverse held on the device in FP64, so that applying it launches no copy (it runs inside
+    captured CUDA graphs)."""
+
+    def __init__(self, box, device):
+        self.cell = as_cell(box)
+        self.words = None
+        if isinstance(self.cell, np.ndarray):
+            w = torch.as_tensor(cell_words(self.cell, np.float64), device=device)
+            self.words = (w[:9].reshape(3, 3), w[9:].reshape(3, 3))
+
+    def __call__(self, rel: torch.Tensor) -> torch.Tensor:
+        if self.cell is None:
+            return rel
+        if self.words is None:
+            return rel - self.cell * torch.round(rel / self.cell)
+        c, inv = self.words
+        f = rel @ inv
+        return (f - torch.round(f)) @ c
 
 
 class PathModel:
@@ -31,13 +47,14 @@ class PathModel:
     def __init__(self, stage, groups, positions, nrows=None, box=None, chunk=256):
         self.stage, self.box = stage, box
         dev = stage.device
+        self.min_image = MinImage(box, dev)
         pos = torch.as_tensor(positions, dtype=torch.float64).to(dev)
         nleg_max = max(int(np.asarray(g[0]).shape[1]) for g in groups)
         atoms, bgroups = [], []
         for g in groups:
             a = torch.as_tensor(np.asarray(g[0]), dtype=torch.long)
             B, n = a.shape
-            rel = min_image(pos[a.to(dev)] - pos[a[:, :1].to(dev)], box).cpu().numpy()
+            rel = self.min_image(pos[a.to(dev)] - pos[a[:, :1].to(dev)]).cpu().numpy()
             bgroups.append((rel, g[1], g[2] if len(g) > 2 else None, g[3] if len(g) > 3 else None))
             pad = torch.cat([a, a[:, :1].expand(B, nleg_max - n)], 1)
             atoms.append(pad)
@@ -49,7 +66,7 @@ class PathModel:
     def coords(self, pos: torch.Tensor) -> torch.Tensor:
         """(n, nleg_max, 3) relative coordinates of every path at positions pos (N, 3), differentiable."""
         rel = pos[self.atoms] - pos[self.atoms[:, :1]]
-        return min_image(rel, self.box) * self.mask
+        return self.min_image(rel) * self.mask
 
     def rows(self, pos: torch.Tensor, q: torch.Tensor, S: torch.Tensor, sigma2=None) -> torch.Tensor:
         return self.stage.chi_reduce(self.batch, q, S, coords=self.coords(pos), sigma2=sigma2)

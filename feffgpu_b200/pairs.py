@@ -23,21 +23,22 @@ import torch
 
 from . import _lib
 from .batch import PathBatch
+from .cell import as_cell, cell_words
 from .stage import GPUPathStage
 
 ETOK = 0.2624684236075176   # 2 m_e / hbar^2 in 1/(eV A^2): k^2 = ETOK (E - E0) (exafs/transform.py:22)
 
 
-def _box_length(box):
-    if box is None:
-        return -1.0
-    if torch.is_tensor(box):
-        if box.dim() != 0:
-            raise NotImplementedError("only cubic boxes (a length) or clusters (None) are supported")
-        return float(box)
-    if not np.isscalar(box):
-        raise NotImplementedError("only cubic boxes (a length) or clusters (None) are supported")
-    return float(box)
+def _box_args(box, device):
+    """(cubic length or -1, cell words (18,) FP64 on the device or None) of a box in any of the reference's forms."""
+    cell = as_cell(box)
+    if isinstance(cell, np.ndarray):
+        return -1.0, torch.as_tensor(cell_words(cell, np.float64), device=device)
+    return (cell if cell is not None else -1.0), None
+
+
+def _ptr(t):
+    return t.data_ptr() if t is not None else None
 
 
 class PairTables:
@@ -101,7 +102,8 @@ class PairTables:
         ip = self._ipot(ipot, n)
         hist = torch.empty(self.nph + 1, self.nr, device=self.device, dtype=torch.float64)
         short = torch.empty(1, device=self.device, dtype=torch.int64)
-        _lib.check(self._lib.fg_pair_histogram(pos.data_ptr(), 1, n, _box_length(box), ab.data_ptr(), int(ab.numel()),
+        bl, cw = _box_args(box, self.device)
+        _lib.check(self._lib.fg_pair_histogram(pos.data_ptr(), 1, n, bl, _ptr(cw), ab.data_ptr(), int(ab.numel()),
                                                ip.data_ptr(), self.nph, self.r0, self.dr, self.nr, self.rmax,
                                                hist.data_ptr(), short.data_ptr(), self._stream()))
         return hist, int(short.item())
@@ -125,7 +127,8 @@ class PairTables:
         C, n, _ = pos64.shape
         hist = torch.empty(self.nph + 1, self.nr, device=self.device, dtype=torch.float64)
         short = torch.empty(1, device=self.device, dtype=torch.int64)
-        _lib.check(self._lib.fg_pair_histogram(pos64.data_ptr(), C, n, _box_length(self.box), None, 0, ip.data_ptr(),
+        bl, cw = _box_args(self.box, self.device)
+        _lib.check(self._lib.fg_pair_histogram(pos64.data_ptr(), C, n, bl, _ptr(cw), None, 0, ip.data_ptr(),
                                                self.nph, self.r0, self.dr, self.nr, self.rmax, hist.data_ptr(),
                                                short.data_ptr(), self._stream()))
         return hist
@@ -149,7 +152,8 @@ class _SingleScattering(torch.autograd.Function):
         C, n, _ = pos64.shape
         D = torch.einsum("prk,k->pr", pt.T, g.to(torch.float64)).contiguous()          # (nph, nr)
         grad = torch.empty_like(pos64)
-        _lib.check(pt._lib.fg_pair_ss_grad(pos64.data_ptr(), C, n, _box_length(pt.box), ctx.ip.data_ptr(), pt.nph,
+        bl, cw = _box_args(pt.box, pt.device)
+        _lib.check(pt._lib.fg_pair_ss_grad(pos64.data_ptr(), C, n, bl, _ptr(cw), ctx.ip.data_ptr(), pt.nph,
                                            D.data_ptr(), pt.r0, pt.dr, pt.nr, pt.rmax, 1.0 / (C * n), grad.data_ptr(),
                                            pt._stream()))
         return grad.to(ctx.dtype), None, None

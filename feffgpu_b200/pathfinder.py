@@ -25,6 +25,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .cell import as_cell, cell_words
 from .pad import BOHR, load_phase, read_phase_pad
 
 NBETA = 40
@@ -152,7 +153,7 @@ class GPUPathFinder:
 
     def enumerate_many(self, pos, box, absorbers, ipot):
         """Every path of every absorber of every frame in one set of launches.  pos (n, 3) A, or (F, n, 3) for F
-        frames of the same atoms (an MD trajectory); box a cubic length or None; absorbers (A,) atom indices, or
+        frames of the same atoms (an MD trajectory); box None, a cubic length, (3,) edges or a 3 x 3 cell (rows); absorbers (A,) atom indices, or
         (F, A) per frame; ipot (n,) potential per atom.  Returns {"paths": {nleg: (coords, ipots, deg, xport, atoms,
         slot)}, "ref": (slots,) reference importance}, slot = frame * A + absorber, paths grouped by slot in the
         reference's order, atoms as indices within the frame."""
@@ -168,24 +169,28 @@ class GPUPathFinder:
         if ab_np.shape[0] != F:
             raise ValueError("absorbers must be (A,) or (frames, A)")
         per_frame = max(int(ab_np.shape[1]), 1)
-        if box is not None and not np.isscalar(box) and not (torch.is_tensor(box) and box.dim() == 0):
-            raise NotImplementedError("only cubic boxes (a length) or clusters (None) are supported")
-        boxf = float(box) if box is not None else -1.0
+        cell = as_cell(box)
+        cellw = None
+        if isinstance(cell, np.ndarray):
+            cellw = torch.as_tensor(cell_words(cell, np.float32), device=dev)
+        boxf = cell if isinstance(cell, float) else -1.0
+        cptr = cellw.data_ptr() if cellw is not None else None
         ab = torch.as_tensor(ab_np.reshape(-1), device=dev).contiguous()
         A = int(ab.shape[0])
-        ipot_of = torch.as_tensor(np.asarray(ipot), device=dev, dtype=torch.int64).contiguous()
+        ipot_of = (ipot.to(dev, torch.int64) if torch.is_tensor(ipot)
+                   else torch.as_tensor(np.asarray(ipot), device=dev, dtype=torch.int64)).contiguous()
         # candidates
         cnt = torch.zeros(A, device=dev, dtype=torch.int32)
         if A == 0:
             return {"paths": {}, "ref": torch.ones(0, device=dev)}
-        _lib.check(lib.fg_pf_candidates(posd.data_ptr(), n, boxf, ab.data_ptr(), A, per_frame, self.rmax,
+        _lib.check(lib.fg_pf_candidates(posd.data_ptr(), n, boxf, cptr, ab.data_ptr(), A, per_frame, self.rmax,
                                         cnt.data_ptr(), None, None, None, st))
         off = torch.zeros(A + 1, device=dev, dtype=torch.int64)
         off[1:] = torch.cumsum(cnt.long(), 0)
         total = int(off[-1])
         cand_atom = torch.empty(max(total, 1), device=dev, dtype=torch.int64)
         cand_rel = torch.empty(max(total, 1), 3, device=dev, dtype=torch.float32)
-        _lib.check(lib.fg_pf_candidates(posd.data_ptr(), n, boxf, ab.data_ptr(), A, per_frame, self.rmax, None,
+        _lib.check(lib.fg_pf_candidates(posd.data_ptr(), n, boxf, cptr, ab.data_ptr(), A, per_frame, self.rmax, None,
                                         off.data_ptr(), cand_atom.data_ptr(), cand_rel.data_ptr(), st))
         slot = torch.repeat_interleave(torch.arange(A, device=dev, dtype=torch.int32), cnt.long())
         seq = (torch.arange(total, device=dev) - off[slot.long()]).to(torch.int32)[:, None].contiguous()

@@ -205,12 +205,14 @@ typedef struct fg_pf_tables {
     const float *trap;       /* (E - ik0) trapezoid weights */
 } fg_pf_tables;
 
-/* Candidates (atoms within rmax of each absorber, minimum image in a cubic box of length box, box <= 0: a cluster,
- * the absorber excluded), in atom order.  pos holds F frames of n atoms (F n, 3); slot a belongs to frame
- * a / per_frame and absorbers[a] is an atom index within that frame.  offset == NULL: count (A) = candidates per
- * slot.  Else offset (A + 1) is the exclusive scan of count and cand_atom (total, frame-local atom indices),
- * cand_rel (total, 3) are written.  pathfinder.py:219-224. */
-FG_API fg_status fg_pf_candidates(const float *pos, int64_t n, float box, const int64_t *absorbers, int32_t A,
+/* Candidates (atoms within rmax of each absorber, the absorber excluded), in atom order, with the minimum image of
+ * cell.py:26-35: cell == NULL: a cubic box of length box (box <= 0: a cluster); else cell holds 18 floats, the
+ * periodic cell's lattice vectors as rows (3 x 3, row-major) and then its inverse, and box is ignored.  pos holds F
+ * frames of n atoms (F n, 3); slot a belongs to frame a / per_frame and absorbers[a] is an atom index within that
+ * frame.  offset == NULL: count (A) = candidates per slot.  Else offset (A + 1) is the exclusive scan of count and
+ * cand_atom (total, frame-local atom indices), cand_rel (total, 3) are written.  pathfinder.py:219-224. */
+FG_API fg_status fg_pf_candidates(const float *pos, int64_t n, float box, const float *cell,
+                                  const int64_t *absorbers, int32_t A,
                                   int32_t per_frame, float rmax, int32_t *count, const int64_t *offset,
                                   int64_t *cand_atom, float *cand_rel, void *stream);
 /* One level of growth: P partial paths of m atoms (seq (P, m), closed-so-far lengths len (P), slots (P)) get every
@@ -242,20 +244,23 @@ FG_API fg_status fg_pf_windows(const float *sorted_len, const int64_t *seg_off, 
 /* ---------------------------------------------------------------------------------------------- pair tables
  * Single scattering of whole configurations from tabulated two-leg signals (the reference's PairTables,
  * src/feffgpu/exafs/forward.py:178-320); the tables themselves are rows of fg_chi_reduce.  pos (C, n, 3) FP64
- * angstrom, C copies of n atoms; box: cubic length, <= 0 for a cluster; ipot (n) int32 scatterer potential 0..nph
+ * angstrom, C copies of n atoms; box: cubic length, <= 0 for a cluster; cell: NULL, or 18 doubles, the periodic
+ * cell's lattice vectors as rows (3 x 3, row-major) and then its inverse (the minimum image of the reference's
+ * cell.py:26-35; box is then ignored); ipot (n) int32 scatterer potential 0..nph
  * (0: never a neighbour in the spectrum); the distance grid r_min + dr i, i < nr. */
 
 /* Histogram of absorber-neighbour distances (forward.py:248-289): every pair with 1e-6 < r^2 <= rmax^2 adds its
  * linear-interpolation weights to row ipot[j] of hist (nph + 1, nr) FP64; absorbers (A) atom indices, the same in
  * every copy, or NULL for every atom; n_short (device, 1) = pairs closer than r_min.  Deterministic: the weights are
  * summed in 2^-32 fixed point (exact, order-free), each pair adding exactly one. */
-FG_API fg_status fg_pair_histogram(const double *pos, int32_t C, int64_t n, double box, const int64_t *absorbers,
-                                   int32_t A, const int32_t *ipot, int32_t nph, double r_min, double dr, int32_t nr,
+FG_API fg_status fg_pair_histogram(const double *pos, int32_t C, int64_t n, double box, const double *cell,
+                                   const int64_t *absorbers, int32_t A, const int32_t *ipot, int32_t nph, double r_min, double dr, int32_t nr,
                                    double rmax, double *hist, uint64_t *n_short, void *stream);
 /* Gradient (C, n, 3) of sum_k g_k chi_k with respect to pos, chi = scale * sum over every ordered pair of every
  * copy of the interpolated table row (PairTables.single_scattering, forward.py:303-319, with scale = 1 / (C n)),
  * given D = T g (nph, nr) FP64 (T the tables of potentials 1..nph).  One atom per block, fixed-order sums. */
-FG_API fg_status fg_pair_ss_grad(const double *pos, int32_t C, int64_t n, double box, const int32_t *ipot, int32_t nph,
+FG_API fg_status fg_pair_ss_grad(const double *pos, int32_t C, int64_t n, double box, const double *cell,
+                                 const int32_t *ipot, int32_t nph,
                                  const double *D, double r_min, double dr, int32_t nr, double rmax, double scale,
                                  double *grad, void *stream);
 

@@ -39,8 +39,14 @@ def tables(P, q, r_min=1.5, rmax=9.4, dr=0.002):
 
 def _pairs(pos, a, box, rmax):
     rel = pos - pos[a]
-    if box is not None:
+    if box is not None and np.ndim(box) == 0:
         rel = rel - box * np.round(rel / box)
+    elif box is not None:
+        # a cell (cell.py:11-35): (3,) edges -> the diagonal cell; f = rel inv(cell), rel = (f - round(f)) cell
+        c = np.asarray(box, float)
+        c = np.diag(c) if c.shape == (3,) else c
+        f = rel @ np.linalg.inv(c)
+        rel = (f - np.round(f)) @ c
     r2 = (rel * rel).sum(-1)
     mask = (r2 <= rmax * rmax) & (r2 > 1e-6)
     return np.nonzero(mask)[0], rel[mask], np.sqrt(r2[mask])

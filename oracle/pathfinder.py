@@ -139,9 +139,15 @@ class Finder:
         and the reference importance."""
         pos = np.asarray(pos, np.float32)
         rel = pos - pos[absorber]
-        if box is not None:
+        if box is not None and np.ndim(box) == 0:
             b = np.float32(box)
             rel = rel - b * np.round(rel / b)
+        elif box is not None:
+            # a cell (cell.py:11-35): (3,) edges -> the diagonal cell; f = rel inv(cell), rel = (f - round(f)) cell
+            c = np.asarray(box, np.float32)
+            c = np.diag(c) if c.shape == (3,) else c
+            f = rel @ np.linalg.inv(c).astype(np.float32)
+            rel = ((f - np.round(f)) @ c).astype(np.float32)
         d0 = np.sqrt((rel * rel).sum(-1)).astype(np.float32)
         n = len(pos)
         cl = np.nonzero((d0 <= np.float32(self.rmax)) & (np.arange(n) != absorber))[0]

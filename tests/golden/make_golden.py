@@ -25,10 +25,12 @@ The reference is imported read-only from its source tree and run on the CPU in F
 * finder_cu.npz, finder_pack.npz, finder_bcc.npz -- the reference's path finder on the Cu cluster (rmax 6, 4 legs),
   a 400-atom periodic Fe/O/Pt packing (rmax 6.5, 7 legs) and a thermal bcc Fe frame (rmax 5.5, 3 legs), each without
   and with an importance cut; finder_feopt.npz -- the reference finder's paths on the benchmark packing (counts,
-  hashes and ends of the atom sequences per leg count, two absorbers, rmax 8 A, 8 legs).
+  hashes and ends of the atom sequences per leg count, two absorbers, rmax 8 A, 8 legs); finder_tri.npz -- a thermal
+  bcc Fe frame in a triclinic cell (the supercell sheared by SHEAR, rmax 5, 4 legs), the reference finder given the
+  3 x 3 cell.
 * feffdat_W.npz -- FEFF's own feff0001..0008.dat of the W case: path geometry and the seven columns.
 * pairs_nio.npz -- the reference's single-scattering pair tables, histogram, all-pairs spectrum and its position
-  gradient on a thermal rock-salt NiO supercell (Ni K edge).
+  gradient on a thermal rock-salt NiO supercell (Ni K edge); pairs_nio_tri.npz -- the same in a triclinic cell.
 * cfg2_phase.npz -- Fe K-edge phase tables (potentials Fe*, Fe, O, Pt, lmax 24) of a cluster cut from the seeded
   3000-atom Fe/O/Pt packing, on FEFF's own energy grid; cfg2_sample.npz -- the reference stage's cchi on those
   tables resampled to 401 k points, for a sample of synthetic paths.
@@ -336,7 +338,17 @@ FINDER_CASES = {
     "cu": ("fcc", "cfg1_cu", None, 6.0, 4, (0.0, 2.5)),
     "pack": ("pack", "cfg2_phase", "Fe", 6.5, 7, (0.0, 1.0)),
     "bcc": ("bcc", "cfg4_fe_phase", None, 5.5, 3, (0.0, 2.0)),
+    "tri": ("tri", "cfg4_fe_phase", None, 5.0, 4, (0.0, 2.0)),
 }
+
+# triclinic cells of the fixtures: a cubic supercell of edge L sheared to these lattice vectors (rows, units of L)
+SHEAR = np.array([[1.0, 0.0, 0.0], [0.21, 1.0, 0.0], [0.13, -0.17, 1.0]])
+
+
+def sheared(pos, L):
+    """Positions and the 3 x 3 cell (rows) of a cubic supercell of edge L sheared by SHEAR."""
+    cell = L * SHEAR
+    return (np.asarray(pos, float) / L) @ cell, cell
 
 
 def finder_structure(kind):
@@ -348,21 +360,31 @@ def finder_structure(kind):
         pos, lab, box = W.random_packing(400, 0.08, 1.8, seed=77)
         ab = int(W.central_atom(pos, box, lab, "Fe", 1)[0])
         return pos, box, ab, np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
+    if kind == "tri":
+        base, L = W.bcc_supercell(6, 2.87)
+        pos, cell = sheared(base, L)
+        pos = W.thermal(pos, 0.08, seed=4)
+        return pos, cell, 0, np.ones(len(pos), int)
     base, box = W.bcc_supercell(6, 2.87)
     pos = W.thermal(base, 0.08, seed=3)
     return pos, box, int(W.central_atom(pos, box, None, None, 1)[0]), np.ones(len(pos), int)
 
 
-def make_finder():
+def make_finder(names=None):
     """finder_<name>.npz -- the reference's GPUPathFinder (src/feffgpu/pathfinder.py) run on the CPU: the structure,
     parameters, and per importance cut the kept paths' atoms, degeneracies and importances, and the reference
     importance.  The phase tables are those of the named fixture."""
     from feffgpu.pathfinder import GPUPathFinder
     for name, (kind, phase_name, _sp, rmax, nlegmax, crits) in FINDER_CASES.items():
+        if names is not None and name not in names:
+            continue
         P = phase_from_npz(np.load(HERE / f"{phase_name}.npz"), prefix="ph_")
         pos, box, ab, ipot = finder_structure(kind)
-        out = {"pos": pos, "box": np.asarray(-1.0 if box is None else box), "absorber": np.asarray(ab),
+        cellbox = box is not None and np.ndim(box) == 2
+        out = {"pos": pos, "box": np.asarray(-1.0 if box is None or cellbox else box), "absorber": np.asarray(ab),
                "ipot": ipot, "rmax": np.asarray(rmax), "nlegmax": np.asarray(nlegmax), "crit": np.asarray(crits)}
+        if cellbox:
+            out["cell"] = np.asarray(box)
         t = time.time()
         for ci, crit in enumerate(crits):
             f = GPUPathFinder(P, device="cpu", rmax=rmax, nlegmax=nlegmax, critpw=crit)
@@ -437,6 +459,34 @@ def make_pairs():
     print(f"pairs_nio: nr {pt.nr}, {time.time() - t:.1f} s")
 
 
+def make_pairs_cell():
+    """pairs_nio_tri.npz -- as pairs_nio.npz on a triclinic cell: the NiO supercell (3^3 cells) sheared by SHEAR,
+    thermally displaced (sigma 0.1 A), the reference's PairTables given the 3 x 3 cell."""
+    from feffgpu.exafs.forward import PairTables
+    P = phase_from_npz(np.load(HERE / "cfg5_nik_phase.npz"), prefix="ph_")
+    pos0, lab, L = W.rock_salt_supercell(3, 4.177)
+    pos0, cell = sheared(pos0, L)
+    pos = np.stack([W.thermal(pos0, 0.1, seed=31), W.thermal(pos0, 0.1, seed=32)])
+    ipot = np.array([{"Ni": 1, "O": 2}[x] for x in lab])
+    k = np.arange(401) * 0.05
+    t = time.time()
+    pt = PairTables(P, k, np.zeros(len(k)), 0.0, box=cell, rmax=5.0, r_min=1.5, dr=0.02, ms=False, device="cpu",
+                    dtype=torch.complex128)
+    pt.ipot = torch.tensor(ipot)
+    out = {"pos": pos, "cell": cell, "ipot": ipot, "k": k, "rmax": np.asarray(5.0), "r_min": np.asarray(1.5),
+           "dr": np.asarray(0.02), "nr": np.asarray(pt.nr)}
+    absorbers = np.array([0, 7, 100, 150])
+    hist, short = pt.histogram(torch.tensor(pos[0]), torch.tensor(absorbers), torch.tensor(ipot), box=torch.tensor(cell))
+    out["absorbers"], out["hist"], out["short"] = absorbers, hist.numpy(), np.asarray(short)
+    x = torch.tensor(pos, dtype=torch.float32, requires_grad=True)
+    chi = pt.single_scattering(x)
+    w = torch.tensor(np.random.default_rng(3).normal(size=len(k)))
+    (chi.double() * w).sum().backward()
+    out["chi"], out["w"], out["grad"] = chi.detach().double().numpy(), w.numpy(), x.grad.numpy()
+    np.savez_compressed(HERE / "pairs_nio_tri.npz", **out)
+    print(f"pairs_nio_tri: nr {pt.nr}, {time.time() - t:.1f} s")
+
+
 def make_feffdat():
     """feffdat_W.npz -- FEFF's own per-path column files feff0001..0008.dat of the W case (tests/data/W): each path's
     geometry (absorber first), potentials, degeneracy and reff from the file header, and its seven columns (k,
@@ -463,7 +513,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
-    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder", "pairs", "feffdat"])
+    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder", "pairs", "pairs_tri",
+                             "feffdat"])
     with tempfile.TemporaryDirectory() as tmp:
         if "cases" in want:
             import shutil
@@ -487,8 +538,12 @@ def main():
         if "finder" in want:
             make_finder()
             make_finder_feopt()
+        if "finder_tri" in want:
+            make_finder(["tri"])
         if "pairs" in want:
             make_pairs()
+        if "pairs_tri" in want:
+            make_pairs_cell()
         if "feffdat" in want:
             make_feffdat()
 

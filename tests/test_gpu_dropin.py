@@ -1,0 +1,76 @@
+"""The unmodified reference's own front end with this package installed in place of its path finder and path stage
+(feffgpu_b200.install()), against the same front end on the reference's own classes, on the same GPU.
+
+The reference is the copy installed under baseline/_ref (pip, unmodified); without it these tests are skipped.  The
+front end is its PathSpectra (src/feffgpu/exafs/forward.py:67-168): path lists from the finder, coordinates rebuilt
+from the positions under the minimum image of its cell, the path stage per chunk under checkpointing, the
+degeneracy-weighted sum per copy.  The structure is a thermal bcc Fe frame in a triclinic cell (tests/golden/
+finder_tri.npz), four absorbers.  Compared: the path counts per leg count (equal), chi per copy and its gradient with
+respect to every position, both through the reference's checkpointed autograd -- complex128 to 1e-9 and 1e-7 of the
+largest value, complex64 to 2e-4 and 2e-3 (two FP32 chains in different orders)."""
+import dataclasses
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from tests.fixtures import npz, phase
+
+pytestmark = pytest.mark.gpu
+
+REF = Path(__file__).resolve().parents[1] / "baseline" / "_ref"
+
+
+@pytest.fixture
+def reference(monkeypatch):
+    if not (REF / "feffgpu" / "exafs" / "forward.py").exists():
+        pytest.skip("the reference is not installed under baseline/_ref")
+    monkeypatch.syspath_prepend(str(REF))
+    import feffgpu
+    import feffgpu.chain
+    import feffgpu.exafs.forward as F
+    import feffgpu.pathfinder
+    import feffgpu.stage
+    # the reference's own classes come back after the test
+    for mod in (feffgpu, feffgpu.chain, F, feffgpu.stage, feffgpu.pathfinder):
+        for name in ("GPUPathStage", "GPUPathFinder"):
+            if hasattr(mod, name):
+                monkeypatch.setattr(mod, name, getattr(mod, name))
+    return feffgpu, F
+
+
+def _spectra(F, P, pos, cell, absorbers, dtype, w):
+    k = np.arange(401) * 0.05
+    ps = F.PathSpectra(P, k, np.zeros(len(k)), 0.0, box=torch.tensor(cell), rmax=5.0, nlegmax=3, critpw=0.5,
+                       device="cuda", dtype=dtype)
+    counts = ps.refresh(pos[None], absorbers[None])
+    x = torch.tensor(pos, device="cuda", dtype=torch.float32 if dtype == torch.complex64 else torch.float64,
+                     requires_grad=True)
+    chi = ps.spectra(x)
+    (chi.double() * w[None]).sum().backward()
+    return counts, chi.detach().double().cpu().numpy(), x.grad.double().cpu().numpy()
+
+
+@pytest.mark.parametrize("dtype,tchi,tgrad", [(torch.complex128, 1e-9, 1e-7), (torch.complex64, 2e-4, 2e-3)])
+def test_reference_front_end_with_this_package_installed(reference, dtype, tchi, tgrad):
+    feffgpu, F = reference
+    import feffgpu_b200
+    from feffgpu.pad import PhaseData as RefPhase
+    ours = phase("cfg4_fe_phase")
+    P = RefPhase(**{f.name: getattr(ours, f.name) for f in dataclasses.fields(RefPhase)})
+    z = npz("finder_tri")
+    pos, cell = z["pos"], z["cell"]
+    absorbers = np.array([0, 57, 190, 301])
+    w = torch.tensor(np.random.default_rng(6).normal(size=401) * (np.arange(401) * 0.05) ** 2, device="cuda")
+    c_ref, chi_ref, g_ref = _spectra(F, P, pos, cell, absorbers, dtype, w)
+    done = feffgpu_b200.install()
+    assert "feffgpu.exafs.forward.GPUPathStage" in done and "feffgpu.exafs.forward.GPUPathFinder" in done
+    assert F.GPUPathStage is feffgpu_b200.GPUPathStage
+    c_b200, chi_b200, g_b200 = _spectra(F, P, pos, cell, absorbers, dtype, w)
+    assert c_b200 == c_ref, (c_b200, c_ref)
+    e_chi = np.abs(chi_b200 - chi_ref).max() / np.abs(chi_ref).max()
+    e_grad = np.abs(g_b200 - g_ref).max() / np.abs(g_ref).max()
+    print(f"{dtype}: paths {c_ref}; chi {e_chi:.2e}, gradient {e_grad:.2e} against the reference's own classes")
+    assert e_chi <= tchi and e_grad <= tgrad

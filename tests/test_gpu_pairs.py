@@ -1,4 +1,5 @@
-"""Pair tables on a B200 against the reference's PairTables (tests/golden/pairs_nio.npz) and the oracle.
+"""Pair tables on a B200 against the reference's PairTables (tests/golden/pairs_nio.npz, a cubic periodic box, and
+pairs_nio_tri.npz, a triclinic cell) and the oracle.
 
 Tables: every 25th row against the reference's (FP64 stage here, FP32 copies there: 1e-6 of the largest entry; the
 mixed form to 2e-5).  Histogram of chosen absorbers: the reference's to 1e-9 (weights summed in 2^-32 fixed point),
@@ -12,38 +13,43 @@ import torch
 
 from oracle import pairs as OP
 from tests.fixtures import npz, phase
+from tests.test_oracle_pairs import pairs_case
+
+CASES = ["pairs_nio", "pairs_nio_tri"]
 
 pytestmark = pytest.mark.gpu
 
 
-def _tables(dtype=torch.complex128):
+def _tables(dtype=torch.complex128, name="pairs_nio"):
     from feffgpu_b200.pairs import PairTables
-    z = npz("pairs_nio")
-    pt = PairTables(phase("cfg5_nik_phase"), z["k"], np.zeros(len(z["k"])), 0.0, box=float(z["box"]),
-                    rmax=float(z["rmax"]), r_min=float(z["r_min"]), dr=float(z["dr"]), device="cuda", dtype=dtype)
+    z, box, r0, dr, rmax = pairs_case(name)
+    pt = PairTables(phase("cfg5_nik_phase"), z["k"], np.zeros(len(z["k"])), 0.0, box=box,
+                    rmax=rmax, r_min=r0, dr=dr, device="cuda", dtype=dtype)
     pt.ipot = torch.tensor(z["ipot"])
-    return pt, z
+    return pt, z, box
 
 
 @pytest.mark.parametrize("dtype,tol", [(torch.complex128, 1e-6), (torch.complex64, 2e-5)])
 def test_tables_equal_reference(dtype, tol):
-    pt, z = _tables(dtype)
+    pt, z, _ = _tables(dtype)
     assert pt.nr == int(z["nr"])
     for p, t in pt.tables.items():
         ref = z[f"table_{p}"]
         assert np.abs(t.cpu().numpy()[::25] - ref).max() <= tol * np.abs(ref).max()
 
 
-def test_histogram_equals_reference_and_repeats():
-    pt, z = _tables()
-    h1, s1 = pt.histogram(z["pos"][0], z["absorbers"], z["ipot"], box=float(z["box"]))
-    h2, s2 = pt.histogram(z["pos"][0], z["absorbers"], z["ipot"], box=float(z["box"]))
+@pytest.mark.parametrize("name", CASES)
+def test_histogram_equals_reference_and_repeats(name):
+    pt, z, box = _tables(name=name)
+    h1, s1 = pt.histogram(z["pos"][0], z["absorbers"], z["ipot"], box=box)
+    h2, s2 = pt.histogram(z["pos"][0], z["absorbers"], z["ipot"], box=box)
     assert torch.equal(h1, h2) and s1 == s2 == int(z["short"])
     assert np.abs(h1.cpu().numpy() - z["hist"]).max() <= 1e-9
 
 
-def test_single_scattering_and_gradient():
-    pt, z = _tables()
+@pytest.mark.parametrize("name", CASES)
+def test_single_scattering_and_gradient(name):
+    pt, z, box = _tables(name=name)
     w = torch.tensor(z["w"], device="cuda")
     out = []
     for _ in range(2):
@@ -56,7 +62,7 @@ def test_single_scattering_and_gradient():
     assert np.abs(chi - z["chi"]).max() <= 1e-5 * np.abs(z["chi"]).max()
     assert np.abs(grad - z["grad"]).max() <= 1e-4 * np.abs(z["grad"]).max()
     T = pt.T.cpu().numpy()
-    oc, og = OP.single_scattering(z["pos"], float(z["box"]), z["ipot"], T, pt.r0, pt.dr, pt.rmax, w=z["w"])
+    oc, og = OP.single_scattering(z["pos"], box, z["ipot"], T, pt.r0, pt.dr, pt.rmax, w=z["w"])
     assert np.abs(chi - oc).max() <= 1e-10 * np.abs(oc).max()
     assert np.abs(grad - og).max() <= 1e-9 * np.abs(og).max()
     # central differences on the largest gradient entries

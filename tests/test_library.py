@@ -50,15 +50,15 @@ def test_new_entry_points_refuse_bad_arguments_on_the_host():
     """The path finder, pair-table, misfit and column entry points check sizes and pointers before any launch."""
     lib = _lib.load()
     V = _lib.FG_ERR_VALUE
-    assert lib.fg_pf_candidates(None, 10, 1.0, None, 1, 1, 5.0, None, None, None, None, None) == V       # null pos
-    assert lib.fg_pf_candidates(None, 10, 1.0, None, 1, 0, 5.0, None, None, None, None, None) == V       # per_frame 0
+    assert lib.fg_pf_candidates(None, 10, 1.0, None, None, 1, 1, 5.0, None, None, None, None, None) == V       # null pos
+    assert lib.fg_pf_candidates(None, 10, 1.0, None, None, 1, 0, 5.0, None, None, None, None, None) == V       # per_frame 0
     assert lib.fg_pf_extend(1, 0, None, None, None, None, None, 10.0, None, None, None, None, None, None) == V
     assert lib.fg_pf_extend(1, 9, None, None, None, None, None, 10.0, None, None, None, None, None, None) == V
     assert lib.fg_pf_terminal(-1, 2, None, None, None, None, None, None) == V
     assert lib.fg_pf_describe(1, 10, None, None, None, None, None, None, None, None, None, None, None, None, None, None,
                               None) == V
-    assert lib.fg_pair_histogram(None, 1, 4, 0.0, None, 0, None, 1, 1.5, 0.01, 1, 5.0, None, None, None) == V   # nr 1
-    assert lib.fg_pair_ss_grad(None, 1, 4, 0.0, None, 1, None, 1.5, 0.0, 10, 5.0, 1.0, None, None) == V        # dr 0
+    assert lib.fg_pair_histogram(None, 1, 4, 0.0, None, None, 0, None, 1, 1.5, 0.01, 1, 5.0, None, None, None) == V   # nr 1
+    assert lib.fg_pair_ss_grad(None, 1, 4, 0.0, None, None, 1, None, 1.5, 0.0, 10, 5.0, 1.0, None, None) == V        # dr 0
     assert lib.fg_rspace_misfit(-1, 401, 100, None, None, None, 1.0, None, None, None) == V
     assert lib.fg_rspace_misfit(1, 401, 100, None, None, None, 1.0, None, None, None) == V                  # nulls
     assert lib.fg_path_columns(1, 0, 0, None, None, None, None, None, None) == V                            # E 0

@@ -7,11 +7,14 @@ import pytest
 from oracle import pathfinder as OF
 from tests.fixtures import npz, phase
 
-CASES = {"cu": "cfg1_cu", "pack": "cfg2_phase", "bcc": "cfg4_fe_phase"}
+CASES = {"cu": "cfg1_cu", "pack": "cfg2_phase", "bcc": "cfg4_fe_phase", "tri": "cfg4_fe_phase"}
 
 
 def finder_case(name):
+    """(fixture, box: None, the cubic length or the 3 x 3 triclinic cell)."""
     z = npz(f"finder_{name}")
+    if "cell" in z:
+        return z, z["cell"]
     box = float(z["box"]) if float(z["box"]) > 0 else None
     return z, box
 
