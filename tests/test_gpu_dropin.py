@@ -7,7 +7,8 @@ from the positions under the minimum image of its cell, the path stage per chunk
 degeneracy-weighted sum per copy.  The structure is a thermal bcc Fe frame in a triclinic cell (tests/golden/
 finder_tri.npz), four absorbers.  Compared: the path counts per leg count (equal), chi per copy and its gradient with
 respect to every position, both through the reference's checkpointed autograd -- complex128 to 1e-9 and 1e-7 of the
-largest value, complex64 to 2e-4 and 2e-3 (two FP32 chains in different orders)."""
+largest value, complex64 to 2e-4 and 2e-3 (two FP32 chains in different orders).  The same for its
+MultipleScattering (rows per absorber, the exact gradient of a loss of the mean spectrum)."""
 import dataclasses
 import sys
 from pathlib import Path
@@ -74,3 +75,36 @@ def test_reference_front_end_with_this_package_installed(reference, dtype, tchi,
     e_grad = np.abs(g_b200 - g_ref).max() / np.abs(g_ref).max()
     print(f"{dtype}: paths {c_ref}; chi {e_chi:.2e}, gradient {e_grad:.2e} against the reference's own classes")
     assert e_chi <= tchi and e_grad <= tgrad
+
+
+def _multiple(F, P, pos, cell, absorbers):
+    k = np.arange(401) * 0.05
+    ms = F.MultipleScattering(P, k, 0.0, torch.tensor(cell), rmax=5.0, critpw=2.0, nlegmax=4, device="cuda")
+    counts = ms.enumerate(pos[None], absorbers=absorbers)
+    x = torch.tensor(pos, device="cuda", dtype=torch.float32)
+    rows = ms.full_pass(x).double().cpu().numpy()
+    w = torch.tensor(np.random.default_rng(7).normal(size=len(k)) * k ** 2, device="cuda")
+    g = ms.full_gradient(x, lambda chi: (chi.double() * w).sum()).double().cpu().numpy()
+    return counts, rows, g
+
+
+def test_reference_multiple_scattering_with_this_package_installed(reference):
+    """The reference's MultipleScattering (exafs/forward.py:330-760, complex64, its memory-probed batches under
+    checkpointing): the same paths of 3 and 4 legs, rows per absorber and the exact gradient of a loss of the mean
+    spectrum, to 2e-4 and 2e-3 of the largest value."""
+    feffgpu, F = reference
+    import feffgpu_b200
+    from feffgpu.pad import PhaseData as RefPhase
+    ours = phase("cfg4_fe_phase")
+    P = RefPhase(**{f.name: getattr(ours, f.name) for f in dataclasses.fields(RefPhase)})
+    z = npz("finder_tri")
+    pos, cell = z["pos"], z["cell"]
+    absorbers = np.array([0, 57, 190])
+    c_ref, rows_ref, g_ref = _multiple(F, P, pos, cell, absorbers)
+    feffgpu_b200.install()
+    c_b200, rows_b200, g_b200 = _multiple(F, P, pos, cell, absorbers)
+    assert c_b200 == c_ref, (c_b200, c_ref)
+    e_rows = np.abs(rows_b200 - rows_ref).max() / np.abs(rows_ref).max()
+    e_grad = np.abs(g_b200 - g_ref).max() / np.abs(g_ref).max()
+    print(f"MultipleScattering: paths {c_ref}; rows {e_rows:.2e}, gradient {e_grad:.2e} against the reference's classes")
+    assert e_rows <= 2e-4 and e_grad <= 2e-3
