@@ -8,7 +8,8 @@ degeneracy-weighted sum per copy.  The structure is a thermal bcc Fe frame in a 
 finder_tri.npz), four absorbers.  Compared: the path counts per leg count (equal), chi per copy and its gradient with
 respect to every position, both through the reference's checkpointed autograd -- complex128 to 1e-9 and 1e-7 of the
 largest value, complex64 to 2e-4 and 2e-3 (two FP32 chains in different orders).  The same for its
-MultipleScattering (rows per absorber, the exact gradient of a loss of the mean spectrum)."""
+MultipleScattering (rows per absorber, the exact gradient of a loss of the mean spectrum), and for its chain.run from a
+feff.inp (the Cu fcc cluster, complex128)."""
 import dataclasses
 import sys
 from pathlib import Path
@@ -108,3 +109,30 @@ def test_reference_multiple_scattering_with_this_package_installed(reference):
     e_grad = np.abs(g_b200 - g_ref).max() / np.abs(g_ref).max()
     print(f"MultipleScattering: paths {c_ref}; rows {e_rows:.2e}, gradient {e_grad:.2e} against the reference's classes")
     assert e_rows <= 2e-4 and e_grad <= 2e-3
+
+
+def test_reference_chain_with_this_package_installed(reference, tmp_path):
+    """feff.inp to chi(k) through the reference's chain.run (src/feffgpu/chain.py:16-51: potentials, phase shifts,
+    path finder, path stage in complex128) on the Cu fcc cluster (a = 3.61 A, 6 A, K edge, NLEG 4): once on its own
+    classes, once after install() with the same potentials and phases.  The same paths, chi to 1e-9 of its largest
+    value."""
+    feffgpu, F = reference
+    import feffgpu.chain as chain
+    import feffgpu_b200
+    from feffgpu_b200 import workloads as W
+    pts = W.fcc_cluster(3.61, 6.0)
+    lines = ["TITLE Cu fcc a=3.61 cluster 6 A", "CONTROL 1 1 1 1 1 1", "PRINT 0 0 0 0 0 0", "EDGE K", "S02 1.0",
+             "NLEG 4", "RPATH 6.0", "", "POTENTIALS", "     0   29  Cu", "     1   29  Cu", "", "ATOMS"]
+    lines += [f"  {x:12.6f} {y:12.6f} {z:12.6f}  {0 if i == 0 else 1:d}" for i, (x, y, z) in enumerate(pts)]
+    inp = tmp_path / "feff.inp"
+    inp.write_text("\n".join(lines + ["END", ""]))
+    kf = np.arange(401) * 0.05
+    ref = chain.run(str(inp), device="cuda", kgrid=kf)
+    feffgpu_b200.install()
+    assert chain.GPUPathStage is feffgpu_b200.GPUPathStage
+    ours = chain.run(str(inp), device="cuda", kgrid=kf, pot=ref["pot"], phase=ref["phase"])
+    assert ours["counts"] == ref["counts"], (ours["counts"], ref["counts"])
+    e = np.abs(np.asarray(ours["chi"]) - np.asarray(ref["chi"])).max() / np.abs(np.asarray(ref["chi"])).max()
+    print(f"chain.run Cu fcc: paths {ref['counts']}; chi {e:.2e} against the reference's own classes; "
+          f"path stage {ref['timing']['chi']:.3f} s -> {ours['timing']['chi']:.3f} s")
+    assert e <= 1e-9
