@@ -8,8 +8,8 @@ degeneracy-weighted sum per copy.  The structure is a thermal bcc Fe frame in a 
 finder_tri.npz), four absorbers.  Compared: the path counts per leg count (equal), chi per copy and its gradient with
 respect to every position, both through the reference's checkpointed autograd -- complex128 to 1e-9 and 1e-7 of the
 largest value, complex64 to 2e-4 and 2e-3 (two FP32 chains in different orders).  The same for its
-MultipleScattering (rows per absorber, the exact gradient of a loss of the mean spectrum), and for its chain.run from a
-feff.inp (the Cu fcc cluster, complex128)."""
+MultipleScattering (rows per absorber, the exact gradient of a loss of the mean spectrum), its chain.run from a
+feff.inp (the Cu fcc cluster, complex128) and its MD-EXAFS EdgeSpectra (pair tables + multiple scattering)."""
 import dataclasses
 import sys
 from pathlib import Path
@@ -136,3 +136,35 @@ def test_reference_chain_with_this_package_installed(reference, tmp_path):
     print(f"chain.run Cu fcc: paths {ref['counts']}; chi {e:.2e} against the reference's own classes; "
           f"path stage {ref['timing']['chi']:.3f} s -> {ours['timing']['chi']:.3f} s")
     assert e <= 1e-9
+
+
+def test_reference_md_edge_spectra_with_this_package_installed(reference):
+    """The reference's MD-EXAFS front end, EdgeSpectra.spectrum (src/feffgpu/md/spectrum.py:101-340: its own
+    PairTables, whose two-leg tables come from the path stage, and MultipleScattering, complex64), on the triclinic
+    bcc Fe frame, eight absorbers, 3 legs within 5 A: the same path counts, chi and its single- and
+    multiple-scattering parts to 2e-4 of the largest value."""
+    feffgpu, F = reference
+    import feffgpu_b200
+    from feffgpu.md.spectrum import EdgeSpectra, phase_k_range
+    from feffgpu.pad import PhaseData as RefPhase
+    ours = phase("cfg4_fe_phase")
+    P = RefPhase(**{f.name: getattr(ours, f.name) for f in dataclasses.fields(RefPhase)})
+    z = npz("finder_tri")
+    pos, cell = z["pos"], z["cell"]
+    k = np.arange(int(min(20.0, phase_k_range(P)) / 0.05) + 1) * 0.05
+    absorbers = np.array([0, 31, 57, 102, 190, 250, 301, 400])
+    symbols = np.array(["Fe"] * len(pos))
+
+    def run():
+        es = EdgeSpectra(P, "Fe", {"Fe": 1}, ["Fe"], k, rpath=5.0, nleg=3, criteria=2.0, device="cuda")
+        return es.spectrum(pos, cell, absorbers, symbols)
+
+    ref = run()
+    feffgpu_b200.install()
+    got = run()
+    assert got.n_paths == ref.n_paths and got.n_short_pairs == ref.n_short_pairs
+    errs = {f: np.abs(getattr(got, f) - getattr(ref, f)).max() / np.abs(getattr(ref, f)).max()
+            for f in ("chi", "chi_ss", "chi_ms", "ss_histogram")}
+    print(f"EdgeSpectra: paths {ref.n_paths}; " + ", ".join(f"{f} {e:.2e}" for f, e in errs.items()))
+    assert errs["ss_histogram"] == 0.0
+    assert max(errs.values()) <= 2e-4
