@@ -9,7 +9,8 @@ finder_tri.npz), four absorbers.  Compared: the path counts per leg count (equal
 respect to every position, both through the reference's checkpointed autograd -- complex128 to 1e-9 and 1e-7 of the
 largest value, complex64 to 2e-4 and 2e-3 (two FP32 chains in different orders).  The same for its
 MultipleScattering (rows per absorber, the exact gradient of a loss of the mean spectrum), its chain.run from a
-feff.inp (the Cu fcc cluster, complex128) and its MD-EXAFS EdgeSpectra (pair tables + multiple scattering)."""
+feff.inp (the Cu fcc cluster, complex128), its MD-EXAFS EdgeSpectra (pair tables + multiple scattering) and its RMC
+GpuRmc (spectrum, misfit and five refinement steps)."""
 import dataclasses
 import sys
 from pathlib import Path
@@ -168,3 +169,40 @@ def test_reference_md_edge_spectra_with_this_package_installed(reference):
     print(f"EdgeSpectra: paths {ref.n_paths}; " + ", ".join(f"{f} {e:.2e}" for f, e in errs.items()))
     assert errs["ss_histogram"] == 0.0
     assert max(errs.values()) <= 2e-4
+
+
+def test_reference_rmc_with_this_package_installed(reference):
+    """The reference's RMC front end, GpuRmc (src/feffgpu/rmc/refine.py:36-260: its PairTables for single scattering,
+    MultipleScattering for 3-leg paths, complex64): the exact spectrum and misfit of the triclinic bcc Fe frame
+    against a target from a displaced copy, then five seeded gradient steps (sampled absorbers, SGD).  The same
+    spectrum to 2e-4 and misfit to 5e-4 relative (a ratio of differences of FP32 spectra); the refined positions to
+    1e-4 A."""
+    feffgpu, F = reference
+    import feffgpu_b200
+    from feffgpu.pad import PhaseData as RefPhase
+    from feffgpu.rmc.refine import GpuRmc
+    ours = phase("cfg4_fe_phase")
+    P = RefPhase(**{f.name: getattr(ours, f.name) for f in dataclasses.fields(RefPhase)})
+    z = npz("finder_tri")
+    pos, cell = z["pos"][None].astype(np.float32), z["cell"]
+    k = np.arange(301) * 0.05
+    moved = pos + np.random.default_rng(9).normal(0.0, 0.03, pos.shape).astype(np.float32)
+
+    def run():
+        target = GpuRmc(P, k, np.zeros(len(k)), 0.0, torch.tensor(cell), window=(3.0, 14.0), rmax=5.0, nleg=3,
+                        device="cuda").spectrum_only(moved)[0].double().cpu().numpy()
+        rmc = GpuRmc(P, k, target, 0.0, torch.tensor(cell), window=(3.0, 14.0), rmax=5.0, nleg=3, device="cuda")
+        chi, mis = rmc.spectrum_only(pos)
+        out, _ = rmc.refine(pos, 5, lr=0.003, ms_absorbers=64, value_every=5, refresh_every=250, seed=2,
+                            verbose=False, log=lambda *a, **k: None)
+        return chi.double().cpu().numpy(), mis, out
+
+    chi_r, mis_r, pos_r = run()
+    feffgpu_b200.install()
+    chi_b, mis_b, pos_b = run()
+    e_chi = np.abs(chi_b - chi_r).max() / np.abs(chi_r).max()
+    e_mis = abs(mis_b - mis_r) / abs(mis_r)
+    e_pos = np.abs(pos_b - pos_r).max()
+    print(f"GpuRmc: chi {e_chi:.2e}, misfit {mis_r:.4e} ({e_mis:.2e}), positions after 5 steps {e_pos:.2e} A "
+          f"(moved {np.abs(pos_r - pos).max():.2e} A)")
+    assert e_chi <= 2e-4 and e_mis <= 5e-4 and e_pos <= 1e-4
