@@ -13,7 +13,8 @@ own two absorbers (weak scaling, no collective on the data path).
 Beside the headline line's value: the end-to-end form (host buffers, copies timed), forward+backward, the plain FP64
 form, the MD-EXAFS batch (bcc Fe, 500 frames x 32 absorbers in one launch) and the RMC refinement (NiO, two edges,
 each step one CUDA graph replay), the path finder itself, the single-scattering pair tables and the reference's own
-GPUPathStage on this GPU (when it is installed under baseline/_ref), each in its own key of the JSON line.
+GPUPathStage on this GPU and on the host cores (when it is installed under baseline/_ref), each in its own key of the
+JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -400,6 +401,55 @@ def reference_gpu_leg(args, P, groups, dev, ours: dict):
     return out
 
 
+def reference_cpu_leg(P, groups, per_leg: int = 48):
+    """The reference's own GPUPathStage on the host cores (device="cpu", torch's default thread count, as the
+    reference requires): per leg count its first `per_leg` paths through cchi -> chi_fine -> weighted sum, timed
+    after a warm-up call and extrapolated by the paths of that leg count; complex64 and complex128."""
+    import dataclasses
+    import torch
+    ref = ROOT / "baseline" / "_ref"
+    if not (ref / "feffgpu" / "stage.py").exists():
+        return {"unavailable": "reference not installed under baseline/_ref"}
+    sys.path.insert(0, str(ref))
+    try:
+        from feffgpu.pad import PhaseData as RefPhase
+        from feffgpu.stage import GPUPathStage as RefStage
+    except Exception as err:                                   # noqa: BLE001 - report, do not fail the bench
+        return {"unavailable": f"reference import failed: {err!r}"[:200]}
+    finally:
+        sys.path.remove(str(ref))
+    refP = RefPhase(**{f.name: getattr(P, f.name) for f in dataclasses.fields(RefPhase)})
+    by_leg: dict = {}
+    for c, ip, deg, _row in groups:
+        by_leg.setdefault(c.shape[1], []).append((c, ip, deg))
+    by_leg = {n: tuple(np.concatenate([x[i] for x in v]) for i in range(3)) for n, v in sorted(by_leg.items())}
+    n_paths = sum(len(v[0]) for v in by_leg.values())
+    out = {"source": "the reference's GPUPathStage(device='cpu'), pip-installed unmodified into baseline/_ref",
+           "cores": torch.get_num_threads()}
+    for key, dtype in (("fwd_c64", torch.complex64), ("fwd_c128", torch.complex128)):
+        stage = RefStage(refP, device="cpu", dtype=dtype)
+        S = stage.linear_matrix(Q)
+        total, sampled = 0.0, 0
+        with torch.no_grad():
+            for n, (c, ip, deg) in by_leg.items():
+                m = min(len(c), per_leg)
+                x = torch.as_tensor(c[:m]).to(stage.rdtype)
+                ipt = torch.as_tensor(ip[:m], dtype=torch.long)
+                w = torch.as_tensor(deg[:m], dtype=torch.float64)[:, None]
+
+                def step():
+                    return (w * stage.chi_fine(*stage.cchi(x, ipt), Q, S, "feff").to(torch.float64)).sum(0)
+
+                step()
+                t0 = time.perf_counter()
+                step()
+                total += (time.perf_counter() - t0) * len(c) / m
+                sampled += m
+        out[key] = {"value": n_paths * NK / total, "unit": UNIT, "s_full_batch": total,
+                    "sample": f"{sampled} of {n_paths} paths (the first {per_leg} of every leg count), extrapolated"}
+    return out
+
+
 def pairs_leg(args, dev, world, rank):
     """Single scattering from pair tables: rock-salt NiO 8^3 cells (5 % vacancies, 0.1 A disorder, 3,891 atoms), Ni K
     tables on r = 1.5..6 A step 0.002 (2,251 points x 401 k, one fused-stage call), then the all-pairs
@@ -515,7 +565,7 @@ def main():
     ap.add_argument("--md-frames", type=int, default=500, help="frames of the MD-batch leg (0: skip it)")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (profiling runs)")
     ap.add_argument("--rmc-steps", type=int, default=200, help="steps of the RMC leg (0: skip it)")
-    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's own stage on this GPU")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's own stage (GPU and host legs)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -637,10 +687,12 @@ def main():
             "peak_source": "measured on this GPU by fg_fp32_fma_peak (FFMA chains on every SM); "
                            "MEASURED_PEAKS.json holds no FP32 figure"}
 
-    cpu = None
+    cpu = ref_cpu = None
     if rank == 0 and not args.no_cpu:
         v, desc = cpu_sample(P, groups, budget_s=args.cpu_budget, nthreads=nthreads)
         cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc}
+        if not args.no_ref_gpu:
+            ref_cpu = reference_cpu_leg(P, groups)
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -650,7 +702,7 @@ def main():
                        l2="flushed between steps (256 MB write)"),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "fwd_bwd": fwd_bwd, "plain_fp64": plain,
         "md_batch": md, "rmc_refinement": rmc, "path_finder": pf,
-        "pair_tables": pairs, "reference_gpu": ref_gpu,
+        "pair_tables": pairs, "reference_gpu": ref_gpu, "reference_cpu": ref_cpu,
         "autotune": {"fwd_warps": stage._launch[0], "bwd_warps": stage._launch[1],
                      "timed": [{"kind": k, "warps": w_, "ms": round(t_, 3)} for sig, k, w_, t_ in tuner.log
                                if sig.split("|")[1] == "p0"]},
