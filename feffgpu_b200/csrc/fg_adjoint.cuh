@@ -972,9 +972,9 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
         if (frame) reframe_path<R>(g, nleg, lane, frame);
         ParGrad pg;
         for (int j = 0; j <= kMaxLeg; ++j) pg.ri[j] = pg.beta[j] = pg.eta[j] = 0.0;
-        for (int e0 = 0; e0 < E; e0 += 32) {
+        for (int e0 = first_chunk(E); e0 < E; e0 += 32) {
             const int e = e0 + lane;
-            if (e < E) path_energy_adj<R, EDGE>(g, dh, dhd, as.dterm_db, T, e, nleg, gbar[p * E + e], pg);
+            if (e >= 0 && e < E) path_energy_adj<R, EDGE>(g, dh, dhd, as.dterm_db, T, e, nleg, gbar[p * E + e], pg);
         }
         // fixed-order warp reduction of the per-lane sums
         for (int j = 1; j <= nleg; ++j) {

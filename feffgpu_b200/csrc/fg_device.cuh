@@ -163,6 +163,11 @@ __host__ __device__ constexpr int dcanon(int MM, int m1, int m2)
 {
     return m1 == 0 ? m2 : (MM + 1) + (m1 - 1) * (2 * MM + 1) + (m2 + MM);
 }
+// First energy of a path's loop over chunks of 32 energies (a lane per energy).  When E is not a multiple of 32 the
+// partial chunk comes first, over the lowest energies, whose partial-wave limits are the smallest, rather than last,
+// over the highest and most expensive: its idle lanes then wait on the cheapest chunk (for E = 401 the chunks are
+// -15..16, 17..48, ..., 369..400).
+__host__ __device__ constexpr int first_chunk(int E) { return (E % 32) ? (E % 32) - 32 : 0; }
 __host__ __device__ constexpr int ncanon(int MM) { return (MM + 1) + MM * (2 * MM + 1); }
 // Row stride of the rotation tables: the canonical entries rounded up to a 16-byte multiple of FP32 (and of FP64)
 // so rows load as float4 / double2 (28 for MM = 3 instead of a 32-entry row: less shared memory per warp, more of

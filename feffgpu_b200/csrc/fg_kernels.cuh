@@ -64,9 +64,9 @@ __global__ void __launch_bounds__(256) k_cchi(Tables<R> T, const CT *__restrict_
     const int MM = nleg == 2 ? K::MMSS : K::MMMS;
     for (int64_t p = (int64_t)blockIdx.x * nw + w; p < B; p += (int64_t)gridDim.x * nw) {
         path_setup<R, CT>(g, dh, T, coords + p * nleg * 3, ipots + p * nleg, nleg, lane, bad, MM);
-        for (int e0 = 0; e0 < E; e0 += 32) {
+        for (int e0 = first_chunk(E); e0 < E; e0 += 32) {
             const int e = e0 + lane;
-            if (e < E) out[p * E + e] = path_energy<R, EDGE>(g, dh, T, e, nleg);
+            if (e >= 0 && e < E) out[p * E + e] = path_energy<R, EDGE>(g, dh, T, e, nleg);
         }
         if (lane == 0) reff[p] = (R)(g.reff * kBohr);
         __syncwarp();
@@ -195,9 +195,9 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
         const int nleg = P.nleg[p];
         path_setup<R, double>(g, dh, T, P.coords + p * P.nleg_max * 3, P.ipots + p * P.nleg_max, nleg, lane, bad,
                               nleg == 2 ? K::MMSS : K::MMMS);
-        for (int e0 = 0; e0 < E; e0 += 32) {
+        for (int e0 = first_chunk(E); e0 < E; e0 += 32) {
             const int e = e0 + lane;
-            if (e < E) {
+            if (e >= 0 && e < E) {
                 const C2<R> v = path_energy<R, EDGE>(g, dh, T, e, nleg);
                 cbuf[e] = v;
                 if (cchi_save) cchi_save[p * E + e] = v;
