@@ -29,6 +29,8 @@ The reference is imported read-only from its source tree and run on the CPU in F
   bcc Fe frame in a triclinic cell (the supercell sheared by SHEAR, rmax 5, 4 legs), the reference finder given the
   3 x 3 cell.
 * feffdat_W.npz -- FEFF's own feff0001..0008.dat of the W case: path geometry and the seven columns.
+* larch_W.npz -- the reference stage's cubic-spline interpolation matrix and its "larch"-convention fine-grid chi of
+  the W case's stored paths.
 * pairs_nio.npz -- the reference's single-scattering pair tables, histogram, all-pairs spectrum and its position
   gradient on a thermal rock-salt NiO supercell (Ni K edge); pairs_nio_tri.npz -- the same in a triclinic cell.
 * cfg2_phase.npz -- Fe K-edge phase tables (potentials Fe*, Fe, O, Pt, lmax 24) of a cluster cut from the seeded
@@ -487,6 +489,24 @@ def make_pairs_cell():
     print(f"pairs_nio_tri: nr {pt.nr}, {time.time() - t:.1f} s")
 
 
+def make_larch():
+    """larch_W.npz -- the reference stage's cubic-spline ("larch") fine grid on the W case: its spline_matrix
+    (src/feffgpu/stage.py:341-351) for q = 0..20 1/A step 0.05 and chi_fine(..., "larch") of the stored paths' cchi."""
+    from feffgpu.pad import read_phase_pad
+    P = read_phase_pad(str(CASES["W"] / "phase.pad"))
+    g = ref_stage(P)
+    z = np.load(HERE / "case_W.npz")
+    q = np.arange(401) * 0.05
+    S = g.spline_matrix(q)
+    out = {"q": q, "S": S.numpy()}
+    for nleg in (2, 3, 4):
+        cc = torch.tensor(z[f"ref_cchi_{nleg}"])
+        rf = torch.tensor(z[f"ref_reff_{nleg}"])
+        out[f"chi_{nleg}"] = g.chi_fine(cc, rf, q, S, "larch").numpy()
+    np.savez_compressed(HERE / "larch_W.npz", **out)
+    print("larch_W written")
+
+
 def make_feffdat():
     """feffdat_W.npz -- FEFF's own per-path column files feff0001..0008.dat of the W case (tests/data/W): each path's
     geometry (absorber first), potentials, degeneracy and reff from the file header, and its seven columns (k,
@@ -514,7 +534,7 @@ def main():
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
     want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder", "pairs", "pairs_tri",
-                             "feffdat"])
+                             "feffdat", "larch"])
     with tempfile.TemporaryDirectory() as tmp:
         if "cases" in want:
             import shutil
@@ -544,6 +564,8 @@ def main():
             make_pairs()
         if "pairs_tri" in want:
             make_pairs_cell()
+        if "larch" in want:
+            make_larch()
         if "feffdat" in want:
             make_feffdat()
 

@@ -189,3 +189,24 @@ def test_edge_cases():
     b = PathBatch([(coords, ipots, None, np.array([0, 2]))], nrows=3, device="cuda")
     rows = st.chi_reduce(b, np.arange(1, 101) * 0.1)
     assert rows.shape == (3, 100) and torch.all(rows[1] == 0)
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_larch_spline_convention_equals_reference(dtype):
+    """spline_matrix (scipy UnivariateSpline s=0, the reference's stage.py:341-351) and chi_fine(..., "larch") on the
+    W case's stored paths against the reference's (tests/golden/larch_W.npz): the matrix to 1e-12, chi to 1e-10 of its
+    largest value in FP64 (the mixed form: 5e-5; its spline weights are FP32, as the reference's complex64 form casts
+    them, and the spline's weights alternate in sign, so their rounding is not damped as linear weights' is)."""
+    from feffgpu_b200 import GPUPathStage
+    z = npz("larch_W")
+    case = npz("case_W")
+    st = GPUPathStage(phase("case_W"), device="cuda", dtype=dtype)
+    S = st.spline_matrix(z["q"])
+    assert np.abs(S.double().cpu().numpy() - z["S"]).max() <= (1e-12 if dtype == torch.complex128 else 1e-6)
+    for nleg in (2, 3, 4):
+        cc = torch.tensor(case[f"ref_cchi_{nleg}"], device="cuda").to(dtype)
+        rf = torch.tensor(case[f"ref_reff_{nleg}"], device="cuda")
+        chi = st.chi_fine(cc, rf, z["q"], convention="larch").double().cpu().numpy()
+        e = _rel(chi, z[f"chi_{nleg}"])
+        print(f"larch nleg {nleg} {dtype}: chi vs reference {e:.2e}")
+        assert e <= (1e-10 if dtype == torch.complex128 else 5e-5), (nleg, e)
