@@ -126,3 +126,28 @@ def test_frames_batched_equal_per_frame():
             for x, y in zip(v[:5], w[:5]):
                 assert torch.equal(x, y[sel]), (fr, nleg)
             assert torch.equal(v[5] + fr * A, w[5][sel])
+
+
+def test_symmetry_degeneracy_totals_on_ideal_lattice():
+    """FEFF's merge of symmetry-equivalent paths on an ideal simple cubic cluster: single scattering in its three
+    shells (6, 8, 12); triangles through two first neighbours total 24, first-second neighbour triangles 48."""
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    from tests.test_oracle_pathfinder import check_lattice_degeneracies, simple_cubic
+    f = GPUPathFinder(phase("case_W"), device="cuda", rmax=5.32, nlegmax=3, critpw=0.0)
+    pos = simple_cubic()
+    kept, _ = f.enumerate(pos, None, 0, np.ones(len(pos), int))
+    check_lattice_degeneracies(kept, lambda c, d: GPUPathFinder.degenerate_total(c, d).cpu().numpy())
+
+
+def test_paths_of_up_to_eight_legs_equal_a_plain_enumeration():
+    """Every path of up to eight legs of a compact 7-atom cluster (rmax 7.4 A, no merge, no cut) against a plain
+    recursive enumeration; nine legs is the largest count accepted."""
+    from feffgpu_b200.pathfinder import NLEG_MAX, GPUPathFinder
+    from tests.test_oracle_pathfinder import check_plain_enumeration, compact_cluster, plain_enumeration
+    pos = compact_cluster()
+    f = GPUPathFinder(phase("case_W"), device="cuda", rmax=7.4, nlegmax=9, critpw=0.0, merge_degenerate=False)
+    kept, _ = f.enumerate(pos, None, 0, np.ones(len(pos), int))
+    check_plain_enumeration(kept, plain_enumeration(pos, 7.4))
+    assert NLEG_MAX == 9
+    with pytest.raises(ValueError, match="between 2 and 9"):
+        GPUPathFinder(phase("case_W"), device="cuda", rmax=7.4, nlegmax=10)
