@@ -76,3 +76,36 @@ def test_single_scattering_and_gradient(name):
             fd = float(((pt.single_scattering(torch.tensor(xp, device="cuda")) -
                          pt.single_scattering(torch.tensor(xm, device="cuda"))) * w).sum()) / (2 * h)
             assert abs(fd - grad[c, i, q]) <= 1e-6 * np.abs(grad).max(), (idx, fd, grad[c, i, q])
+
+
+def test_pair_tables_equal_the_two_leg_paths_of_the_path_stage():
+    """One element, every atom an absorber (a thermal bcc W block, periodic, e0 = 2 eV): the histogram of pair
+    distances times the tables equals the two-leg paths of every absorber through the path finder and the fused stage,
+    to the tables' 0.002 A grid (2e-3 of the largest value over k = 3..20; the reference's own check of its
+    PairTables, tests/test_shared_layer.py:116-137 there), and is differentiable in the positions."""
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    from feffgpu_b200.pairs import ETOK, PairTables
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    from feffgpu_b200 import workloads as W
+    P = phase("case_W")
+    sites, box = W.bcc_supercell(4, 3.1652)
+    pos = sites + np.random.default_rng(0).normal(0, 0.05, sites.shape)
+    k = np.arange(401) * 0.05
+    pt = PairTables(P, k, np.zeros(len(k)), 2.0, box=box, rmax=6.0, device="cuda", dtype=torch.complex64)
+    x = torch.tensor(pos, device="cuda", dtype=torch.float32)[None]
+    chi = pt.single_scattering(x).cpu().numpy()
+    f = GPUPathFinder(P, device="cuda", rmax=6.0, nlegmax=2, critpw=0.0, merge_degenerate=False)
+    res = f.enumerate_many(pos, box, np.arange(len(pos)), np.ones(len(pos), int))
+    coords, ipots, deg, _xp, _atoms, _slot = res["paths"][2]
+    st = GPUPathStage(P, device="cuda", dtype=torch.complex64)
+    batch = PathBatch([(coords.double(), ipots, deg.double(), None)], nrows=1, device="cuda")
+    en = k ** 2 - 2.0 * ETOK
+    q = np.sign(en) * np.sqrt(np.abs(en))
+    ref = st.chi_reduce(batch, q)[0].cpu().numpy() / len(pos)
+    sel = (k > 3) & (k < 20)
+    e = np.abs(chi - ref)[sel].max() / np.abs(ref[sel]).max()
+    print(f"pair tables vs two-leg paths of the stage: {e:.2e}")
+    assert e < 2e-3
+    xg = x.clone().requires_grad_(True)
+    (pt.single_scattering(xg) ** 2).sum().backward()
+    assert torch.isfinite(xg.grad).all() and float(xg.grad.abs().max()) > 0
