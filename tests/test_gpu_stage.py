@@ -210,3 +210,51 @@ def test_larch_spline_convention_equals_reference(dtype):
         e = _rel(chi, z[f"chi_{nleg}"])
         print(f"larch nleg {nleg} {dtype}: chi vs reference {e:.2e}")
         assert e <= (1e-10 if dtype == torch.complex128 else 5e-5), (nleg, e)
+
+
+def test_gaussian_frames_damp_the_first_shell_like_the_sigma2_factor():
+    """Frames of independent Gaussian displacements (s = 0.04 A per component, 40 frames of a bcc W block, every atom
+    an absorber, the first shell's two-leg paths through the batched finder and the fused stage): the frame average
+    decays against the ideal lattice like exp(-2 k^2 sigma^2) with sigma^2 = 2 s^2 (the reference's check of its MD
+    averaging, tests/md/test_spectrum.py:166-201 there), and its envelope equals that of the ideal lattice's spectrum
+    with the per-path factor exp(-2 sigma^2 q^2) of sigma^2 = 2 s^2 to 3 % over k = 3..14 (the spectra themselves
+    differ by the phase of the mean-distance shift of a 3D Gaussian, sigma_perp^2 / R, which the factor leaves out).
+    Envelopes: the magnitude of the analytic signal (scipy's hilbert) on q = 0.05..19.95."""
+    from scipy.signal import hilbert
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    from feffgpu_b200 import workloads as W
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    s, F = 0.04, 40
+    sites, box = W.bcc_supercell(4, 3.1652)
+    n = len(sites)
+    frames = sites[None] + np.random.default_rng(1).normal(0.0, s, (F, n, 3))
+    P = phase("case_W")
+    f = GPUPathFinder(P, device="cuda", rmax=2.95, nlegmax=2, critpw=0.0, merge_degenerate=False)
+    st = GPUPathStage(P, device="cuda", dtype=torch.complex128)
+    q = np.arange(1, 400) * 0.05          # to 19.95: the envelope's edge effects stay away from the fit window
+
+    def rows(pos, sigma2=None):
+        fr = pos if pos.ndim == 3 else pos[None]
+        res = f.enumerate_many(fr, box, np.arange(n), np.ones(n, int))
+        coords, ipots, deg, _xp, _atoms, slot = res["paths"][2]
+        b = PathBatch([(coords.double(), ipots, deg.double(), torch.div(slot, n, rounding_mode="floor"))],
+                      nrows=fr.shape[0], device="cuda")
+        s2 = None if sigma2 is None else torch.full((b.n,), sigma2, device="cuda", dtype=torch.float64)
+        return st.chi_reduce(b, q, sigma2=s2).cpu().numpy() / n
+
+    avg = rows(frames).mean(0)
+    ideal = rows(sites)[0]
+    damped = rows(sites, 2 * s * s)[0]
+    m = (q >= 5.0) & (q <= 14.0)
+    env = lambda y: np.abs(hilbert(y))
+    y = np.log(env(avg)[m] / env(ideal)[m])
+    A = np.vstack([np.ones(m.sum()), q[m] ** 2]).T
+    (c, slope), *_ = np.linalg.lstsq(A, y, rcond=None)
+    sigma2 = -slope / 2
+    print(f"sigma^2 from the frames' spectrum {sigma2:.5f} (2 s^2 = {2 * s * s:.5f}), offset {c:.3f}")
+    assert np.abs(y - A @ np.array([c, slope])).max() < 0.05 and abs(c) < 0.03
+    assert abs(sigma2 - 2 * s * s) < 0.1 * 2 * s * s
+    w = (q >= 3.0) & (q <= 14.0)
+    e = np.abs(env(avg)[w] / env(damped)[w] - 1.0).max()
+    print(f"envelope of the frame average vs the sigma^2 factor on the ideal lattice: {e:.3f}")
+    assert e < 0.03
