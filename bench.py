@@ -17,6 +17,7 @@ GPUPathStage on this GPU and on the host cores (when it is installed under basel
 JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --frontends      # the reference's MD and RMC front ends, its classes vs install()
 
 --impl reference times the reference's path stage on the CPU (the FP64 oracle port of its algorithm with all host
 threads) on a bounded stratified sample of the same workload, rank 0 only.
@@ -454,6 +455,72 @@ def reference_cpu_leg(P, groups, per_leg: int = 48):
     return out
 
 
+def frontends_leg(dev):
+    """The reference's own front ends (installed unmodified under baseline/_ref) timed on its own classes and then
+    after feffgpu_b200.install(), each after one warm-up call, wall clock with the device synchronised:
+    * MD: EdgeSpectra.spectrum of one thermal bcc Fe frame (16^3 cells, 8192 atoms, sigma 0.08 A) for 32 absorbers,
+      paths of up to 3 legs within 5.5 A (src/feffgpu/md/spectrum.py:303-340);
+    * RMC: MultipleScattering.full_pass and full_gradient of the same frame for 32 absorbers, 3 legs, critpw 2
+      (src/feffgpu/exafs/forward.py:691-723).
+    The front ends' own orchestration (per-absorber finder calls, chunk loops, host syncs) is timed too: this is what
+    the one-line drop-in buys, not the fused API's figure."""
+    import dataclasses
+    import torch
+    ref = ROOT / "baseline" / "_ref"
+    if not (ref / "feffgpu" / "md" / "spectrum.py").exists():
+        return {"unavailable": "reference not installed under baseline/_ref"}
+    sys.path.insert(0, str(ref))
+    try:
+        import feffgpu.exafs.forward as F
+        from feffgpu.md.spectrum import EdgeSpectra
+        from feffgpu.pad import PhaseData as RefPhase
+    except Exception as err:                                   # noqa: BLE001 - report, do not fail the bench
+        return {"unavailable": f"reference import failed: {err!r}"[:200]}
+    import feffgpu_b200
+    from feffgpu_b200 import workloads as W
+    from feffgpu_b200.pad import phase_from_npz
+    ours = phase_from_npz(np.load(ROOT / "tests" / "golden" / "cfg4_fe_phase.npz"), prefix="ph_")
+    P = RefPhase(**{f.name: getattr(ours, f.name) for f in dataclasses.fields(RefPhase)})
+    base, L = W.bcc_supercell(16, 2.87)
+    pos = W.thermal(base, 0.08, seed=11)
+    cell = np.eye(3) * L
+    absorbers = np.random.default_rng(12).choice(len(pos), 32, replace=False)
+    symbols = np.array(["Fe"] * len(pos))
+    k = np.arange(401) * 0.05
+
+    def wall(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize(dev)
+        return (time.perf_counter() - t0) * 1e3
+
+    def md():
+        es = EdgeSpectra(P, "Fe", {"Fe": 1}, ["Fe"], k, rpath=5.5, nleg=3, criteria=2.0, device=str(dev))
+        return lambda: es.spectrum(pos, cell, absorbers, symbols)
+
+    def rmc():
+        ms = F.MultipleScattering(P, k, 0.0, torch.tensor(cell), rmax=5.5, critpw=2.0, nlegmax=3, device=str(dev))
+        x = torch.tensor(pos, device=dev, dtype=torch.float32)
+        ms.enumerate(x[None], absorbers=absorbers)
+        w = torch.tensor(np.random.default_rng(7).normal(size=len(k)), device=dev)
+
+        def step():
+            ms.full_pass(x)
+            ms.full_gradient(x, lambda chi: (chi.double() * w).sum())
+        return step
+
+    out = {"workload": "bcc Fe 16^3 cells (8192 atoms), 32 absorbers, 3 legs within 5.5 A, 401 k"}
+    res = {"reference": {"md_frame_ms": wall(md()), "rmc_pass_and_gradient_ms": wall(rmc())}}
+    feffgpu_b200.install()
+    res["installed"] = {"md_frame_ms": wall(md()), "rmc_pass_and_gradient_ms": wall(rmc())}
+    out.update(res)
+    out["speedup"] = {key: res["reference"][key] / res["installed"][key] for key in res["reference"]}
+    sys.path.remove(str(ref))
+    return out
+
+
 def pairs_leg(args, dev, world, rank):
     """Single scattering from pair tables: rock-salt NiO 8^3 cells (5 % vacancies, 0.1 A disorder, 3,891 atoms), Ni K
     tables on r = 1.5..6 A step 0.002 (2,251 points x 401 k, one fused-stage call), then the all-pairs
@@ -570,11 +637,18 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (profiling runs)")
     ap.add_argument("--rmc-steps", type=int, default=200, help="steps of the RMC leg (0: skip it)")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's own stage (GPU and host legs)")
+    ap.add_argument("--frontends", action="store_true",
+                    help="only time the reference's MD and RMC front ends on its own classes and after install()")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     nthreads = os.cpu_count() or 1
+
+    if args.frontends:
+        import torch
+        print(json.dumps({"frontends": frontends_leg(torch.device("cuda", 0))}))
+        return
 
     if args.impl == "reference":
         if rank != 0:
