@@ -198,8 +198,8 @@ class GPUPathFinder:
         length = torch.sqrt(cr[:, 0] * cr[:, 0] + cr[:, 1] * cr[:, 1] + cr[:, 2] * cr[:, 2]).contiguous()
         groups = {2: (seq, slot, torch.ones(total, device=dev))}
         # multiple scattering needs two candidates (pathfinder.py:237, 243, 262)
-        grow = cnt[slot.long()] > 1
-        seq, slot, length = seq[grow].contiguous(), slot[grow].contiguous(), length[grow].contiguous()
+        grow = torch.nonzero(cnt[slot.long()] > 1).squeeze(1)         # one index vector: one sync for three gathers
+        seq, slot, length = seq.index_select(0, grow), slot.index_select(0, grow), length.index_select(0, grow)
         two_r = float(np.float32(2 * self.rmax))
         for m in range(1, self.nlegmax - 1):
             P = int(seq.shape[0])
@@ -227,8 +227,8 @@ class GPUPathFinder:
             deg = torch.empty(Cn, device=dev, dtype=torch.float32)
             _lib.check(lib.fg_pf_terminal(Cn, m + 1, seq.data_ptr(), slot.data_ptr(), off.data_ptr(), keep.data_ptr(),
                                           deg.data_ptr(), st))
-            k = keep.bool()
-            groups[m + 2] = (seq[k].contiguous(), slot[k].contiguous(), deg[k])
+            k = torch.nonzero(keep).squeeze(1)
+            groups[m + 2] = (seq.index_select(0, k), slot.index_select(0, k), deg.index_select(0, k))
         out = {}
         for nleg, (s, sl, dg) in groups.items():
             d = self._describe(int(s.shape[0]), nleg, s, sl, off, cand_rel, cand_atom, ipot_of, ab,
@@ -299,8 +299,9 @@ class GPUPathFinder:
             else:
                 dtot = dg
             frac = 100 * dtot * v["xport"] / refs[v["slot"].long()]
-            k = frac >= self.critpw
-            paths[nleg] = (v["coords"][k], v["ipots"][k], dg[k], v["xport"][k], v["atoms"][k], v["slot"][k])
+            k = torch.nonzero(frac >= self.critpw).squeeze(1)
+            paths[nleg] = tuple(t.index_select(0, k) for t in (v["coords"], v["ipots"], dg, v["xport"], v["atoms"],
+                                                                v["slot"]))
         return {"paths": paths, "ref": refs}
 
     def _windows(self, out, A):
