@@ -222,3 +222,52 @@ def test_cfg1_end_to_end_from_the_path_finder(dtype, tol):
     R = _R(K401, z["ref_chi"], rows)
     print(f"cfg1 from the path finder {dtype}: R {R:.2e}")
     assert R <= tol
+
+
+def test_path_model_and_graph_in_a_triclinic_cell():
+    """PathModel and GraphedRefinement with a triclinic cell (the bcc Fe frame of tests/golden/finder_tri.npz): the
+    paths of four absorbers from the CUDA finder (the cell's minimum image, FP32), held as atom indices and rebuilt by
+    the model's FP64 minimum image of the cell, give the finder's coordinates to 1e-5 A and the same rows to 1e-6;
+    two graph-replayed refinement steps equal the same steps run eagerly."""
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    from feffgpu_b200.model import GraphedRefinement, PathModel
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    from feffgpu_b200.rspace import FitWindow, RSpaceMisfit
+    z = npz("finder_tri")
+    pos, cell = z["pos"], z["cell"]
+    P = phase("cfg4_fe_phase")
+    f = GPUPathFinder(P, device="cuda", rmax=5.0, nlegmax=4, critpw=2.0)
+    res = f.enumerate_many(pos, cell, np.array([0, 57, 190, 301]), np.ones(len(pos), int))
+    absorbers = np.array([0, 57, 190, 301])
+    st = GPUPathStage(P, device="cuda", dtype=torch.complex64)
+    gs, cg = [], []
+    for nleg, (coords, ipots, deg, _xp, atoms, slot) in sorted(res["paths"].items()):
+        ab = torch.as_tensor(absorbers, device="cuda")[slot.long()][:, None]
+        gs.append((torch.cat([ab, atoms], 1).cpu().numpy(), ipots.cpu().numpy(), deg.cpu().numpy(),
+                   np.zeros(len(deg), int)))
+        cg.append((coords.double(), ipots, deg.double(), None))
+    model = PathModel(st, gs, pos, nrows=1, box=cell)
+    x = torch.tensor(pos, device="cuda")
+    mc = model.coords(x)
+    fc = PathBatch(cg, nrows=1, device="cuda").coords
+    assert torch.abs(mc - fc).max() < 1e-5
+    q = torch.tensor(K401, device="cuda")
+    S = st.linear_matrix(K401).double().contiguous()
+    with torch.no_grad():
+        rows = model.rows(x, q, S)
+        ref = st.chi_reduce(PathBatch(cg, nrows=1, device="cuda"), q, S)
+    assert torch.abs(rows - ref).max() <= 1e-6 * torch.abs(ref).max()
+    target = (model.rows(torch.tensor(pos + 0.02, device="cuda"), q, S)[0]).detach()
+    mis = RSpaceMisfit(len(K401), target, FitWindow(kmin=3.0, kmax=14.0, rmin=1.0, rmax=5.0))
+    g = GraphedRefinement([(model, q, S, mis)], pos, lr=0.002)
+    eager = torch.tensor(pos, device="cuda", requires_grad=True)
+    opt = torch.optim.Adam([eager], lr=0.002, capturable=True)
+    for _ in range(2):
+        g.step()
+        opt.zero_grad()
+        loss = mis(model.rows(eager, q, S).mean(0, keepdim=True))[0]
+        loss.backward()
+        opt.step()
+        torch.cuda.synchronize()
+        assert abs(float(g.loss) - float(loss)) <= 1e-9 * abs(float(loss))
+    assert torch.allclose(g.pos.detach(), eager.detach(), rtol=0, atol=1e-9)
