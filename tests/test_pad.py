@@ -1,5 +1,4 @@
 """The phase-file boundary: PhaseData fields, the packed-ASCII reader, npz round trip, resampling."""
-from pathlib import Path
 
 import numpy as np
 import pytest
@@ -7,8 +6,6 @@ import pytest
 from feffgpu_b200.pad import PhaseData, load_phase, phase_from_npz, phase_to_arrays, read_phase_pad, resample_phase
 from oracle import oracle as O
 from tests.fixtures import GOLDEN, npz, phase
-
-REF_L001 = Path("/root/reference/data/validation/L001/phase.pad")
 
 
 def test_reader_matches_the_reference_tables():
