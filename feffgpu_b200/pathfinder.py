@@ -6,7 +6,10 @@ Same constructor and ``enumerate(pos, box, absorber, ipot)`` output as the refer
 every frame of an MD or RMC job in one set of launches.  The enumeration, the path geometry, the plane-wave
 importance and the degeneracy keys are CUDA kernels (``csrc/fg_paths.cu``, C ABI ``fg_pf_*``); the merges and the
 importance cut are index bookkeeping done here with torch on the device (sorts, unique, gathers), the greedy
-length windows of the accidental-degeneracy merge on the host (``fg_pf_windows``).
+length windows of the accidental-degeneracy merge on the host (``fg_pf_windows``).  A call for one absorber (how
+the reference's front ends call it) does the merges and the cut on the host after one copy of the fields they
+read, with the same arithmetic, and gathers the kept paths on the device: a few hundred paths are not worth the
+launch and synchronisation latency of the device version's many small steps.
 
 Algorithm (pathfinder.py:159-279): a path of nleg legs is a sequence of nleg - 1 intermediates (the absorber's
 candidates -- atoms within rmax, minimum image, in atom order -- then the absorber itself), first and last a
@@ -252,7 +255,94 @@ class GPUPathFinder:
                                                 _ptr(key), st))
         return {"coords": coords, "ipots": ipots, "atoms": atoms, "rtot": rtot, "xport": xport, "key": key}
 
+    def _merge_and_cut_one(self, out, off):
+        """_merge_and_cut for a single absorber slot, on the host after one copy of the fields the merges read: the
+        reference's front ends call the finder once per absorber, and for a few hundred paths the device version is
+        bound by the launch and synchronisation latency of its many small steps.  Every step is the device version's
+        in the same FP32 arithmetic and order (the kept paths are bit-identical, asserted against enumerate_many)."""
+        dev = self.device
+        legs = sorted(out)
+        nb = {n: int(out[n]["rtot"].shape[0]) for n in legs}
+        f32 = [torch.stack([out[n]["xport"], out[n]["deg"].to(torch.float32)], 1).reshape(-1) for n in legs]
+        f32.append(out[2]["coords"][:, 1].reshape(-1))
+        f32.append(torch.cat([out[n]["rtot"] for n in legs]))
+        i64 = [off.reshape(-1), out[2]["ipots"][:, 1].reshape(-1)]
+        keyed = [n for n in legs if n > 2 and out[n]["key"] is not None]
+        i64 += [out[n]["key"].reshape(-1) for n in keyed]
+        hf = torch.cat(f32).cpu().numpy()
+        hi = torch.cat(i64).cpu().numpy()
+        s = 0
+        xport, deg = {}, {}
+        for n in legs:
+            v = hf[s:s + 2 * nb[n]].reshape(-1, 2)
+            xport[n], deg[n] = v[:, 0], v[:, 1]
+            s += 2 * nb[n]
+        c1 = hf[s:s + 3 * nb[2]].reshape(-1, 3)
+        s += 3 * nb[2]
+        rtot_all = hf[s:]
+        cnt = int(hi[1] - hi[0])
+        ip1 = hi[2:2 + nb[2]]
+        s = 2 + nb[2]
+        key = {}
+        for n in keyed:
+            key[n] = hi[s:s + nb[n] * 2 * n].reshape(nb[n], 2 * n)
+            s += nb[n] * 2 * n
+        d = np.sqrt(c1[:, 0] * c1[:, 0] + c1[:, 1] * c1[:, 1] + c1[:, 2] * c1[:, 2])
+        ref = np.float32(1.0)
+        rep = np.arange(nb[2])
+        ss_deg = deg[2]
+        if not self.merge_degenerate or nb[2] == 0:
+            if nb[2] and cnt > 0:
+                ref = xport[2][int(np.argmin(d))]                  # the first of equal minima, as np.argmin gives
+        if self.merge_degenerate and nb[2]:
+            # greedy 1e-3 A windows over the sorted closed lengths of every path (the device version's _windows)
+            o = np.argsort(rtot_all, kind="stable")
+            sr = np.ascontiguousarray(rtot_all[o], dtype=np.float32)
+            seg = np.array([0, len(sr)], np.int64)
+            win_sorted = np.zeros(len(sr), np.int64)
+            _lib.check(self._lib.fg_pf_windows(sr.ctypes.data, seg.ctypes.data, 1, float(np.float32(1e-3)),
+                                               win_sorted.ctypes.data))
+            win = np.empty(len(sr), np.int64)
+            win[o] = win_sorted
+            o = np.argsort(d, kind="stable")
+            keys = np.stack([np.round(d[o] * np.float32(1000)).astype(np.int64), ip1[o], win[:nb[2]][o]], 1)
+            _, inv = np.unique(keys, axis=0, return_inverse=True)
+            inv = inv.reshape(-1)
+            G = int(inv.max()) + 1
+            firstp = np.full(G, len(o), np.int64)
+            np.minimum.at(firstp, inv, np.arange(len(o)))
+            gcount = np.bincount(inv, minlength=G).astype(np.float32)
+            go = np.argsort(firstp, kind="stable")
+            rep = o[firstp[go]]
+            ss_deg = gcount[go]
+            first = int(np.argmin(d[rep]))
+            ref = xport[2][rep[first]] * ss_deg[first]
+        refs = np.float32(ref)
+        paths = {}
+        for n in legs:
+            if n == 2:
+                idx, dg = rep, ss_deg
+            else:
+                idx, dg = np.arange(nb[n]), deg[n]
+            dtot = dg
+            if n > 2 and self.merge_degenerate and nb[n] and cnt > 1:
+                _, inv = np.unique(key[n], axis=0, return_inverse=True)
+                inv = inv.reshape(-1)
+                tot = np.zeros(int(inv.max()) + 1, np.float32)
+                np.add.at(tot, inv, dg)
+                dtot = tot[inv]
+            frac = np.float32(100) * dtot * xport[n][idx] / refs
+            k = np.nonzero(frac >= np.float32(self.critpw))[0]
+            ki = torch.as_tensor(idx[k], device=dev)
+            v = out[n]
+            dsel = torch.as_tensor(dg[k], device=dev) if n == 2 else v["deg"].index_select(0, ki)
+            paths[n] = (v["coords"].index_select(0, ki), v["ipots"].index_select(0, ki), dsel,
+                        v["xport"].index_select(0, ki), v["atoms"].index_select(0, ki), v["slot"].index_select(0, ki))
+        return {"paths": paths, "ref": torch.full((1,), float(refs), device=dev, dtype=torch.float32)}
+
     def _merge_and_cut(self, out, A, off, cand_rel):
+        if A == 1:
+            return self._merge_and_cut_one(out, off)
         dev = self.device
         ss = out[2]
         c1 = ss["coords"][:, 1]

@@ -48,20 +48,24 @@ def test_finder_equals_reference(name):
             print(f"finder_{name} critpw {crit} nleg {nleg}: {len(ra)} paths equal")
 
 
-def test_batched_absorbers_equal_single_calls():
+@pytest.mark.parametrize("merge,crit", [(True, 0.5), (True, 0.0), (False, 0.5)])
+def test_batched_absorbers_equal_single_calls(merge, crit):
+    """enumerate_many over six absorbers (merges and cut on the device) against one enumerate per absorber (the
+    single-slot merges and cut on the host): the same paths bit for bit, the same reference importance."""
     from feffgpu_b200.pathfinder import GPUPathFinder
     z, box = finder_case("pack")
     pos, ipot = z["pos"], z["ipot"]
     abs_ = [int(a) for a in np.nonzero(ipot == 1)[0][:6]]
-    f = GPUPathFinder(phase("cfg2_phase"), device="cuda", rmax=5.5, nlegmax=5, critpw=0.5)
+    f = GPUPathFinder(phase("cfg2_phase"), device="cuda", rmax=5.5, nlegmax=5, critpw=crit, merge_degenerate=merge)
     many = f.enumerate_many(pos, box, abs_, ipot)
     for s, a in enumerate(abs_):
         kept, ref = f.enumerate(pos, box, a, ipot)
-        assert abs(float(many["ref"][s]) - ref) <= 1e-7 * abs(ref)
+        assert float(many["ref"][s]) == ref
+        assert set(kept) == set(many["paths"])
         for nleg, v in kept.items():
             sel = many["paths"][nleg][5] == s
             for x, y in zip(v, many["paths"][nleg][:5]):
-                assert torch.equal(x, y[sel]), (a, nleg)
+                assert x.dtype == y.dtype and torch.equal(x, y[sel]), (a, nleg)
 
 
 def test_feopt_paths_equal_reference():
