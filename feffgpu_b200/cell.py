@@ -36,3 +36,13 @@ def cell_words(cell: np.ndarray, dtype) -> np.ndarray:
     c = torch.tensor(cell, dtype=tdt)
     inv = torch.linalg.inv(c)
     return np.concatenate([c.numpy().ravel(), inv.numpy().ravel()]).astype(dtype)
+
+
+def min_width(cell) -> float:
+    """The smallest perpendicular width of a cell from as_cell (A): the length of a cubic box, inf for a cluster."""
+    if cell is None:
+        return float("inf")
+    if isinstance(cell, float):
+        return cell
+    vol = abs(np.linalg.det(cell))
+    return float(min(vol / np.linalg.norm(np.cross(cell[(i + 1) % 3], cell[(i + 2) % 3])) for i in range(3)))

@@ -23,7 +23,7 @@ import torch
 
 from . import _lib
 from .batch import PathBatch
-from .cell import as_cell, cell_words
+from .cell import as_cell, cell_words, min_width
 from .stage import GPUPathStage
 
 ETOK = 0.2624684236075176   # 2 m_e / hbar^2 in 1/(eV A^2): k^2 = ETOK (E - E0) (exafs/transform.py:22)
@@ -52,6 +52,12 @@ class PairTables:
         if ms:
             raise NotImplementedError("multiple scattering is the path finder and the path stage of this package "
                                       "(feffgpu_b200.pathfinder, GPUPathStage.chi_reduce); build PairTables with ms=False")
+        width = min_width(as_cell(box))
+        if width < 2 * float(rmax):
+            # the reference refuses such a cell in the same place (its PathSpectra, exafs/forward.py:71-73)
+            raise ValueError(f"the periodic cell (smallest width {width:.2f} A) is narrower than twice the cutoff "
+                             f"({float(rmax)} A): a pair would have more than one image within it; use a larger "
+                             f"supercell or a smaller cutoff")
         self.device = torch.device(device)
         self.stage = phase if isinstance(phase, GPUPathStage) else GPUPathStage(phase, device=device, dtype=dtype)
         self.device = self.stage.device

@@ -40,3 +40,17 @@ def test_min_image_matches_the_reference_rule():
     cub = MinImage(12.0, "cpu")(torch.tensor(rel)).numpy()
     assert np.allclose(cub, rel - 12.0 * np.round(rel / 12.0))
     assert np.array_equal(MinImage(None, "cpu")(torch.tensor(rel)).numpy(), rel)
+
+
+def test_min_width_and_the_pair_tables_refuse_narrow_cells():
+    """The smallest perpendicular width of a cell; PairTables refuses a cell narrower than twice its cutoff, as the
+    reference's front end does, before it touches a device."""
+    from feffgpu_b200.cell import min_width
+    from feffgpu_b200.pairs import PairTables
+    assert min_width(None) == float("inf") and min_width(11.0) == 11.0
+    c = np.array([[10.0, 0, 0], [5.0, 10.0, 0], [0, 0, 12.0]])
+    assert abs(min_width(c) - 10.0 * 10.0 / np.hypot(5.0, 10.0)) < 1e-12
+    with pytest.raises(ValueError, match="narrower than twice the cutoff"):
+        PairTables(None, np.arange(10) * 0.1, box=11.0, rmax=6.0)
+    with pytest.raises(ValueError, match="narrower than twice the cutoff"):
+        PairTables(None, np.arange(10) * 0.1, box=c, rmax=5.0)
