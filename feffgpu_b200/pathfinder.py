@@ -195,7 +195,8 @@ class GPUPathFinder:
         cand_rel = torch.empty(max(total, 1), 3, device=dev, dtype=torch.float32)
         _lib.check(lib.fg_pf_candidates(posd.data_ptr(), n, boxf, cptr, ab.data_ptr(), A, per_frame, self.rmax, None,
                                         off.data_ptr(), cand_atom.data_ptr(), cand_rel.data_ptr(), st))
-        slot = torch.repeat_interleave(torch.arange(A, device=dev, dtype=torch.int32), cnt.long())
+        slot = torch.repeat_interleave(torch.arange(A, device=dev, dtype=torch.int32), cnt.long(),
+                                       output_size=total)          # the size is known: no synchronisation
         seq = (torch.arange(total, device=dev) - off[slot.long()]).to(torch.int32)[:, None].contiguous()
         cr = cand_rel[:total]
         length = torch.sqrt(cr[:, 0] * cr[:, 0] + cr[:, 1] * cr[:, 1] + cr[:, 2] * cr[:, 2]).contiguous()
@@ -318,7 +319,7 @@ class GPUPathFinder:
             first = int(np.argmin(d[rep]))
             ref = xport[2][rep[first]] * ss_deg[first]
         refs = np.float32(ref)
-        paths = {}
+        paths, kept, ss_kept_deg = {}, {}, np.zeros(0, np.float32)
         for n in legs:
             if n == 2:
                 idx, dg = rep, ss_deg
@@ -333,9 +334,23 @@ class GPUPathFinder:
                 dtot = tot[inv]
             frac = np.float32(100) * dtot * xport[n][idx] / refs
             k = np.nonzero(frac >= np.float32(self.critpw))[0]
-            ki = torch.as_tensor(idx[k], device=dev)
+            kept[n] = idx[k]
+            if n == 2:
+                ss_kept_deg = dg[k]
+        # every leg's kept indices and the merged single-scattering degeneracies in one copy to the device
+        sizes = [len(kept[n]) for n in legs]
+        packed = np.concatenate([kept[n].astype(np.int64) for n in legs] +
+                                [ss_kept_deg.astype(np.float32).view(np.int32).astype(np.int64)])
+        dpk = torch.as_tensor(packed, device=dev)
+        s = 0
+        for n, m in zip(legs, sizes):
+            ki = dpk[s:s + m]
+            s += m
             v = out[n]
-            dsel = torch.as_tensor(dg[k], device=dev) if n == 2 else v["deg"].index_select(0, ki)
+            if n == 2:
+                dsel = dpk[-m:].to(torch.int32).view(torch.float32) if m else v["deg"][:0]
+            else:
+                dsel = v["deg"].index_select(0, ki)
             paths[n] = (v["coords"].index_select(0, ki), v["ipots"].index_select(0, ki), dsel,
                         v["xport"].index_select(0, ki), v["atoms"].index_select(0, ki), v["slot"].index_select(0, ki))
         return {"paths": paths, "ref": torch.full((1,), float(refs), device=dev, dtype=torch.float32)}
