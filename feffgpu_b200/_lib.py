@@ -123,6 +123,8 @@ def check(status: int) -> None:
     if status == FG_OK:
         return
     msg = (_lib.fg_last_error() or b"").decode(errors="replace")
+    if status == FG_ERR_VALUE and msg.startswith("potential index"):
+        raise IndexError(msg)                    # the reference's table lookup (stage.py:244) raises IndexError
     if status in (FG_ERR_VALUE, FG_ERR_WORKSPACE):
         raise ValueError(msg)
     if status == FG_ERR_NOT_IMPLEMENTED:

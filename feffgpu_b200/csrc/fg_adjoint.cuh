@@ -945,7 +945,7 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
                                                   const int *__restrict__ order, const C2<R> *__restrict__ gbar,
                                                   const double *__restrict__ greff_d, const R *__restrict__ greff_r,
                                                   R *__restrict__ gout_r, double *__restrict__ gout_d,
-                                                  unsigned long long *counter, int nsc_max, size_t wbytes)
+                                                  unsigned long long *counter, int *status, int nsc_max, size_t wbytes)
 {
     using K = Kinds<EDGE>;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -963,9 +963,13 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
         tk = __shfl_sync(0xffffffffu, tk, 0);
         if (tk >= (unsigned long long)B) break;
         const int64_t p = order ? order[tk] : (int64_t)tk;
-        const int nleg = nlegs ? nlegs[p] : nleg_uniform;
+        const int nleg = (p >= 0 && p < B) ? (nlegs ? nlegs[p] : nleg_uniform) : 0;
+        if (nleg < 2 || nleg > stride) {              // a malformed batch: report it, never index past the arrays
+            if (lane == 0) atomicOr(status, kBadLayout);
+            continue;
+        }
         const int MM = nleg == 2 ? K::MMSS : K::MMMS;
-        path_setup<R, CT>(g, dh, T, coords + p * stride * 3, ipots + p * stride, nleg, lane, nullptr, MM);
+        path_setup<R, CT>(g, dh, T, coords + p * stride * 3, ipots + p * stride, nleg, lane, status, MM);
         adj_setup<R>(g, dhd, as.dterm_db, T, nleg, lane, MM);
         __syncwarp();
         const int frame = choose_frame<R>(g, nleg, lane);
@@ -1021,10 +1025,10 @@ __global__ void __launch_bounds__(256) k_fine_adjoint(int64_t B, int E, int NK, 
                                                        const double *__restrict__ S_d, const int *__restrict__ span,
                                                        const int *__restrict__ tspan, const R *__restrict__ gchi,
                                                        const double *__restrict__ grows, const int *__restrict__ row,
-                                                       const double *__restrict__ deg, const double *__restrict__ sigma2,
-                                                       C2<R> *__restrict__ gbar, R *__restrict__ greff_r,
-                                                       double *__restrict__ greff_d, double *__restrict__ gsig,
-                                                       size_t wbytes)
+                                                       int nrows, const double *__restrict__ deg,
+                                                       const double *__restrict__ sigma2, C2<R> *__restrict__ gbar,
+                                                       R *__restrict__ greff_r, double *__restrict__ greff_d,
+                                                       double *__restrict__ gsig, int *status, size_t wbytes)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -1041,7 +1045,9 @@ __global__ void __launch_bounds__(256) k_fine_adjoint(int64_t B, int E, int NK, 
         const double rf = reff_d ? reff_d[p] : (double)reff_r[p];
         const double s2 = (mode == 1 && sigma2) ? sigma2[p] : 0.0;
         const double wd = mode == 1 ? deg[p] : 1.0;
-        const double *gr = mode == 1 ? grows + (int64_t)row[p] * NK : nullptr;
+        const int rp = mode == 1 ? row[p] : 0;
+        if (mode == 1 && (rp < 0 || rp >= nrows) && lane == 0) atomicOr(status, kBadLayout);
+        const double *gr = (mode == 1 && rp >= 0 && rp < nrows) ? grows + (int64_t)rp * NK : nullptr;
         double g_reff = 0.0, g_s2 = 0.0;
         for (int k0 = 0; k0 < NK; k0 += 32) {
             const int k = k0 + lane;
@@ -1056,7 +1062,7 @@ __global__ void __launch_bounds__(256) k_fine_adjoint(int64_t B, int E, int NK, 
                 }
                 const double qk = q_d ? q_d[k] : (double)q_r[k];
                 const double damp = s2 != 0.0 ? exp(-2.0 * s2 * qk * qk) : 1.0;
-                const double G = (mode == 1 ? gr[k] * wd : (double)gchi[p * NK + k]) * damp;
+                const double G = (mode == 1 ? (gr ? gr[k] * wd : 0.0) : (double)gchi[p * NK + k]) * damp;
                 const double arg = ph + 2.0 * qk * rf;
                 const double sn = sin_arg<R>(arg), cs = sin_arg<R>(arg + 1.5707963267948966);
                 da = G * sn;
@@ -1109,7 +1115,7 @@ template <typename R, int EDGE, typename CT>
 fg_status launch_adjoint(const StageView &sv, const Tables<R> &T, const CT *coords, const int64_t *ipots, int stride,
                          const int *nlegs, int nleg_uniform, int nsc_max, int64_t B, const int *order,
                          const C2<R> *gbar, const double *greff_d, const R *greff_r, R *gout_r, double *gout_d,
-                         unsigned long long *counter, int warps, cudaStream_t st)
+                         unsigned long long *counter, int *status, int warps, cudaStream_t st)
 {
     using K = Kinds<EDGE>;
     const size_t wb = adj_warp_bytes<R>(sv.L1, nsc_max, K::MM);
@@ -1118,10 +1124,9 @@ fg_status launch_adjoint(const StageView &sv, const Tables<R> &T, const CT *coor
     auto kern = k_adjoint<R, EDGE, CT>;
     int blocks = 0;
     if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;
-    FG_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
     timer_begin(st);
     kern<<<blocks, threads, wb * warps, st>>>(T, coords, ipots, stride, nlegs, nleg_uniform, B, order, gbar, greff_d,
-                                              greff_r, gout_r, gout_d, counter, nsc_max, wb);
+                                              greff_r, gout_r, gout_d, counter, status, nsc_max, wb);
     timer_end(st);
     FG_CUDA(cudaGetLastError());
     return FG_OK;
@@ -1131,8 +1136,8 @@ template <typename R>
 fg_status launch_fine_adjoint(const StageView &sv, int64_t B, int NK, int mode, const void *cchi, const R *reff_r,
                               const double *reff_d, const R *q_r, const double *q_d, const R *S_r, const double *S_d,
                               const int *span, const int *tspan, const R *gchi, const double *grows, const int *row,
-                              const double *deg, const double *sigma2, C2<R> *gbar, R *greff_r, double *greff_d,
-                              double *gsig, cudaStream_t st)
+                              int nrows, const double *deg, const double *sigma2, C2<R> *gbar, R *greff_r,
+                              double *greff_d, double *gsig, int *status, cudaStream_t st)
 {
     const size_t wb = 2 * align_up((size_t)sv.E * 8, 16) + align_up((size_t)NK * 16, 16);
     const int warps = fit_warps(4, wb, sv.max_smem), threads = warps * 32;
@@ -1140,8 +1145,8 @@ fg_status launch_fine_adjoint(const StageView &sv, int64_t B, int NK, int mode, 
     int blocks = 0;
     if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;
     kern<<<blocks, threads, wb * warps, st>>>(B, sv.E, NK, mode, static_cast<const C2<R> *>(cchi), reff_r, reff_d, q_r,
-                                              q_d, S_r, S_d, span, tspan, gchi, grows, row, deg, sigma2, gbar, greff_r,
-                                              greff_d, gsig, wb);
+                                              q_d, S_r, S_d, span, tspan, gchi, grows, row, nrows, deg, sigma2, gbar,
+                                              greff_r, greff_d, gsig, status, wb);
     FG_CUDA(cudaGetLastError());
     return FG_OK;
 }
@@ -1152,15 +1157,17 @@ fg_status Launch<R, EDGE>::cchi_bwd(const StageView &sv, const Tables<R> &T, int
                                     void *grad_coords, unsigned char *ws, int warps, cudaStream_t st)
 {
     unsigned long long *counter = reinterpret_cast<unsigned long long *>(ws);
+    int *status = reinterpret_cast<int *>(ws + kStatusOffset);
     const C2<R> *gb = static_cast<const C2<R> *>(grad_cchi);
     const R *gr = static_cast<const R *>(grad_reff);
+    FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes, st));
     if (coords_f64)
         return launch_adjoint<R, EDGE, double>(sv, T, static_cast<const double *>(coords), ipots, nleg, nullptr, nleg,
                                                nleg - 1, B, nullptr, gb, nullptr, gr, static_cast<R *>(grad_coords),
-                                               nullptr, counter, warps, st);
+                                               nullptr, counter, status, warps, st);
     return launch_adjoint<R, EDGE, float>(sv, T, static_cast<const float *>(coords), ipots, nleg, nullptr, nleg,
                                           nleg - 1, B, nullptr, gb, nullptr, gr, static_cast<R *>(grad_coords),
-                                          nullptr, counter, warps, st);
+                                          nullptr, counter, status, warps, st);
 }
 
 template <typename R, int EDGE>
@@ -1171,15 +1178,18 @@ fg_status Launch<R, EDGE>::fused_bwd(const StageView &sv, const Tables<R> &T, co
                                      cudaStream_t st)
 {
     unsigned long long *counter = reinterpret_cast<unsigned long long *>(ws);
+    int *status = reinterpret_cast<int *>(ws + kStatusOffset);
     C2<R> *gbar = reinterpret_cast<C2<R> *>(ws + kCounterBytes);
     double *greff = reinterpret_cast<double *>(ws + kCounterBytes + align_up((size_t)P->n * sv.E * sizeof(C2<double>), 256));
+    FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes, st));
     if (P->n == 0) return FG_OK;
     if (fg_status rc = launch_fine_adjoint<R>(sv, P->n, NK, 1, cchi_saved, nullptr, reff_saved, nullptr, q, nullptr, S,
-                                              span, tspan, nullptr, grad_rows, P->row, P->deg, P->sigma2, gbar, nullptr,
-                                              greff, grad_sigma2, st))
+                                              span, tspan, nullptr, grad_rows, P->row, P->nrows, P->deg, P->sigma2,
+                                              gbar, nullptr, greff, grad_sigma2, status, st))
         return rc;
     return launch_adjoint<R, EDGE, double>(sv, T, P->coords, P->ipots, P->nleg_max, P->nleg, 0, P->nleg_max - 1, P->n,
-                                           P->order, gbar, greff, nullptr, nullptr, grad_coords, counter, warps, st);
+                                           P->order, gbar, greff, nullptr, nullptr, grad_coords, counter, status,
+                                           warps, st);
 }
 
 template <typename R>
@@ -1189,8 +1199,9 @@ fg_status LaunchCommon<R>::chi_fine_bwd(const StageView &sv, int64_t B, const vo
 {
     return launch_fine_adjoint<R>(sv, B, NK, 0, cchi, static_cast<const R *>(reff), nullptr, static_cast<const R *>(q),
                                   nullptr, static_cast<const R *>(S), nullptr, span, tspan,
-                                  static_cast<const R *>(grad_chi), nullptr, nullptr, nullptr, nullptr,
-                                  static_cast<C2<R> *>(grad_cchi), static_cast<R *>(grad_reff), nullptr, nullptr, st);
+                                  static_cast<const R *>(grad_chi), nullptr, nullptr, 0, nullptr, nullptr,
+                                  static_cast<C2<R> *>(grad_cchi), static_cast<R *>(grad_reff), nullptr, nullptr,
+                                  nullptr, st);
 }
 
 }  // namespace fg

@@ -35,6 +35,10 @@ struct fg_stage {
     int num_sms = 148;
     int max_smem = 227 * 1024;
     int fwd_warps = 0, bwd_warps = 0;   // launch shape of this stage's calls, 0 = the process default
+    // device address of the no-allocation scratch in this stage's context, looked up by its first
+    // fg_chi_reduce_noalloc call (a device reset invalidates the stage, and with it this address)
+    void *noalloc_scratch = nullptr;
+    std::mutex noalloc_mu;
     std::vector<int> lmax_host;     // (E, nph1)
     std::vector<double> xk_host;    // (E)
     Tables<float> tf{};
@@ -380,14 +384,19 @@ template <class F> fg_status by_kind(const fg_stage *s, fg_precision prec, F &&f
     }
 }
 
+// Host-side checks of a batch's sizes and pointers; the kernels check the contents (indices and offsets) and report
+// through the call's status word.
 fg_status check_paths(const fg_paths *P)
 {
     if (!P) return fail(FG_ERR_VALUE, "null paths");
     if (P->n < 0 || P->nrows < 0 || P->nchunks < 0) return fail(FG_ERR_VALUE, "negative size");
     if (P->nleg_max < 2 || P->nleg_max > kMaxLeg) return fail(FG_ERR_VALUE, "nleg_max must be 2..9");
-    if (P->n > 0 && (!P->coords || !P->ipots || !P->nleg || !P->deg || !P->order || !P->sorted || !P->chunk_bounds ||
-                     !P->row_chunks || !P->row))
+    if (P->n > 0 && (!P->coords || !P->ipots || !P->nleg || !P->deg || !P->order || !P->row))
         return fail(FG_ERR_VALUE, "null array in paths");
+    if (P->nrows > 0 && !P->row_chunks) return fail(FG_ERR_VALUE, "null row_chunks with nrows > 0");
+    if (P->nchunks > 0 && (!P->chunk_bounds || !P->sorted))
+        return fail(FG_ERR_VALUE, "null chunk_bounds or sorted with nchunks > 0");
+    if (P->n > 0 && P->nchunks == 0) return fail(FG_ERR_VALUE, "paths but no summation chunks");
     if (P->n > 0x7fffffff) return fail(FG_ERR_VALUE, "at most 2^31-1 paths per call");
     return FG_OK;
 }
@@ -500,10 +509,12 @@ extern "C" fg_status fg_chi_reduce(const fg_stage *s, fg_precision prec, const f
     if (fg_status rc = set_device(s)) return rc;
     const StageView sv = view(s);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    return by_kind(s, prec, [&](auto L, const auto &T) {
-        return decltype(L)::fused(sv, T, P, NK, q, S, span, rows, cchi_save, reff_save,
-                                  static_cast<unsigned char *>(workspace), fwd_warps(s), st);
-    });
+    if (fg_status rc = by_kind(s, prec, [&](auto L, const auto &T) {
+            return decltype(L)::fused(sv, T, P, NK, q, S, span, rows, cchi_save, reff_save,
+                                      static_cast<unsigned char *>(workspace), fwd_warps(s), st);
+        }))
+        return rc;
+    return read_status(reinterpret_cast<const int *>(static_cast<unsigned char *>(workspace) + kStatusOffset), st);
 }
 
 extern "C" size_t fg_chi_reduce_backward_workspace(const fg_stage *s, const fg_paths *P, int32_t NK)
@@ -531,11 +542,13 @@ extern "C" fg_status fg_chi_reduce_backward(const fg_stage *s, fg_precision prec
     if (fg_status rc = set_device(s)) return rc;
     const StageView sv = view(s);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    return by_kind(s, prec, [&](auto L, const auto &T) {
-        return decltype(L)::fused_bwd(sv, T, P, NK, q, S, span, tspan, grad_rows, cchi_saved, reff_saved,
-                                      grad_coords, grad_sigma2, static_cast<unsigned char *>(workspace), bwd_warps(s),
-                                      st);
-    });
+    if (fg_status rc = by_kind(s, prec, [&](auto L, const auto &T) {
+            return decltype(L)::fused_bwd(sv, T, P, NK, q, S, span, tspan, grad_rows, cchi_saved, reff_saved,
+                                          grad_coords, grad_sigma2, static_cast<unsigned char *>(workspace),
+                                          bwd_warps(s), st);
+        }))
+        return rc;
+    return read_status(reinterpret_cast<const int *>(static_cast<unsigned char *>(workspace) + kStatusOffset), st);
 }
 
 // ------------------------------------------------------------------------------------------------ no-allocation variant
@@ -544,23 +557,20 @@ extern "C" fg_status fg_chi_reduce_backward(const fg_stage *s, fg_precision prec
 static __device__ __align__(256) unsigned char g_noalloc_scratch[FG_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-constexpr int kMaxDevices = 128;
-std::mutex g_noalloc_mu;
-void *g_noalloc_addr[kMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on `device` (which must be current); looked up once per device.
-fg_status noalloc_scratch(int device, void **out)
+// Device address of g_noalloc_scratch in the context of stage s, whose device must be current: looked up once per
+// stage (a stage belongs to one device and one context; a device reset invalidates the stage with its tables, so a
+// stage created after a reset looks the address up again).
+fg_status noalloc_scratch(fg_stage *s, void **out)
 {
-    if (device < 0 || device >= kMaxDevices) return fail(FG_ERR_VALUE, "device index out of range");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[device]) {
+    std::lock_guard<std::mutex> lock(s->noalloc_mu);
+    if (!s->noalloc_scratch) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
             return fail(FG_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
-        g_noalloc_addr[device] = p;
+        s->noalloc_scratch = p;
     }
-    *out = g_noalloc_addr[device];
+    *out = s->noalloc_scratch;
     return FG_OK;
 }
 }  // namespace
@@ -582,11 +592,13 @@ extern "C" fg_status fg_chi_reduce_noalloc(const fg_stage *s, fg_precision prec,
                                       std::to_string((size_t)FG_NOALLOC_SCRATCH_BYTES) + " bytes; split it by rows");
     if (fg_status rc = set_device(s)) return rc;
     void *ws = nullptr;
-    if (fg_status rc = noalloc_scratch(s->device, &ws)) return rc;
+    if (fg_status rc = noalloc_scratch(const_cast<fg_stage *>(s), &ws)) return rc;
     const StageView sv = view(s);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    return by_kind(s, prec, [&](auto L, const auto &T) {
-        return decltype(L)::fused(sv, T, P, NK, q, S, span, rows, nullptr, nullptr, static_cast<unsigned char *>(ws),
-                                  fwd_warps(s), st);
-    });
+    if (fg_status rc = by_kind(s, prec, [&](auto L, const auto &T) {
+            return decltype(L)::fused(sv, T, P, NK, q, S, span, rows, nullptr, nullptr,
+                                      static_cast<unsigned char *>(ws), fwd_warps(s), st);
+        }))
+        return rc;
+    return read_status(reinterpret_cast<const int *>(static_cast<unsigned char *>(ws) + kStatusOffset), st);
 }

@@ -16,6 +16,12 @@ constexpr double kBohr = 0.52917721067;   // pad.py:13
 constexpr int kMaxLeg = 9;                 // pathfinder.py:26 (NLEG_MAX)
 constexpr int kLamTot = 15;                // genfmt.py:18
 
+// Bits of the status word the per-path kernels raise (atomicOr) instead of reading out of bounds: a potential index
+// outside 0..nph (clamped, as the reference's tables would raise IndexError), and a malformed batch layout (a path
+// index, leg count, summation index or chunk offset outside its range; that path or term is skipped).
+constexpr int kBadIpot = 1;
+constexpr int kBadLayout = 2;
+
 // ------------------------------------------------------------------------------------------------ complex helpers
 template <typename R> struct C2 { R x, y; };
 

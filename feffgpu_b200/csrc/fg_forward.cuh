@@ -51,7 +51,7 @@ __device__ void path_setup(WarpPath<R> &g, R *dh, const Tables<R> &T, const CT *
     if (lane <= nleg) {
         int64_t v = ipots[(lane == 0 || lane == nleg) ? 0 : lane];
         if (v < 0 || v >= T.nph1) {
-            if (bad_ipot) atomicExch(bad_ipot, 1);
+            if (bad_ipot) atomicOr(bad_ipot, kBadIpot);
             v = v < 0 ? 0 : T.nph1 - 1;
         }
         g.ip[lane] = (int)v;

@@ -192,7 +192,11 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= (unsigned long long)P.n) break;
         const int64_t p = P.order[t];
-        const int nleg = P.nleg[p];
+        const int nleg = (p >= 0 && p < P.n) ? P.nleg[p] : 0;
+        if (nleg < 2 || nleg > P.nleg_max) {          // a malformed batch: report it, never index past the arrays
+            if (lane == 0) atomicOr(bad, kBadLayout);
+            continue;
+        }
         path_setup<R, double>(g, dh, T, P.coords + p * P.nleg_max * 3, P.ipots + p * P.nleg_max, nleg, lane, bad,
                               nleg == 2 ? K::MMSS : K::MMMS);
         for (int e0 = first_chunk(E); e0 < E; e0 += 32) {
@@ -276,7 +280,7 @@ fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const 
 {
     using K = Kinds<EDGE>;
     unsigned long long *counter = reinterpret_cast<unsigned long long *>(ws);
-    int *bad = reinterpret_cast<int *>(ws + 64);
+    int *bad = reinterpret_cast<int *>(ws + kStatusOffset);
     double *terms = reinterpret_cast<double *>(ws + kCounterBytes);
     double *partial = reinterpret_cast<double *>(ws + kCounterBytes + align_up((size_t)P->n * NK * sizeof(double), 256));
     FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes, st));
@@ -295,7 +299,7 @@ fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const 
         timer_end(st);
         FG_CUDA(cudaGetLastError());
     }
-    return launch_reductions(P, NK, terms, partial, rows, st);
+    return launch_reductions(P, NK, terms, partial, rows, bad, st);
 }
 
 template <typename R>

@@ -15,6 +15,7 @@ fg_status fail(fg_status s, const std::string &m);  // records the message for f
 __host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 constexpr size_t kCounterBytes = 256;   // head of every fused workspace: work-queue counters and flags
+constexpr size_t kStatusOffset = 64;    // the int status word (kBadIpot | kBadLayout) within that head
 
 // What the launches need to know about a stage.
 struct StageView {
@@ -58,8 +59,14 @@ template <typename R> struct LaunchCommon {
 };
 
 // Fused reduction kernels (precision independent, FP64).
-fg_status launch_reductions(const fg_paths *P, int NK, const double *terms, double *partial, double *rows,
+// Rows of a call whose status word is set are written as NaN (so that a result can never look valid).
+fg_status launch_reductions(const fg_paths *P, int NK, const double *terms, double *partial, double *rows, int *status,
                             cudaStream_t st);
+
+// The status word of a call's kernels (device int) turned into a return code: outside stream capture the call waits
+// for its stream and reads the word (FG_ERR_VALUE with a message if a bit is set); under capture it returns FG_OK
+// without waiting (the rows of a replay that meets a bad input are NaN).
+fg_status read_status(const int *status, cudaStream_t st);
 
 // Events around the main kernel of a call when kernel timing is on (fg_set_kernel_timing)
 void timer_begin(cudaStream_t st);

@@ -16,42 +16,73 @@ struct KSum {
     __device__ __forceinline__ double value() const { return s + c; }
 };
 
-__global__ void k_chunk_sums(int NK, const double *__restrict__ terms, const int *__restrict__ sorted,
-                             const int64_t *__restrict__ bounds, double *__restrict__ partial)
+__global__ void k_chunk_sums(int NK, int64_t n, int64_t nchunks, const double *__restrict__ terms,
+                             const int *__restrict__ sorted, const int64_t *__restrict__ bounds,
+                             double *__restrict__ partial, int *status)
 {
     const int64_t c = blockIdx.x;
     const int k = blockIdx.y * blockDim.x + threadIdx.x;
     if (k >= NK) return;
+    int64_t lo = bounds[c], hi = bounds[c + 1];
+    if (lo < 0 || hi < lo || hi > n) {         // chunk offsets must cut 0..n in order
+        atomicOr(status, kBadLayout);
+        lo = hi = 0;
+    }
     KSum s;
-    for (int64_t i = bounds[c]; i < bounds[c + 1]; ++i) s.add(terms[(int64_t)sorted[i] * NK + k]);
+    for (int64_t i = lo; i < hi; ++i) {
+        const int p = sorted[i];
+        if (p < 0 || p >= n) { atomicOr(status, kBadLayout); continue; }
+        s.add(terms[(int64_t)p * NK + k]);
+    }
     partial[c * NK + k] = s.value();
 }
 
-__global__ void k_row_sums(int NK, int nrows, const double *__restrict__ partial,
-                           const int64_t *__restrict__ row_chunks, double *__restrict__ rows)
+__global__ void k_row_sums(int NK, int nrows, int64_t nchunks, const double *__restrict__ partial,
+                           const int64_t *__restrict__ row_chunks, double *__restrict__ rows, int *status)
 {
     const int r = blockIdx.x;
     const int k = blockIdx.y * blockDim.x + threadIdx.x;
     if (k >= NK || r >= nrows) return;
+    int64_t lo = row_chunks[r], hi = row_chunks[r + 1];
+    if (lo < 0 || hi < lo || hi > nchunks) {
+        atomicOr(status, kBadLayout);
+        lo = hi = 0;
+    }
     KSum s;
-    for (int64_t c = row_chunks[r]; c < row_chunks[r + 1]; ++c) s.add(partial[c * NK + k]);
-    rows[(int64_t)r * NK + k] = s.value();
+    for (int64_t c = lo; c < hi; ++c) s.add(partial[c * NK + k]);
+    // the earlier kernels of the call have finished (same stream): a set status word makes the whole call's rows NaN
+    rows[(int64_t)r * NK + k] = *(volatile int *)status ? __longlong_as_double(0x7ff8000000000000ll) : s.value();
 }
 }  // namespace
 
-fg_status launch_reductions(const fg_paths *P, int NK, const double *terms, double *partial, double *rows,
+fg_status launch_reductions(const fg_paths *P, int NK, const double *terms, double *partial, double *rows, int *status,
                             cudaStream_t st)
 {
     if (P->nchunks > 0) {
         dim3 g1((unsigned)P->nchunks, (NK + 127) / 128);
-        k_chunk_sums<<<g1, 128, 0, st>>>(NK, terms, P->sorted, P->chunk_bounds, partial);
+        k_chunk_sums<<<g1, 128, 0, st>>>(NK, P->n, P->nchunks, terms, P->sorted, P->chunk_bounds, partial, status);
         FG_CUDA(cudaGetLastError());
     }
     if (P->nrows > 0) {
         dim3 g2((unsigned)P->nrows, (NK + 127) / 128);
-        k_row_sums<<<g2, 128, 0, st>>>(NK, P->nrows, partial, P->row_chunks, rows);
+        k_row_sums<<<g2, 128, 0, st>>>(NK, P->nrows, P->nchunks, partial, P->row_chunks, rows, status);
         FG_CUDA(cudaGetLastError());
     }
+    return FG_OK;
+}
+
+fg_status read_status(const int *status, cudaStream_t st)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    FG_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return FG_OK;
+    int v = 0;
+    FG_CUDA(cudaMemcpyAsync(&v, status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    if (v & kBadIpot) return fail(FG_ERR_VALUE, "potential index outside 0..nph (the rows are NaN)");
+    if (v & kBadLayout)
+        return fail(FG_ERR_VALUE, "malformed path batch: a path index, leg count, summation index or chunk offset is "
+                                  "outside its range (the rows are NaN)");
     return FG_OK;
 }
 

@@ -324,6 +324,8 @@ class GPUPathStage:
         crd = crd.to(self.device, torch.float64)
         s2 = None if sigma2 is None else torch.as_tensor(sigma2).to(self.device, torch.float64)
         prec = self.prec if dtype is None else (_lib.FG_FP64 if dtype == torch.complex128 else _lib.FG_MIXED)
+        if batch.max_ipot > self.P.nph:
+            raise IndexError(f"potential index {batch.max_ipot} out of range 0..{self.P.nph}")
         grad = torch.is_grad_enabled() and (crd.requires_grad or (s2 is not None and s2.requires_grad))
         self._pick_launch(batch, qt, Sd, prec, backward=grad)
         if s2 is None:

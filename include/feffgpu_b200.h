@@ -95,7 +95,7 @@ FG_API fg_status fg_cchi(const fg_stage *stage, fg_precision prec, int64_t B, in
 /* Adjoint of fg_cchi: grad_coords (B, nleg, 3) = d(loss)/d(coords) from grad_cchi (B, E) complex with PyTorch's
  * convention d(loss)/d(Re) + i d(loss)/d(Im), and grad_reff (B) (may be NULL).  grad_coords has the precision's
  * real type.  Recomputes the per-leg scattering matrices (no forward state is kept).  `workspace` must hold
- * fg_cchi_backward_workspace(...) bytes. */
+ * fg_cchi_backward_workspace(...) bytes.  Potential indices are clamped as in fg_cchi (which reports them). */
 FG_API size_t fg_cchi_backward_workspace(const fg_stage *stage, int64_t B, int32_t nleg);
 FG_API fg_status fg_cchi_backward(const fg_stage *stage, fg_precision prec, int64_t B, int32_t nleg, const void *coords,
                            int32_t coords_f64, const int64_t *ipots, const void *grad_cchi, const void *grad_reff,
@@ -126,20 +126,27 @@ typedef struct fg_paths {
     const double *sigma2;    /* (n) per-path sigma^2 in A^2, or NULL (no damping) */
     const int32_t *row;      /* (n) output row of each path, 0..nrows-1 */
     const int32_t *order;    /* (n) launch order: a permutation of 0..n-1, costliest paths first */
-    const int32_t *sorted;   /* (n) path indices grouped by row: the fixed summation order */
-    const int64_t *chunk_bounds; /* (nchunks+1) offsets into `sorted`; each chunk lies within one row */
+    const int32_t *sorted;   /* (n) path indices grouped by row: the fixed summation order (a permutation) */
+    const int64_t *chunk_bounds; /* (nchunks+1) offsets into `sorted` from 0 to n; each chunk lies within one row */
     const int64_t *row_chunks;   /* (nrows+1) offsets into the chunks: row r owns chunks row_chunks[r]..[r+1]-1 */
-    int64_t nchunks;
+    int64_t nchunks;         /* >= 1 when n > 0 */
 } fg_paths;
+/* The fused calls check the contents of these arrays on the device: a path index, leg count (2..nleg_max),
+ * potential index (0..nph), row, summation index or chunk offset outside its range is never used to address memory;
+ * the call's rows become NaN and, outside stream capture, the call waits for its stream and returns FG_ERR_VALUE
+ * naming the fault.  Under stream capture it returns without waiting (a graph replay with such an input gives NaN
+ * rows).  Host pointers and sizes are checked before any launch. */
 
-/* Workspace of the fused calls: a work-queue counter, per-path fine-grid terms and per-chunk partial sums. */
+/* Workspace of the fused calls: a work-queue counter and status word, per-path fine-grid terms and per-chunk partial
+ * sums. */
 FG_API size_t fg_chi_reduce_workspace(const fg_stage *stage, const fg_paths *paths, int32_t NK);
 
 /* rows (nrows, NK) FP64 = sum over paths p of deg_p exp(-2 sigma2_p q^2) chi_p(q), chi_p from cchi and chi_fine
  * as above, summed in a fixed order (deterministic).  Fuses GPUPathStage.cchi + chi_fine with the reduction
  * of the callers (chain.py:48-49, exafs/forward.py:162, md/spectrum.py:298).  q (NK), S (NK, E) and span as in
  * fg_chi_fine but always FP64.  If cchi_save (n, E complex of the precision) and reff_save (n, FP64) are non-NULL
- * the per-path signals are kept for fg_chi_reduce_backward. */
+ * the per-path signals are kept for fg_chi_reduce_backward.  Outside stream capture the call ends by waiting for
+ * its stream (to read the status word of the checks above). */
 FG_API fg_status fg_chi_reduce(const fg_stage *stage, fg_precision prec, const fg_paths *paths, int32_t NK, const double *q,
                         const double *S, const int32_t *span, double *rows, void *cchi_save, double *reff_save,
                         void *workspace, size_t workspace_bytes, void *stream);
@@ -150,11 +157,13 @@ FG_API fg_status fg_chi_reduce(const fg_stage *stage, fg_precision prec, const f
  * the workspace fg_chi_reduce asks for.  Instead of a caller workspace it uses an array compiled into the library,
  * FG_NOALLOC_SCRATCH_BYTES (32 MiB) on every GPU that loads the library, held until the process exits; a batch
  * whose fg_chi_reduce_workspace exceeds that is rejected with FG_ERR_VALUE (split it by rows).  It allocates
- * nothing: no cudaMalloc, no cudaFree, no allocating library call.  The first call on a device looks up the
- * array's device address with that device current; make that first call before any stream capture.  All calls
+ * nothing: no cudaMalloc, no cudaFree, no allocating library call.  The first call with a given stage looks up the
+ * array's device address with the stage's device current and keeps it in the stage; make that first call before any
+ * stream capture.  A cudaDeviceReset invalidates every stage (its tables and this address): create new stages after
+ * one.  All calls
  * share the array and it keeps the last call's contents (each call clears the queue counter it needs): calls whose
  * work overlaps on the GPU -- other streams, other host threads -- race on it and must be serialised by the caller.
- * Same inputs and result as fg_chi_reduce; the per-path signals are not kept (no adjoint). */
+ * Same inputs, checks and result as fg_chi_reduce; the per-path signals are not kept (no adjoint). */
 #define FG_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 FG_API fg_status fg_chi_reduce_noalloc(const fg_stage *stage, fg_precision prec, const fg_paths *paths, int32_t NK,
                                        const double *q, const double *S, const int32_t *span, double *rows,
@@ -162,7 +171,8 @@ FG_API fg_status fg_chi_reduce_noalloc(const fg_stage *stage, fg_precision prec,
 
 /* Adjoint of fg_chi_reduce: grad_coords (n, nleg_max, 3) FP64 and grad_sigma2 (n) FP64 (may be NULL) from
  * grad_rows (nrows, NK), using the saved cchi and reff; tspan as in fg_chi_fine_backward.  No reference
- * counterpart for sigma^2 (a new input). */
+ * counterpart for sigma^2 (a new input).  The batch is checked as in fg_chi_reduce (outside stream capture the call
+ * waits for its stream and returns FG_ERR_VALUE on a bad index). */
 FG_API size_t fg_chi_reduce_backward_workspace(const fg_stage *stage, const fg_paths *paths, int32_t NK);
 FG_API fg_status fg_chi_reduce_backward(const fg_stage *stage, fg_precision prec, const fg_paths *paths, int32_t NK,
                                  const double *q, const double *S, const int32_t *span, const int32_t *tspan,

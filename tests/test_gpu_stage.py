@@ -192,6 +192,71 @@ def test_edge_cases():
 
 
 @pytest.mark.parametrize("dtype", DTYPES)
+def test_fused_stage_reports_bad_potential_indices_and_layouts(dtype):
+    """An out-of-range potential index in a fused batch raises IndexError in the Python layer before any launch, and
+    through the C ABI the kernels clamp it (no out-of-bounds read), turn the rows NaN and the call returns
+    FG_ERR_VALUE; the backward likewise.  A malformed launch order (a path index past n) is reported the same way
+    and never used to address memory.  The reference raises IndexError from its table lookup (stage.py:244)."""
+    import ctypes as C
+    from feffgpu_b200 import GPUPathStage, PathBatch, _lib
+    P = phase("case_L001")
+    st = GPUPathStage(P, device="cuda", dtype=dtype)
+    gs = groups("case_L001")
+    coords, ipots, deg = gs[3]
+    bad = ipots[:4].copy()
+    bad[2, 1] = P.nph + 3
+    b = PathBatch([(coords[:4], bad, deg[:4])], device="cuda")
+    q = np.arange(1, 401) * 0.05
+    with pytest.raises(IndexError):
+        st.chi_reduce(b, q)
+    qt = torch.tensor(q, dtype=torch.float64, device="cuda")
+    S = st.linear_matrix(q).double().contiguous()
+    span = st._span(S)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def call(batch, order=None):
+        ps = st._paths_struct(batch, batch.coords, None)
+        if order is not None:
+            ps.order = order.data_ptr()
+        rows = torch.zeros(batch.nrows, 400, dtype=torch.float64, device="cuda")
+        n = int(st._lib.fg_chi_reduce_workspace(st._h, C.byref(ps), 400))
+        ws = torch.empty(n, dtype=torch.uint8, device="cuda")
+        cc = torch.empty(batch.n, st.E, dtype=st.cdtype, device="cuda")
+        rf = torch.empty(batch.n, dtype=torch.float64, device="cuda")
+        rc = st._lib.fg_chi_reduce(st._h, st.prec, C.byref(ps), 400, qt.data_ptr(), S.data_ptr(), span.data_ptr(),
+                                   rows.data_ptr(), cc.data_ptr(), rf.data_ptr(), ws.data_ptr(), n, stream)
+        return rc, rows, ps, cc, rf
+
+    rc, rows, ps, cc, rf = call(b)
+    msg = st._lib.fg_last_error().decode()
+    assert rc == _lib.FG_ERR_VALUE and "potential index" in msg
+    assert torch.isnan(rows).all()
+    rc2 = st._lib.fg_chi_reduce_noalloc(st._h, st.prec, C.byref(ps), 400, qt.data_ptr(), S.data_ptr(),
+                                        span.data_ptr(), rows.data_ptr(), stream)
+    assert rc2 == _lib.FG_ERR_VALUE and "potential index" in st._lib.fg_last_error().decode()
+    with pytest.raises(IndexError):
+        _lib.check(rc2)
+    # the backward of the same batch reports it too
+    g = torch.ones(1, 400, dtype=torch.float64, device="cuda")
+    gc = torch.empty_like(b.coords)
+    nb = int(st._lib.fg_chi_reduce_backward_workspace(st._h, C.byref(ps), 400))
+    wsb = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    rc3 = st._lib.fg_chi_reduce_backward(st._h, st.prec, C.byref(ps), 400, qt.data_ptr(), S.data_ptr(),
+                                         span.data_ptr(), st._span(S, True).data_ptr(), g.data_ptr(), cc.data_ptr(),
+                                         rf.data_ptr(), gc.data_ptr(), None, wsb.data_ptr(), nb, stream)
+    assert rc3 == _lib.FG_ERR_VALUE and "potential index" in st._lib.fg_last_error().decode()
+    # a valid batch with a launch order that names a path past n: reported, rows NaN
+    good = PathBatch([(coords[:4], ipots[:4], deg[:4])], device="cuda")
+    order = torch.tensor([0, 1, 7, 3], dtype=torch.int32, device="cuda")
+    rc4, rows4, *_ = call(good, order)
+    assert rc4 == _lib.FG_ERR_VALUE and "malformed" in st._lib.fg_last_error().decode()
+    assert torch.isnan(rows4).all()
+    # and the same batch with its own order is fine afterwards (the status word is cleared per call)
+    rc5, rows5, *_ = call(good)
+    assert rc5 == _lib.FG_OK and torch.isfinite(rows5).all()
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
 def test_larch_spline_convention_equals_reference(dtype):
     """spline_matrix (scipy UnivariateSpline s=0, the reference's stage.py:341-351) and chi_fine(..., "larch") on the
     W case's stored paths against the reference's (tests/golden/larch_W.npz): the matrix to 1e-12, chi to 1e-10 of its

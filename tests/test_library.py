@@ -68,3 +68,45 @@ def test_new_entry_points_refuse_bad_arguments_on_the_host():
     off = (C.c_int64 * 2)(0, 3)
     assert lib.fg_pf_windows(sl, off, 1, C.c_float(1e-3), w) == _lib.FG_OK
     assert list(w) == [0, 0, 1]
+
+
+def test_fused_entry_points_refuse_batches_without_their_summation_arrays():
+    """A batch whose rows, chunk offsets or summation order are missing is refused before any launch (the stage
+    handle is not read: the batch is checked first), so no kernel ever reads through a null device pointer."""
+    lib = _lib.load()
+    V = _lib.FG_ERR_VALUE
+    fake_stage = C.create_string_buffer(64)          # never dereferenced: the batch check fails first
+    dummy = C.create_string_buffer(64)
+
+    def paths(n, nrows, nchunks, row_chunks=True, bounds=True, order=True):
+        a = C.addressof(dummy)
+        return _lib.Paths(n, 3, nrows, a, a, a, a, None, a, a, a if order else None, a if bounds else None,
+                          a if row_chunks else None, nchunks)
+
+    bad = [paths(0, 2, 0, row_chunks=False),          # no paths, two rows, no row offsets
+           paths(5, 1, 1, row_chunks=False),
+           paths(5, 1, 1, bounds=False),              # chunks without their bounds
+           paths(5, 1, 0),                            # paths but no summation chunks
+           paths(5, 1, 1, order=False)]
+    for ps in bad:
+        assert lib.fg_chi_reduce(fake_stage, 0, C.byref(ps), 401, None, None, None, None, None, None, None, 0,
+                                 None) == V
+        assert lib.fg_chi_reduce_noalloc(fake_stage, 0, C.byref(ps), 401, None, None, None, None, None) == V
+        assert lib.fg_chi_reduce_backward(fake_stage, 0, C.byref(ps), 401, None, None, None, None, None, None, None,
+                                          None, None, None, 0, None) == V
+    with pytest.raises(ValueError, match="row_chunks"):
+        _lib.check(lib.fg_chi_reduce(fake_stage, 0, C.byref(bad[0]), 401, None, None, None, None, None, None, None,
+                                     0, None))
+
+
+def test_potential_index_errors_raise_index_error():
+    """The library's out-of-range potential report maps to the reference's exception for a bad table index."""
+    _lib.load()
+    import feffgpu_b200._lib as L
+    orig = L._lib.fg_last_error
+    try:
+        L._lib.fg_last_error = lambda: b"potential index outside 0..nph (the rows are NaN)"
+        with pytest.raises(IndexError):
+            L.check(L.FG_ERR_VALUE)
+    finally:
+        L._lib.fg_last_error = orig

@@ -31,10 +31,11 @@ def _ref_rows(st, b, q, S, span):
     return rows
 
 
-def _noalloc_rows(st, b, q, S, span):
+def _noalloc_rows(st, b, q, S, span, rows=None):
     from feffgpu_b200 import _lib
     ps = st._paths_struct(b, b.coords, None)
-    rows = torch.full((b.nrows, q.shape[0]), float("nan"), dtype=torch.float64, device="cuda")
+    if rows is None:
+        rows = torch.full((b.nrows, q.shape[0]), float("nan"), dtype=torch.float64, device="cuda")
     _lib.check(st._lib.fg_chi_reduce_noalloc(st._h, st.prec, C.byref(ps), q.shape[0], q.data_ptr(), S.data_ptr(),
                                              span.data_ptr(), rows.data_ptr(), torch.cuda.current_stream().cuda_stream))
     return rows
@@ -60,6 +61,16 @@ def test_no_alloc_entry_point_equals_fg_chi_reduce(dtype):
     b2 = PathBatch([(gs[3][0][:5], gs[3][1][:5], gs[3][2][:5])], device="cuda")
     np.testing.assert_allclose(_noalloc_rows(st, b2, q, S, span).cpu().numpy(),
                                _ref_rows(st, b2, q, S, span).cpu().numpy(), rtol=0, atol=1e-12 * scale)
+    # the defining property: once the scratch address is known (the calls above), calls take no device memory --
+    # the GPU's free memory is the same before and after two more calls into a buffer allocated beforehand
+    out = torch.empty(b.nrows, q.shape[0], dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        _noalloc_rows(st, b, q, S, span, out)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    np.testing.assert_allclose(out.cpu().numpy(), ref.cpu().numpy(), rtol=0, atol=1e-12 * scale)
 
 
 def test_no_alloc_entry_point_refuses_a_batch_beyond_its_scratch():
