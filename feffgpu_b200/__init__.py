@@ -7,10 +7,9 @@ rebinds the reference's names to them so that its chain, MD-EXAFS and RMC-EXAFS 
 from .pad import BOHR, HART, PhaseData, load_phase, read_phase_pad, resample_phase, save_phase
 from .stage import GPUPathStage
 from .batch import PathBatch
-from .compare import hanning, r_factor
 
 __all__ = ["GPUPathStage", "PathBatch", "PhaseData", "read_phase_pad", "load_phase", "resample_phase", "save_phase",
-           "r_factor", "hanning", "install", "BOHR", "HART"]
+           "install", "BOHR", "HART"]
 
 
 def install(finder: bool = True) -> list[str]:

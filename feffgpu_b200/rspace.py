@@ -3,7 +3,8 @@
 Conventions of the reference's ``src/feffgpu/exafs/transform.py:24-145`` (xraylarch's): uniform k grid from zero with
 step 0.05 1/A, Hanning window with sills centred on kmin and kmax and dk wide, chi(R) = (kstep / sqrt(pi)) FFT of
 k^kweight chi(k) window zero-padded to 2048 points, R = pi / (kstep 2048) * arange(1024), and the R-factor
-sum |chi_R(model) - chi_R(target)|^2 / sum |chi_R(target)|^2 over rmin <= R <= rmax (real and imaginary parts).
+sum |chi_R(model) - chi_R(target)|^2 / sum |chi_R(target)|^2 over rmin <= R <= rmax (real and imaginary parts), the R
+window taken on the reference's FP32 R grid.
 
 The transform restricted to the R window is one dense (NR, NK) complex matrix (``transform_matrix``): the same numbers
 as the padded FFT.  The misfit and its gradient are one CUDA kernel (``fg_rspace_misfit``, one block per row, FP64,
@@ -35,34 +36,60 @@ class FitWindow:
 
 
 def hanning(k: np.ndarray, kmin: float, kmax: float, dk: float = 1.0) -> np.ndarray:
-    k = np.asarray(k, float)
+    """Hanning window with sills centred on kmin and kmax, dk wide (dk = 0: rectangular), in k's precision."""
+    k = np.asarray(k)
+    if not np.issubdtype(k.dtype, np.floating):
+        k = k.astype(float)
     if dk <= 0:
-        return ((k >= kmin) & (k <= kmax)).astype(float)
-    up = 0.5 * (1 - np.cos(np.pi * np.clip((k - (kmin - dk / 2)) / dk, 0, 1)))
-    down = 0.5 * (1 + np.cos(np.pi * np.clip((k - (kmax - dk / 2)) / dk, 0, 1)))
-    return up * down
+        return ((k >= kmin) & (k <= kmax)).astype(k.dtype)
+    t = k.dtype.type
+    rise = t(0.5) * (t(1) - np.cos(t(np.pi) * np.clip((k - t(kmin - dk / 2)) / t(dk), 0, 1)))
+    fall = t(0.5) * (t(1) + np.cos(t(np.pi) * np.clip((k - t(kmax - dk / 2)) / t(dk), 0, 1)))
+    return rise * fall
 
 
-def transform_matrix(nk: int, window: FitWindow = FitWindow()):
-    """(F (NR, NK) complex128, R (NR,)): chi_R = F chi restricted to rmin <= R <= rmax."""
-    k = KSTEP * np.arange(nk)
-    r = RSTEP * np.arange(NFFT // 2)
-    keep = (r >= window.rmin) & (r <= window.rmax)
-    w = hanning(k, window.kmin, window.kmax, window.dk) * k ** window.kweight
+def r_window(window: FitWindow) -> np.ndarray:
+    """Indices of the R points rmin <= R <= rmax.  The reference forms its R grid in FP32
+    (``transform.py:125-127``) and compares it with the window's limits in FP32; so does this mask, so that a limit
+    that falls on a grid point keeps or drops that point as the reference does."""
+    r = (np.float32(RSTEP) * np.arange(NFFT // 2, dtype=np.float32)).astype(np.float32)
+    return np.nonzero((r >= np.float32(window.rmin)) & (r <= np.float32(window.rmax)))[0]
+
+
+def transform_matrix(nk: int, window: FitWindow = FitWindow(), k_dtype=np.float64):
+    """(F (NR, NK) complex128, R (NR,)): chi_R = F chi restricted to rmin <= R <= rmax.
+
+    k_dtype float64: the k grid and window of ``r_factor_torch`` (``transform.py:130-145``); float32: those of
+    ``PathSpectra.misfit`` (``exafs/forward.py:87-90, 165-168``), which holds k and forms the window in FP32 and
+    widens both to FP64 for the transform."""
+    k = (KSTEP * np.arange(nk)).astype(k_dtype)
+    m = r_window(window)
+    w = hanning(k, window.kmin, window.kmax, window.dk).astype(np.float64)
+    k = k.astype(np.float64)
+    w = w * k ** window.kweight
     # FFT restricted to the kept R: sum_n x_n exp(-2 pi i m n / NFFT), m = index of R
-    m = np.nonzero(keep)[0]
     F = np.exp(-2j * np.pi * np.outer(m, np.arange(nk)) / NFFT) * (KSTEP / math.sqrt(math.pi)) * w[None, :]
-    return F, r[keep]
+    return F, RSTEP * m
+
+
+def r_factor(data, fit, window: FitWindow = FitWindow()) -> float:
+    """R-factor of one spectrum ``fit`` against ``data``, both on k = KSTEP * arange(NK) (numpy, host):
+    sum |chi_R(fit) - chi_R(data)|^2 / sum |chi_R(data)|^2 over the R window -- the comparison of the reference's
+    ``compare.py:17-27`` and ``r_factor_torch`` with the transform of ``transform_matrix``."""
+    data, fit = np.asarray(data, float), np.asarray(fit, float)
+    F, _ = transform_matrix(data.shape[-1], window)
+    d = F @ data
+    return float(np.sum(np.abs(F @ fit - d) ** 2) / np.sum(np.abs(d) ** 2))
 
 
 class RSpaceMisfit:
     """R-factor of rows chi (B, NK) on k = KSTEP * arange(NK) against a target (NK,), on a CUDA device."""
 
-    def __init__(self, nk: int, target, window: FitWindow = FitWindow(), device="cuda"):
+    def __init__(self, nk: int, target, window: FitWindow = FitWindow(), device="cuda", k_dtype=np.float64):
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise RuntimeError("feffgpu_b200 evaluates the misfit on CUDA devices only (no CPU path)")
-        F, self.r = transform_matrix(nk, window)
+        F, self.r = transform_matrix(nk, window, k_dtype)
         self.nk = nk
         self.F = torch.tensor(F, dtype=torch.complex128, device=self.device).contiguous()     # (NR, NK)
         self._lib = _lib.load()

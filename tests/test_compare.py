@@ -1,7 +1,8 @@
-"""The package's R-factor equals the oracle's restatement of the reference's compare.py."""
+"""The package's R-factor (rspace.r_factor, the dense restricted transform) equals the oracle's restatement of the
+reference's compare.py (a padded FFT) on the uniform k grid from zero."""
 import numpy as np
 
-from feffgpu_b200 import r_factor
+from feffgpu_b200.rspace import FitWindow, r_factor
 from oracle import oracle as O
 
 
@@ -10,5 +11,7 @@ def test_r_factor_matches():
     rng = np.random.default_rng(0)
     a = np.sin(2 * 2.5 * k) * np.exp(-k / 10) + 0.01 * rng.normal(size=k.size)
     b = a + 1e-3 * rng.normal(size=k.size)
-    assert r_factor(k, a, b, kmin=3, kmax=19) == O.r_factor(k, a, b, kmin=3, kmax=19)
-    assert r_factor(k, a, a) == 0.0
+    for kw in (dict(kmin=3, kmax=19, rmin=1, rmax=6), dict(kmin=2, kmax=14, rmin=1.2, rmax=5.5)):
+        ours = r_factor(a, b, FitWindow(**kw))
+        assert abs(ours - O.r_factor(k, a, b, **kw)) <= 1e-12 * ours
+    assert r_factor(a, a) == 0.0

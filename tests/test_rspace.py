@@ -56,3 +56,47 @@ def test_misfit_kernel_and_gradient():
         assert abs(float(v[b]) - val) <= 1e-12 * max(val, 1e-30) + 1e-15
         assert np.abs(x.grad[b].cpu().numpy() - float(w[b]) * g).max() <= 1e-10 * np.abs(g).max() + 1e-15
     assert float(v[1]) < 1e-28
+
+
+def _fixture_windows():
+    z = np.load(__import__("pathlib").Path(__file__).resolve().parent / "golden" / "rspace_ref.npz")
+    out = []
+    for i in range(3):
+        w = z[f"win_{i}"]
+        out.append((i, FitWindow(w[0], w[1], w[2], int(w[3]), w[4], w[5])))
+    return z, out
+
+
+def test_misfit_pinned_to_the_reference_losses():
+    """The R window, the loss and its gradient equal the reference's own R-space losses (tests/golden/rspace_ref.npz,
+    generated from its source): r_factor_torch (transform.py:130-145) with the FP64 k grid, and PathSpectra.misfit
+    (exafs/forward.py:165-168) with its FP32 k grid and window.  Both keep the R points of the FP32 R grid
+    (transform.py:125-127) -- one window's lower limit falls on a grid point the FP32 grid drops.  Tolerances: 1e-12
+    relative for the FP64 form; 1e-7 for the FP32-grid form (its window values are FP32 cosines, equal to the
+    reference's to an FP32 rounding)."""
+    from feffgpu_b200.rspace import r_window
+    z, wins = _fixture_windows()
+    for i, win in wins:
+        assert np.array_equal(r_window(win), z[f"keep_{i}"])
+        for kd, key, tol in ((np.float64, "", 1e-12), (np.float32, "32", 1e-7)):
+            F, _ = transform_matrix(401, win, kd)
+            for b in range(z["models"].shape[0]):
+                v, g = _misfit_np(F, z["data"], z["models"][b])
+                ref_v, ref_g = z[f"R{key}_{i}"][b], z[f"grad{key}_{i}"][b]
+                assert abs(v - ref_v) <= tol * ref_v, (i, key, b)
+                assert np.abs(g - ref_g).max() <= tol * np.abs(ref_g).max(), (i, key, b)
+
+
+@pytest.mark.gpu
+def test_misfit_kernel_pinned_to_the_reference_losses():
+    """The misfit kernel (value and gradient) against the reference's losses of the fixture, both k-grid forms."""
+    z, wins = _fixture_windows()
+    for i, win in wins:
+        for kd, key, tol in ((np.float64, "", 1e-12), (np.float32, "32", 1e-7)):
+            mis = RSpaceMisfit(401, z["data"], win, device="cuda", k_dtype=kd)
+            x = torch.tensor(z["models"], device="cuda", requires_grad=True)
+            v = mis(x)
+            v.sum().backward()
+            ref_v, ref_g = z[f"R{key}_{i}"], z[f"grad{key}_{i}"]
+            np.testing.assert_allclose(v.detach().cpu().numpy(), ref_v, rtol=tol, atol=0)
+            assert np.abs(x.grad.cpu().numpy() - ref_g).max() <= tol * np.abs(ref_g).max()
