@@ -84,11 +84,17 @@ def workload(rank: int, world: int, scale: float = 1.0, finder: str = "gpu"):
     return P, groups
 
 
-def workload_config(n_paths: int, world: int) -> dict:
-    """The workload's description, the same on both arms of the benchmark."""
+def workload_config(groups, world: int) -> dict:
+    """The workload's description, built from the path groups, the same on both arms of the benchmark."""
+    legs: dict = {}
+    for c, *_ in groups:
+        legs[int(c.shape[1])] = legs.get(int(c.shape[1]), 0) + len(c)
+    n_paths = sum(legs.values())
     return {"workload": f"Fe/O/Pt packing 3000 atoms, 2 Fe K absorbers per GPU, every path finder path of 2-8 legs "
                         f"to 8 A, {n_paths} paths per GPU, lmax 24 x {NK} k, chi on {NK} k",
-            "paths_per_gpu": n_paths, "nk": NK, "parallelism": f"dp{world} (absorbers per rank)"}
+            "paths_per_gpu": n_paths, "nk": NK, "energies": NK, "legs": dict(sorted(legs.items())),
+            "parallelism": f"dp{world} (absorbers per rank)",
+            "l2": "GPU arm: flushed between timed steps (256 MB write)"}
 
 
 def finder_leg(args, dev, world, rank):
@@ -186,7 +192,8 @@ class Clocks:
 # ------------------------------------------------------------------------------------------------ CPU legs
 def cpu_sample(P, groups, budget_s: float, nthreads: int):
     """The oracle (FP64, C, pthreads) on a stratified sample of every leg count, extrapolated to the workload:
-    cchi of the sampled paths, their fine-grid signal and weighted sum.  Returns (path·k/s, description)."""
+    cchi of the sampled paths, their fine-grid signal and sum.  Returns (path·k/s, description, samples) with
+    samples {nleg: (coords, ipots, chi summed over the sampled paths)} for the parity check."""
     from oracle import oracle as O
     orc = O.Oracle(P)
     S = orc.linear_matrix(Q)
@@ -203,21 +210,40 @@ def cpu_sample(P, groups, budget_s: float, nthreads: int):
         t = time.perf_counter()
         cc, rf = orc.cchi(c[sel], ip[sel], nthreads=nthreads)
         chi = O.chi_fine(cc, rf, Q, S).sum(0)
-        return (time.perf_counter() - t) / len(sel), len(sel), chi
+        return (time.perf_counter() - t) / len(sel), len(sel), chi, c[sel], ip[sel]
 
     # calibrate with two paths per leg count, then spend the budget in proportion to each bucket's total time
     per = {n: run(n, 2)[0] for n in counts}
     full = sum(counts[n] * per[n] for n in counts)
     scale = budget_s / max(full, 1e-9)
-    t_total, sampled = 0.0, 0
+    t_total, sampled, samples = 0.0, 0, {}
     for n in sorted(counts):
         m = max(4, int(counts[n] * scale))
-        tp, got, _ = run(n, m)
+        tp, got, chi, c, ip = run(n, m)
         t_total += counts[n] * tp
         sampled += got
+        samples[n] = (c, ip, chi)
     n_paths = sum(counts.values())
     return n_paths * NK / t_total, f"stratified sample of {sampled} of {n_paths} paths (every leg count), " \
-                                    f"timed per leg count and extrapolated to the full batch"
+                                    f"timed per leg count and extrapolated to the full batch", samples
+
+
+def parity_vs_oracle(P, samples, dev):
+    """This package's rows of the CPU baseline's stratified sample (one row per leg count, every sampled path weight
+    one) against the oracle's FP64 sums of the same paths: R-factor per leg count, mixed and FP64 forms."""
+    import torch
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    from feffgpu_b200.rspace import FitWindow, r_factor
+    win = FitWindow(kmin=3.0, kmax=19.0, rmin=1.0, rmax=8.0)
+    legs = sorted(samples)
+    b = PathBatch([(samples[n][0], samples[n][1], None, np.full(len(samples[n][0]), i)) for i, n in enumerate(legs)],
+                  nrows=len(legs), device=dev)
+    res = {"paths": b.n, "legs": {int(n): int(len(samples[n][0])) for n in legs}}
+    for d, key in ((torch.complex64, "R_mixed_vs_oracle"), (torch.complex128, "R_fp64_vs_oracle")):
+        with torch.no_grad():
+            rows = GPUPathStage(P, device=dev, dtype=d).chi_reduce(b, Q).cpu().numpy()
+        res[key] = max(r_factor(samples[n][2], rows[i], win) for i, n in enumerate(legs))
+    return res
 
 
 def extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms):
@@ -274,7 +300,7 @@ def md_extra(args, dev, timed, world, rank):
     import torch
     from feffgpu_b200 import GPUPathStage, PathBatch
     from feffgpu_b200 import workloads as W
-    from feffgpu_b200.compare import r_factor
+    from feffgpu_b200.rspace import FitWindow, r_factor
     from feffgpu_b200.pad import phase_from_npz
     from feffgpu_b200.pathfinder import GPUPathFinder
     P = phase_from_npz(np.load(ROOT / "tests" / "golden" / "cfg4_fe_phase.npz"), prefix="ph_")
@@ -310,7 +336,8 @@ def md_extra(args, dev, timed, world, rank):
         st64 = GPUPathStage(P, device=dev, dtype=torch.complex128, autotune=not args.no_autotune)
         ms64, _ = timed(lambda: st64.chi_reduce(batch, Q, S), 2, 1)
         ref = st64.chi_reduce(batch, Q, S).cpu().numpy()
-    R = [r_factor(Q, ref[f], rows[f], kmin=3.0, kmax=19.0, rmin=1.0, rmax=5.5) for f in range(frames)]
+    win = FitWindow(kmin=3.0, kmax=19.0, rmin=1.0, rmax=5.5)
+    R = [r_factor(ref[f], rows[f], win) for f in range(frames)]
     out = {"value": world * batch.n * NK / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "paths_per_gpu": batch.n,
            "frames": frames, "absorbers_per_frame": absorbers, "legs": batch.counts,
            "path_finder_ms": ms_find, "fp64_ms_per_step": ms64, "r_factor_vs_fp64_max": max(R),
@@ -320,27 +347,39 @@ def md_extra(args, dev, timed, world, rank):
     return out
 
 
-def reference_gpu_leg(args, P, groups, dev, ours: dict):
-    """The reference's own GPUPathStage (installed unmodified under baseline/_ref) on this GPU, on a sample of the
-    same batch: per leg count one chunk of up to 4096 paths, the chunk size of its callers (src/feffgpu/chain.py:47),
-    cchi -> chi_fine -> degeneracy-weighted sum into the absorber rows, timed with CUDA events after a warm-up chunk
-    and extrapolated by paths per leg count.  complex64 (its production default) and complex128 forward; complex64
-    forward+backward through non-reentrant checkpointing (src/feffgpu/exafs/forward.py:158-159) in chunks of up to
-    2048 paths, its PathSpectra's default chunk (forward.py:69).  ``ours`` holds this package's ms per step of the
-    same batch to put beside them."""
-    import dataclasses
-    import torch
+def _ref_stage_class():
+    """The reference's GPUPathStage and PhaseData from baseline/_ref, or (None, reason)."""
     ref = ROOT / "baseline" / "_ref"
     if not (ref / "feffgpu" / "stage.py").exists():
-        return {"unavailable": "reference not installed under baseline/_ref"}
+        return None, "reference not installed under baseline/_ref"
     sys.path.insert(0, str(ref))
     try:
         from feffgpu.pad import PhaseData as RefPhase
         from feffgpu.stage import GPUPathStage as RefStage
     except Exception as err:                                   # noqa: BLE001 - report, do not fail the bench
-        return {"unavailable": f"reference import failed: {err!r}"[:200]}
+        return None, f"reference import failed: {err!r}"[:200]
     finally:
         sys.path.remove(str(ref))
+    return (RefStage, RefPhase), ""
+
+
+def reference_gpu_leg(args, P, groups, dev, ours: dict, uuid):
+    """The reference's own GPUPathStage (installed unmodified under baseline/_ref) on this GPU, on a sample of the
+    same batch, the way its callers run it: per leg count chunks of up to 4096 paths (src/feffgpu/chain.py:47),
+    cchi -> chi_fine -> degeneracy-weighted sum into the absorber rows.  Per leg count three chunks (the first three
+    of that leg count, or the same chunk again when it has fewer paths) are timed with CUDA events after a warm-up
+    chunk; the median time per path is extrapolated by the paths of that leg count.  complex64 (its production
+    default) and complex128 forward; complex64 forward+backward through non-reentrant checkpointing
+    (src/feffgpu/exafs/forward.py:158-159) in chunks of up to 2048 paths, its PathSpectra's default chunk
+    (forward.py:69).  The clocks are sampled over the leg.  ``ours`` holds this package's ms per step of the same
+    batch.  Parity: the first chunk of every leg count is also evaluated by this package (mixed and FP64 forms) and
+    compared with the reference's complex128 rows and per-path cchi."""
+    import torch
+    cls, why = _ref_stage_class()
+    if cls is None:
+        return {"unavailable": why}, None
+    RefStage, RefPhase = cls
+    import dataclasses
     from torch.utils.checkpoint import checkpoint
     refP = RefPhase(**{f.name: getattr(P, f.name) for f in dataclasses.fields(RefPhase)})
     by_leg: dict = {}
@@ -353,57 +392,102 @@ def reference_gpu_leg(args, P, groups, dev, ours: dict):
         torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        fn()
+        res = fn()
         e1.record()
         e1.synchronize()
-        return e0.elapsed_time(e1)
+        return e0.elapsed_time(e1), res
 
-    def arm(dtype, chunk, grad):
+    keep = {}
+
+    def arm(dtype, chunk, grad, save=False):
         stage = RefStage(refP, device=dev, dtype=dtype)
         S = stage.linear_matrix(Q)
-        total, sampled = 0.0, 0
+        total, sampled, chunks = 0.0, 0, 0
         for n, (c, ip, deg, row) in by_leg.items():
             m = min(len(c), chunk)
-            coords = torch.as_tensor(c[:m], device=dev).to(stage.rdtype)
-            ipots = torch.as_tensor(ip[:m], device=dev, dtype=torch.long)
-            w = torch.as_tensor(deg[:m], device=dev, dtype=torch.float64)[:, None]
-            rows = torch.as_tensor(row[:m], device=dev, dtype=torch.long)
+            per_path = []
+            for j in range(4):                                   # chunk 0 twice: warm-up, then timed
+                lo = (max(j - 1, 0) * m) if (max(j - 1, 0) + 1) * m <= len(c) else 0
+                coords = torch.as_tensor(c[lo:lo + m], device=dev).to(stage.rdtype)
+                ipots = torch.as_tensor(ip[lo:lo + m], device=dev, dtype=torch.long)
+                w = torch.as_tensor(deg[lo:lo + m], device=dev, dtype=torch.float64)[:, None]
+                rows = torch.as_tensor(row[lo:lo + m], device=dev, dtype=torch.long)
 
-            def fwd(x):
-                return stage.chi_fine(*stage.cchi(x, ipots), Q, S, "feff")
+                def fwd(x):
+                    return stage.chi_fine(*stage.cchi(x, ipots), Q, S, "feff")
 
-            def step():
-                out = torch.zeros(2, NK, device=dev, dtype=torch.float64)
-                if grad:
-                    x = coords.clone().requires_grad_(True)
-                    chi = checkpoint(fwd, x, use_reentrant=False)
-                    out = out.index_add(0, rows, w * chi.to(torch.float64))
-                    out.sum().backward()
-                else:
-                    with torch.no_grad():
-                        out = out.index_add(0, rows, w * fwd(coords).to(torch.float64))
-                return out.cpu()
+                def step():
+                    out = torch.zeros(2, NK, device=dev, dtype=torch.float64)
+                    if grad:
+                        x = coords.clone().requires_grad_(True)
+                        chi = checkpoint(fwd, x, use_reentrant=False)
+                        out = out.index_add(0, rows, w * chi.to(torch.float64))
+                        out.sum().backward()
+                    else:
+                        with torch.no_grad():
+                            out = out.index_add(0, rows, w * fwd(coords).to(torch.float64))
+                    return out.cpu()
 
-            step()                                              # warm-up: allocator, kernels, caches
-            total += ev_time(step) * len(c) / m
-            sampled += m
+                t, out = ev_time(step)
+                if j == 0:
+                    if save:
+                        with torch.no_grad():
+                            cc, _ = stage.cchi(coords, ipots)
+                        keep[n] = (out.numpy(), cc.cpu().numpy(), lo, m)
+                    continue
+                per_path.append(t / m)
+                sampled += m
+                chunks += 1
+            total += float(np.median(per_path)) * len(c)
             torch.cuda.empty_cache()
-        return total, sampled
+        return total, sampled, chunks
 
     out = {"source": "the reference's GPUPathStage, pip-installed unmodified into baseline/_ref, on this GPU"}
-    for key, dtype, chunk, grad, mine in (("fwd_c64", torch.complex64, 4096, False, ours.get("fwd")),
-                                          ("fwd_c128", torch.complex128, 4096, False, ours.get("fwd64")),
-                                          ("fwd_bwd_c64", torch.complex64, 2048, True, ours.get("fwd_bwd"))):
-        try:
-            ms, sampled = arm(dtype, chunk, grad)
-        except torch.cuda.OutOfMemoryError as err:
-            out[key] = {"unavailable": f"out of memory: {err}"[:200]}
-            torch.cuda.empty_cache()
-            continue
-        out[key] = {"value": n_paths * NK / (ms * 1e-3), "unit": UNIT, "ms_full_batch": ms,
-                    "sample": f"{sampled} of {n_paths} paths (one chunk per leg count), extrapolated per leg count",
-                    "ours_over_reference": (ms / mine) if mine else None}
-    return out
+    with Clocks(uuid) as clk:
+        for key, dtype, chunk, grad, mine in (("fwd_c64", torch.complex64, 4096, False, ours.get("fwd")),
+                                              ("fwd_c128", torch.complex128, 4096, False, ours.get("fwd64")),
+                                              ("fwd_bwd_c64", torch.complex64, 2048, True, ours.get("fwd_bwd"))):
+            try:
+                ms, sampled, chunks = arm(dtype, chunk, grad, save=(key == "fwd_c128"))
+            except torch.cuda.OutOfMemoryError as err:
+                out[key] = {"unavailable": f"out of memory: {err}"[:200]}
+                torch.cuda.empty_cache()
+                continue
+            out[key] = {"value": n_paths * NK / (ms * 1e-3), "unit": UNIT, "ms_full_batch": ms,
+                        "sample": f"{chunks} timed chunks ({sampled} paths of {n_paths}), three per leg count, "
+                                  f"median time per path extrapolated per leg count",
+                        "ours_over_reference": (ms / mine) if mine else None}
+    out["clocks"] = clk.summary()
+    return out, (keep, by_leg)
+
+
+def parity_vs_reference(P, saved, dev):
+    """This package's rows and cchi of the reference leg's first chunk of every leg count against the reference's
+    complex128 ones: R-factor per (leg count, absorber row) of the mixed and FP64 rows, and the largest per-path
+    |cchi - cchi_ref| / max|cchi_ref| of the mixed form."""
+    import torch
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    from feffgpu_b200.rspace import FitWindow, r_factor
+    keep, by_leg = saved
+    win = FitWindow(kmin=3.0, kmax=19.0, rmin=1.0, rmax=8.0)
+    res = {"R_mixed_vs_ref_fp64": 0.0, "R_fp64_vs_ref_fp64": 0.0, "max_rel_cchi_mixed": 0.0, "paths": 0}
+    st = {d: GPUPathStage(P, device=dev, dtype=d) for d in (torch.complex64, torch.complex128)}
+    for n, (ref_rows, ref_cc, lo, m) in keep.items():
+        c, ip, deg, row = (v[lo:lo + m] for v in by_leg[n])
+        b = PathBatch([(c, ip, deg, row)], nrows=2, device=dev)
+        for d, key in ((torch.complex64, "R_mixed_vs_ref_fp64"), (torch.complex128, "R_fp64_vs_ref_fp64")):
+            with torch.no_grad():
+                rows = st[d].chi_reduce(b, Q).cpu().numpy()
+            for r in range(2):
+                if np.abs(ref_rows[r]).max() > 0:
+                    res[key] = max(res[key], r_factor(ref_rows[r], rows[r], win))
+        with torch.no_grad():
+            cc, _ = st[torch.complex64].cchi(torch.as_tensor(c), torch.as_tensor(ip))
+        res["max_rel_cchi_mixed"] = max(res["max_rel_cchi_mixed"],
+                                        float(np.abs(cc.cpu().numpy() - ref_cc).max() / np.abs(ref_cc).max()))
+        res["paths"] += m
+    res["window"] = "k 3-19, R 1-8, kw 2; rows per (leg count, absorber) of the first reference chunk of each leg count"
+    return res
 
 
 def reference_cpu_leg(P, groups, per_leg: int = 48):
@@ -654,19 +738,27 @@ def main():
         if rank != 0:
             return
         P, groups = workload(0, 1, args.paths_scale, finder="oracle")
-        vals = []
+        vals, walls, timed_paths = [], [], 0
         for i in range(args.warmup + args.steps):
-            v, desc = cpu_sample(P, groups, budget_s=max(2.0, args.cpu_budget / 3), nthreads=nthreads)
+            t0 = time.perf_counter()
+            v, desc, smp = cpu_sample(P, groups, budget_s=max(2.0, args.cpu_budget / 3), nthreads=nthreads)
+            wall = time.perf_counter() - t0
             if i >= args.warmup:
                 vals.append(v)
+                walls.append(wall)
+                timed_paths = sum(len(x[0]) for x in smp.values())
         v = float(np.median(vals))
         n_paths = sum(len(g[0]) for g in groups)
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": n_paths * NK / v * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
-            "config": dict(workload_config(n_paths, world=args.gpus),
-                           impl="FP64 C port of the reference's path stage (oracle), host cores"),
+            "warmup": args.warmup, "ms_per_step": float(np.median(walls)) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+            "config": workload_config(groups, world=args.gpus),
+            "reference_impl": "FP64 C port of the reference's path stage (oracle), all host cores",
+            "timing": {"step": "one stratified sample of the batch (every leg count), timed per leg count; value = "
+                               "the batch's path·k over the per-leg-count extrapolated time",
+                       "timed_paths_per_step": timed_paths, "timed_s": float(np.sum(walls)),
+                       "ms_full_batch_extrapolated": n_paths * NK / v * 1e3},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
@@ -732,15 +824,14 @@ def main():
             ms, kern = timed(lambda: stage.chi_reduce(batch, Q, S), args.steps, args.warmup, kernel_time=True)
     value = world * n_paths * NK / (ms * 1e-3)
 
-    e2e = fwd_bwd = plain = md = rmc = pf = pairs = ref_gpu = None
+    e2e = fwd_bwd = plain = md = rmc = pf = pairs = ref_gpu = saved = None
     if not args.no_extras:
         pf = finder_leg(args, dev, world, rank)
         pairs = pairs_leg(args, dev, world, rank)
         e2e, fwd_bwd, plain = extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms)
         if not args.no_ref_gpu and rank == 0:
-            ref_gpu = reference_gpu_leg(args, P, groups, dev, {
-                "fwd": ms, "fwd64": plain["ms_per_step"],
-                "fwd_bwd": (fwd_bwd or {}).get("ms_per_step")})
+            ref_gpu, saved = reference_gpu_leg(args, P, groups, dev, {
+                "fwd": ms, "fwd64": plain["ms_per_step"], "fwd_bwd": (fwd_bwd or {}).get("ms_per_step")}, uuid)
         if args.md_frames > 0:
             md = md_extra(args, dev, timed, world, rank)
         if args.rmc_steps > 0:
@@ -752,39 +843,67 @@ def main():
     flops = batch_flops(batch.nleg.cpu().numpy(), batch.ipots.cpu().numpy(), stage.lmax.cpu().numpy())
     kern_ms = float(np.mean(kern)) if kern else None
     achieved = flops / (kern_ms * 1e-3) / 1e12 if kern_ms else None
-    traffic = None
+    traffic, traffic_src = None, None
     tf = ROOT / "profiles" / "k_fused_feopt_traffic.txt"
     if tf.exists():
         for line in tf.read_text().splitlines():
             if line.startswith("bytes_per_launch"):
                 traffic = float(line.split("=")[1])
+            if line.startswith("captured"):
+                traffic_src = line.split("=", 1)[1].strip()
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
             "frac": achieved / peak.value if achieved else None, "traffic": traffic,
+            "traffic_source": f"not measured in this run: ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                              f"full-size launch, profiles/k_fused_feopt_traffic.txt ({traffic_src})",
             "kernel": "k_fused (per-path signal, all leg counts, one persistent launch)",
             "kernel_ms": kern_ms, "flops_per_launch": flops,
             "peak_source": "measured on this GPU by fg_fp32_fma_peak (FFMA chains on every SM); "
                            "MEASURED_PEAKS.json holds no FP32 figure"}
 
     cpu = ref_cpu = None
+    parity = {}
     if rank == 0 and not args.no_cpu:
-        v, desc = cpu_sample(P, groups, budget_s=args.cpu_budget, nthreads=nthreads)
+        v, desc, samples = cpu_sample(P, groups, budget_s=args.cpu_budget, nthreads=nthreads)
         cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": desc}
+        parity["oracle"] = parity_vs_oracle(P, samples, dev)
         if not args.no_ref_gpu:
             ref_cpu = reference_cpu_leg(P, groups)
+    if saved is not None:
+        parity["reference_gpu_stage"] = parity_vs_reference(P, saved, dev)
 
+    # the figures beside the headline, gathered last so that they close the line
+    def g(d, *k):
+        for key in k:
+            d = (d or {}).get(key) if isinstance(d, dict) else None
+        return d
+    summary = {
+        "fwd_ms": ms, "fwd_bwd_ms": g(fwd_bwd, "ms_per_step"), "fwd_bwd_value": g(fwd_bwd, "value"),
+        "plain_fp64_ms": g(plain, "ms_per_step"), "e2e_value": g(e2e, "value"),
+        "roofline_frac": roof["frac"],
+        "parity_R_mixed_vs_oracle": g(parity, "oracle", "R_mixed_vs_oracle"),
+        "parity_R_fp64_vs_oracle": g(parity, "oracle", "R_fp64_vs_oracle"),
+        "parity_R_mixed_vs_reference_fp64": g(parity, "reference_gpu_stage", "R_mixed_vs_ref_fp64"),
+        "parity_R_fp64_vs_reference_fp64": g(parity, "reference_gpu_stage", "R_fp64_vs_ref_fp64"),
+        "parity_max_rel_cchi_mixed": g(parity, "reference_gpu_stage", "max_rel_cchi_mixed"),
+        "md_ms": g(md, "ms_per_step"), "md_fp64_ms": g(md, "fp64_ms_per_step"),
+        "md_R_vs_fp64_max": g(md, "r_factor_vs_fp64_max"),
+        "rmc_ms_per_step": g(rmc, "ms_per_step"), "path_finder_ms": g(pf, "ms"),
+        "reference_gpu_fwd_c64_ms": g(ref_gpu, "fwd_c64", "ms_full_batch"),
+        "reference_gpu_fwd_c128_ms": g(ref_gpu, "fwd_c128", "ms_full_batch"),
+        "reference_gpu_fwd_bwd_c64_ms": g(ref_gpu, "fwd_bwd_c64", "ms_full_batch"),
+    }
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32 (complex chain) + fp64 (phase argument, sums)", "data": "synthetic",
-        "config": dict(workload_config(n_paths, world), legs=batch.counts, energies=stage.E,
-                       l2="flushed between steps (256 MB write)"),
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "fwd_bwd": fwd_bwd, "plain_fp64": plain,
-        "md_batch": md, "rmc_refinement": rmc, "path_finder": pf,
-        "pair_tables": pairs, "reference_gpu": ref_gpu, "reference_cpu": ref_cpu,
+        "config": workload_config(groups, world),
         "autotune": {"fwd_warps": stage._launch[0], "bwd_warps": stage._launch[1],
                      "timed": [{"kind": k, "warps": w_, "ms": round(t_, 3)} for sig, k, w_, t_ in tuner.log
                                if sig.split("|")[1] == "p0"]},
-        "gpu_launches": 3 * args.steps, "clocks": clk.summary(),
+        "reference_cpu": ref_cpu, "pair_tables": pairs, "path_finder": pf, "md_batch": md, "rmc_refinement": rmc,
+        "reference_gpu": ref_gpu, "plain_fp64": plain, "fwd_bwd": fwd_bwd,
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "parity": parity,
+        "gpu_launches": 3 * args.steps, "clocks": clk.summary(), "summary": summary,
     }
     if rank == 0:
         print(json.dumps(out))

@@ -1,8 +1,8 @@
 """Generates the golden fixtures of tests/golden/ from the reference implementation (nmarcella/feffGPU).
 
-Run in a container where the reference is mounted (default /root/reference, or $FEFFGPU_REFERENCE):
+Run where a copy of the reference's source tree is at hand, giving its root (the directory holding src/feffgpu):
 
-    python tests/golden/make_golden.py [--only NAME ...]
+    python tests/golden/make_golden.py REFERENCE_ROOT [--only NAME ...]
 
 The reference is imported read-only from its source tree and run on the CPU in FP64 (complex128).  Outputs are small
 .npz files; nothing at test time reads the reference itself.
@@ -40,7 +40,6 @@ The reference is imported read-only from its source tree and run on the CPU in F
 from __future__ import annotations
 
 import argparse
-import os
 import sys
 import time
 from pathlib import Path
@@ -49,8 +48,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
-REF = Path(os.environ.get("FEFFGPU_REFERENCE", "/root/reference"))
-sys.path.insert(0, str(REF / "src"))
+REF: Path = Path()      # the reference's source root, set by main() from its required argument
+CASES: dict = {}
 sys.path.insert(0, str(REPO))
 
 import torch  # noqa: E402
@@ -58,8 +57,15 @@ import torch  # noqa: E402
 from feffgpu_b200.pad import phase_to_arrays, phase_from_npz, resample_phase  # noqa: E402
 from feffgpu_b200 import workloads as W  # noqa: E402
 
-CASES = {"W": REF / "tests/data/W", **{c: REF / "data/validation" / c for c in
-                                       ("A000", "A009", "A014", "A018", "L000", "L001")}}
+def set_reference(root: str) -> None:
+    """Import the reference read-only from root/src and locate FEFF's stored cases under root."""
+    global REF, CASES
+    REF = Path(root).resolve()
+    if not (REF / "src" / "feffgpu" / "stage.py").exists():
+        raise SystemExit(f"{REF} does not hold the reference's src/feffgpu")
+    sys.path.insert(0, str(REF / "src"))
+    CASES = {"W": REF / "tests/data/W", **{c: REF / "data/validation" / c for c in
+                                           ("A000", "A009", "A014", "A018", "L000", "L001")}}
 
 
 def parse_paths(fname):
@@ -429,6 +435,103 @@ def make_finder_feopt():
     print(f"finder_feopt: {time.time() - t:.1f} s")
 
 
+def make_bench_sample(per=48, per_cchi=4, seed=31):
+    """bench_sample.npz -- the parity gate on the benchmark's own paths: the reference finder's paths of the benchmark
+    packing (two central Fe absorbers, rmax 8 A, 8 legs, no importance cut, as finder_feopt.npz), a seeded stratified
+    sample of up to `per` paths of every (absorber, leg count) -- their index in the finder's output, atom sequences,
+    coordinates (FP32, as the finder forms them), potentials and degeneracies -- and the reference stage's FP64 (complex128) signals on the resampled 401-k tables:
+    rows (14, 401) = per (absorber, leg count) the degeneracy-weighted sum of chi_fine on q = 0.05 * arange(401)
+    (the benchmark's output grid), and cchi/reff of the first `per_cchi` sampled paths of every (absorber, leg
+    count)."""
+    from feffgpu.pad import PhaseData as RefPhase
+    from feffgpu.pathfinder import GPUPathFinder
+    import dataclasses
+    P0 = phase_from_npz(np.load(HERE / "cfg2_phase.npz"), prefix="ph_")
+    q = np.arange(401) * 0.05
+    P = resample_phase(P0, q)
+    refP = RefPhase(**{f.name: getattr(P, f.name) for f in dataclasses.fields(RefPhase)})
+    st = ref_stage(refP)
+    S = st.linear_matrix(q)
+    pos, lab, box = W.random_packing(3000, 0.08, 1.8, seed=2024)
+    ipot = np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
+    abs2 = W.central_atom(pos, box, lab, "Fe", 2)
+    rng = np.random.default_rng(seed)
+    f = GPUPathFinder(P0, device="cpu", rmax=8.0, nlegmax=8, critpw=0.0)
+    out = {"absorbers": np.asarray(abs2), "q": q, "per": np.asarray(per), "per_cchi": np.asarray(per_cchi)}
+    rows, keys = [], []
+    t = time.time()
+    for s_, ab in enumerate(abs2):
+        kept, _ = f.enumerate(pos, box, int(ab), ipot)
+        for nleg in range(2, 9):
+            coords, ipots, deg, _xp, atoms = kept[nleg]
+            n = int(coords.shape[0])
+            idx = np.sort(rng.choice(n, size=min(per, n), replace=False))
+            c = coords[idx].double()
+            ip = ipots[idx].long()
+            with torch.no_grad():
+                cc, rf = st.cchi(c, ip)
+                chi = st.chi_fine(cc, rf, q, S, "feff")
+            d = deg[idx].double()
+            rows.append((d[:, None] * chi).sum(0).numpy())
+            keys.append((s_, nleg))
+            out[f"idx_{s_}_{nleg}"] = idx.astype(np.int64)
+            out[f"atoms_{s_}_{nleg}"] = atoms[idx].numpy().astype(np.int64)
+            out[f"coords_{s_}_{nleg}"] = coords[idx].numpy()          # FP32, as the finder forms them
+            out[f"ipots_{s_}_{nleg}"] = ipots[idx].numpy().astype(np.int64)
+            out[f"deg_{s_}_{nleg}"] = d.numpy()
+            out[f"count_{s_}_{nleg}"] = np.asarray(n)
+            out[f"cchi_{s_}_{nleg}"] = cc[:per_cchi].numpy()
+            out[f"reff_{s_}_{nleg}"] = rf[:per_cchi].numpy()
+        print(f"bench_sample absorber {int(ab)}: {time.time() - t:.1f} s")
+    out["rows"] = np.stack(rows)
+    out["row_keys"] = np.asarray(keys, np.int64)
+    np.savez_compressed(HERE / "bench_sample.npz", **out)
+    print(f"bench_sample: {sum(len(out[f'idx_{a}_{n}']) for a, n in keys)} paths, {time.time() - t:.1f} s")
+
+
+def make_rspace(seed=41):
+    """rspace_ref.npz -- the reference's R-space loss on seeded spectra: for each window, the R-factor of model rows
+    (B, 401) against data (401,) on k = 0.05 * arange(401) and its gradient with respect to the rows, (a) by
+    r_factor_torch (src/feffgpu/exafs/transform.py:130-145; FP64 k and window) and (b) as PathSpectra.misfit forms it
+    (exafs/forward.py:87-90, 105-110, 165-168: k and the Hanning window in FP32, widened to FP64); both take the R
+    window on the FP32 R grid of transform.py:125-127.  One window's limits fall on R grid points, where the FP32 grid
+    decides which points are kept."""
+    from feffgpu.exafs import transform as T
+    rng = np.random.default_rng(seed)
+    k = T.KSTEP * np.arange(401)
+    kk = k[None, :]
+    data = (np.sin(2 * 2.3 * k) * np.exp(-0.01 * k ** 2) + 0.2 * np.sin(2 * 3.9 * k + 0.4) * np.exp(-0.02 * k ** 2)) \
+        / np.maximum(k, 0.5)
+    models = data[None] * (1 + 0.05 * rng.normal(size=(3, 1))) + 0.01 * rng.normal(size=(3, 401)) * np.exp(-kk / 8)
+    windows = [T.FitWindow(3.0, 14.0, 1.0, 2, 1.0, 6.0), T.FitWindow(2.0, 18.0, 0.5, 3, 1.2, 5.0),
+               T.FitWindow(3.0, 14.0, 1.0, 1, 25 * T.RSTEP, 150 * T.RSTEP)]
+    out = {"k": k, "data": data, "models": models}
+    for i, w in enumerate(windows):
+        out[f"win_{i}"] = np.array([w.kmin, w.kmax, w.dk, w.kweight, w.rmin, w.rmax])
+        m = torch.tensor(models, dtype=torch.float64, requires_grad=True)
+        R = T.r_factor_torch(m, torch.tensor(data), torch.tensor(k), w)
+        R.sum().backward()
+        out[f"R_{i}"], out[f"grad_{i}"] = R.detach().numpy(), m.grad.numpy()
+        r = T.r_grid()
+        out[f"keep_{i}"] = np.nonzero(((r >= w.rmin) & (r <= w.rmax)).numpy())[0]
+        # PathSpectra.misfit's forms: FP32 k and window, FP64 transform
+        kt = torch.tensor(k, dtype=torch.float32)
+        win = T.hanning_window(kt, torch.tensor([w.kmin]), torch.tensor([w.kmax]), dk=w.dk)
+        keep = (r >= w.rmin) & (r <= w.rmax)
+        tr = T.ft(torch.tensor(data)[None], kt.double(), win.double(), kweight=w.kweight)[0][keep]
+        Rs, gs = [], []
+        for b in range(models.shape[0]):
+            x = torch.tensor(models[b], dtype=torch.float64, requires_grad=True)
+            cr = T.ft(x[None], kt.double(), win.double(), kweight=w.kweight)[0][keep]
+            v = ((cr - tr).abs() ** 2).sum() / float((tr.abs() ** 2).sum())
+            v.backward()
+            Rs.append(float(v.detach()))
+            gs.append(x.grad.numpy())
+        out[f"R32_{i}"], out[f"grad32_{i}"] = np.asarray(Rs), np.stack(gs)
+    np.savez_compressed(HERE / "rspace_ref.npz", **out)
+    print(f"rspace_ref: {len(windows)} windows")
+
+
 def make_pairs():
     """pairs_nio.npz -- the reference's single-scattering pair tables (src/feffgpu/exafs/forward.py:178-320) on the
     CPU in FP64: a thermally displaced rock-salt NiO supercell (3^3 cells, 216 sites, sigma 0.1 A, periodic), Ni K
@@ -531,10 +634,12 @@ def make_feffdat():
 def main():
     import tempfile
     ap = argparse.ArgumentParser()
+    ap.add_argument("reference", help="root of the reference's source tree (the directory holding src/feffgpu)")
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
+    set_reference(args.reference)
     want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder", "pairs", "pairs_tri",
-                             "feffdat", "larch"])
+                             "feffdat", "larch", "bench_sample", "rspace"])
     with tempfile.TemporaryDirectory() as tmp:
         if "cases" in want:
             import shutil
@@ -568,6 +673,10 @@ def main():
             make_larch()
         if "feffdat" in want:
             make_feffdat()
+        if "bench_sample" in want:
+            make_bench_sample()
+        if "rspace" in want:
+            make_rspace()
 
 
 if __name__ == "__main__":

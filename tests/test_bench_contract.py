@@ -24,3 +24,8 @@ def test_reference_arm_json_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "port" and cb["value"] == d["value"] and cb["cores"] >= 1 and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    # the timing is checkable from the line: a step is the measured sample, the full batch is extrapolated beside it
+    t = d["timing"]
+    assert t["timed_paths_per_step"] > 0 and t["timed_s"] > 0 and t["ms_full_batch_extrapolated"] > d["ms_per_step"]
+    assert abs(t["timed_s"] * 1e3 - d["ms_per_step"] * d["steps"]) <= 0.5 * t["timed_s"] * 1e3
+    assert sorted(d["config"]["legs"]) == [str(n) for n in range(2, 9)] or sorted(d["config"]["legs"]) == list(range(2, 9))

@@ -90,3 +90,23 @@ def test_wigner_d_unitarity_and_symmetry():
         for a in range(-m, m + 1):
             for b in range(-m, m + 1):
                 assert abs(d[l, a + 3, b + 3] - (-1) ** (a - b) * d[l, -a + 3, -b + 3]) < 1e-12
+
+
+def test_oracle_on_the_benchmark_batch_sample():
+    """The oracle on the reference finder's paths of the benchmark packing (tests/golden/bench_sample.npz: 592 paths,
+    every absorber and leg count of the benchmark batch, phase tables resampled to 401 k) equals the reference
+    stage's FP64 rows to R < 1e-20 and its per-path cchi to 1e-10."""
+    from feffgpu_b200.pad import phase_from_npz, resample_phase
+    z = npz("bench_sample")
+    q = z["q"]
+    P = resample_phase(phase_from_npz(npz("cfg2_phase"), prefix="ph_"), q)
+    orc = O.Oracle(P)
+    S = orc.linear_matrix(q)
+    per = int(z["per_cchi"])
+    for r, (s, nleg) in enumerate(z["row_keys"]):
+        c = z[f"coords_{s}_{nleg}"].astype(np.float64)
+        cc, rf = orc.cchi(c, z[f"ipots_{s}_{nleg}"])
+        row = (z[f"deg_{s}_{nleg}"][:, None] * O.chi_fine(cc, rf, q, S)).sum(0)
+        assert O.r_factor(q, z["rows"][r], row, kmin=3, kmax=19, rmin=1, rmax=8) < 1e-20
+        refc = z[f"cchi_{s}_{nleg}"]
+        assert np.abs(cc[:per] - refc).max() <= 1e-10 * np.abs(refc).max()
