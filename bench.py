@@ -648,15 +648,20 @@ def pairs_leg(args, dev, world, rank):
 
 def rmc_extra(args, dev, world, rank):
     """RMC refinement: rock-salt NiO 8^3 cells (4096 sites, a = 4.177 A) with 5 % vacancies and 0.1 A disorder; Ni K
-    and O K edges, 32 absorbers each (seeded paths of 2-4 legs, rmax 5 A); targets from a hidden 0.03 A perturbation;
+    and O K edges, 32 absorbers each, their paths from the CUDA path finder (rmax 5 A, 4 legs, importance cut 2 %,
+    single scattering unmerged: the reference GpuRmc's defaults, src/feffgpu/rmc/refine.py:84-89 and
+    exafs/forward.py:68-75); targets from a hidden 0.03 A perturbation;
     each step (both edges' rows, R-space misfits, backward, Adam on all positions) one CUDA graph replay with the
-    autotuned launch shapes; `rmc_steps` steps timed with CUDA events and the host clock."""
+    autotuned launch shapes; every `rmc_refresh` steps (the reference's default cadence, refine.py:176-179) the
+    paths are found again at the current positions and the step is captured again.  `rmc_steps` steps timed with
+    CUDA events and the host clock, refreshes included; the refreshes' own cost is reported beside."""
     import time as _time
     import torch
     from feffgpu_b200 import GPUPathStage
     from feffgpu_b200 import workloads as W
-    from feffgpu_b200.model import GraphedRefinement, PathModel
+    from feffgpu_b200.model import GraphedRefinement, PathModel, finder_groups
     from feffgpu_b200.pad import phase_from_npz
+    from feffgpu_b200.pathfinder import GPUPathFinder
     from feffgpu_b200.rspace import FitWindow, RSpaceMisfit
     pos0, lab, box = W.rock_salt_supercell(8, 4.177)
     rng = np.random.default_rng(5 + rank)
@@ -665,27 +670,30 @@ def rmc_extra(args, dev, world, rank):
     pos = W.thermal(pos0, 0.1, seed=6 + rank)
     hidden = W.thermal(pos, 0.03, seed=7 + rank)
     q = torch.tensor(Q, device=dev)
-    models, npaths = [], 0
+    ipot_of = np.array([{"Ni": 1, "O": 2}[x] for x in lab])
+    edges = []
     for edge, fname in (("Ni", "cfg5_nik_phase"), ("O", "cfg5_ok_phase")):
-        st = GPUPathStage(phase_from_npz(np.load(ROOT / "tests" / "golden" / f"{fname}.npz"), prefix="ph_"),
-                          device=dev, dtype=torch.complex64, autotune=not args.no_autotune)
-        ipot_of = np.array([{"Ni": 1, "O": 2}[x] for x in lab])
-        gs = []
-        for a in W.central_atom(pos, box, lab, edge, 32):
-            paths = W.random_paths(pos, box, int(a), {2: 24, 3: 120, 4: 200}, rmax=5.0, leg_max=5.0,
-                                   seed=int(a) + 17 * rank, ipot_of=ipot_of)
-            for nleg, (c, ip, atoms) in paths.items():
-                # deg 1/32: the row is the absorbers' average spectrum
-                gs.append((np.concatenate([np.full((len(atoms), 1), a), atoms], 1), ip, np.full(len(atoms), 1 / 32),
-                           np.zeros(len(atoms), int)))
-        model = PathModel(st, gs, pos, nrows=1, box=box)
+        P = phase_from_npz(np.load(ROOT / "tests" / "golden" / f"{fname}.npz"), prefix="ph_")
+        st = GPUPathStage(P, device=dev, dtype=torch.complex64, autotune=not args.no_autotune)
+        finder = GPUPathFinder(P, device=dev, rmax=5.0, nlegmax=4, critpw=2.0, merge_degenerate=False)
+        edges.append((st, finder, W.central_atom(pos, box, lab, edge, 32)))
+
+    def build(x):
+        return [PathModel(st, finder_groups(f, x, box, ab, ipot_of), x, nrows=1, box=box) for st, f, ab in edges]
+
+    models, npaths = [], 0
+    for (st, _f, _ab), model in zip(edges, build(pos)):
         npaths += model.batch.n
         S = st.linear_matrix(Q).double().contiguous()
         with torch.no_grad():
             target = model.rows(torch.tensor(hidden, device=dev), q, S)[0]
         models.append((model, q, S, RSpaceMisfit(NK, target, FitWindow(kmin=3.0, kmax=14.0, rmin=1.0, rmax=5.0),
                                                  device=dev)))
-    g = GraphedRefinement(models, pos, lr=0.002)
+
+    def rebuild(x, old):
+        return [(m, qq, SS, mis) for m, (_m, qq, SS, mis) in zip(build(x.cpu().numpy()), old)]
+
+    g = GraphedRefinement(models, pos, lr=0.002, rebuild=rebuild, refresh_every=args.rmc_refresh)
     torch.cuda.synchronize(dev)
     g.step()
     torch.cuda.synchronize(dev)
@@ -700,10 +708,15 @@ def rmc_extra(args, dev, world, rank):
         g.step()
     e1.record()
     e1.synchronize()
-    wall = (_time.perf_counter() - t0) * 1e3 / n
-    return {"steps": n, "ms_per_step": e0.elapsed_time(e1) / n, "wall_ms_per_step": wall, "atoms": len(pos),
-            "paths_per_gpu": npaths, "misfit_first_step": first, "misfit_final": float(g.loss),
-            "launch_warps": [list(m[0].stage._launch) for m in models], "graph": "one CUDA graph replay per step"}
+    wall = (_time.perf_counter() - t0) * 1e3
+    refresh_ms = [ms for _s, ms in g.refreshes]
+    return {"steps": n, "ms_per_step": e0.elapsed_time(e1) / n, "wall_ms_per_step": wall / n,
+            "wall_ms_per_step_between_refreshes": (wall - sum(refresh_ms)) / n, "atoms": len(pos),
+            "paths_per_gpu": npaths, "paths_after_refresh": sum(m[0].batch.n for m in g.models),
+            "refresh_every": args.rmc_refresh, "refreshes_ms": refresh_ms,
+            "misfit_first_step": first, "misfit_final": float(g.loss),
+            "launch_warps": [list(m[0].stage._launch) for m in g.models],
+            "graph": "one CUDA graph replay per step; paths found again and the step re-captured at each refresh"}
 
 
 # ------------------------------------------------------------------------------------------------ main
@@ -719,7 +732,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="only the headline forward (profiling runs)")
     ap.add_argument("--md-frames", type=int, default=500, help="frames of the MD-batch leg (0: skip it)")
     ap.add_argument("--no-autotune", action="store_true", help="default launch shapes (profiling runs)")
-    ap.add_argument("--rmc-steps", type=int, default=200, help="steps of the RMC leg (0: skip it)")
+    ap.add_argument("--rmc-steps", type=int, default=500, help="steps of the RMC leg (0: skip it)")
+    ap.add_argument("--rmc-refresh", type=int, default=250, help="steps between path searches in the RMC leg")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's own stage (GPU and host legs)")
     ap.add_argument("--frontends", action="store_true",
                     help="only time the reference's MD and RMC front ends on its own classes and after install()")

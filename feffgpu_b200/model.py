@@ -7,9 +7,12 @@ absorber/copy.  ``PathModel`` does the same with one ``PathBatch`` and one fused
 the coordinates is a differentiable torch indexing (its backward scatters the per-path gradients onto the atoms),
 the stage is ``GPUPathStage.chi_reduce``.  ``GraphedRefinement`` captures one refinement step -- model, R-space
 misfit, backward and the Adam update -- in a CUDA graph and replays it (the RMC loop of
-``src/feffgpu/rmc/refine.py:120-260`` with a fixed path list).
+``src/feffgpu/rmc/refine.py:120-260``), re-enumerating the paths and capturing the step again every
+``refresh_every`` steps as that loop does (``refine.py:176-179``).
 """
 from __future__ import annotations
+
+import time
 
 import numpy as np
 import torch
@@ -72,20 +75,52 @@ class PathModel:
         return self.stage.chi_reduce(self.batch, q, S, coords=self.coords(pos), sigma2=sigma2)
 
 
+def finder_groups(finder, positions, box, absorbers, ipot_of, weight=None):
+    """PathModel groups of every path the finder (``GPUPathFinder``) returns for the absorbers at positions (N, 3):
+    atoms as global indices with the absorber first, degeneracy times ``weight`` (default 1 / the number of absorbers:
+    the row is the absorbers' mean spectrum, as the reference's PathSpectra.spectra divides by them,
+    ``exafs/forward.py:141-163``), row 0."""
+    ab_np = np.asarray(absorbers, np.int64)
+    w = 1.0 / max(len(ab_np), 1) if weight is None else float(weight)
+    res = finder.enumerate_many(positions, box, ab_np, ipot_of)
+    groups = []
+    for nleg, (_c, ipots, deg, _xp, atoms, slot) in sorted(res["paths"].items()):
+        ab = torch.as_tensor(ab_np, device=atoms.device)[slot.long()][:, None]
+        groups.append((torch.cat([ab, atoms.long()], 1).cpu().numpy(), ipots.cpu().numpy(),
+                       deg.double().cpu().numpy() * w, np.zeros(len(deg), int)))
+    return groups
+
+
 class GraphedRefinement:
     """One refinement step -- rows of every model, mean spectrum per model, R-space misfit summed over the models,
     backward, Adam -- captured once in a CUDA graph, then replayed.  models: list of (PathModel, q as a device
     tensor, S, misfit); the positions are shared by all models (several edges of one structure).  The warm-up steps
     that precede the capture (they allocate every buffer the step uses) are undone afterwards: the first replay
-    is the first step from `positions` with a fresh optimiser state."""
+    is the first step from `positions` with a fresh optimiser state.
 
-    def __init__(self, models, positions, lr=0.002, warmup=2):
+    rebuild(positions (N, 3) FP64 tensor, models) -> models, with refresh_every > 0: every refresh_every steps the
+    path lists are found again at the current positions (the reference's loop re-enumerates every refresh_every
+    steps, ``rmc/refine.py:176-179``) and the step is captured again; positions and optimiser state carry over.
+    ``refreshes`` records (step, milliseconds of finding and capturing)."""
+
+    def __init__(self, models, positions, lr=0.002, warmup=2, rebuild=None, refresh_every=0):
         self.models = models
         dev = models[0][0].stage.device
+        self.dev = dev
         self.pos0 = torch.as_tensor(positions, dtype=torch.float64).to(dev).clone()
         self.pos = self.pos0.clone().requires_grad_(True)
         self.opt = torch.optim.Adam([self.pos], lr=lr, capturable=True)
         self.loss = torch.zeros((), dtype=torch.float64, device=dev)
+        self.rebuild, self.refresh_every = rebuild, int(refresh_every)
+        if self.refresh_every and rebuild is None:
+            raise ValueError("refresh_every needs a rebuild function")
+        self.nstep = 0
+        self.refreshes: list = []
+        self._capture(warmup)
+        self.reset()
+
+    def _capture(self, warmup):
+        dev = self.dev
         s = torch.cuda.Stream(dev)
         s.wait_stream(torch.cuda.current_stream(dev))
         with torch.cuda.stream(s):
@@ -96,11 +131,33 @@ class GraphedRefinement:
         self.opt.zero_grad(set_to_none=False)
         with torch.cuda.graph(self.graph):
             self._step()
-        self.reset()
+
+    @torch.no_grad()
+    def refresh(self) -> None:
+        """New path lists at the current positions and a new capture of the step; the positions, the optimiser state
+        and the loss are kept (the warm-up before the capture runs on copies' behalf and is undone)."""
+        torch.cuda.synchronize(self.dev)
+        t0 = time.perf_counter()
+        pos = self.pos.detach().clone()
+        state = [{k: v.clone() for k, v in st.items() if torch.is_tensor(v)} for st in self.opt.state.values()]
+        loss = self.loss.clone()
+        self.models = self.rebuild(pos, self.models)
+        del self.graph
+        with torch.enable_grad():
+            self._capture(1)
+        self.pos.copy_(pos)
+        for st, saved in zip(self.opt.state.values(), state):
+            for k, v in saved.items():
+                st[k].copy_(v)
+        self.loss.copy_(loss)
+        torch.cuda.synchronize(self.dev)
+        self.refreshes.append((self.nstep, (time.perf_counter() - t0) * 1e3))
 
     @torch.no_grad()
     def reset(self, positions=None) -> None:
-        """Back to `positions` (default: the initial ones) with a fresh optimiser state, in place."""
+        """Back to `positions` (default: the initial ones) with a fresh optimiser state and step count, in place
+        (the path lists stay those of the last refresh)."""
+        self.nstep = 0
         self.pos.copy_(self.pos0 if positions is None else torch.as_tensor(positions, dtype=torch.float64))
         for st in self.opt.state.values():
             for v in st.values():
@@ -123,4 +180,7 @@ class GraphedRefinement:
         self.loss.copy_(loss.detach())
 
     def step(self) -> None:
+        if self.refresh_every and self.nstep and self.nstep % self.refresh_every == 0:
+            self.refresh()
         self.graph.replay()
+        self.nstep += 1

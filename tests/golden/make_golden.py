@@ -33,6 +33,9 @@ The reference is imported read-only from its source tree and run on the CPU in F
   the W case's stored paths.
 * pairs_nio.npz -- the reference's single-scattering pair tables, histogram, all-pairs spectrum and its position
   gradient on a thermal rock-salt NiO supercell (Ni K edge); pairs_nio_tri.npz -- the same in a triclinic cell.
+* bench_sample.npz -- a stratified sample of the benchmark batch with the reference's FP64 signals (make_bench_sample);
+  rspace_ref.npz -- the reference's R-space losses and gradients (make_rspace); cfg3_adjoint.npz -- configuration 3's
+  loss and position gradient through the reference's PathSpectra and autograd (make_cfg3).
 * cfg2_phase.npz -- Fe K-edge phase tables (potentials Fe*, Fe, O, Pt, lmax 24) of a cluster cut from the seeded
   3000-atom Fe/O/Pt packing, on FEFF's own energy grid; cfg2_sample.npz -- the reference stage's cchi on those
   tables resampled to 401 k points, for a sample of synthetic paths.
@@ -532,6 +535,42 @@ def make_rspace(seed=41):
     print(f"rspace_ref: {len(windows)} windows")
 
 
+def make_cfg3(n_absorbers=16, seed=31):
+    """cfg3_adjoint.npz -- configuration 3 through the reference's own forward model: a seeded 800-atom Fe/O/Pt
+    packing (feffgpu_b200.workloads, seed 31), its 16 most central Fe absorbers, the reference's PathSpectra
+    (src/feffgpu/exafs/forward.py:33-176: its path finder, rmax 5 A, 4 legs, its default importance cut 0.5 %; its
+    stage in complex128 on the CPU; chunks through non-reentrant checkpointing) on the Fe K tables resampled to 401 k;
+    the target is its spectrum of the same path lists at positions displaced by seeded Gaussian noise (sigma 0.05 A);
+    the loss its R-space misfit (k 3-16, R 1-6, kw 2) and the gradient of the loss with respect to every position
+    by its autograd.  Stored: positions, box, absorbers, potentials, path counts per leg count, target, loss and the
+    (800, 3) gradient."""
+    import dataclasses
+    from feffgpu.exafs.forward import PathSpectra
+    from feffgpu.pad import PhaseData as RefPhase
+    q = np.arange(401) * 0.05
+    P = resample_phase(phase_from_npz(np.load(HERE / "cfg2_phase.npz"), prefix="ph_"), q)
+    refP = RefPhase(**{f.name: getattr(P, f.name) for f in dataclasses.fields(RefPhase)})
+    pos, lab, box = W.random_packing(800, 0.08, 1.8, seed=seed)
+    ipot = np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
+    absorbers = np.asarray(W.central_atom(pos, box, lab, "Fe", n_absorbers))
+    t = time.time()
+    ps = PathSpectra(refP, q, np.zeros(401), 0.0, window=(3.0, 16.0), r_range=(1.0, 6.0), box=box, rmax=5.0,
+                     nlegmax=4, critpw=0.5, device="cpu", dtype=torch.complex128)
+    counts = ps.refresh(pos[None], absorbers[None], ipot=torch.tensor(ipot))
+    target_pos = W.thermal(pos, 0.05, seed=77)
+    with torch.no_grad():
+        target = ps.spectra(torch.tensor(target_pos, dtype=torch.float64).reshape(-1, 3), use_checkpoint=False)[0]
+    ps.set_target(target.numpy())
+    x = torch.tensor(pos, dtype=torch.float64).reshape(-1, 3).requires_grad_(True)
+    loss = ps.misfit(ps.spectra(x).mean(0))
+    loss.backward()
+    np.savez_compressed(HERE / "cfg3_adjoint.npz", pos=pos, box=np.asarray(box), absorbers=absorbers, ipot=ipot,
+                        legs=np.asarray(sorted(counts)), counts=np.asarray([counts[n] for n in sorted(counts)]),
+                        target=target.numpy(), target_pos=target_pos, loss=np.asarray(float(loss.detach())),
+                        grad=x.grad.numpy().reshape(-1, 3), q=q)
+    print(f"cfg3_adjoint: {counts}, loss {float(loss.detach()):.4e}, {time.time() - t:.1f} s")
+
+
 def make_pairs():
     """pairs_nio.npz -- the reference's single-scattering pair tables (src/feffgpu/exafs/forward.py:178-320) on the
     CPU in FP64: a thermally displaced rock-salt NiO supercell (3^3 cells, 216 sites, sigma 0.1 A, periodic), Ni K
@@ -639,7 +678,7 @@ def main():
     args = ap.parse_args()
     set_reference(args.reference)
     want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder", "pairs", "pairs_tri",
-                             "feffdat", "larch", "bench_sample", "rspace"])
+                             "feffdat", "larch", "bench_sample", "rspace", "cfg3"])
     with tempfile.TemporaryDirectory() as tmp:
         if "cases" in want:
             import shutil
@@ -677,6 +716,8 @@ def main():
             make_bench_sample()
         if "rspace" in want:
             make_rspace()
+        if "cfg3" in want:
+            make_cfg3()
 
 
 if __name__ == "__main__":

@@ -2,8 +2,9 @@
 
 1. Cu fcc 6 A cluster, K edge: the reference chain's own phases and path finder output (317 paths), chi on
    k = 0..20 step 0.05 against the reference's FP64 chi (R <= 1e-6 mixed, 1e-12 FP64).
-3. Adjoint on an 800-atom Fe/O/Pt packing: gradient of an R-space misfit with respect to every position and every
-   per-path sigma^2 against central differences (h = 1e-4 A), FP32-vs-FP64 gradient error stated.
+3. Adjoint on an 800-atom Fe/O/Pt packing: the path finder's paths, the gradient of the reference's R-space misfit
+   with respect to every position against the reference's own autograd, per-path sigma^2 against central
+   differences, FP32-vs-FP64 gradient error stated.
 4. MD batch: frames of a thermally displaced bcc Fe supercell x absorbers in one launch, chi averaged per frame,
    against the oracle's FP64 sums.
 5. Two-edge refinement (Ni K + O K of a rock-salt NiO model with vacancies): the step captured as a CUDA graph equals
@@ -47,69 +48,61 @@ def test_cfg1_cu_cluster(dtype, tol):
     assert _R(K401, z["ref_chi"], chi.cpu().numpy()) <= tol
 
 
-def _distinct(atoms):
-    a = np.asarray(atoms)
-    return np.array([len(set(r.tolist())) == len(r) for r in a])
-
-
-def _feopt_model(dtype, n_atoms=800, seed=31):
-    from feffgpu_b200 import GPUPathStage
-    from feffgpu_b200.model import PathModel
-    from tests.fixtures import cfg2_phase
-    pos, lab, box = W.random_packing(n_atoms, 0.08, 1.8, seed=seed)
-    ab = int(W.central_atom(pos, box, lab, "Fe", 1)[0])
-    ipot_of = np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
-    paths = W.random_paths(pos, box, ab, {2: 40, 3: 300, 4: 400, 5: 300}, rmax=6.0, seed=5, ipot_of=ipot_of)
-    gs = []
-    for nleg, (c, ip, atoms) in paths.items():
-        full = np.concatenate([np.full((len(atoms), 1), ab), atoms], 1)
-        keep = _distinct(full)            # revisiting paths are not differentiable at the revisit
-        gs.append((full[keep], ip[keep], np.ones(int(keep.sum())), np.zeros(int(keep.sum()), int)))
-    st = GPUPathStage(cfg2_phase(), device="cuda", dtype=dtype)
-    return st, PathModel(st, gs, pos, nrows=1, box=box), pos, box
-
-
 def test_cfg3_adjoint_800_atoms():
+    """Configuration 3 against the reference's own forward model and autograd (tests/golden/cfg3_adjoint.npz: its
+    PathSpectra -- path finder, complex128 stage under non-reentrant checkpointing, R-space misfit -- on the seeded
+    800-atom Fe/O/Pt packing, 16 Fe absorbers, rmax 5 A, 4 legs, importance cut 0.5 %, target from a 0.05 A Gaussian
+    displacement).  This package: the CUDA finder's paths (the same lists), PathModel + chi_reduce, the misfit with
+    PathSpectra's FP32 k grid; the loss and the gradient with respect to all 3 x 800 positions against the reference's
+    (FP64 form: 1e-9 relative to the largest component; mixed form: 1e-4), and per-path
+    sigma^2 gradients (no reference counterpart) against central differences.  The FP32-vs-FP64 gradient error is
+    printed."""
+    from feffgpu_b200 import GPUPathStage
+    from feffgpu_b200.model import PathModel, finder_groups
+    from feffgpu_b200.pathfinder import GPUPathFinder
     from feffgpu_b200.rspace import FitWindow, RSpaceMisfit
+    from tests.fixtures import cfg2_phase
+    z = npz("cfg3_adjoint")
+    P = cfg2_phase()
+    pos, box, absorbers, ipot = z["pos"], float(z["box"]), z["absorbers"], z["ipot"]
+    # PathSpectra's finder keeps single-scattering paths unmerged (its merge_degenerate=False, forward.py:68-75)
+    finder = GPUPathFinder(P, device="cuda", rmax=5.0, nlegmax=4, critpw=0.5, merge_degenerate=False)
+    gs = finder_groups(finder, pos, box, absorbers, ipot)
+    assert {int(np.asarray(g[0]).shape[1]): len(g[0]) for g in gs} == dict(zip(z["legs"].tolist(), z["counts"].tolist()))
     q = torch.tensor(K401, device="cuda")
+    win = FitWindow(kmin=3.0, kmax=16.0, dk=1.0, kweight=2, rmin=1.0, rmax=6.0)
     grads = {}
-    for dtype in (torch.complex128, torch.complex64):
-        st, model, pos, box = _feopt_model(dtype)
+    for dtype, tol in ((torch.complex128, 1e-9), (torch.complex64, 1e-4)):
+        st = GPUPathStage(P, device="cuda", dtype=dtype)
+        model = PathModel(st, gs, pos, nrows=1, box=box)
         S = st.linear_matrix(K401).double()
-        target_pos = W.thermal(pos, 0.05, seed=77)
-        with torch.no_grad():
-            target = model.rows(torch.tensor(target_pos, device="cuda"), q, S)[0]
-        mis = RSpaceMisfit(len(K401), target, FitWindow(kmin=3.0, kmax=16.0, rmin=1.0, rmax=6.0))
+        mis = RSpaceMisfit(len(K401), z["target"], win, k_dtype=np.float32)
         x = torch.tensor(pos, device="cuda", requires_grad=True)
-        s2 = torch.full((model.batch.n,), 0.003, dtype=torch.float64, device="cuda", requires_grad=True)
+        s2 = torch.zeros(model.batch.n, dtype=torch.float64, device="cuda", requires_grad=True)
         loss = mis(model.rows(x, q, S, sigma2=s2))[0]
         loss.backward()
-        grads[dtype] = (x.grad.cpu().numpy(), s2.grad.cpu().numpy(), float(loss))
+        gx = x.grad.cpu().numpy()
+        err_l = abs(float(loss.detach()) - float(z["loss"])) / float(z["loss"])
+        err_g = np.abs(gx - z["grad"]).max() / np.abs(z["grad"]).max()
+        print(f"cfg3 {dtype}: loss {float(loss.detach()):.6e} (reference {float(z['loss']):.6e}, rel {err_l:.1e}), "
+              f"gradient vs reference autograd {err_g:.2e}")
+        assert err_l <= tol and err_g <= tol
+        grads[dtype] = (gx, s2.grad.cpu().numpy())
         if dtype != torch.complex128:
             continue
-        # central differences on the atoms with the largest gradients and on a few sigma^2
-        gx = grads[dtype][0]
-        top = np.argsort(-np.abs(gx).ravel())[:6]
+        # per-path sigma^2 (new, no reference counterpart): central differences on the largest components
+        gsig = grads[dtype][1]
         with torch.no_grad():
-            for idx in top:
-                i, k = divmod(int(idx), 3)
-                xp, xm = pos.copy(), pos.copy()
-                xp[i, k] += 1e-4
-                xm[i, k] -= 1e-4
-                lp = float(mis(model.rows(torch.tensor(xp, device="cuda"), q, S, sigma2=s2.detach()))[0])
-                lm = float(mis(model.rows(torch.tensor(xm, device="cuda"), q, S, sigma2=s2.detach()))[0])
-                fd = (lp - lm) / 2e-4
-                assert abs(gx[i, k] - fd) <= 1e-4 * abs(gx).max(), (i, k, gx[i, k], fd)
-            gs = grads[dtype][1]
-            for p in np.argsort(-np.abs(gs))[:4]:
+            for p in np.argsort(-np.abs(gsig))[:4]:
                 sp, sm = s2.detach().clone(), s2.detach().clone()
                 sp[p] += 1e-6
                 sm[p] -= 1e-6
                 fd = (float(mis(model.rows(x.detach(), q, S, sigma2=sp))[0]) -
                       float(mis(model.rows(x.detach(), q, S, sigma2=sm))[0])) / 2e-6
-                assert abs(gs[p] - fd) <= 1e-4 * abs(gs).max(), (p, gs[p], fd)
-    e_x = np.abs(grads[torch.complex64][0] - grads[torch.complex128][0]).max() / np.abs(grads[torch.complex128][0]).max()
-    e_s = np.abs(grads[torch.complex64][1] - grads[torch.complex128][1]).max() / np.abs(grads[torch.complex128][1]).max()
+                assert abs(gsig[p] - fd) <= 1e-4 * abs(gsig).max(), (p, gsig[p], fd)
+    g64, g32 = grads[torch.complex128], grads[torch.complex64]
+    e_x = np.abs(g32[0] - g64[0]).max() / np.abs(g64[0]).max()
+    e_s = np.abs(g32[1] - g64[1]).max() / np.abs(g64[1]).max()
     print(f"cfg3: FP32 vs FP64 gradient error: positions {e_x:.2e}, sigma2 {e_s:.2e}")
     assert e_x < 1e-4 and e_s < 1e-4
 
@@ -271,3 +264,57 @@ def test_path_model_and_graph_in_a_triclinic_cell():
         torch.cuda.synchronize()
         assert abs(float(g.loss) - float(loss)) <= 1e-9 * abs(float(loss))
     assert torch.allclose(g.pos.detach(), eager.detach(), rtol=0, atol=1e-9)
+
+
+def test_refinement_refreshes_the_path_lists_and_recaptures():
+    """GraphedRefinement with refresh_every: every third step the CUDA finder lists the paths again at the current
+    positions (the reference's refinement loop does this every refresh_every steps, src/feffgpu/rmc/refine.py:176-179)
+    and the step is captured again.  The graph-replayed run equals an eager run with the same refreshes (losses and
+    positions to 1e-9), the optimiser state carries over the refreshes, and the model after a refresh holds the
+    finder's paths at those positions."""
+    from feffgpu_b200 import GPUPathStage
+    from feffgpu_b200.model import GraphedRefinement, PathModel, finder_groups
+    from feffgpu_b200.pathfinder import GPUPathFinder
+    from feffgpu_b200.rspace import FitWindow, RSpaceMisfit
+    pos0, lab, box = W.rock_salt_supercell(3, 4.177)
+    pos = W.thermal(pos0, 0.1, seed=6)
+    hidden = W.thermal(pos, 0.05, seed=7)
+    P = phase("cfg5_nik_phase")
+    st = GPUPathStage(P, device="cuda", dtype=torch.complex64)
+    ipot_of = np.array([{"Ni": 1, "O": 2}[x] for x in lab])
+    absorbers = W.central_atom(pos, box, lab, "Ni", 4)
+    finder = GPUPathFinder(P, device="cuda", rmax=4.5, nlegmax=4, critpw=0.5)
+    q = torch.tensor(K401, device="cuda")
+    S = st.linear_matrix(K401).double().contiguous()
+
+    def build(x):
+        return PathModel(st, finder_groups(finder, np.asarray(x), box, absorbers, ipot_of), np.asarray(x), nrows=1,
+                         box=box)
+
+    m0 = build(pos)
+    with torch.no_grad():
+        target = m0.rows(torch.tensor(hidden, device="cuda"), q, S)[0]
+    mis = RSpaceMisfit(len(K401), target, FitWindow(kmin=3.0, kmax=14.0, rmin=1.0, rmax=4.5))
+
+    def rebuild(x, models):
+        return [(build(x.cpu().numpy()), q, S, mis)]
+
+    g = GraphedRefinement([(m0, q, S, mis)], pos, lr=0.01, rebuild=rebuild, refresh_every=3)
+    eager = torch.tensor(pos, device="cuda", requires_grad=True)
+    opt = torch.optim.Adam([eager], lr=0.01, capturable=True)
+    model = m0
+    for it in range(8):
+        if it and it % 3 == 0:
+            model = build(eager.detach().cpu().numpy())
+        g.step()
+        opt.zero_grad()
+        loss = mis(model.rows(eager, q, S).mean(0, keepdim=True))[0]
+        loss.backward()
+        opt.step()
+        torch.cuda.synchronize()
+        assert abs(float(g.loss) - float(loss)) <= 1e-9 * abs(float(loss)), (it, float(g.loss), float(loss))
+    assert torch.allclose(g.pos.detach(), eager.detach(), rtol=0, atol=1e-9)
+    assert [s for s, _ in g.refreshes] == [3, 6]
+    assert g.models[0][0].batch.n == model.batch.n
+    assert torch.equal(g.models[0][0].atoms, model.atoms)
+    print(f"refresh: {[round(ms, 1) for _, ms in g.refreshes]} ms to find and re-capture")
