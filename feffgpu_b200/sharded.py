@@ -25,18 +25,15 @@ def path_cost(nleg: np.ndarray) -> np.ndarray:
 
 def shard(nleg: np.ndarray, world: int, cost=None) -> np.ndarray:
     """Rank of every path: longest-processing-time-first assignment of the path costs (default: by leg count; pass
-    roofline.path_flops for the FLOP cost over all energies) to the least-loaded rank.  Deterministic for a given
-    input."""
+    roofline.path_flops for the FLOP cost over all energies) to the least-loaded rank, by the library's host routine
+    fg_shard_lpt (a heap over the ranks' loads).  Deterministic for a given input."""
+    from . import _lib
     nleg = np.asarray(nleg)
-    cost = path_cost(nleg) if cost is None else np.asarray(cost, float)
-    order = np.argsort(-cost, kind="stable")
-    load = np.zeros(world)
-    owner = np.zeros(len(nleg), np.int64)
-    for i in order:
-        r = int(np.argmin(load))
-        owner[i] = r
-        load[r] += cost[i]
-    return owner
+    cost = np.ascontiguousarray(path_cost(nleg) if cost is None else np.asarray(cost, float), dtype=np.float64)
+    owner = np.zeros(len(nleg), np.int32)
+    lib = _lib.load()
+    _lib.check(lib.fg_shard_lpt(cost.ctypes.data, len(cost), int(world), owner.ctypes.data))
+    return owner.astype(np.int64)
 
 
 def split_groups(groups, world: int, rank: int, lmax=None):

@@ -291,6 +291,12 @@ FG_API fg_status fg_path_columns(int64_t B, int32_t E, fg_precision prec, const 
 FG_API fg_status fg_rspace_misfit(int64_t B, int32_t NK, int32_t NR, const double *rows, const double *F,
                                   const double *target, double inv_norm, double *R, double *grad, void *stream);
 
+/* ---------------------------------------------------------------------------------------------- multi-GPU split
+ * Host: owner (n) = the rank of every path for a split over `world` ranks -- paths in order of decreasing cost (equal
+ * costs in index order) each to the least-loaded rank (equal loads: the lowest rank).  The reference shards whole MD
+ * frames across processes (src/feffgpu/parallel/__init__.py:78-133); this splits one path list by its cost. */
+FG_API fg_status fg_shard_lpt(const double *cost, int64_t n, int32_t world, int32_t *owner);
+
 #ifdef __cplusplus
 }
 #endif
