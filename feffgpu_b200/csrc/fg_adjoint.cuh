@@ -439,15 +439,47 @@ __device__ __forceinline__ void cfac_grad(const WarpPath<R> &g, const Tables<R> 
 }
 
 // ------------------------------------------------------------------------------------------------ one energy
+// Prefix products kept by the adjoint's first sweep: P_k for k a multiple of FG_ADJ_CKPT (0: none), the others
+// recomputed in the second sweep from the nearest kept one and the stored F~_k.  Every prefix kept (1) put 3.9 KB
+// of local memory on every lane, which spilled from L2 to DRAM at 8 warps per SM.
+#ifndef FG_ADJ_CKPT
+#define FG_ADJ_CKPT 1
+#endif
+
+// P <- e^{-i eta m} F~ P (F~ by its canonical entries f; P, N x N0, in per-lane local memory), one column at a time.
+template <typename R, int KIND, int N, int N0, int MM>
+__device__ __forceinline__ void chain_step(C2<R> (&P)[N][N0], const C2<R> (&f)[RepTab<KIND, N, N>().n],
+                                           const C2<R> (&ph)[2 * MM + 1])
+{
+    constexpr RepTab<KIND, N, N> RT{};
+    constexpr LamTab L = lamtab(KIND);
+#pragma unroll 1
+    for (int b = 0; b < N0; ++b) {
+        C2<R> col[N];
+#pragma unroll
+        for (int c = 0; c < N; ++c) col[c] = P[c][b];
+#pragma unroll
+        for (int a = 0; a < N; ++a) {
+            C2<R> s = cz<R>();
+#pragma unroll
+            for (int c = 0; c < N; ++c) {
+                const C2<R> v = f[RT.rep[a][c]];
+                s = RT.sg[a][c] > 0 ? pfma(v, col[c], s) : pfms(v, col[c], s);
+            }
+            P[a][b] = cmul(ph[L.m[a] + MM], s);
+        }
+    }
+}
+
 // Multiple scattering (nleg >= 3).  Adds this energy's parameter gradients into pg.  Every scattering matrix is
 // handled as a full lamx x lamx matrix (one code path for the first, middle and last matrices): the first matrix's
 // columns beyond laml0x meet the zero rows of P_0 (the lamx x laml0x identity) and the last matrix's rows beyond
-// laml0x meet the zero columns of R_nsc = [T 0].  Sweep 1 keeps every F~_k and P_k in per-lane local memory, so that
-// sweep 2's partial-wave loop carries only the contraction.  The small matrix products between the partial-wave
-// loops run as rolled loops over one index of the local-memory operand: the per-energy code then stays within the
-// instruction cache (the unrolled products made the kernel several times larger than its two hot loops); their
-// complex multiply-adds are FP32-pair instructions (3 % faster; in the forward's register-resident chain product the
-// pairing measured slower and is not used).
+// laml0x meet the zero columns of R_nsc = [T 0].  Sweep 1 keeps every F~_k and the checkpoint prefixes in per-lane
+// local memory, so that sweep 2's partial-wave loop carries only the contraction.  The small matrix products between
+// the partial-wave loops run as rolled loops over one index of the local-memory operand: the per-energy code then
+// stays within the instruction cache (the unrolled products made the kernel several times larger than its two hot
+// loops); their complex multiply-adds are FP32-pair instructions (3 % faster; in the forward's register-resident
+// chain product the pairing measured slower and is not used).
 template <typename R, int KIND>
 __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, const R (*dterm_db)[49],
                               const Tables<R> &T, int e, int nleg, C2<R> gbar, ParGrad &pg)
@@ -455,6 +487,8 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     constexpr LamTab L = lamtab(KIND);
     constexpr int N = L.N, N0 = L.N0, MM = L.MM, DS = dstride(MM);
     constexpr RepTab<KIND, N, N> RT{};
+    constexpr int CK = FG_ADJ_CKPT;
+    constexpr int NCK = CK > 0 ? (kMaxLeg - 2) / CK : 0;     // checkpoints P_CK, P_2CK, ... below P_nsc
     const int E = T.E, nsc = nleg - 1;
     const size_t dleg = (size_t)(T.L1 + 1) * DS, tlip = (size_t)(T.L1 + 1) * E;
     const C2<R> ck = T.ck[e];
@@ -463,16 +497,19 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     const C2<R> cf = cfac(g, T, e, nleg, ck);
     const C2<R> sd = cmul(C2<R>{gbar.x, -gbar.y}, cf);      // s = conj(gbar) cfac: dL = Re(s dptrac)
     const C2<R> sck = cmul(sd, ck);
-    // per-lane local memory: F~_k (k = 1..nsc), P_k = F_k ... F_1 P_0 (k = 0..nsc), R_k.  (Measured on B200: loading
-    // the next column while the current one is in use, or forming P_0 on the fly instead of storing it, is slower.)
+    // per-lane local memory: F~_k (k = 1..nsc), the checkpoint prefixes, the working prefix P and the suffix R_k
     C2<R> Fst[kMaxLeg - 1][RT.n];
-    C2<R> Pst[kMaxLeg][N][N0];
+    C2<R> Pck[NCK > 0 ? NCK : 1][N][N0];
+    C2<R> Pw[N][N0];
     C2<R> Rst[N0][N];
+    auto identity = [&]() {
 #pragma unroll
-    for (int a = 0; a < N; ++a)
+        for (int a = 0; a < N; ++a)
 #pragma unroll
-        for (int b = 0; b < N0; ++b) Pst[0][a][b] = a == b ? C2<R>{R(1), R(0)} : cz<R>();
-    // sweep 1
+            for (int b = 0; b < N0; ++b) Pw[a][b] = a == b ? C2<R>{R(1), R(0)} : cz<R>();
+    };
+    identity();
+    // sweep 1: F~_k and P_k = e^{-i eta_(k+1) m} F~_k P_(k-1); the last, P_nsc, stays in Pw for the termination
     for (int k = 1; k <= nsc; ++k) {
         C2<R> acc[RT.n];
         const int ip = g.ip[k];
@@ -482,22 +519,12 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
         for (int r = 0; r < RT.n; ++r) Fst[k - 1][r] = acc[r];
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
-        // P_k = e^{-i eta_(k+1) m} F~_k P_(k-1), one column of P at a time
+        chain_step<R, KIND, N, N0, MM>(Pw, acc, ph);
+        if (CK > 0 && k < nsc && k % CK == 0) {
 #pragma unroll 1
-        for (int b = 0; b < N0; ++b) {
-            C2<R> col[N];
+            for (int a = 0; a < N; ++a)
 #pragma unroll
-            for (int c = 0; c < N; ++c) col[c] = Pst[k - 1][c][b];
-#pragma unroll
-            for (int a = 0; a < N; ++a) {
-                C2<R> s = cz<R>();
-#pragma unroll
-                for (int c = 0; c < N; ++c) {
-                    const C2<R> f = acc[RT.rep[a][c]];
-                    s = RT.sg[a][c] > 0 ? pfma(f, col[c], s) : pfms(f, col[c], s);
-                }
-                Pst[k][a][b] = cmul(ph[L.m[a] + MM], s);
-            }
+                for (int b = 0; b < N0; ++b) Pck[k / CK - 1][a][b] = Pw[a][b];
         }
     }
     // the termination with P_nsc: its own gradients, ptrac and cfac's gradient
@@ -510,7 +537,7 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
         for (int a = 0; a < N0; ++a)
 #pragma unroll
             for (int b = N0; b < N; ++b) Rst[a][b] = cz<R>();
-        const C2<R> ptrac = term_adj<R, KIND>(g, dterm_db, T, e, tl, [&](int b, int a) { return Pst[nsc][b][a]; },
+        const C2<R> ptrac = term_adj<R, KIND>(g, dterm_db, T, e, tl, [&](int b, int a) { return Pw[b][a]; },
                                               ge1, gbn, gr1, grn, &Rst[0][0], N);
         add_re(pg.eta[1], sd, ge1);
         add_re(pg.beta[nleg], sd, gbn);
@@ -520,6 +547,27 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     }
     // sweep 2, k = nsc .. 1 with R_k = T F_nsc ... F_(k+1) and M_k = P_(k-1) R_k
     for (int k = nsc; k >= 1; --k) {
+        // P_(k-1) into Pw: from the nearest checkpoint at or below it, or from P_0
+        {
+            const int j0 = CK > 0 ? ((k - 1) / CK) * CK : 0;
+            if (j0 == 0) {
+                identity();
+            } else {
+#pragma unroll 1
+                for (int a = 0; a < N; ++a)
+#pragma unroll
+                    for (int b = 0; b < N0; ++b) Pw[a][b] = Pck[j0 / CK - 1][a][b];
+            }
+#pragma unroll 1
+            for (int j = j0 + 1; j <= k - 1; ++j) {
+                C2<R> f[RT.n];
+#pragma unroll
+                for (int r = 0; r < RT.n; ++r) f[r] = Fst[j - 1][r];
+                C2<R> phj[2 * MM + 1];
+                phase_powers<R, MM>(g.phs[j + 1], phj);
+                chain_step<R, KIND, N, N0, MM>(Pw, f, phj);
+            }
+        }
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
         // Wh[r] = sum over the flip orbit of r of sign * e^{-i eta m_a} M(b, a), We the same times -i m_a;
@@ -533,7 +581,7 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
             for (int c = 0; c < N0; ++c) {
                 C2<R> pc[N], rr[N], re[N];
 #pragma unroll
-                for (int b = 0; b < N; ++b) pc[b] = Pst[k - 1][b][c];
+                for (int b = 0; b < N; ++b) pc[b] = Pw[b][c];
 #pragma unroll
                 for (int a = 0; a < N; ++a) {
                     rr[a] = cmul(ph[L.m[a] + MM], Rst[c][a]);

@@ -21,6 +21,28 @@ constexpr int kLamTot = 15;                // genfmt.py:18
 // index, leg count, summation index or chunk offset outside its range; that path or term is skipped).
 constexpr int kBadIpot = 1;
 constexpr int kBadLayout = 2;
+constexpr int kBadRange = 4;    // a weighted path term not finite or beyond the exact row sums' range (|v| >= 2^31)
+
+// The fused stage's row sums: per path and k point the term is added to its row exactly, as a fixed-point number of
+// resolution 2^-64 held in two 64-bit integer sums: a signed word of resolution 2^-32 (its additions wrap modulo
+// 2^64, which leaves the final sum exact whenever the row itself is below 2^31) and a low word of the next 32 bits
+// (non-negative, below 2^32 per term, so up to 2^31 terms cannot overflow it).  Integer addition is associative,
+// so the rows do not depend on the order in which paths finish, the launch shape or the GPU.
+#ifndef FG_EXACT_ROWS
+#define FG_EXACT_ROWS 0
+#endif
+// Adds v to the fixed-point sum whose two words are a[0] and a[stride]; false (nothing added) if v is not finite or
+// |v| >= 2^31.
+__device__ __forceinline__ bool fixed_add(unsigned long long *a, size_t stride, double v)
+{
+    if (!(fabs(v) < 2147483648.0)) return false;
+    const double x = v * 4294967296.0;                  // exact: v * 2^32, |x| < 2^63
+    const double hi = floor(x);
+    const double lo = rint((x - hi) * 4294967296.0);    // the next 32 bits, 0 <= lo <= 2^32; rounding below 2^-64
+    atomicAdd(a, (unsigned long long)(long long)hi);
+    atomicAdd(a + stride, (unsigned long long)lo);
+    return true;
+}
 
 // ------------------------------------------------------------------------------------------------ complex helpers
 template <typename R> struct C2 { R x, y; };

@@ -154,12 +154,14 @@ __global__ void __launch_bounds__(256) k_chi_fine(int64_t B, int E, const C2<R> 
 struct PathsDev {
     int64_t n;
     int nleg_max;
+    int nrows;
     const double *coords;
     const int64_t *ipots;
     const int *nleg;
     const double *deg;
     const double *sigma2;
     const int *order;
+    const int *row;
 };
 
 // Fused forward: every path of the batch, all leg counts, from one work queue (costliest first); per path the
@@ -172,7 +174,8 @@ template <typename R, int EDGE>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
     k_fused(Tables<R> T, PathsDev P, int NK, const double *__restrict__ q,
                                                 const double *__restrict__ S, const int *__restrict__ span,
-                                                double *__restrict__ terms, C2<R> *__restrict__ cchi_save,
+                                                double *__restrict__ terms, unsigned long long *__restrict__ racc,
+                                                C2<R> *__restrict__ cchi_save,
                                                 double *__restrict__ reff_save, unsigned long long *counter, int *bad,
                                                 int nsc_max, size_t wbytes)
 {
@@ -211,6 +214,13 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
         amp_phase<R>(E, lane, [&](int e) { return cbuf[e]; }, amp, pha);
         __syncwarp();
         const double rf = g.reff * kBohr, wdeg = P.deg[p], s2 = P.sigma2 ? P.sigma2[p] : 0.0;
+#if FG_EXACT_ROWS
+        int prow = P.row[p];
+        if (prow < 0 || prow >= P.nrows) {
+            if (lane == 0) atomicOr(bad, kBadLayout);
+            prow = -1;
+        }
+#endif
         for (int k0 = 0; k0 < NK; k0 += 32) {
             const int k = k0 + lane;
             if (k < NK) {
@@ -223,7 +233,13 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
                 }
                 const double qk = q[k];
                 const double damp = s2 != 0.0 ? exp(-2.0 * s2 * qk * qk) : 1.0;   // exact 1 without sigma^2
-                terms[p * NK + k] = wdeg * a * sin_arg<R>(ph + 2.0 * qk * rf) * damp;
+                const double v = wdeg * a * sin_arg<R>(ph + 2.0 * qk * rf) * damp;
+#if FG_EXACT_ROWS
+                const size_t stride = (size_t)P.nrows * NK;
+                if (prow < 0 || !fixed_add(racc + (size_t)prow * NK + k, stride, v)) atomicOr(bad, kBadRange);
+#else
+                terms[p * NK + k] = v;
+#endif
             }
         }
         if (lane == 0 && reff_save) reff_save[p] = rf;
@@ -281,9 +297,16 @@ fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const 
     using K = Kinds<EDGE>;
     unsigned long long *counter = reinterpret_cast<unsigned long long *>(ws);
     int *bad = reinterpret_cast<int *>(ws + kStatusOffset);
+#if FG_EXACT_ROWS
+    double *terms = nullptr, *partial = nullptr;
+    unsigned long long *racc = reinterpret_cast<unsigned long long *>(ws + kCounterBytes);
+    FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes + (size_t)2 * P->nrows * NK * sizeof(unsigned long long), st));
+#else
+    unsigned long long *racc = nullptr;
     double *terms = reinterpret_cast<double *>(ws + kCounterBytes);
     double *partial = reinterpret_cast<double *>(ws + kCounterBytes + align_up((size_t)P->n * NK * sizeof(double), 256));
     FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes, st));
+#endif
     if (P->n > 0) {
         const int nsc_max = P->nleg_max - 1;
         const size_t wb = warp_bytes<R>(sv.L1, nsc_max, K::MM, sv.E, true);
@@ -292,14 +315,18 @@ fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const 
         auto kern = k_fused<R, EDGE>;
         int blocks = 0;
         if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, P->n, blocks)) return rc;
-        PathsDev pd{P->n, P->nleg_max, P->coords, P->ipots, P->nleg, P->deg, P->sigma2, P->order};
+        PathsDev pd{P->n, P->nleg_max, P->nrows, P->coords, P->ipots, P->nleg, P->deg, P->sigma2, P->order, P->row};
         timer_begin(st);
-        kern<<<blocks, threads, wb * warps, st>>>(T, pd, NK, q, S, span, terms, static_cast<C2<R> *>(cchi_save),
+        kern<<<blocks, threads, wb * warps, st>>>(T, pd, NK, q, S, span, terms, racc, static_cast<C2<R> *>(cchi_save),
                                                   reff_save, counter, bad, nsc_max, wb);
         timer_end(st);
         FG_CUDA(cudaGetLastError());
     }
+#if FG_EXACT_ROWS
+    return launch_row_finish(P, NK, racc, rows, bad, st);
+#else
     return launch_reductions(P, NK, terms, partial, rows, bad, st);
+#endif
 }
 
 template <typename R>

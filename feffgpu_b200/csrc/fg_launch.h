@@ -63,6 +63,10 @@ template <typename R> struct LaunchCommon {
 fg_status launch_reductions(const fg_paths *P, int NK, const double *terms, double *partial, double *rows, int *status,
                             cudaStream_t st);
 
+// Rows (nrows, NK) from the exact fixed-point sums (two word arrays of nrows * NK), NaN where the status is set.
+fg_status launch_row_finish(const fg_paths *P, int NK, const unsigned long long *racc, double *rows, const int *status,
+                            cudaStream_t st);
+
 // The status word of a call's kernels (device int) turned into a return code: outside stream capture the call waits
 // for its stream and reads the word (FG_ERR_VALUE with a message if a bit is set); under capture it returns FG_OK
 // without waiting (the rows of a replay that meets a bad input are NaN).

@@ -53,7 +53,30 @@ __global__ void k_row_sums(int NK, int nrows, int64_t nchunks, const double *__r
     // the earlier kernels of the call have finished (same stream): a set status word makes the whole call's rows NaN
     rows[(int64_t)r * NK + k] = *(volatile int *)status ? __longlong_as_double(0x7ff8000000000000ll) : s.value();
 }
+// rows from the fixed-point sums: the low word's carry moved into the signed word in integers, then one value in FP64
+__global__ void k_row_finish(int64_t count, const unsigned long long *__restrict__ racc, double *__restrict__ rows,
+                             const int *status)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    unsigned long long lo = racc[count + i];
+    const long long hi = (long long)(racc[i] + (lo >> 32));   // value * 2^32 (integer part), wraps modulo 2^64
+    lo &= 0xffffffffull;
+    const double v = (double)(hi >> 32) + ((double)(hi & 0xffffffffll) + (double)lo * 0x1p-32) * 0x1p-32;
+    rows[i] = *(volatile const int *)status ? __longlong_as_double(0x7ff8000000000000ll) : v;
+}
 }  // namespace
+
+fg_status launch_row_finish(const fg_paths *P, int NK, const unsigned long long *racc, double *rows,
+                            const int *status, cudaStream_t st)
+{
+    const int64_t count = (int64_t)P->nrows * NK;
+    if (count > 0) {
+        k_row_finish<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(count, racc, rows, status);
+        FG_CUDA(cudaGetLastError());
+    }
+    return FG_OK;
+}
 
 fg_status launch_reductions(const fg_paths *P, int NK, const double *terms, double *partial, double *rows, int *status,
                             cudaStream_t st)
@@ -80,6 +103,9 @@ fg_status read_status(const int *status, cudaStream_t st)
     FG_CUDA(cudaMemcpyAsync(&v, status, sizeof(int), cudaMemcpyDeviceToHost, st));
     FG_CUDA(cudaStreamSynchronize(st));
     if (v & kBadIpot) return fail(FG_ERR_VALUE, "potential index outside 0..nph (the rows are NaN)");
+    if (v & kBadRange)
+        return fail(FG_ERR_VALUE, "a weighted path term is not finite or its magnitude is 2^31 or more (the rows are "
+                                  "NaN)");
     if (v & kBadLayout)
         return fail(FG_ERR_VALUE, "malformed path batch: a path index, leg count, summation index or chunk offset is "
                                   "outside its range (the rows are NaN)");
@@ -88,8 +114,12 @@ fg_status read_status(const int *status, cudaStream_t st)
 
 size_t fused_workspace(const fg_paths *P, int NK)
 {
+#if FG_EXACT_ROWS
+    return kCounterBytes + align_up((size_t)2 * P->nrows * NK * sizeof(unsigned long long), 256);
+#else
     return kCounterBytes + align_up((size_t)P->n * NK * sizeof(double), 256) +
            align_up((size_t)P->nchunks * NK * sizeof(double), 256);
+#endif
 }
 
 }  // namespace fg
