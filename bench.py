@@ -52,48 +52,58 @@ def packing():
     return pos, lab, box, ipot_of
 
 
-def workload(rank: int, world: int, scale: float = 1.0, finder: str = "gpu"):
-    """Phase tables (resampled to 401 k) and the path groups of this rank's two absorbers: every path of 2-8 legs
-    within 8 A that the path finder returns (no importance cut), degeneracies included, row = absorber.  finder
-    "gpu": this package's CUDA path finder (the paths are the reference finder's, bit for bit); "oracle": the CPU
-    restatement (the reference arm, which runs nothing of this package).  scale < 1 keeps every k-th path per leg
-    count (profiling runs)."""
+def workload(world: int, scale: float = 1.0, finder: str = "gpu"):
+    """Phase tables (resampled to 401 k) and the path groups of the job's 2 x world absorbers (the most central Fe
+    atoms): every path of 2-8 legs within 8 A that the path finder returns (no importance cut), degeneracies
+    included, row = absorber.  finder "gpu": this package's CUDA path finder (the paths are the reference finder's,
+    bit for bit); "oracle": the CPU restatement (the reference arm, which runs nothing of this package).  scale < 1
+    keeps every k-th path per leg count (profiling runs)."""
     from feffgpu_b200 import workloads as W
     from feffgpu_b200.pad import phase_from_npz, resample_phase
     z = np.load(ROOT / "tests" / "golden" / "cfg2_phase.npz")
     P0 = phase_from_npz(z, prefix="ph_")
     P = resample_phase(P0, Q)
-    pos, lab, box, ipot_of = packing()
-    absorbers = W.central_atom(pos, box, lab, "Fe", 2 * world)[2 * rank:2 * rank + 2]
+    pos, lab, box = packing()[:3]
+    ipot_of = packing()[3]
+    absorbers = W.central_atom(pos, box, lab, "Fe", 2 * world)
     groups = []
-    for i, ab in enumerate(absorbers):
-        if finder == "gpu":
-            from feffgpu_b200.pathfinder import GPUPathFinder
-            kept, _ = GPUPathFinder(P0, device="cuda", rmax=8.0, nlegmax=8, critpw=0.0).enumerate(pos, box, int(ab),
-                                                                                                  ipot_of)
-            kept = {n: tuple(t.cpu().numpy() for t in v) for n, v in kept.items()}
-        else:
-            from oracle.pathfinder import Finder
+    if finder == "gpu":
+        from feffgpu_b200.pathfinder import GPUPathFinder
+        res = GPUPathFinder(P0, device="cuda", rmax=8.0, nlegmax=8, critpw=0.0).enumerate_many(pos, box, absorbers,
+                                                                                               ipot_of)
+        for nleg, (coords, ip, deg, _xp, _atoms, slot) in sorted(res["paths"].items()):
+            sl = slot.cpu().numpy()
+            c, i, d = coords.cpu().numpy(), ip.cpu().numpy(), deg.cpu().numpy()
+            for a in range(len(absorbers)):
+                sel = np.nonzero(sl == a)[0]
+                groups.append((a, nleg, c[sel], i[sel], d[sel]))
+    else:
+        from oracle.pathfinder import Finder
+        for a, ab in enumerate(absorbers):
             kept, _ = Finder(P0, rmax=8.0, nlegmax=8, critpw=0.0).enumerate(pos, box, int(ab), ipot_of)
-        for nleg, (coords, ip, deg, _xp, _atoms) in sorted(kept.items()):
-            if len(coords) == 0:
-                continue
-            step = max(1, int(round(1.0 / scale)))
-            sel = np.arange(0, len(coords), step)
-            groups.append((coords[sel].astype(np.float64), ip[sel], deg[sel].astype(np.float64), np.full(len(sel), i)))
-    return P, groups
+            for nleg, (coords, ip, deg, _xp, _atoms) in sorted(kept.items()):
+                groups.append((a, nleg, coords, ip, deg))
+    out = []
+    for a, nleg, coords, ip, deg in sorted(groups, key=lambda g: (g[0], g[1])):
+        if len(coords) == 0:
+            continue
+        step = max(1, int(round(1.0 / scale)))
+        sel = np.arange(0, len(coords), step)
+        out.append((coords[sel].astype(np.float64), ip[sel], deg[sel].astype(np.float64), np.full(len(sel), a)))
+    return P, out
 
 
 def workload_config(groups, world: int) -> dict:
-    """The workload's description, built from the path groups, the same on both arms of the benchmark."""
+    """The job's description, built from the path groups of all its absorbers, the same on both arms."""
     legs: dict = {}
     for c, *_ in groups:
         legs[int(c.shape[1])] = legs.get(int(c.shape[1]), 0) + len(c)
     n_paths = sum(legs.values())
-    return {"workload": f"Fe/O/Pt packing 3000 atoms, 2 Fe K absorbers per GPU, every path finder path of 2-8 legs "
-                        f"to 8 A, {n_paths} paths per GPU, lmax 24 x {NK} k, chi on {NK} k",
-            "paths_per_gpu": n_paths, "nk": NK, "energies": NK, "legs": dict(sorted(legs.items())),
-            "parallelism": f"dp{world} (absorbers per rank)",
+    return {"workload": f"Fe/O/Pt packing 3000 atoms, {2 * world} Fe K absorbers (2 per GPU), every path finder path "
+                        f"of 2-8 legs to 8 A, {n_paths} paths, lmax 24 x {NK} k, chi on {NK} k",
+            "paths_total": n_paths, "paths_per_gpu": n_paths // world, "nk": NK, "energies": NK,
+            "legs": dict(sorted(legs.items())),
+            "parallelism": f"dp{world}: the paths of all absorbers split over the GPUs by FLOP cost, rows all-reduced",
             "l2": "GPU arm: flushed between timed steps (256 MB write)"}
 
 
@@ -106,7 +116,7 @@ def finder_leg(args, dev, world, rank):
     from feffgpu_b200.pathfinder import GPUPathFinder
     P0 = phase_from_npz(np.load(ROOT / "tests" / "golden" / "cfg2_phase.npz"), prefix="ph_")
     pos, lab, box, ipot_of = packing()
-    absorbers = W.central_atom(pos, box, lab, "Fe", 2 * world)[2 * rank:2 * rank + 2]
+    absorbers = W.central_atom(pos, box, lab, "Fe", 2 * world)[2 * rank:2 * rank + 2]     # this GPU's two
     f = GPUPathFinder(P0, device=dev, rmax=8.0, nlegmax=8, critpw=0.0)
     res = f.enumerate_many(pos, box, absorbers, ipot_of)
     torch.cuda.synchronize(dev)
@@ -246,46 +256,48 @@ def parity_vs_oracle(P, samples, dev):
     return res
 
 
-def extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms):
-    """End-to-end, forward+backward and plain-FP64 measurements beside the headline."""
+def extras(args, stage, batch, P, S, dev, timed, n_total, ms):
+    """End-to-end, forward+backward and plain-FP64 measurements beside the headline, each step the same job as the
+    headline's (this GPU's share of the paths, rows all-reduced over the GPUs)."""
     import torch
     from feffgpu_b200 import GPUPathStage
+    from feffgpu_b200.sharded import allreduce_rows
     coords_h = batch.coords.cpu().pin_memory()
     coords_d = torch.empty_like(batch.coords)
     rows_h = torch.empty(batch.nrows, NK, dtype=torch.float64).pin_memory()
 
     def e2e_step():
         coords_d.copy_(coords_h, non_blocking=True)
-        rows = stage.chi_reduce(batch, Q, S, coords=coords_d)
+        rows = allreduce_rows(stage.chi_reduce(batch, Q, S, coords=coords_d))
         rows_h.copy_(rows, non_blocking=True)
 
     with torch.no_grad():
         ms_e2e, _ = timed(e2e_step, args.steps, 1)
-    e2e = {"value": world * n_paths * NK / (ms_e2e * 1e-3), "unit": UNIT,
+    e2e = {"value": n_total * NK / (ms_e2e * 1e-3), "unit": UNIT,
            "h2d_bytes_per_step": int(coords_h.numel() * coords_h.element_size()),
            "d2h_bytes_per_step": int(rows_h.numel() * rows_h.element_size())}
 
     # forward + backward (gradients with respect to every path coordinate and per-path sigma^2)
     fwd_bwd = None
     try:
-        s2 = torch.zeros(n_paths, dtype=torch.float64, device=dev, requires_grad=True)
+        s2 = torch.zeros(batch.n, dtype=torch.float64, device=dev, requires_grad=True)
         cg = batch.coords.clone().requires_grad_(True)
         w = torch.randn(batch.nrows, NK, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
 
         def fb():
-            rows = stage.chi_reduce(batch, Q, S, coords=cg, sigma2=s2)
+            rows = allreduce_rows(stage.chi_reduce(batch, Q, S, coords=cg, sigma2=s2))
             (rows * w).sum().backward()
 
         ms_fb, _ = timed(fb, max(2, args.steps // 2), 1)
-        fwd_bwd = {"value": world * n_paths * NK / (ms_fb * 1e-3), "unit": UNIT, "ms_per_step": ms_fb}
+        fwd_bwd = {"value": n_total * NK / (ms_fb * 1e-3), "unit": UNIT, "ms_per_step": ms_fb}
     except NotImplementedError as err:
         fwd_bwd = {"value": None, "unit": UNIT, "note": f"not available: {err}"}
 
     # the plain FP64 drop-in (complex128) on the same batch
     stage64 = GPUPathStage(P, device=dev, dtype=torch.complex128, autotune=not args.no_autotune)
     with torch.no_grad():
-        ms64, _ = timed(lambda: stage64.chi_reduce(batch, Q, S), 2, 1)
-    plain = {"value": world * n_paths * NK / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
+        ms64, _ = timed(lambda: allreduce_rows(stage64.chi_reduce(batch, Q, S)), 2, 1)
+    plain = {"value": n_total * NK / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
              "speedup_mixed_over_fp64": ms64 / ms, "launch_warps": list(stage64._launch)}
 
     return e2e, fwd_bwd, plain
@@ -387,6 +399,7 @@ def reference_gpu_leg(args, P, groups, dev, ours: dict, uuid):
         by_leg.setdefault(c.shape[1], []).append((c, ip, deg, row))
     by_leg = {n: tuple(np.concatenate([x[i] for x in v]) for i in range(4)) for n, v in sorted(by_leg.items())}
     n_paths = sum(len(v[0]) for v in by_leg.values())
+    nrows = 1 + max(int(v[3].max()) for v in by_leg.values())
 
     def ev_time(fn):
         torch.cuda.synchronize(dev)
@@ -417,7 +430,7 @@ def reference_gpu_leg(args, P, groups, dev, ours: dict, uuid):
                     return stage.chi_fine(*stage.cchi(x, ipots), Q, S, "feff")
 
                 def step():
-                    out = torch.zeros(2, NK, device=dev, dtype=torch.float64)
+                    out = torch.zeros(nrows, NK, device=dev, dtype=torch.float64)
                     if grad:
                         x = coords.clone().requires_grad_(True)
                         chi = checkpoint(fwd, x, use_reentrant=False)
@@ -474,11 +487,11 @@ def parity_vs_reference(P, saved, dev):
     st = {d: GPUPathStage(P, device=dev, dtype=d) for d in (torch.complex64, torch.complex128)}
     for n, (ref_rows, ref_cc, lo, m) in keep.items():
         c, ip, deg, row = (v[lo:lo + m] for v in by_leg[n])
-        b = PathBatch([(c, ip, deg, row)], nrows=2, device=dev)
+        b = PathBatch([(c, ip, deg, row)], nrows=ref_rows.shape[0], device=dev)
         for d, key in ((torch.complex64, "R_mixed_vs_ref_fp64"), (torch.complex128, "R_fp64_vs_ref_fp64")):
             with torch.no_grad():
                 rows = st[d].chi_reduce(b, Q).cpu().numpy()
-            for r in range(2):
+            for r in range(ref_rows.shape[0]):
                 if np.abs(ref_rows[r]).max() > 0:
                     res[key] = max(res[key], r_factor(ref_rows[r], rows[r], win))
         with torch.no_grad():
@@ -751,7 +764,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        P, groups = workload(0, 1, args.paths_scale, finder="oracle")
+        P, groups = workload(args.gpus, args.paths_scale, finder="oracle")
         vals, walls, timed_paths = [], [], 0
         for i in range(args.warmup + args.steps):
             t0 = time.perf_counter()
@@ -789,9 +802,15 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
-    P, groups = workload(rank, world, args.paths_scale)
+    P, all_groups = workload(world, args.paths_scale)
     stage = GPUPathStage(P, device=dev, dtype=torch.complex64, autotune=not args.no_autotune)
-    batch = PathBatch(groups, nrows=2, device=dev)
+    from feffgpu_b200.sharded import allreduce_rows, split_groups
+    groups = split_groups(all_groups, world, rank, lmax=stage.lmax.cpu().numpy()) if world > 1 else all_groups
+    batch = PathBatch(groups, nrows=2 * world, device=dev)
+    n_total = sum(len(g[0]) for g in all_groups)
+
+    def step_rows(**kw):
+        return allreduce_rows(stage.chi_reduce(batch, Q, S, **kw))
     S = stage.linear_matrix(Q)
     lib = _lib.load()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2, written between steps
@@ -835,14 +854,14 @@ def main():
     uuid = uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"
     with torch.no_grad():
         with Clocks(uuid) as clk:
-            ms, kern = timed(lambda: stage.chi_reduce(batch, Q, S), args.steps, args.warmup, kernel_time=True)
-    value = world * n_paths * NK / (ms * 1e-3)
+            ms, kern = timed(lambda: step_rows(), args.steps, args.warmup, kernel_time=True)
+    value = n_total * NK / (ms * 1e-3)
 
     e2e = fwd_bwd = plain = md = rmc = pf = pairs = ref_gpu = saved = None
     if not args.no_extras:
         pf = finder_leg(args, dev, world, rank)
         pairs = pairs_leg(args, dev, world, rank)
-        e2e, fwd_bwd, plain = extras(args, stage, batch, P, S, dev, timed, world, n_paths, ms)
+        e2e, fwd_bwd, plain = extras(args, stage, batch, P, S, dev, timed, n_total, ms)
         if not args.no_ref_gpu and rank == 0:
             ref_gpu, saved = reference_gpu_leg(args, P, groups, dev, {
                 "fwd": ms, "fwd64": plain["ms_per_step"], "fwd_bwd": (fwd_bwd or {}).get("ms_per_step")}, uuid)
@@ -910,7 +929,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32 (complex chain) + fp64 (phase argument, sums)", "data": "synthetic",
-        "config": workload_config(groups, world),
+        "config": workload_config(all_groups, world),
         "autotune": {"fwd_warps": stage._launch[0], "bwd_warps": stage._launch[1],
                      "timed": [{"kind": k, "warps": w_, "ms": round(t_, 3)} for sig, k, w_, t_ in tuner.log
                                if sig.split("|")[1] == "p0"]},

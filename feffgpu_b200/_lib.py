@@ -28,7 +28,7 @@ EXPORTS = ("fg_stage_create", "fg_stage_destroy", "fg_stage_get_info", "fg_stage
            "fg_chi_reduce_backward", "fg_set_kernel_timing", "fg_kernel_time_ms", "fg_fp32_fma_peak", "fg_set_launch",
            "fg_stage_set_launch", "fg_pf_candidates", "fg_pf_extend", "fg_pf_terminal", "fg_pf_describe",
            "fg_pf_windows", "fg_pair_histogram", "fg_pair_ss_grad", "fg_rspace_misfit",
-           "fg_path_columns", "fg_shard_lpt")
+           "fg_path_columns", "fg_shard_lpt", "fg_pf_enumerate_one", "fg_pf_result_gather", "fg_pf_result_destroy")
 
 
 class PhaseDesc(C.Structure):
@@ -46,8 +46,7 @@ class StageInfo(C.Structure):
 class Paths(C.Structure):
     _fields_ = [("n", C.c_int64), ("nleg_max", C.c_int32), ("nrows", C.c_int32), ("coords", C.c_void_p),
                 ("ipots", C.c_void_p), ("nleg", C.c_void_p), ("deg", C.c_void_p), ("sigma2", C.c_void_p),
-                ("row", C.c_void_p), ("order", C.c_void_p), ("sorted", C.c_void_p), ("chunk_bounds", C.c_void_p),
-                ("row_chunks", C.c_void_p), ("nchunks", C.c_int64)]
+                ("row", C.c_void_p), ("order", C.c_void_p)]
 
 
 class PfTables(C.Structure):
@@ -94,6 +93,11 @@ _SIGS = {
     "fg_rspace_misfit": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, _P, _P, _P, C.c_double, _P, _P, _P]),
     "fg_path_columns": (C.c_int, [C.c_int64, C.c_int32, C.c_int, _P, _P, _P, _P, _P, _P]),
     "fg_shard_lpt": (C.c_int, [_P, C.c_int64, C.c_int32, _P]),
+    "fg_pf_enumerate_one": (C.c_int, [_P, C.c_int64, C.c_float, _P, C.c_int64, _P, C.POINTER(PfTables), C.c_float,
+                                      C.c_int32, C.c_float, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
+                                      C.POINTER(C.c_float), _P]),
+    "fg_pf_result_gather": (C.c_int, [_P, C.c_int32, _P, _P, _P, _P, _P, _P]),
+    "fg_pf_result_destroy": (None, [_P]),
 }
 
 _lock = threading.Lock()

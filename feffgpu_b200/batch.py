@@ -6,9 +6,8 @@ path once, padded to the largest leg count, together with
 
 * ``order``  -- the launch order of the persistent work queue: costliest paths (most legs) first, so that the last
   paths to start are the cheapest (longest-processing-time-first scheduling);
-* ``sorted`` / ``chunk_bounds`` / ``row_chunks`` -- the fixed summation order of the cross-path sum: paths grouped
-  by row, each row cut into chunks of at most ``chunk`` paths; chunk partial sums, then row sums of the partials,
-  both in index order, so the result does not depend on scheduling.
+* ``row`` -- the output row of every path; the stage adds each path's terms to its row exactly (integer sums of the
+  terms rounded to 2^-64), so the result does not depend on scheduling.
 
 The layout is built once per path list (on the host) and reused: only the coordinates change from call to call
 (``GPUPathStage.chi_reduce(batch, q, coords=...)``).
@@ -26,9 +25,8 @@ class PathBatch:
     one entry per leg count (or any grouping); nrows defaults to max(row) + 1.
     """
 
-    def __init__(self, groups, nrows: int | None = None, device="cuda", chunk: int = 256):
+    def __init__(self, groups, nrows: int | None = None, device="cuda"):
         self.device = torch.device(device)
-        self.chunk = chunk
         cs, ips, nl, dg, rw = [], [], [], [], []
         nleg_max = 2
         groups = [tuple(g) + (None,) * (4 - len(g)) for g in groups]
@@ -71,19 +69,6 @@ class PathBatch:
         # launch order: most legs first (stable), the persistent queue's LPT schedule
         nl_np = nleg.numpy()
         order = np.argsort(-nl_np, kind="stable").astype(np.int32)
-        # summation order: by row, then by index; chunks of at most `chunk` paths within a row
-        row_np = row.numpy()
-        srt = np.argsort(row_np, kind="stable").astype(np.int32)
-        counts = np.bincount(row_np, minlength=self.nrows) if self.n else np.zeros(self.nrows, int)
-        bounds, row_chunks = [0], [0]
-        pos = 0
-        for r in range(self.nrows):
-            c = int(counts[r])
-            for s in range(0, c, chunk):
-                bounds.append(pos + min(s + chunk, c))
-            pos += c
-            row_chunks.append(len(bounds) - 1)
-        self.nchunks = len(bounds) - 1
         d = self.device
         self.coords = coords.to(d)
         self.ipots = ipots.to(d)
@@ -91,9 +76,6 @@ class PathBatch:
         self.deg = deg.to(d)
         self.row = row.to(d)
         self.order = torch.as_tensor(order).to(d)
-        self.sorted = torch.as_tensor(srt).to(d)
-        self.chunk_bounds = torch.as_tensor(np.asarray(bounds, np.int64)).to(d)
-        self.row_chunks = torch.as_tensor(np.asarray(row_chunks, np.int64)).to(d)
         self.counts = {int(k): int(v) for k, v in zip(*np.unique(nl_np, return_counts=True))}
         self._ws = {}
         self._tuned = {}             # launch shapes chosen for this batch, per (stage, precision, k points)
@@ -111,7 +93,7 @@ class PathBatch:
             sel = idx[nl == n]
             groups.append((self.coords[sel, :n].cpu(), self.ipots[sel, :n].cpu(), self.deg[sel].cpu(),
                            self.row[sel].cpu()))
-        return PathBatch(groups, nrows=self.nrows, device=self.device, chunk=self.chunk)
+        return PathBatch(groups, nrows=self.nrows, device=self.device)
 
     def workspace(self, nbytes: int, backward: bool = False) -> torch.Tensor:
         """A cached device scratch buffer of at least nbytes (one per direction)."""

@@ -237,7 +237,7 @@ __device__ __forceinline__ void accumulate_f_adj(C2<R> (&acc)[RepTab<KIND, NR, N
 // weighted sums along rho_in, rho_out and beta_k, with the spherical-wave values and tangents streamed.  Every
 // complex operation of the loop runs as FP32-pair instructions (forward + backward of 2e5 paths 321 -> 299 ms).
 template <typename R, int KIND, int NR, int NC>
-__device__ __forceinline__ void contract_f_adj(const C2<R> (&Wh)[RepTab<KIND, NR, NC>().n], const R *dhk,
+__device__ __forceinline__ void contract_f_adj_tangent(const C2<R> (&Wh)[RepTab<KIND, NR, NC>().n], const R *dhk,
                                                const R *dhdk, const C2<R> *tlk, int E, int ilx, C2<R> z_in,
                                                C2<R> z_out, C2<R> &g_in, C2<R> &g_out, C2<R> &g_beta)
 {
@@ -320,6 +320,107 @@ __device__ __forceinline__ void contract_f_adj(const C2<R> (&Wh)[RepTab<KIND, NR
     g_in = gi;
     g_out = go;
     g_beta = gb;
+}
+
+// -i z v: the factor of the rho-derivative of the spherical-wave factors
+template <typename R> __device__ __forceinline__ C2<R> mi_z(C2<R> z, C2<R> v)
+{
+    const C2<R> zv = pmul(z, v);
+    return C2<R>{zv.y, -zv.x};
+}
+
+// contract_f_adj with the rho-derivatives of the spherical-wave factors from the factors themselves: column j (m = j - 1)
+// of c(z), z = -i / rho, obeys dc_j/drho = -i z ((j - 1) c_j + j c_(j+1)) (verified against finite differences of the
+// recursion), so one more column of the value recursion replaces the tangent recursions and their state.
+template <typename R, int KIND, int NR, int NC>
+__device__ __forceinline__ void contract_f_adj_identity(const C2<R> (&Wh)[RepTab<KIND, NR, NC>().n], const R *dhk,
+                                                        const R *dhdk, const C2<R> *tlk, int E, int ilx, C2<R> z_in,
+                                                        C2<R> z_out, C2<R> &g_in, C2<R> &g_out, C2<R> &g_beta)
+{
+    constexpr RepTab<KIND, NR, NC> RT{};
+    constexpr LamTab L = lamtab(KIND);
+    constexpr int DS = dstride(L.MM);
+    constexpr int NCAN = ncanon(L.MM);
+    constexpr int CI = L.CI, CO = L.CO;
+    C2<R> pi[CI + 2], ci[CI + 2], po[CO + 2], co[CO + 2];
+#pragma unroll
+    for (int j = 0; j <= CI + 1; ++j) pi[j] = ci[j] = cz<R>();
+#pragma unroll
+    for (int j = 0; j <= CO + 1; ++j) po[j] = co[j] = cz<R>();
+    pi[1] = ci[1] = po[1] = co[1] = C2<R>{R(1), R(0)};
+    C2<R> gi = cz<R>(), go = cz<R>(), gb = cz<R>();
+    C2<R> t1 = tlk[E], t2 = ilx >= 2 ? tlk[(size_t)2 * E] : cz<R>();
+    for (int il = 1; il <= ilx; ++il) {
+        const C2<R> t = t1;
+        t1 = t2;
+        if (il + 2 <= ilx) t2 = tlk[(size_t)(il + 2) * E];
+        R d[NCAN], dd[NCAN];
+        load_row<R, NCAN>(dhk + (size_t)il * DS, d);
+        load_row<R, NCAN>(dhdk + (size_t)il * DS, dd);
+        C2<R> tco[CO + 1], tdco[CO + 1];
+#pragma unroll
+        for (int j = 1; j <= CO; ++j) {
+            tco[j] = pmul(t, co[j]);
+            tdco[j] = pmul(t, mi_z(z_out, pfmr(co[j], R(j - 1), cscl(co[j + 1], R(j)))));
+        }
+        C2<R> X[CI + 1][CO + 1], Y[CI + 1][CO + 1];
+#pragma unroll
+        for (int a = 0; a <= CI; ++a)
+#pragma unroll
+            for (int b = 0; b <= CO; ++b) X[a][b] = Y[a][b] = cz<R>();
+#pragma unroll
+        for (int r = 0; r < RT.n; ++r) {
+            X[RT.ci[r]][RT.co[r]] = pfmr(Wh[r], d[RT.d[r]], X[RT.ci[r]][RT.co[r]]);
+            Y[RT.ci[r]][RT.co[r]] = pfmr(Wh[r], dd[RT.d[r]], Y[RT.ci[r]][RT.co[r]]);
+        }
+#pragma unroll
+        for (int a = 1; a <= CI; ++a) {
+            C2<R> v = cz<R>(), y = cz<R>();
+#pragma unroll
+            for (int b = 1; b <= CO; ++b) {
+                v = pfma(X[a][b], tco[b], v);
+                y = pfma(Y[a][b], tco[b], y);
+            }
+            gi = pfma(mi_z(z_in, pfmr(ci[a], R(a - 1), cscl(ci[a + 1], R(a)))), v, gi);
+            gb = pfma(ci[a], y, gb);
+        }
+#pragma unroll
+        for (int b = 1; b <= CO; ++b) {
+            C2<R> v = cz<R>();
+#pragma unroll
+            for (int a = 1; a <= CI; ++a) v = pfma(X[a][b], ci[a], v);
+            go = pfma(tdco[b], v, go);
+        }
+        const R w = R(2 * il - 1);
+        const C2<R> wi = cscl(z_in, w), wo = cscl(z_out, w);
+        C2<R> ni[CI + 2], no[CO + 2];
+#pragma unroll
+        for (int j = 1; j <= CI + 1; ++j) ni[j] = pfms(wi, j > 1 ? padd(ci[j], ci[j - 1]) : ci[j], pi[j]);
+#pragma unroll
+        for (int j = 1; j <= CO + 1; ++j) no[j] = pfms(wo, j > 1 ? padd(co[j], co[j - 1]) : co[j], po[j]);
+#pragma unroll
+        for (int j = 1; j <= CI + 1; ++j) { pi[j] = ci[j]; ci[j] = ni[j]; }
+#pragma unroll
+        for (int j = 1; j <= CO + 1; ++j) { po[j] = co[j]; co[j] = no[j]; }
+    }
+    g_in = gi;
+    g_out = go;
+    g_beta = gb;
+}
+
+#ifndef FG_ADJ_DERIV
+#define FG_ADJ_DERIV 0
+#endif
+template <typename R, int KIND, int NR, int NC>
+__device__ __forceinline__ void contract_f_adj(const C2<R> (&Wh)[RepTab<KIND, NR, NC>().n], const R *dhk,
+                                               const R *dhdk, const C2<R> *tlk, int E, int ilx, C2<R> z_in,
+                                               C2<R> z_out, C2<R> &g_in, C2<R> &g_out, C2<R> &g_beta)
+{
+#if FG_ADJ_DERIV
+    contract_f_adj_identity<R, KIND, NR, NC>(Wh, dhk, dhdk, tlk, E, ilx, z_in, z_out, g_in, g_out, g_beta);
+#else
+    contract_f_adj_tangent<R, KIND, NR, NC>(Wh, dhk, dhdk, tlk, E, ilx, z_in, z_out, g_in, g_out, g_beta);
+#endif
 }
 
 // Weights of the contraction: Wh[r] = sum over the orbit of r of sign * ph(m_a) * M(b, a), and the same with an
@@ -439,47 +540,17 @@ __device__ __forceinline__ void cfac_grad(const WarpPath<R> &g, const Tables<R> 
 }
 
 // ------------------------------------------------------------------------------------------------ one energy
-// Prefix products kept by the adjoint's first sweep: P_k for k a multiple of FG_ADJ_CKPT (0: none), the others
-// recomputed in the second sweep from the nearest kept one and the stored F~_k.  Every prefix kept (1) put 3.9 KB
-// of local memory on every lane, which spilled from L2 to DRAM at 8 warps per SM.
-#ifndef FG_ADJ_CKPT
-#define FG_ADJ_CKPT 1
-#endif
-
-// P <- e^{-i eta m} F~ P (F~ by its canonical entries f; P, N x N0, in per-lane local memory), one column at a time.
-template <typename R, int KIND, int N, int N0, int MM>
-__device__ __forceinline__ void chain_step(C2<R> (&P)[N][N0], const C2<R> (&f)[RepTab<KIND, N, N>().n],
-                                           const C2<R> (&ph)[2 * MM + 1])
-{
-    constexpr RepTab<KIND, N, N> RT{};
-    constexpr LamTab L = lamtab(KIND);
-#pragma unroll 1
-    for (int b = 0; b < N0; ++b) {
-        C2<R> col[N];
-#pragma unroll
-        for (int c = 0; c < N; ++c) col[c] = P[c][b];
-#pragma unroll
-        for (int a = 0; a < N; ++a) {
-            C2<R> s = cz<R>();
-#pragma unroll
-            for (int c = 0; c < N; ++c) {
-                const C2<R> v = f[RT.rep[a][c]];
-                s = RT.sg[a][c] > 0 ? pfma(v, col[c], s) : pfms(v, col[c], s);
-            }
-            P[a][b] = cmul(ph[L.m[a] + MM], s);
-        }
-    }
-}
-
 // Multiple scattering (nleg >= 3).  Adds this energy's parameter gradients into pg.  Every scattering matrix is
 // handled as a full lamx x lamx matrix (one code path for the first, middle and last matrices): the first matrix's
 // columns beyond laml0x meet the zero rows of P_0 (the lamx x laml0x identity) and the last matrix's rows beyond
-// laml0x meet the zero columns of R_nsc = [T 0].  Sweep 1 keeps every F~_k and the checkpoint prefixes in per-lane
-// local memory, so that sweep 2's partial-wave loop carries only the contraction.  The small matrix products between
-// the partial-wave loops run as rolled loops over one index of the local-memory operand: the per-energy code then
-// stays within the instruction cache (the unrolled products made the kernel several times larger than its two hot
-// loops); their complex multiply-adds are FP32-pair instructions (3 % faster; in the forward's register-resident
-// chain product the pairing measured slower and is not used).
+// laml0x meet the zero columns of R_nsc = [T 0].  Sweep 1 keeps every F~_k and P_k in per-lane local memory, so that
+// sweep 2's partial-wave loop carries only the contraction.  The small matrix products between the partial-wave
+// loops run as rolled loops over one index of the local-memory operand: the per-energy code then stays within the
+// instruction cache (the unrolled products made the kernel several times larger than its two hot loops); their
+// complex multiply-adds are FP32-pair instructions (3 % faster; in the forward's register-resident chain product the
+// pairing measured slower and is not used).  Keeping only every second or third prefix and recomputing the others
+// from F~_k (1.5-2.3 KB instead of 3.7 KB of local memory per lane) measured 1-3 % slower on B200: the local memory is
+// not what bounds this kernel.
 template <typename R, int KIND>
 __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, const R (*dterm_db)[49],
                               const Tables<R> &T, int e, int nleg, C2<R> gbar, ParGrad &pg)
@@ -487,8 +558,6 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     constexpr LamTab L = lamtab(KIND);
     constexpr int N = L.N, N0 = L.N0, MM = L.MM, DS = dstride(MM);
     constexpr RepTab<KIND, N, N> RT{};
-    constexpr int CK = FG_ADJ_CKPT;
-    constexpr int NCK = CK > 0 ? (kMaxLeg - 2) / CK : 0;     // checkpoints P_CK, P_2CK, ... below P_nsc
     const int E = T.E, nsc = nleg - 1;
     const size_t dleg = (size_t)(T.L1 + 1) * DS, tlip = (size_t)(T.L1 + 1) * E;
     const C2<R> ck = T.ck[e];
@@ -497,19 +566,16 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     const C2<R> cf = cfac(g, T, e, nleg, ck);
     const C2<R> sd = cmul(C2<R>{gbar.x, -gbar.y}, cf);      // s = conj(gbar) cfac: dL = Re(s dptrac)
     const C2<R> sck = cmul(sd, ck);
-    // per-lane local memory: F~_k (k = 1..nsc), the checkpoint prefixes, the working prefix P and the suffix R_k
+    // per-lane local memory: F~_k (k = 1..nsc), P_k = F_k ... F_1 P_0 (k = 0..nsc), R_k.  (Measured on B200: loading
+    // the next column while the current one is in use, or forming P_0 on the fly instead of storing it, is slower.)
     C2<R> Fst[kMaxLeg - 1][RT.n];
-    C2<R> Pck[NCK > 0 ? NCK : 1][N][N0];
-    C2<R> Pw[N][N0];
+    C2<R> Pst[kMaxLeg][N][N0];
     C2<R> Rst[N0][N];
-    auto identity = [&]() {
 #pragma unroll
-        for (int a = 0; a < N; ++a)
+    for (int a = 0; a < N; ++a)
 #pragma unroll
-            for (int b = 0; b < N0; ++b) Pw[a][b] = a == b ? C2<R>{R(1), R(0)} : cz<R>();
-    };
-    identity();
-    // sweep 1: F~_k and P_k = e^{-i eta_(k+1) m} F~_k P_(k-1); the last, P_nsc, stays in Pw for the termination
+        for (int b = 0; b < N0; ++b) Pst[0][a][b] = a == b ? C2<R>{R(1), R(0)} : cz<R>();
+    // sweep 1
     for (int k = 1; k <= nsc; ++k) {
         C2<R> acc[RT.n];
         const int ip = g.ip[k];
@@ -519,12 +585,22 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
         for (int r = 0; r < RT.n; ++r) Fst[k - 1][r] = acc[r];
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
-        chain_step<R, KIND, N, N0, MM>(Pw, acc, ph);
-        if (CK > 0 && k < nsc && k % CK == 0) {
+        // P_k = e^{-i eta_(k+1) m} F~_k P_(k-1), one column of P at a time
 #pragma unroll 1
-            for (int a = 0; a < N; ++a)
+        for (int b = 0; b < N0; ++b) {
+            C2<R> col[N];
 #pragma unroll
-                for (int b = 0; b < N0; ++b) Pck[k / CK - 1][a][b] = Pw[a][b];
+            for (int c = 0; c < N; ++c) col[c] = Pst[k - 1][c][b];
+#pragma unroll
+            for (int a = 0; a < N; ++a) {
+                C2<R> s = cz<R>();
+#pragma unroll
+                for (int c = 0; c < N; ++c) {
+                    const C2<R> f = acc[RT.rep[a][c]];
+                    s = RT.sg[a][c] > 0 ? pfma(f, col[c], s) : pfms(f, col[c], s);
+                }
+                Pst[k][a][b] = cmul(ph[L.m[a] + MM], s);
+            }
         }
     }
     // the termination with P_nsc: its own gradients, ptrac and cfac's gradient
@@ -537,7 +613,7 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
         for (int a = 0; a < N0; ++a)
 #pragma unroll
             for (int b = N0; b < N; ++b) Rst[a][b] = cz<R>();
-        const C2<R> ptrac = term_adj<R, KIND>(g, dterm_db, T, e, tl, [&](int b, int a) { return Pw[b][a]; },
+        const C2<R> ptrac = term_adj<R, KIND>(g, dterm_db, T, e, tl, [&](int b, int a) { return Pst[nsc][b][a]; },
                                               ge1, gbn, gr1, grn, &Rst[0][0], N);
         add_re(pg.eta[1], sd, ge1);
         add_re(pg.beta[nleg], sd, gbn);
@@ -547,27 +623,6 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     }
     // sweep 2, k = nsc .. 1 with R_k = T F_nsc ... F_(k+1) and M_k = P_(k-1) R_k
     for (int k = nsc; k >= 1; --k) {
-        // P_(k-1) into Pw: from the nearest checkpoint at or below it, or from P_0
-        {
-            const int j0 = CK > 0 ? ((k - 1) / CK) * CK : 0;
-            if (j0 == 0) {
-                identity();
-            } else {
-#pragma unroll 1
-                for (int a = 0; a < N; ++a)
-#pragma unroll
-                    for (int b = 0; b < N0; ++b) Pw[a][b] = Pck[j0 / CK - 1][a][b];
-            }
-#pragma unroll 1
-            for (int j = j0 + 1; j <= k - 1; ++j) {
-                C2<R> f[RT.n];
-#pragma unroll
-                for (int r = 0; r < RT.n; ++r) f[r] = Fst[j - 1][r];
-                C2<R> phj[2 * MM + 1];
-                phase_powers<R, MM>(g.phs[j + 1], phj);
-                chain_step<R, KIND, N, N0, MM>(Pw, f, phj);
-            }
-        }
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
         // Wh[r] = sum over the flip orbit of r of sign * e^{-i eta m_a} M(b, a), We the same times -i m_a;
@@ -581,7 +636,7 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
             for (int c = 0; c < N0; ++c) {
                 C2<R> pc[N], rr[N], re[N];
 #pragma unroll
-                for (int b = 0; b < N; ++b) pc[b] = Pw[b][c];
+                for (int b = 0; b < N; ++b) pc[b] = Pst[k - 1][b][c];
 #pragma unroll
                 for (int a = 0; a < N; ++a) {
                     rr[a] = cmul(ph[L.m[a] + MM], Rst[c][a]);
@@ -997,6 +1052,7 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
 {
     using K = Kinds<EDGE>;
     extern __shared__ __align__(16) unsigned char smem[];
+    if (*(volatile const int *)status & kBadLayout) return;     // a batch that k_validate refused
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int E = T.E, L1 = T.L1;
     unsigned char *base = smem + (size_t)w * wbytes;
@@ -1011,11 +1067,7 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
         tk = __shfl_sync(0xffffffffu, tk, 0);
         if (tk >= (unsigned long long)B) break;
         const int64_t p = order ? order[tk] : (int64_t)tk;
-        const int nleg = (p >= 0 && p < B) ? (nlegs ? nlegs[p] : nleg_uniform) : 0;
-        if (nleg < 2 || nleg > stride) {              // a malformed batch: report it, never index past the arrays
-            if (lane == 0) atomicOr(status, kBadLayout);
-            continue;
-        }
+        const int nleg = nlegs ? nlegs[p] : nleg_uniform;
         const int MM = nleg == 2 ? K::MMSS : K::MMMS;
         path_setup<R, CT>(g, dh, T, coords + p * stride * 3, ipots + p * stride, nleg, lane, status, MM);
         adj_setup<R>(g, dhd, as.dterm_db, T, nleg, lane, MM);
@@ -1073,12 +1125,13 @@ __global__ void __launch_bounds__(256) k_fine_adjoint(int64_t B, int E, int NK, 
                                                        const double *__restrict__ S_d, const int *__restrict__ span,
                                                        const int *__restrict__ tspan, const R *__restrict__ gchi,
                                                        const double *__restrict__ grows, const int *__restrict__ row,
-                                                       int nrows, const double *__restrict__ deg,
+                                                       const double *__restrict__ deg,
                                                        const double *__restrict__ sigma2, C2<R> *__restrict__ gbar,
                                                        R *__restrict__ greff_r, double *__restrict__ greff_d,
                                                        double *__restrict__ gsig, int *status, size_t wbytes)
 {
     extern __shared__ __align__(16) unsigned char smem[];
+    if (status && (*(volatile const int *)status & kBadLayout)) return;   // a batch that k_validate refused
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     unsigned char *base = smem + (size_t)w * wbytes;
     double *amp = reinterpret_cast<double *>(base);        // FP64, as the forward forms it
@@ -1093,9 +1146,7 @@ __global__ void __launch_bounds__(256) k_fine_adjoint(int64_t B, int E, int NK, 
         const double rf = reff_d ? reff_d[p] : (double)reff_r[p];
         const double s2 = (mode == 1 && sigma2) ? sigma2[p] : 0.0;
         const double wd = mode == 1 ? deg[p] : 1.0;
-        const int rp = mode == 1 ? row[p] : 0;
-        if (mode == 1 && (rp < 0 || rp >= nrows) && lane == 0) atomicOr(status, kBadLayout);
-        const double *gr = (mode == 1 && rp >= 0 && rp < nrows) ? grows + (int64_t)rp * NK : nullptr;
+        const double *gr = mode == 1 ? grows + (int64_t)row[p] * NK : nullptr;
         double g_reff = 0.0, g_s2 = 0.0;
         for (int k0 = 0; k0 < NK; k0 += 32) {
             const int k = k0 + lane;
@@ -1110,7 +1161,7 @@ __global__ void __launch_bounds__(256) k_fine_adjoint(int64_t B, int E, int NK, 
                 }
                 const double qk = q_d ? q_d[k] : (double)q_r[k];
                 const double damp = s2 != 0.0 ? exp(-2.0 * s2 * qk * qk) : 1.0;
-                const double G = (mode == 1 ? (gr ? gr[k] * wd : 0.0) : (double)gchi[p * NK + k]) * damp;
+                const double G = (mode == 1 ? gr[k] * wd : (double)gchi[p * NK + k]) * damp;
                 const double arg = ph + 2.0 * qk * rf;
                 const double sn = sin_arg<R>(arg), cs = sin_arg<R>(arg + 1.5707963267948966);
                 da = G * sn;
@@ -1184,7 +1235,7 @@ template <typename R>
 fg_status launch_fine_adjoint(const StageView &sv, int64_t B, int NK, int mode, const void *cchi, const R *reff_r,
                               const double *reff_d, const R *q_r, const double *q_d, const R *S_r, const double *S_d,
                               const int *span, const int *tspan, const R *gchi, const double *grows, const int *row,
-                              int nrows, const double *deg, const double *sigma2, C2<R> *gbar, R *greff_r,
+                              const double *deg, const double *sigma2, C2<R> *gbar, R *greff_r,
                               double *greff_d, double *gsig, int *status, cudaStream_t st)
 {
     const size_t wb = 2 * align_up((size_t)sv.E * 8, 16) + align_up((size_t)NK * 16, 16);
@@ -1193,7 +1244,7 @@ fg_status launch_fine_adjoint(const StageView &sv, int64_t B, int NK, int mode, 
     int blocks = 0;
     if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;
     kern<<<blocks, threads, wb * warps, st>>>(B, sv.E, NK, mode, static_cast<const C2<R> *>(cchi), reff_r, reff_d, q_r,
-                                              q_d, S_r, S_d, span, tspan, gchi, grows, row, nrows, deg, sigma2, gbar,
+                                              q_d, S_r, S_d, span, tspan, gchi, grows, row, deg, sigma2, gbar,
                                               greff_r, greff_d, gsig, status, wb);
     FG_CUDA(cudaGetLastError());
     return FG_OK;
@@ -1231,8 +1282,9 @@ fg_status Launch<R, EDGE>::fused_bwd(const StageView &sv, const Tables<R> &T, co
     double *greff = reinterpret_cast<double *>(ws + kCounterBytes + align_up((size_t)P->n * sv.E * sizeof(C2<double>), 256));
     FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes, st));
     if (P->n == 0) return FG_OK;
+    if (fg_status rc = launch_validate(P, sv.nph1, status, st)) return rc;
     if (fg_status rc = launch_fine_adjoint<R>(sv, P->n, NK, 1, cchi_saved, nullptr, reff_saved, nullptr, q, nullptr, S,
-                                              span, tspan, nullptr, grad_rows, P->row, P->nrows, P->deg, P->sigma2,
+                                              span, tspan, nullptr, grad_rows, P->row, P->deg, P->sigma2,
                                               gbar, nullptr, greff, grad_sigma2, status, st))
         return rc;
     return launch_adjoint<R, EDGE, double>(sv, T, P->coords, P->ipots, P->nleg_max, P->nleg, 0, P->nleg_max - 1, P->n,
@@ -1247,7 +1299,7 @@ fg_status LaunchCommon<R>::chi_fine_bwd(const StageView &sv, int64_t B, const vo
 {
     return launch_fine_adjoint<R>(sv, B, NK, 0, cchi, static_cast<const R *>(reff), nullptr, static_cast<const R *>(q),
                                   nullptr, static_cast<const R *>(S), nullptr, span, tspan,
-                                  static_cast<const R *>(grad_chi), nullptr, nullptr, 0, nullptr, nullptr,
+                                  static_cast<const R *>(grad_chi), nullptr, nullptr, nullptr, nullptr,
                                   static_cast<C2<R> *>(grad_cchi), static_cast<R *>(grad_reff), nullptr, nullptr,
                                   nullptr, st);
 }

@@ -384,19 +384,16 @@ template <class F> fg_status by_kind(const fg_stage *s, fg_precision prec, F &&f
     }
 }
 
-// Host-side checks of a batch's sizes and pointers; the kernels check the contents (indices and offsets) and report
-// through the call's status word.
+// Host-side checks of a batch's sizes and pointers; k_validate checks the contents (indices) on the device and
+// reports through the call's status word.
 fg_status check_paths(const fg_paths *P)
 {
     if (!P) return fail(FG_ERR_VALUE, "null paths");
-    if (P->n < 0 || P->nrows < 0 || P->nchunks < 0) return fail(FG_ERR_VALUE, "negative size");
+    if (P->n < 0 || P->nrows < 0) return fail(FG_ERR_VALUE, "negative size");
     if (P->nleg_max < 2 || P->nleg_max > kMaxLeg) return fail(FG_ERR_VALUE, "nleg_max must be 2..9");
     if (P->n > 0 && (!P->coords || !P->ipots || !P->nleg || !P->deg || !P->order || !P->row))
         return fail(FG_ERR_VALUE, "null array in paths");
-    if (P->nrows > 0 && !P->row_chunks) return fail(FG_ERR_VALUE, "null row_chunks with nrows > 0");
-    if (P->nchunks > 0 && (!P->chunk_bounds || !P->sorted))
-        return fail(FG_ERR_VALUE, "null chunk_bounds or sorted with nchunks > 0");
-    if (P->n > 0 && P->nchunks == 0) return fail(FG_ERR_VALUE, "paths but no summation chunks");
+    if (P->n > 0 && P->nrows == 0) return fail(FG_ERR_VALUE, "paths but no rows");
     if (P->n > 0x7fffffff) return fail(FG_ERR_VALUE, "at most 2^31-1 paths per call");
     return FG_OK;
 }

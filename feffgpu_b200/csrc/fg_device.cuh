@@ -27,10 +27,9 @@ constexpr int kBadRange = 4;    // a weighted path term not finite or beyond the
 // resolution 2^-64 held in two 64-bit integer sums: a signed word of resolution 2^-32 (its additions wrap modulo
 // 2^64, which leaves the final sum exact whenever the row itself is below 2^31) and a low word of the next 32 bits
 // (non-negative, below 2^32 per term, so up to 2^31 terms cannot overflow it).  Integer addition is associative,
-// so the rows do not depend on the order in which paths finish, the launch shape or the GPU.
-#ifndef FG_EXACT_ROWS
-#define FG_EXACT_ROWS 0
-#endif
+// so the rows do not depend on the order in which paths finish, the launch shape or the GPU.  (Measured on B200:
+// 45.80 ms against 45.99 for per-path terms in memory summed in a fixed order afterwards on the 189,419-path benchmark
+// batch, 137.5 against 149.1 ms on the 4.2e6-path MD batch, and no workspace beyond the rows.)
 // Adds v to the fixed-point sum whose two words are a[0] and a[stride]; false (nothing added) if v is not finite or
 // |v| >= 2^31.
 __device__ __forceinline__ bool fixed_add(unsigned long long *a, size_t stride, double v)

@@ -170,9 +170,8 @@ __device__ __forceinline__ void accumulate_f(C2<R> (&acc)[RepTab<KIND, NR, NC>()
         const C2<R> t = t1;
         t1 = t2;
         if (il + 2 <= ilx) t2 = tlk[(size_t)(il + 2) * E];
-        const R *dr = dhk + (size_t)il * DS;
         R d[NCAN];
-        load_row<R, NCAN>(dr, d);
+        load_row<R, NCAN>(dhk + (size_t)il * DS, d);
         C2<R> tco[CO + 1];
 #pragma unroll
         for (int j = 1; j <= CO; ++j) tco[j] = pmul(t, co[j]);

@@ -166,21 +166,20 @@ struct PathsDev {
 
 // Fused forward: every path of the batch, all leg counts, from one work queue (costliest first); per path the
 // signal at all E, its amplitude and unwrapped phase, and the weighted fine-grid terms
-// deg exp(-2 sigma2 q^2) a(q) sin(phi(q) + 2 q reff) for the deterministic reduction that follows.
+// deg exp(-2 sigma2 q^2) a(q) sin(phi(q) + 2 q reff), each added exactly to its row (fixed_add).  The batch's
+// indices were checked by k_validate before the launch: with a malformed batch the kernel returns at once.
 #ifndef FG_FUSED_MIN_BLOCKS
 #define FG_FUSED_MIN_BLOCKS 2
 #endif
 template <typename R, int EDGE>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
-    k_fused(Tables<R> T, PathsDev P, int NK, const double *__restrict__ q,
-                                                const double *__restrict__ S, const int *__restrict__ span,
-                                                double *__restrict__ terms, unsigned long long *__restrict__ racc,
-                                                C2<R> *__restrict__ cchi_save,
-                                                double *__restrict__ reff_save, unsigned long long *counter, int *bad,
-                                                int nsc_max, size_t wbytes)
+    k_fused(Tables<R> T, PathsDev P, int NK, const double *__restrict__ q, const double *__restrict__ S,
+            const int *__restrict__ span, unsigned long long *__restrict__ racc, C2<R> *__restrict__ cchi_save,
+            double *__restrict__ reff_save, unsigned long long *counter, int *status, int nsc_max, size_t wbytes)
 {
     using K = Kinds<EDGE>;
     extern __shared__ __align__(16) unsigned char smem[];
+    if (*(volatile const int *)status & kBadLayout) return;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int E = T.E, L1 = T.L1;
     unsigned char *base = smem + (size_t)w * wbytes;
@@ -195,12 +194,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= (unsigned long long)P.n) break;
         const int64_t p = P.order[t];
-        const int nleg = (p >= 0 && p < P.n) ? P.nleg[p] : 0;
-        if (nleg < 2 || nleg > P.nleg_max) {          // a malformed batch: report it, never index past the arrays
-            if (lane == 0) atomicOr(bad, kBadLayout);
-            continue;
-        }
-        path_setup<R, double>(g, dh, T, P.coords + p * P.nleg_max * 3, P.ipots + p * P.nleg_max, nleg, lane, bad,
+        const int nleg = P.nleg[p];
+        path_setup<R, double>(g, dh, T, P.coords + p * P.nleg_max * 3, P.ipots + p * P.nleg_max, nleg, lane, status,
                               nleg == 2 ? K::MMSS : K::MMMS);
         for (int e0 = first_chunk(E); e0 < E; e0 += 32) {
             const int e = e0 + lane;
@@ -214,13 +209,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
         amp_phase<R>(E, lane, [&](int e) { return cbuf[e]; }, amp, pha);
         __syncwarp();
         const double rf = g.reff * kBohr, wdeg = P.deg[p], s2 = P.sigma2 ? P.sigma2[p] : 0.0;
-#if FG_EXACT_ROWS
-        int prow = P.row[p];
-        if (prow < 0 || prow >= P.nrows) {
-            if (lane == 0) atomicOr(bad, kBadLayout);
-            prow = -1;
-        }
-#endif
+        unsigned long long *acc_row = racc + (size_t)P.row[p] * NK;
         for (int k0 = 0; k0 < NK; k0 += 32) {
             const int k = k0 + lane;
             if (k < NK) {
@@ -234,12 +223,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
                 const double qk = q[k];
                 const double damp = s2 != 0.0 ? exp(-2.0 * s2 * qk * qk) : 1.0;   // exact 1 without sigma^2
                 const double v = wdeg * a * sin_arg<R>(ph + 2.0 * qk * rf) * damp;
-#if FG_EXACT_ROWS
-                const size_t stride = (size_t)P.nrows * NK;
-                if (prow < 0 || !fixed_add(racc + (size_t)prow * NK + k, stride, v)) atomicOr(bad, kBadRange);
-#else
-                terms[p * NK + k] = v;
-#endif
+                if (!fixed_add(acc_row + k, (size_t)P.nrows * NK, v)) atomicOr(status, kBadRange);
             }
         }
         if (lane == 0 && reff_save) reff_save[p] = rf;
@@ -296,17 +280,10 @@ fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const 
 {
     using K = Kinds<EDGE>;
     unsigned long long *counter = reinterpret_cast<unsigned long long *>(ws);
-    int *bad = reinterpret_cast<int *>(ws + kStatusOffset);
-#if FG_EXACT_ROWS
-    double *terms = nullptr, *partial = nullptr;
+    int *status = reinterpret_cast<int *>(ws + kStatusOffset);
     unsigned long long *racc = reinterpret_cast<unsigned long long *>(ws + kCounterBytes);
-    FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes + (size_t)2 * P->nrows * NK * sizeof(unsigned long long), st));
-#else
-    unsigned long long *racc = nullptr;
-    double *terms = reinterpret_cast<double *>(ws + kCounterBytes);
-    double *partial = reinterpret_cast<double *>(ws + kCounterBytes + align_up((size_t)P->n * NK * sizeof(double), 256));
-    FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes, st));
-#endif
+    FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes + row_sum_bytes(P->nrows, NK), st));
+    if (fg_status rc = launch_validate(P, sv.nph1, status, st)) return rc;
     if (P->n > 0) {
         const int nsc_max = P->nleg_max - 1;
         const size_t wb = warp_bytes<R>(sv.L1, nsc_max, K::MM, sv.E, true);
@@ -317,16 +294,12 @@ fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const 
         if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, P->n, blocks)) return rc;
         PathsDev pd{P->n, P->nleg_max, P->nrows, P->coords, P->ipots, P->nleg, P->deg, P->sigma2, P->order, P->row};
         timer_begin(st);
-        kern<<<blocks, threads, wb * warps, st>>>(T, pd, NK, q, S, span, terms, racc, static_cast<C2<R> *>(cchi_save),
-                                                  reff_save, counter, bad, nsc_max, wb);
+        kern<<<blocks, threads, wb * warps, st>>>(T, pd, NK, q, S, span, racc, static_cast<C2<R> *>(cchi_save),
+                                                  reff_save, counter, status, nsc_max, wb);
         timer_end(st);
         FG_CUDA(cudaGetLastError());
     }
-#if FG_EXACT_ROWS
-    return launch_row_finish(P, NK, racc, rows, bad, st);
-#else
-    return launch_reductions(P, NK, terms, partial, rows, bad, st);
-#endif
+    return launch_row_finish(P, NK, racc, rows, status, st);
 }
 
 template <typename R>

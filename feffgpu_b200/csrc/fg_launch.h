@@ -58,10 +58,13 @@ template <typename R> struct LaunchCommon {
                                   const void *grad_chi, void *grad_cchi, void *grad_reff, cudaStream_t st);
 };
 
-// Fused reduction kernels (precision independent, FP64).
-// Rows of a call whose status word is set are written as NaN (so that a result can never look valid).
-fg_status launch_reductions(const fg_paths *P, int NK, const double *terms, double *partial, double *rows, int *status,
-                            cudaStream_t st);
+// The fused calls' batch check (precision independent): every path's launch-order entry, leg count (2..nleg_max),
+// row and potential indices; a bad one raises kBadLayout / kBadIpot in the status word (the per-path kernels then
+// return at once on kBadLayout, and clamp potentials).
+fg_status launch_validate(const fg_paths *P, int nph1, int *status, cudaStream_t st);
+
+// Bytes of the exact row sums of nrows x NK (two 64-bit words per entry)
+size_t row_sum_bytes(int nrows, int NK);
 
 // Rows (nrows, NK) from the exact fixed-point sums (two word arrays of nrows * NK), NaN where the status is set.
 fg_status launch_row_finish(const fg_paths *P, int NK, const unsigned long long *racc, double *rows, const int *status,

@@ -1,0 +1,513 @@
+// fg_pf_one.cu -- the path finder for one absorber, driven from the host in C++ (the reference's front ends call the
+// finder once per absorber: src/feffgpu/exafs/forward.py:122-123, md/spectrum.py:275-277).  The kernels are the
+// batched finder's (fg_paths.cu); what changes is the driver: one call runs candidates, growth, description, merges
+// and importance cut with one synchronisation per growth level plus two, instead of a Python sequence of small torch
+// operations whose launch and dispatch latency dominated a call of a few hundred paths.  The merges and the cut run
+// on the host in FP32 with the arithmetic and order of the batched path (and so of the reference, pathfinder.py:
+// 102-157, 271-279), so the kept paths are bit for bit those of fg_pf_* driven by feffgpu_b200/pathfinder.py.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "fg_launch.h"
+
+namespace fg {
+namespace {
+
+// The finder's own stream-ordered memory pool per device: its scratch comes and goes with every call, so the pool
+// keeps up to 1 GiB reserved between calls instead of returning it to the driver at each synchronisation (the
+// device's default pool, and its settings, are left alone).
+constexpr int kMaxDevices = 128;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxDevices] = {};
+
+fg_status finder_pool(cudaMemPool_t *out)
+{
+    int dev = 0;
+    FG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(FG_ERR_VALUE, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        FG_CUDA(cudaMemPoolCreate(&g_pool[dev], &props));
+        uint64_t keep = uint64_t(1) << 30;
+        FG_CUDA(cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    *out = g_pool[dev];
+    return FG_OK;
+}
+
+// device scratch of one call, stream-ordered from the finder's pool
+struct Scratch {
+    cudaStream_t st = nullptr;
+    cudaMemPool_t pool = nullptr;
+    std::vector<void *> bufs;
+    template <typename T> fg_status get(size_t count, T **out)
+    {
+        if (!pool)
+            if (fg_status rc = finder_pool(&pool)) return rc;
+        void *p = nullptr;
+        FG_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(count, 1) * sizeof(T), pool, st));
+        bufs.push_back(p);
+        *out = static_cast<T *>(p);
+        return FG_OK;
+    }
+    void release()
+    {
+        for (void *p : bufs) cudaFreeAsync(p, st);
+        bufs.clear();
+    }
+};
+
+__global__ void k_cand_len(int64_t nc, const float *__restrict__ rel, float *__restrict__ len, int32_t *__restrict__ seq,
+                           int32_t *__restrict__ slot)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nc) return;
+    const float x = rel[3 * i], y = rel[3 * i + 1], z = rel[3 * i + 2];
+    len[i] = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
+    seq[i] = (int32_t)i;
+    slot[i] = 0;
+}
+
+// out[i] = in[idx[i]] for rows of w elements
+template <typename T>
+__global__ void k_gather_rows(int64_t B, int w, const int64_t *__restrict__ idx, const T *__restrict__ in,
+                              T *__restrict__ out)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= B * w) return;
+    const int64_t b = t / w, j = t % w;
+    out[t] = in[idx[b] * w + j];
+}
+
+template <typename T> fg_status gather(int64_t B, int w, const int64_t *idx, const T *in, T *out, cudaStream_t st)
+{
+    if (B == 0 || !out) return FG_OK;
+    const int64_t n = B * w;
+    k_gather_rows<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(B, w, idx, in, out);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+// indices that sort v ascending, equal values in index order (numpy's argsort(kind="stable"))
+template <typename T> std::vector<int64_t> stable_argsort(const std::vector<T> &v)
+{
+    std::vector<int64_t> o(v.size());
+    std::iota(o.begin(), o.end(), int64_t(0));
+    std::stable_sort(o.begin(), o.end(), [&](int64_t a, int64_t b) { return v[a] < v[b]; });
+    return o;
+}
+
+// numpy.unique(rows, axis=0, return_inverse=True)[1]: the rank of each row among the distinct rows in lexicographic
+// order; rows of width w, row i at keys[i * w]
+std::vector<int64_t> unique_inverse(const std::vector<int64_t> &keys, int64_t n, int w, int64_t *groups)
+{
+    std::vector<int64_t> o(n);
+    std::iota(o.begin(), o.end(), int64_t(0));
+    auto less = [&](int64_t a, int64_t b) {
+        return std::lexicographical_compare(keys.begin() + a * w, keys.begin() + (a + 1) * w, keys.begin() + b * w,
+                                            keys.begin() + (b + 1) * w);
+    };
+    std::stable_sort(o.begin(), o.end(), less);
+    std::vector<int64_t> inv(n);
+    int64_t g = -1;
+    for (int64_t i = 0; i < n; ++i) {
+        if (i == 0 || less(o[i - 1], o[i])) ++g;
+        inv[o[i]] = g;
+    }
+    *groups = g + 1;
+    return inv;
+}
+
+}  // namespace
+}  // namespace fg
+
+using namespace fg;
+
+// One leg count of the result: its device arrays (all paths described, before the cut) and the kept indices.
+struct fg_pf_leg {
+    int nleg = 0;
+    int64_t nb = 0;                     // paths described
+    float *coords = nullptr;            // (nb, nleg, 3)
+    int64_t *ipots = nullptr, *atoms = nullptr;
+    float *rtot = nullptr, *xport = nullptr, *deg = nullptr;
+    int64_t *key = nullptr;
+    uint8_t *keep = nullptr;            // terminal flags (nleg > 2), null for single scattering
+    std::vector<int64_t> kept;          // indices into the described paths
+    std::vector<float> kept_deg;        // degeneracies of the kept paths
+};
+
+struct fg_pf_result {
+    Scratch scratch;
+    std::vector<fg_pf_leg> legs;
+    float ref = 1.f;
+};
+
+namespace {
+// pinned staging for the device -> host copies of one call (per host thread, grown as needed)
+struct Pinned {
+    void *p = nullptr;
+    size_t n = 0;
+    ~Pinned()
+    {
+        if (p) cudaFreeHost(p);
+    }
+};
+thread_local Pinned t_pinned;
+
+fg_status pinned(size_t bytes, unsigned char **out)
+{
+    if (t_pinned.n < bytes) {
+        if (t_pinned.p) cudaFreeHost(t_pinned.p);
+        t_pinned.p = nullptr;
+        t_pinned.n = 0;
+        const size_t want = std::max<size_t>(bytes, size_t(1) << 20);
+        FG_CUDA(cudaMallocHost(&t_pinned.p, want));
+        t_pinned.n = want;
+    }
+    *out = static_cast<unsigned char *>(t_pinned.p);
+    return FG_OK;
+}
+
+constexpr int64_t kPartialLimit = 30000000;   // partial paths per absorber (the reference's limit, pathfinder.py:25)
+
+// The merges and the importance cut of one absorber (the host side of feffgpu_b200/pathfinder.py's one-absorber
+// path, itself pathfinder.py:102-157, 271-279 of the reference), FP32 throughout in the same operation order.
+struct LegHost {
+    int nleg;
+    int64_t nb;                            // terminal paths
+    std::vector<int64_t> idx;              // their indices among the described sequences
+    std::vector<float> xport, deg, rtot;   // per terminal path
+    std::vector<int64_t> key;              // (nb, 2 nleg) when keyed
+};
+
+void merge_and_cut(std::vector<LegHost> &L, int64_t cnt, const std::vector<float> &c1, const std::vector<int64_t> &ip1,
+                   bool merge, float critpw, std::vector<fg_pf_leg> &legs, float &ref_out)
+{
+    LegHost &ss = L[0];
+    const int64_t nb2 = ss.nb;
+    std::vector<float> d(nb2);
+    for (int64_t i = 0; i < nb2; ++i) {
+        const float x = c1[3 * i], y = c1[3 * i + 1], z = c1[3 * i + 2];
+        d[i] = std::sqrt(x * x + y * y + z * z);
+    }
+    float ref = 1.f;
+    std::vector<int64_t> rep(nb2);
+    std::iota(rep.begin(), rep.end(), int64_t(0));
+    std::vector<float> ss_deg = ss.deg;
+    auto first_min = [](const std::vector<float> &v, const std::vector<int64_t> &at) {
+        int64_t best = 0;
+        for (int64_t i = 1; i < (int64_t)at.size(); ++i)
+            if (v[at[i]] < v[at[best]]) best = i;
+        return best;
+    };
+    if (!merge || nb2 == 0) {
+        if (nb2 && cnt > 0) ref = ss.xport[rep[first_min(d, rep)]];
+    }
+    if (merge && nb2) {
+        // greedy 1e-3 A windows over the sorted closed lengths of every path
+        std::vector<float> all;
+        for (const LegHost &l : L) all.insert(all.end(), l.rtot.begin(), l.rtot.end());
+        const std::vector<int64_t> o = stable_argsort(all);
+        std::vector<float> sr(all.size());
+        for (size_t i = 0; i < all.size(); ++i) sr[i] = all[o[i]];
+        std::vector<int64_t> seg{0, (int64_t)sr.size()}, win_sorted(sr.size()), win(sr.size());
+        fg_pf_windows(sr.data(), seg.data(), 1, 1e-3f, win_sorted.data());
+        for (size_t i = 0; i < sr.size(); ++i) win[o[i]] = win_sorted[i];
+        const std::vector<int64_t> od = stable_argsort(d);
+        std::vector<int64_t> keys((size_t)nb2 * 3);
+        for (int64_t i = 0; i < nb2; ++i) {
+            keys[3 * i] = (int64_t)std::nearbyint(d[od[i]] * 1000.f);
+            keys[3 * i + 1] = ip1[od[i]];
+            keys[3 * i + 2] = win[od[i]];
+        }
+        int64_t G = 0;
+        const std::vector<int64_t> inv = unique_inverse(keys, nb2, 3, &G);
+        std::vector<int64_t> firstp(G, nb2);
+        std::vector<float> gcount(G, 0.f);
+        for (int64_t i = 0; i < nb2; ++i) {
+            firstp[inv[i]] = std::min(firstp[inv[i]], i);
+            gcount[inv[i]] += 1.f;
+        }
+        const std::vector<int64_t> go = stable_argsort(firstp);
+        rep.assign(G, 0);
+        ss_deg.assign(G, 0.f);
+        for (int64_t g = 0; g < G; ++g) {
+            rep[g] = od[firstp[go[g]]];
+            ss_deg[g] = gcount[go[g]];
+        }
+        const int64_t f = first_min(d, rep);
+        ref = ss.xport[rep[f]] * ss_deg[f];
+    }
+    ref_out = ref;
+    legs.resize(L.size());
+    for (size_t li = 0; li < L.size(); ++li) {
+        const LegHost &l = L[li];
+        std::vector<int64_t> idx;
+        std::vector<float> dg;
+        if (l.nleg == 2) {
+            idx = rep;
+            dg = ss_deg;
+        } else {
+            idx.resize(l.nb);
+            std::iota(idx.begin(), idx.end(), int64_t(0));
+            dg = l.deg;
+        }
+        std::vector<float> dtot = dg;
+        if (l.nleg > 2 && merge && l.nb && cnt > 1) {
+            int64_t G = 0;
+            const std::vector<int64_t> inv = unique_inverse(l.key, l.nb, 2 * l.nleg, &G);
+            std::vector<float> tot(G, 0.f);
+            for (int64_t i = 0; i < l.nb; ++i) tot[inv[i]] += dg[i];
+            for (int64_t i = 0; i < l.nb; ++i) dtot[i] = tot[inv[i]];
+        }
+        fg_pf_leg &out = legs[li];
+        out.nleg = l.nleg;
+        out.kept.clear();
+        out.kept_deg.clear();
+        for (size_t i = 0; i < idx.size(); ++i) {
+            const float frac = 100.f * dtot[i] * l.xport[idx[i]] / ref;
+            if (frac >= critpw) {
+                out.kept.push_back(l.idx[idx[i]]);
+                out.kept_deg.push_back(dg[i]);
+            }
+        }
+    }
+}
+}  // namespace
+
+extern "C" fg_status fg_pf_enumerate_one(const float *pos, int64_t n, float box, const float *cell, int64_t absorber,
+                                         const int64_t *ipot_of, const fg_pf_tables *T, float rmax, int32_t nlegmax,
+                                         float critpw, int32_t merge, fg_pf_result **out, int64_t *counts, float *ref,
+                                         void *stream)
+{
+    if (!pos || !ipot_of || !T || !out || !counts || !ref) return fail(FG_ERR_VALUE, "null argument");
+    if (n < 1 || absorber < 0 || absorber >= n) return fail(FG_ERR_VALUE, "absorber outside the atoms");
+    if (nlegmax < 2 || nlegmax > kMaxLeg) return fail(FG_ERR_VALUE, "nlegmax must be 2..9");
+    *out = nullptr;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    fg_pf_result *r = new fg_pf_result();
+    r->scratch.st = st;
+    Scratch &S = r->scratch;
+    auto bail = [&](fg_status rc) {
+        S.release();
+        delete r;
+        return rc;
+    };
+#define FG_TRY(x)                            \
+    do {                                     \
+        if (fg_status rc_ = (x)) return bail(rc_); \
+    } while (0)
+    auto cuda = [&](cudaError_t e, const char *what) -> fg_status {
+        return e == cudaSuccess ? FG_OK : fail(FG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    unsigned char *hp = nullptr;
+    // candidates: count, then write (one synchronisation for the count)
+    int64_t *d_ab = nullptr, *d_off = nullptr;
+    int32_t *d_cnt = nullptr;
+    FG_TRY(S.get(1, &d_ab));
+    FG_TRY(S.get(2, &d_off));
+    FG_TRY(S.get(1, &d_cnt));
+    FG_TRY(cuda(cudaMemcpyAsync(d_ab, &absorber, sizeof(int64_t), cudaMemcpyHostToDevice, st), "copy"));
+    FG_TRY(fg_pf_candidates(pos, n, box, cell, d_ab, 1, 1, rmax, d_cnt, nullptr, nullptr, nullptr, stream));
+    FG_TRY(pinned(64, &hp));
+    FG_TRY(cuda(cudaMemcpyAsync(hp, d_cnt, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "copy"));
+    FG_TRY(cuda(cudaStreamSynchronize(st), "synchronize"));
+    int32_t nc32 = 0;
+    std::memcpy(&nc32, hp, sizeof(int32_t));
+    const int64_t nc = nc32;
+    const int64_t off_h[2] = {0, nc};
+    FG_TRY(cuda(cudaMemcpyAsync(d_off, off_h, sizeof(off_h), cudaMemcpyHostToDevice, st), "copy"));
+    int64_t *cand_atom = nullptr;
+    float *cand_rel = nullptr;
+    FG_TRY(S.get(nc, &cand_atom));
+    FG_TRY(S.get(3 * nc, &cand_rel));
+    if (nc > 0)
+        FG_TRY(fg_pf_candidates(pos, n, box, cell, d_ab, 1, 1, rmax, nullptr, d_off, cand_atom, cand_rel, stream));
+    // single scattering: every candidate
+    int32_t *seq = nullptr, *slot = nullptr;
+    float *len = nullptr;
+    FG_TRY(S.get(nc, &seq));
+    FG_TRY(S.get(nc, &slot));
+    FG_TRY(S.get(nc, &len));
+    if (nc > 0) {
+        k_cand_len<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(nc, cand_rel, len, seq, slot);
+        FG_TRY(cuda(cudaGetLastError(), "launch"));
+    }
+    auto describe = [&](fg_pf_leg &l, const int32_t *s, const int32_t *sl, bool want_key) -> fg_status {
+        const int64_t B = l.nb;
+        if (fg_status rc = S.get(B * l.nleg * 3, &l.coords)) return rc;
+        if (fg_status rc = S.get(B * l.nleg, &l.ipots)) return rc;
+        if (fg_status rc = S.get(B * (l.nleg - 1), &l.atoms)) return rc;
+        if (fg_status rc = S.get(B, &l.rtot)) return rc;
+        if (fg_status rc = S.get(B, &l.xport)) return rc;
+        if (want_key)
+            if (fg_status rc = S.get(B * 2 * l.nleg, &l.key)) return rc;
+        if (B == 0) return FG_OK;
+        return fg_pf_describe(B, l.nleg, s, sl, d_off, cand_rel, cand_atom, ipot_of, d_ab, T, l.coords, l.ipots,
+                              l.atoms, l.rtot, l.xport, l.key, stream);
+    };
+    std::vector<fg_pf_leg> &legs = r->legs;
+    legs.reserve(kMaxLeg);
+    legs.emplace_back();
+    legs[0].nleg = 2;
+    legs[0].nb = nc;
+    FG_TRY(describe(legs[0], seq, slot, false));
+    // growth, one level per extra leg: one synchronisation per level (the number of children sizes the next)
+    int64_t P = nc > 1 ? nc : 0;     // multiple scattering needs two candidates (pathfinder.py:237, 243, 262)
+    const float two_r = 2.f * rmax;
+    for (int m = 1; m <= nlegmax - 2 && P > 0; ++m) {
+        int32_t *cc = nullptr;
+        FG_TRY(S.get(P, &cc));
+        FG_TRY(fg_pf_extend(P, m, seq, len, slot, d_off, cand_rel, two_r, cc, nullptr, nullptr, nullptr, nullptr,
+                            stream));
+        FG_TRY(pinned((size_t)P * sizeof(int32_t), &hp));
+        FG_TRY(cuda(cudaMemcpyAsync(hp, cc, (size_t)P * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "copy"));
+        FG_TRY(cuda(cudaStreamSynchronize(st), "synchronize"));
+        std::vector<int64_t> coff((size_t)P + 1, 0);
+        const int32_t *ch = reinterpret_cast<const int32_t *>(hp);
+        for (int64_t i = 0; i < P; ++i) coff[i + 1] = coff[i] + ch[i];
+        const int64_t Cn = coff[P];
+        if (Cn > kPartialLimit || Cn * (4 * (m + 2) + 8) > (int64_t(8) << 30))
+            return bail(fail(FG_ERR_VALUE, std::to_string(Cn) + " partial paths of " + std::to_string(m + 2) +
+                                               " legs: lower the path cutoff or the largest number of legs"));
+        if (Cn == 0) break;
+        int64_t *d_coff = nullptr;
+        int32_t *cseq = nullptr, *cslot = nullptr;
+        float *clen = nullptr;
+        FG_TRY(S.get(P + 1, &d_coff));
+        FG_TRY(S.get(Cn * (m + 1), &cseq));
+        FG_TRY(S.get(Cn, &cslot));
+        FG_TRY(S.get(Cn, &clen));
+        FG_TRY(cuda(cudaMemcpyAsync(d_coff, coff.data(), coff.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st),
+                    "copy"));
+        FG_TRY(fg_pf_extend(P, m, seq, len, slot, d_off, cand_rel, two_r, nullptr, d_coff, cseq, clen, cslot, stream));
+        fg_pf_leg l;
+        l.nleg = m + 2;
+        l.nb = Cn;
+        FG_TRY(S.get(Cn, &l.keep));
+        FG_TRY(S.get(Cn, &l.deg));
+        FG_TRY(fg_pf_terminal(Cn, m + 1, cseq, cslot, d_off, l.keep, l.deg, stream));
+        FG_TRY(describe(l, cseq, cslot, merge != 0));
+        legs.push_back(l);
+        seq = cseq;
+        slot = cslot;
+        len = clen;
+        P = Cn;
+    }
+    // the fields the merges and the cut read, in one copy through pinned memory
+    size_t bytes = 0;
+    auto reserve = [&](size_t b) {
+        const size_t at = bytes;
+        bytes += (b + 15) / 16 * 16;
+        return at;
+    };
+    struct At { size_t xport, deg, rtot, keep, key; };
+    std::vector<At> at(legs.size());
+    for (size_t i = 0; i < legs.size(); ++i) {
+        const fg_pf_leg &l = legs[i];
+        at[i].xport = reserve(l.nb * sizeof(float));
+        at[i].rtot = reserve(l.nb * sizeof(float));
+        at[i].deg = l.deg ? reserve(l.nb * sizeof(float)) : 0;
+        at[i].keep = l.keep ? reserve(l.nb) : 0;
+        at[i].key = l.key ? reserve(l.nb * 2 * l.nleg * sizeof(int64_t)) : 0;
+    }
+    const size_t at_c1 = reserve(nc * 3 * sizeof(float)), at_ip1 = reserve(nc * sizeof(int64_t));
+    FG_TRY(pinned(bytes, &hp));
+    auto d2h = [&](size_t o, const void *src, size_t b) {
+        return b ? cuda(cudaMemcpyAsync(hp + o, src, b, cudaMemcpyDeviceToHost, st), "copy") : FG_OK;
+    };
+    for (size_t i = 0; i < legs.size(); ++i) {
+        const fg_pf_leg &l = legs[i];
+        FG_TRY(d2h(at[i].xport, l.xport, l.nb * sizeof(float)));
+        FG_TRY(d2h(at[i].rtot, l.rtot, l.nb * sizeof(float)));
+        if (l.deg) FG_TRY(d2h(at[i].deg, l.deg, l.nb * sizeof(float)));
+        if (l.keep) FG_TRY(d2h(at[i].keep, l.keep, l.nb));
+        if (l.key) FG_TRY(d2h(at[i].key, l.key, l.nb * 2 * l.nleg * sizeof(int64_t)));
+    }
+    if (nc > 0) {
+        // candidate j's coordinates are row 1 of single-scattering path j; its potential likewise
+        FG_TRY(cuda(cudaMemcpy2DAsync(hp + at_c1, 3 * sizeof(float), legs[0].coords + 3, 6 * sizeof(float),
+                                      3 * sizeof(float), nc, cudaMemcpyDeviceToHost, st), "copy"));
+        FG_TRY(cuda(cudaMemcpy2DAsync(hp + at_ip1, sizeof(int64_t), legs[0].ipots + 1, 2 * sizeof(int64_t),
+                                      sizeof(int64_t), nc, cudaMemcpyDeviceToHost, st), "copy"));
+    }
+    FG_TRY(cuda(cudaStreamSynchronize(st), "synchronize"));
+    std::vector<LegHost> H(legs.size());
+    for (size_t i = 0; i < legs.size(); ++i) {
+        const fg_pf_leg &l = legs[i];
+        LegHost &h = H[i];
+        h.nleg = l.nleg;
+        const float *xp = reinterpret_cast<const float *>(hp + at[i].xport);
+        const float *rt = reinterpret_cast<const float *>(hp + at[i].rtot);
+        const float *dg = l.deg ? reinterpret_cast<const float *>(hp + at[i].deg) : nullptr;
+        const uint8_t *kp = l.keep ? hp + at[i].keep : nullptr;
+        const int64_t *ky = l.key ? reinterpret_cast<const int64_t *>(hp + at[i].key) : nullptr;
+        for (int64_t j = 0; j < l.nb; ++j) {
+            if (kp && !kp[j]) continue;              // not a path (ends at the absorber, or after its reverse)
+            h.idx.push_back(j);
+            h.xport.push_back(xp[j]);
+            h.rtot.push_back(rt[j]);
+            h.deg.push_back(dg ? dg[j] : 1.f);
+            if (ky) h.key.insert(h.key.end(), ky + j * 2 * l.nleg, ky + (j + 1) * 2 * l.nleg);
+        }
+        h.nb = (int64_t)h.idx.size();
+    }
+    std::vector<float> c1(nc * 3);
+    std::vector<int64_t> ip1(nc);
+    if (nc > 0) {
+        std::memcpy(c1.data(), hp + at_c1, c1.size() * sizeof(float));
+        std::memcpy(ip1.data(), hp + at_ip1, ip1.size() * sizeof(int64_t));
+    }
+    std::vector<fg_pf_leg> kept;
+    merge_and_cut(H, nc, c1, ip1, merge != 0, critpw, kept, r->ref);
+    for (int i = 0; i <= kMaxLeg; ++i) counts[i] = -1;
+    for (size_t i = 0; i < legs.size(); ++i) {
+        legs[i].kept = std::move(kept[i].kept);
+        legs[i].kept_deg = std::move(kept[i].kept_deg);
+        counts[legs[i].nleg] = (int64_t)legs[i].kept.size();
+    }
+    *ref = r->ref;
+    *out = r;
+    return FG_OK;
+#undef FG_TRY
+}
+
+extern "C" fg_status fg_pf_result_gather(fg_pf_result *r, int32_t nleg, float *coords, int64_t *ipots, float *deg,
+                                         float *xport, int64_t *atoms, void *stream)
+{
+    if (!r) return fail(FG_ERR_VALUE, "null result");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    for (fg_pf_leg &l : r->legs) {
+        if (l.nleg != nleg) continue;
+        const int64_t B = (int64_t)l.kept.size();
+        if (B == 0) return FG_OK;
+        if (!coords || !ipots || !deg || !xport || !atoms) return fail(FG_ERR_VALUE, "null output");
+        int64_t *d_idx = nullptr;
+        if (fg_status rc = r->scratch.get(B, &d_idx)) return rc;
+        FG_CUDA(cudaMemcpyAsync(d_idx, l.kept.data(), B * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+        FG_CUDA(cudaMemcpyAsync(deg, l.kept_deg.data(), B * sizeof(float), cudaMemcpyHostToDevice, st));
+        if (fg_status rc = gather<float>(B, nleg * 3, d_idx, l.coords, coords, st)) return rc;
+        if (fg_status rc = gather<int64_t>(B, nleg, d_idx, l.ipots, ipots, st)) return rc;
+        if (fg_status rc = gather<float>(B, 1, d_idx, l.xport, xport, st)) return rc;
+        return gather<int64_t>(B, nleg - 1, d_idx, l.atoms, atoms, st);
+    }
+    return fail(FG_ERR_VALUE, "no paths of " + std::to_string(nleg) + " legs in the result");
+}
+
+extern "C" void fg_pf_result_destroy(fg_pf_result *r)
+{
+    if (!r) return;
+    r->scratch.release();
+    delete r;
+}

@@ -1,58 +1,33 @@
-// fg_reduce.cu -- the deterministic cross-path sum of the fused stage: per-chunk partial sums of the per-path
-// fine-grid terms in a fixed order, then per-row sums of the chunk partials, both Neumaier-compensated in FP64.
+// fg_reduce.cu -- the fused stage's batch check and its exact row sums: every weighted path term is added to its row as
+// a fixed-point number of resolution 2^-64 (fixed_add, two 64-bit integer words per row entry), and the rows are read
+// out once all paths are done.  Integer addition is associative, so the rows are exact sums of the rounded terms,
+// bit for bit the same whatever the order in which paths finish, the launch shape or the GPU.
 #include "fg_launch.h"
 
 namespace fg {
 
 namespace {
-struct KSum {
-    double s = 0.0, c = 0.0;
-    __device__ __forceinline__ void add(double x)
-    {
-        const double t = s + x;
-        c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
-        s = t;
-    }
-    __device__ __forceinline__ double value() const { return s + c; }
-};
-
-__global__ void k_chunk_sums(int NK, int64_t n, int64_t nchunks, const double *__restrict__ terms,
-                             const int *__restrict__ sorted, const int64_t *__restrict__ bounds,
-                             double *__restrict__ partial, int *status)
+__global__ void k_validate(int64_t n, int nleg_max, int nrows, int nph1, const int *__restrict__ order,
+                           const int *__restrict__ nleg, const int *__restrict__ row, const int64_t *__restrict__ ipots,
+                           int *status)
 {
-    const int64_t c = blockIdx.x;
-    const int k = blockIdx.y * blockDim.x + threadIdx.x;
-    if (k >= NK) return;
-    int64_t lo = bounds[c], hi = bounds[c + 1];
-    if (lo < 0 || hi < lo || hi > n) {         // chunk offsets must cut 0..n in order
-        atomicOr(status, kBadLayout);
-        lo = hi = 0;
-    }
-    KSum s;
-    for (int64_t i = lo; i < hi; ++i) {
-        const int p = sorted[i];
-        if (p < 0 || p >= n) { atomicOr(status, kBadLayout); continue; }
-        s.add(terms[(int64_t)p * NK + k]);
-    }
-    partial[c * NK + k] = s.value();
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int bad = 0;
+    const int o = order[i];
+    if (o < 0 || o >= n) bad |= kBadLayout;
+    const int nl = nleg[i];
+    if (nl < 2 || nl > nleg_max) bad |= kBadLayout;
+    const int r = row[i];
+    if (r < 0 || r >= nrows) bad |= kBadLayout;
+    if (!(bad & kBadLayout))
+        for (int j = 0; j < nl; ++j) {
+            const int64_t v = ipots[i * nleg_max + j];
+            if (v < 0 || v >= nph1) bad |= kBadIpot;
+        }
+    if (bad) atomicOr(status, bad);
 }
 
-__global__ void k_row_sums(int NK, int nrows, int64_t nchunks, const double *__restrict__ partial,
-                           const int64_t *__restrict__ row_chunks, double *__restrict__ rows, int *status)
-{
-    const int r = blockIdx.x;
-    const int k = blockIdx.y * blockDim.x + threadIdx.x;
-    if (k >= NK || r >= nrows) return;
-    int64_t lo = row_chunks[r], hi = row_chunks[r + 1];
-    if (lo < 0 || hi < lo || hi > nchunks) {
-        atomicOr(status, kBadLayout);
-        lo = hi = 0;
-    }
-    KSum s;
-    for (int64_t c = lo; c < hi; ++c) s.add(partial[c * NK + k]);
-    // the earlier kernels of the call have finished (same stream): a set status word makes the whole call's rows NaN
-    rows[(int64_t)r * NK + k] = *(volatile int *)status ? __longlong_as_double(0x7ff8000000000000ll) : s.value();
-}
 // rows from the fixed-point sums: the low word's carry moved into the signed word in integers, then one value in FP64
 __global__ void k_row_finish(int64_t count, const unsigned long long *__restrict__ racc, double *__restrict__ rows,
                              const int *status)
@@ -67,28 +42,24 @@ __global__ void k_row_finish(int64_t count, const unsigned long long *__restrict
 }
 }  // namespace
 
+fg_status launch_validate(const fg_paths *P, int nph1, int *status, cudaStream_t st)
+{
+    if (P->n > 0) {
+        k_validate<<<(unsigned)((P->n + 255) / 256), 256, 0, st>>>(P->n, P->nleg_max, P->nrows, nph1, P->order,
+                                                                   P->nleg, P->row, P->ipots, status);
+        FG_CUDA(cudaGetLastError());
+    }
+    return FG_OK;
+}
+
+size_t row_sum_bytes(int nrows, int NK) { return align_up((size_t)2 * nrows * NK * sizeof(unsigned long long), 256); }
+
 fg_status launch_row_finish(const fg_paths *P, int NK, const unsigned long long *racc, double *rows,
                             const int *status, cudaStream_t st)
 {
     const int64_t count = (int64_t)P->nrows * NK;
     if (count > 0) {
         k_row_finish<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(count, racc, rows, status);
-        FG_CUDA(cudaGetLastError());
-    }
-    return FG_OK;
-}
-
-fg_status launch_reductions(const fg_paths *P, int NK, const double *terms, double *partial, double *rows, int *status,
-                            cudaStream_t st)
-{
-    if (P->nchunks > 0) {
-        dim3 g1((unsigned)P->nchunks, (NK + 127) / 128);
-        k_chunk_sums<<<g1, 128, 0, st>>>(NK, P->n, P->nchunks, terms, P->sorted, P->chunk_bounds, partial, status);
-        FG_CUDA(cudaGetLastError());
-    }
-    if (P->nrows > 0) {
-        dim3 g2((unsigned)P->nrows, (NK + 127) / 128);
-        k_row_sums<<<g2, 128, 0, st>>>(NK, P->nrows, P->nchunks, partial, P->row_chunks, rows, status);
         FG_CUDA(cudaGetLastError());
     }
     return FG_OK;
@@ -112,15 +83,7 @@ fg_status read_status(const int *status, cudaStream_t st)
     return FG_OK;
 }
 
-size_t fused_workspace(const fg_paths *P, int NK)
-{
-#if FG_EXACT_ROWS
-    return kCounterBytes + align_up((size_t)2 * P->nrows * NK * sizeof(unsigned long long), 256);
-#else
-    return kCounterBytes + align_up((size_t)P->n * NK * sizeof(double), 256) +
-           align_up((size_t)P->nchunks * NK * sizeof(double), 256);
-#endif
-}
+size_t fused_workspace(const fg_paths *P, int NK) { return kCounterBytes + row_sum_bytes(P->nrows, NK); }
 
 }  // namespace fg
 

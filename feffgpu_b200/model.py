@@ -47,7 +47,7 @@ class PathModel:
     """groups: (atoms (B, nleg) global indices with the absorber first, ipots (B, nleg), deg (B,) or None,
     row (B,) or None) per leg count; positions (N, 3) A."""
 
-    def __init__(self, stage, groups, positions, nrows=None, box=None, chunk=256):
+    def __init__(self, stage, groups, positions, nrows=None, box=None):
         self.stage, self.box = stage, box
         dev = stage.device
         self.min_image = MinImage(box, dev)
@@ -61,7 +61,7 @@ class PathModel:
             bgroups.append((rel, g[1], g[2] if len(g) > 2 else None, g[3] if len(g) > 3 else None))
             pad = torch.cat([a, a[:, :1].expand(B, nleg_max - n)], 1)
             atoms.append(pad)
-        self.batch = PathBatch(bgroups, nrows=nrows, device=dev, chunk=chunk)
+        self.batch = PathBatch(bgroups, nrows=nrows, device=dev)
         self.atoms = torch.cat(atoms).to(dev)
         legs = torch.arange(nleg_max, device=dev)
         self.mask = (legs[None, :] < self.batch.nleg[:, None].long()).to(torch.float64)[:, :, None]

@@ -7,9 +7,9 @@ every frame of an MD or RMC job in one set of launches.  The enumeration, the pa
 importance and the degeneracy keys are CUDA kernels (``csrc/fg_paths.cu``, C ABI ``fg_pf_*``); the merges and the
 importance cut are index bookkeeping done here with torch on the device (sorts, unique, gathers), the greedy
 length windows of the accidental-degeneracy merge on the host (``fg_pf_windows``).  A call for one absorber (how
-the reference's front ends call it) does the merges and the cut on the host after one copy of the fields they
-read, with the same arithmetic, and gathers the kept paths on the device: a few hundred paths are not worth the
-launch and synchronisation latency of the device version's many small steps.
+the reference's front ends call it) is one library call, ``fg_pf_enumerate_one``: the same kernels driven from C++,
+the merges and the cut on the host after one copy of the fields they read, with the same FP32 arithmetic and order
+(a few hundred paths are not worth the dispatch latency of many small host-driven steps).
 
 Algorithm (pathfinder.py:159-279): a path of nleg legs is a sequence of nleg - 1 intermediates (the absorber's
 candidates -- atoms within rmax, minimum image, in atom order -- then the absorber itself), first and last a
@@ -149,10 +149,47 @@ class GPUPathFinder:
     def enumerate(self, pos, box, absorber, ipot, chunk=256):
         """The reference's enumerate for one absorber: ({nleg: (coords (B, nleg, 3) relative to the absorber,
         ipots (B, nleg), deg (B,), xport (B,), atoms (B, nleg - 1))} after the importance cut, the reference
-        importance)."""
-        res = self.enumerate_many(pos, box, [int(absorber)], ipot)
-        kept = {n: v[:5] for n, v in res["paths"].items()}
-        return kept, float(res["ref"][0])
+        importance).  One library call drives the whole search (fg_pf_enumerate_one): the reference's front ends call
+        this once per absorber, and for a few hundred paths a sequence of small host-driven steps would be bound by
+        its launch and dispatch latency.  The paths are those enumerate_many gives, bit for bit."""
+        dev, lib, st = self.device, self._lib, self._stream()
+        posd = torch.as_tensor(np.asarray(pos) if not torch.is_tensor(pos) else pos, device=dev,
+                               dtype=torch.float32).contiguous()
+        if posd.dim() == 3:
+            if posd.shape[0] != 1:
+                raise ValueError("enumerate takes one frame of positions (n, 3)")
+            posd = posd[0]
+        n = int(posd.shape[0])
+        if not 0 <= int(absorber) < n:
+            raise IndexError(f"absorber {int(absorber)} outside the {n} atoms")
+        cell = as_cell(box)
+        cellw = torch.as_tensor(cell_words(cell, np.float32), device=dev) if isinstance(cell, np.ndarray) else None
+        boxf = cell if isinstance(cell, float) else -1.0
+        ipot_of = (ipot.to(dev, torch.int64) if torch.is_tensor(ipot)
+                   else torch.as_tensor(np.asarray(ipot), device=dev, dtype=torch.int64)).contiguous()
+        h = C.c_void_p()
+        counts = (C.c_int64 * (NLEG_MAX + 1))()
+        ref = C.c_float()
+        _lib.check(lib.fg_pf_enumerate_one(posd.data_ptr(), n, boxf, _ptr(cellw), int(absorber), ipot_of.data_ptr(),
+                                           C.byref(self._tables), self.rmax, self.nlegmax, self.critpw,
+                                           int(bool(self.merge_degenerate)), C.byref(h), counts, C.byref(ref), st))
+        try:
+            kept = {}
+            for nleg in range(2, NLEG_MAX + 1):
+                B = int(counts[nleg])
+                if B < 0:
+                    continue
+                f32 = torch.empty(B * (3 * nleg + 2), device=dev, dtype=torch.float32)
+                i64 = torch.empty(B * (2 * nleg - 1), device=dev, dtype=torch.int64)
+                coords = f32[:3 * nleg * B].view(B, nleg, 3)
+                deg, xport = f32[3 * nleg * B:(3 * nleg + 1) * B], f32[(3 * nleg + 1) * B:]
+                ipots, atoms = i64[:nleg * B].view(B, nleg), i64[nleg * B:].view(B, nleg - 1)
+                _lib.check(lib.fg_pf_result_gather(h, nleg, coords.data_ptr(), ipots.data_ptr(), deg.data_ptr(),
+                                                   xport.data_ptr(), atoms.data_ptr(), st))
+                kept[nleg] = (coords, ipots, deg, xport, atoms)
+        finally:
+            lib.fg_pf_result_destroy(h)
+        return kept, float(ref.value)
 
     def enumerate_many(self, pos, box, absorbers, ipot):
         """Every path of every absorber of every frame in one set of launches.  pos (n, 3) A, or (F, n, 3) for F
@@ -256,108 +293,7 @@ class GPUPathFinder:
                                                 _ptr(key), st))
         return {"coords": coords, "ipots": ipots, "atoms": atoms, "rtot": rtot, "xport": xport, "key": key}
 
-    def _merge_and_cut_one(self, out, off):
-        """_merge_and_cut for a single absorber slot, on the host after one copy of the fields the merges read: the
-        reference's front ends call the finder once per absorber, and for a few hundred paths the device version is
-        bound by the launch and synchronisation latency of its many small steps.  Every step is the device version's
-        in the same FP32 arithmetic and order (the kept paths are bit-identical, asserted against enumerate_many)."""
-        dev = self.device
-        legs = sorted(out)
-        nb = {n: int(out[n]["rtot"].shape[0]) for n in legs}
-        f32 = [torch.stack([out[n]["xport"], out[n]["deg"].to(torch.float32)], 1).reshape(-1) for n in legs]
-        f32.append(out[2]["coords"][:, 1].reshape(-1))
-        f32.append(torch.cat([out[n]["rtot"] for n in legs]))
-        i64 = [off.reshape(-1), out[2]["ipots"][:, 1].reshape(-1)]
-        keyed = [n for n in legs if n > 2 and out[n]["key"] is not None]
-        i64 += [out[n]["key"].reshape(-1) for n in keyed]
-        hf = torch.cat(f32).cpu().numpy()
-        hi = torch.cat(i64).cpu().numpy()
-        s = 0
-        xport, deg = {}, {}
-        for n in legs:
-            v = hf[s:s + 2 * nb[n]].reshape(-1, 2)
-            xport[n], deg[n] = v[:, 0], v[:, 1]
-            s += 2 * nb[n]
-        c1 = hf[s:s + 3 * nb[2]].reshape(-1, 3)
-        s += 3 * nb[2]
-        rtot_all = hf[s:]
-        cnt = int(hi[1] - hi[0])
-        ip1 = hi[2:2 + nb[2]]
-        s = 2 + nb[2]
-        key = {}
-        for n in keyed:
-            key[n] = hi[s:s + nb[n] * 2 * n].reshape(nb[n], 2 * n)
-            s += nb[n] * 2 * n
-        d = np.sqrt(c1[:, 0] * c1[:, 0] + c1[:, 1] * c1[:, 1] + c1[:, 2] * c1[:, 2])
-        ref = np.float32(1.0)
-        rep = np.arange(nb[2])
-        ss_deg = deg[2]
-        if not self.merge_degenerate or nb[2] == 0:
-            if nb[2] and cnt > 0:
-                ref = xport[2][int(np.argmin(d))]                  # the first of equal minima, as np.argmin gives
-        if self.merge_degenerate and nb[2]:
-            # greedy 1e-3 A windows over the sorted closed lengths of every path (the device version's _windows)
-            o = np.argsort(rtot_all, kind="stable")
-            sr = np.ascontiguousarray(rtot_all[o], dtype=np.float32)
-            seg = np.array([0, len(sr)], np.int64)
-            win_sorted = np.zeros(len(sr), np.int64)
-            _lib.check(self._lib.fg_pf_windows(sr.ctypes.data, seg.ctypes.data, 1, float(np.float32(1e-3)),
-                                               win_sorted.ctypes.data))
-            win = np.empty(len(sr), np.int64)
-            win[o] = win_sorted
-            o = np.argsort(d, kind="stable")
-            keys = np.stack([np.round(d[o] * np.float32(1000)).astype(np.int64), ip1[o], win[:nb[2]][o]], 1)
-            _, inv = np.unique(keys, axis=0, return_inverse=True)
-            inv = inv.reshape(-1)
-            G = int(inv.max()) + 1
-            firstp = np.full(G, len(o), np.int64)
-            np.minimum.at(firstp, inv, np.arange(len(o)))
-            gcount = np.bincount(inv, minlength=G).astype(np.float32)
-            go = np.argsort(firstp, kind="stable")
-            rep = o[firstp[go]]
-            ss_deg = gcount[go]
-            first = int(np.argmin(d[rep]))
-            ref = xport[2][rep[first]] * ss_deg[first]
-        refs = np.float32(ref)
-        paths, kept, ss_kept_deg = {}, {}, np.zeros(0, np.float32)
-        for n in legs:
-            if n == 2:
-                idx, dg = rep, ss_deg
-            else:
-                idx, dg = np.arange(nb[n]), deg[n]
-            dtot = dg
-            if n > 2 and self.merge_degenerate and nb[n] and cnt > 1:
-                _, inv = np.unique(key[n], axis=0, return_inverse=True)
-                inv = inv.reshape(-1)
-                tot = np.zeros(int(inv.max()) + 1, np.float32)
-                np.add.at(tot, inv, dg)
-                dtot = tot[inv]
-            frac = np.float32(100) * dtot * xport[n][idx] / refs
-            k = np.nonzero(frac >= np.float32(self.critpw))[0]
-            kept[n] = idx[k]
-            if n == 2:
-                ss_kept_deg = dg[k]
-        # every leg's kept indices and the merged single-scattering degeneracies in one copy to the device
-        sizes = [len(kept[n]) for n in legs]
-        packed = np.concatenate([kept[n].astype(np.int64) for n in legs] +
-                                [ss_kept_deg.astype(np.float32).view(np.int32).astype(np.int64)])
-        dpk = torch.as_tensor(packed, device=dev)
-        s = 0
-        for n, m in zip(legs, sizes):
-            ki = dpk[s:s + m]
-            s += m
-            v = out[n]
-            if n == 2:
-                dsel = dpk[-m:].to(torch.int32).view(torch.float32) if m else v["deg"][:0]
-            else:
-                dsel = v["deg"].index_select(0, ki)
-            paths[n] = (v["coords"].index_select(0, ki), v["ipots"].index_select(0, ki), dsel,
-                        v["xport"].index_select(0, ki), v["atoms"].index_select(0, ki), v["slot"].index_select(0, ki))
-        return {"paths": paths, "ref": torch.full((1,), float(refs), device=dev, dtype=torch.float32)}
-
     def _merge_and_cut(self, out, A, off, cand_rel):
-        if A == 1:
-            return self._merge_and_cut_one(out, off)
         dev = self.device
         ss = out[2]
         c1 = ss["coords"][:, 1]

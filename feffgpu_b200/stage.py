@@ -12,7 +12,8 @@ MD-EXAFS and RMC-EXAFS front ends and their forward model (``src/feffgpu/exafs/f
 
 New beside them: ``chi_reduce(batch, q, ...)``, the fused stage: every path of a ``PathBatch`` (mixed leg counts,
 one persistent launch), the fine-grid signal, an optional per-path exp(-2 sigma^2 q^2) and the degeneracy-weighted
-deterministic FP64 sum into rows, differentiable in the coordinates and in sigma^2.
+sum into FP64 rows (exact integer sums of the terms rounded to 2^-64: deterministic), differentiable in the
+coordinates and in sigma^2.
 
 All computation runs in the CUDA library (``_build/libfeffgpu_b200.so``); there is no CPU path.
 """
@@ -313,7 +314,7 @@ class GPUPathStage:
     # -- fused stage ----------------------------------------------------------------------------------------
     def chi_reduce(self, batch: "PathBatch", q, S=None, coords=None, sigma2=None, dtype=None):
         """rows (nrows, len(q)) FP64: sum over the batch's paths of deg exp(-2 sigma2 q^2) chi_path(q) into each
-        path's row, in a fixed order.  ``coords`` (n, nleg_max, 3) A replaces the batch's coordinates (same
+        path's row, exact in the terms (the result does not depend on the evaluation order).  ``coords`` (n, nleg_max, 3) A replaces the batch's coordinates (same
         paths, new positions); ``sigma2`` (n,) A^2 per path.  Differentiable in coords and sigma2.  ``dtype``
         complex64 / complex128 overrides the stage's precision for this call."""
         if S is None:
@@ -335,8 +336,7 @@ class GPUPathStage:
     def _paths_struct(self, batch, coords, sigma2):
         return _lib.Paths(batch.n, batch.nleg_max, batch.nrows, coords.data_ptr(), batch.ipots.data_ptr(),
                           batch.nleg.data_ptr(), batch.deg.data_ptr(), _ptr(sigma2), batch.row.data_ptr(),
-                          batch.order.data_ptr(), batch.sorted.data_ptr(), batch.chunk_bounds.data_ptr(),
-                          batch.row_chunks.data_ptr(), batch.nchunks)
+                          batch.order.data_ptr())
 
     def _chi_reduce_forward(self, batch, coords, sigma2, q, S, prec, save: bool):
         coords = coords.contiguous()

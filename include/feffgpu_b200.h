@@ -121,28 +121,26 @@ typedef struct fg_paths {
     int32_t nrows;           /* output rows */
     const double *coords;    /* (n, nleg_max, 3) angstrom, absorber first; legs past nleg[p] are ignored */
     const int64_t *ipots;    /* (n, nleg_max) */
-    const int32_t *nleg;     /* (n) legs of each path, 2..9 */
+    const int32_t *nleg;     /* (n) legs of each path, 2..nleg_max */
     const double *deg;       /* (n) degeneracy weight */
     const double *sigma2;    /* (n) per-path sigma^2 in A^2, or NULL (no damping) */
     const int32_t *row;      /* (n) output row of each path, 0..nrows-1 */
     const int32_t *order;    /* (n) launch order: a permutation of 0..n-1, costliest paths first */
-    const int32_t *sorted;   /* (n) path indices grouped by row: the fixed summation order (a permutation) */
-    const int64_t *chunk_bounds; /* (nchunks+1) offsets into `sorted` from 0 to n; each chunk lies within one row */
-    const int64_t *row_chunks;   /* (nrows+1) offsets into the chunks: row r owns chunks row_chunks[r]..[r+1]-1 */
-    int64_t nchunks;         /* >= 1 when n > 0 */
 } fg_paths;
-/* The fused calls check the contents of these arrays on the device: a path index, leg count (2..nleg_max),
- * potential index (0..nph), row, summation index or chunk offset outside its range is never used to address memory;
- * the call's rows become NaN and, outside stream capture, the call waits for its stream and returns FG_ERR_VALUE
- * naming the fault.  Under stream capture it returns without waiting (a graph replay with such an input gives NaN
- * rows).  Host pointers and sizes are checked before any launch. */
+/* The fused calls check the contents of these arrays on the device before their kernels read them: a launch-order
+ * entry, leg count, row or potential index outside its range is never used to address memory; the call's rows become
+ * NaN and, outside stream capture, the call waits for its stream and returns FG_ERR_VALUE naming the fault.  Under
+ * stream capture it returns without waiting (a graph replay with such an input gives NaN rows).  Host pointers and
+ * sizes are checked before any launch. */
 
-/* Workspace of the fused calls: a work-queue counter and status word, per-path fine-grid terms and per-chunk partial
- * sums. */
+/* Workspace of the fused calls: a work-queue counter and status word, and the rows' exact sums (2 x nrows x NK 64-bit
+ * words; no per-path storage). */
 FG_API size_t fg_chi_reduce_workspace(const fg_stage *stage, const fg_paths *paths, int32_t NK);
 
 /* rows (nrows, NK) FP64 = sum over paths p of deg_p exp(-2 sigma2_p q^2) chi_p(q), chi_p from cchi and chi_fine
- * as above, summed in a fixed order (deterministic).  Fuses GPUPathStage.cchi + chi_fine with the reduction
+ * as above; every term is rounded to 2^-64 and summed exactly in 64-bit integers, so the rows do not depend on the
+ * order in which paths are evaluated (deterministic, bit for bit); a term that is not finite or reaches 2^31 in
+ * magnitude is an error.  Fuses GPUPathStage.cchi + chi_fine with the reduction
  * of the callers (chain.py:48-49, exafs/forward.py:162, md/spectrum.py:298).  q (NK), S (NK, E) and span as in
  * fg_chi_fine but always FP64.  If cchi_save (n, E complex of the precision) and reff_save (n, FP64) are non-NULL
  * the per-path signals are kept for fg_chi_reduce_backward.  Outside stream capture the call ends by waiting for
@@ -156,7 +154,8 @@ FG_API fg_status fg_chi_reduce(const fg_stage *stage, fg_precision prec, const f
  * control (a simulation code that reserves the whole device for its own pool at start-up) and so cannot provide
  * the workspace fg_chi_reduce asks for.  Instead of a caller workspace it uses an array compiled into the library,
  * FG_NOALLOC_SCRATCH_BYTES (32 MiB) on every GPU that loads the library, held until the process exits; a batch
- * whose fg_chi_reduce_workspace exceeds that is rejected with FG_ERR_VALUE (split it by rows).  It allocates
+ * whose fg_chi_reduce_workspace exceeds that (more than about 5,200 rows at 401 k points, whatever the number of
+ * paths) is rejected with FG_ERR_VALUE (split it by rows).  It allocates
  * nothing: no cudaMalloc, no cudaFree, no allocating library call.  The first call with a given stage looks up the
  * array's device address with the stage's device current and keeps it in the stage; make that first call before any
  * stream capture.  A cudaDeviceReset invalidates every stage (its tables and this address): create new stages after
@@ -250,6 +249,24 @@ FG_API fg_status fg_pf_describe(int64_t B, int32_t nleg, const int32_t *seq, con
  * of FEFF's accidental-degeneracy merge, pathfinder.py:110-119); window ids restart at 0 per segment. */
 FG_API fg_status fg_pf_windows(const float *sorted_len, const int64_t *seg_off, int64_t nseg, float eps,
                                int64_t *window);
+
+/* The whole finder for one absorber in one call -- the reference's GPUPathFinder.enumerate (pathfinder.py:213-279),
+ * which its front ends call once per absorber (exafs/forward.py:122-123, md/spectrum.py:275-277): candidates,
+ * growth, description, the merges and the importance cut, with one synchronisation per growth level plus two.  pos
+ * (n, 3) FP32 one frame on the device, box / cell as in fg_pf_candidates, ipot_of (n) on the device, T the
+ * importance tables.  counts (10): kept paths per leg count (index nleg; -1 for a leg count the growth did not
+ * reach), *ref the reference importance.  The paths stay in *result until fg_pf_result_gather copies those of one leg
+ * count into caller arrays -- coords (B, nleg, 3) FP32, ipots (B, nleg), deg (B) FP32, xport (B) FP32, atoms
+ * (B, nleg - 1) -- and fg_pf_result_destroy frees them (stream ordered).  The kept paths are those of the batched
+ * entry points above, bit for bit.  Scratch comes from the library's own stream-ordered pool on the device. */
+typedef struct fg_pf_result fg_pf_result;
+FG_API fg_status fg_pf_enumerate_one(const float *pos, int64_t n, float box, const float *cell, int64_t absorber,
+                                     const int64_t *ipot_of, const fg_pf_tables *T, float rmax, int32_t nlegmax,
+                                     float critpw, int32_t merge_degenerate, fg_pf_result **result, int64_t *counts,
+                                     float *ref, void *stream);
+FG_API fg_status fg_pf_result_gather(fg_pf_result *result, int32_t nleg, float *coords, int64_t *ipots, float *deg,
+                                     float *xport, int64_t *atoms, void *stream);
+FG_API void fg_pf_result_destroy(fg_pf_result *result);
 
 /* ---------------------------------------------------------------------------------------------- pair tables
  * Single scattering of whole configurations from tabulated two-leg signals (the reference's PairTables,

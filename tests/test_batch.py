@@ -1,4 +1,4 @@
-"""PathBatch's launch order and fixed summation order (host-side layout, no GPU)."""
+"""PathBatch's layout and launch order (host side, no GPU)."""
 import numpy as np
 import torch
 
@@ -18,22 +18,15 @@ def _groups(rng):
 def test_layout_and_orders():
     rng = np.random.default_rng(0)
     gs = _groups(rng)
-    b = PathBatch(gs, nrows=4, device="cpu", chunk=64)
+    b = PathBatch(gs, nrows=4, device="cpu")
     assert b.n == 347 and b.nleg_max == 5 and b.nrows == 4
     nleg = b.nleg.numpy()
     order = b.order.numpy()
     assert sorted(order.tolist()) == list(range(b.n))
     assert np.all(np.diff(nleg[order]) <= 0)             # costliest (most legs) first
     row = b.row.numpy()
-    srt = b.sorted.numpy()
-    assert np.all(np.diff(row[srt]) >= 0)               # grouped by row
-    bounds, rc = b.chunk_bounds.numpy(), b.row_chunks.numpy()
-    assert bounds[0] == 0 and bounds[-1] == b.n and np.all(np.diff(bounds) <= 64) and np.all(np.diff(bounds) > 0)
-    assert rc[0] == 0 and rc[-1] == b.nchunks and len(rc) == b.nrows + 1
-    for r in range(b.nrows):                            # every chunk of a row holds only that row's paths
-        for c in range(rc[r], rc[r + 1]):
-            assert np.all(row[srt[bounds[c]:bounds[c + 1]]] == r)
-    assert rc[4] - rc[3] == 0                           # an empty row owns no chunk
+    assert np.array_equal(row, np.concatenate([g[3] for g in gs]))
+    assert b.max_ipot == 1 and b.counts == {2: 7, 3: 40, 5: 300}
     # padding: legs past nleg are zero
     c = b.coords.numpy()
     assert np.all(c[nleg == 2][:, 2:] == 0)

