@@ -233,95 +233,6 @@ __device__ __forceinline__ void accumulate_f_adj(C2<R> (&acc)[RepTab<KIND, NR, N
     g_beta = gb;
 }
 
-// The contraction part of accumulate_f_adj alone (F~_k itself is known from the first sweep): per partial wave the
-// weighted sums along rho_in, rho_out and beta_k, with the spherical-wave values and tangents streamed.  Every
-// complex operation of the loop runs as FP32-pair instructions (forward + backward of 2e5 paths 321 -> 299 ms).
-template <typename R, int KIND, int NR, int NC>
-__device__ __forceinline__ void contract_f_adj_tangent(const C2<R> (&Wh)[RepTab<KIND, NR, NC>().n], const R *dhk,
-                                               const R *dhdk, const C2<R> *tlk, int E, int ilx, C2<R> z_in,
-                                               C2<R> z_out, C2<R> &g_in, C2<R> &g_out, C2<R> &g_beta)
-{
-    constexpr RepTab<KIND, NR, NC> RT{};
-    constexpr LamTab L = lamtab(KIND);
-    constexpr int DS = dstride(L.MM);
-    constexpr int NCAN = ncanon(L.MM);
-    constexpr int CI = L.CI, CO = L.CO;
-    const C2<R> dz_in = cmul(C2<R>{R(0), R(-1)}, cmul(z_in, z_in));
-    const C2<R> dz_out = cmul(C2<R>{R(0), R(-1)}, cmul(z_out, z_out));
-    C2<R> pi[CI + 1], ci[CI + 1], po[CO + 1], co[CO + 1];
-    C2<R> dpi[CI + 1], dci[CI + 1], dpo[CO + 1], dco[CO + 1];
-#pragma unroll
-    for (int j = 0; j <= CI; ++j) pi[j] = ci[j] = dpi[j] = dci[j] = cz<R>();
-#pragma unroll
-    for (int j = 0; j <= CO; ++j) po[j] = co[j] = dpo[j] = dco[j] = cz<R>();
-    pi[1] = ci[1] = po[1] = co[1] = C2<R>{R(1), R(0)};
-    C2<R> gi = cz<R>(), go = cz<R>(), gb = cz<R>();
-    C2<R> t1 = tlk[E], t2 = ilx >= 2 ? tlk[(size_t)2 * E] : cz<R>();
-    for (int il = 1; il <= ilx; ++il) {
-        const C2<R> t = t1;
-        t1 = t2;
-        if (il + 2 <= ilx) t2 = tlk[(size_t)(il + 2) * E];
-        R d[NCAN], dd[NCAN];
-        load_row<R, NCAN>(dhk + (size_t)il * DS, d);
-        load_row<R, NCAN>(dhdk + (size_t)il * DS, dd);
-        C2<R> tco[CO + 1], tdco[CO + 1];
-#pragma unroll
-        for (int j = 1; j <= CO; ++j) { tco[j] = pmul(t, co[j]); tdco[j] = pmul(t, dco[j]); }
-        C2<R> X[CI + 1][CO + 1], Y[CI + 1][CO + 1];
-#pragma unroll
-        for (int a = 0; a <= CI; ++a)
-#pragma unroll
-            for (int b = 0; b <= CO; ++b) X[a][b] = Y[a][b] = cz<R>();
-#pragma unroll
-        for (int r = 0; r < RT.n; ++r) {
-            X[RT.ci[r]][RT.co[r]] = pfmr(Wh[r], d[RT.d[r]], X[RT.ci[r]][RT.co[r]]);
-            Y[RT.ci[r]][RT.co[r]] = pfmr(Wh[r], dd[RT.d[r]], Y[RT.ci[r]][RT.co[r]]);
-        }
-#pragma unroll
-        for (int a = 1; a <= CI; ++a) {
-            C2<R> v = cz<R>(), y = cz<R>();
-#pragma unroll
-            for (int b = 1; b <= CO; ++b) {
-                v = pfma(X[a][b], tco[b], v);
-                y = pfma(Y[a][b], tco[b], y);
-            }
-            gi = pfma(dci[a], v, gi);
-            gb = pfma(ci[a], y, gb);
-        }
-#pragma unroll
-        for (int b = 1; b <= CO; ++b) {
-            C2<R> v = cz<R>();
-#pragma unroll
-            for (int a = 1; a <= CI; ++a) v = pfma(X[a][b], ci[a], v);
-            go = pfma(tdco[b], v, go);
-        }
-        const R w = R(2 * il - 1);
-        const C2<R> wi = cscl(z_in, w), wo = cscl(z_out, w), wdi = cscl(dz_in, w), wdo = cscl(dz_out, w);
-        C2<R> ni[CI + 1], no[CO + 1], dni[CI + 1], dno[CO + 1];
-#pragma unroll
-        for (int j = 1; j <= CI; ++j) {
-            const C2<R> sv = j > 1 ? padd(ci[j], ci[j - 1]) : ci[j];
-            const C2<R> dsv = j > 1 ? padd(dci[j], dci[j - 1]) : dci[j];
-            ni[j] = pfms(wi, sv, pi[j]);
-            dni[j] = pfms(wdi, sv, pfms(wi, dsv, dpi[j]));
-        }
-#pragma unroll
-        for (int j = 1; j <= CO; ++j) {
-            const C2<R> sv = j > 1 ? padd(co[j], co[j - 1]) : co[j];
-            const C2<R> dsv = j > 1 ? padd(dco[j], dco[j - 1]) : dco[j];
-            no[j] = pfms(wo, sv, po[j]);
-            dno[j] = pfms(wdo, sv, pfms(wo, dsv, dpo[j]));
-        }
-#pragma unroll
-        for (int j = 1; j <= CI; ++j) { pi[j] = ci[j]; ci[j] = ni[j]; dpi[j] = dci[j]; dci[j] = dni[j]; }
-#pragma unroll
-        for (int j = 1; j <= CO; ++j) { po[j] = co[j]; co[j] = no[j]; dpo[j] = dco[j]; dco[j] = dno[j]; }
-    }
-    g_in = gi;
-    g_out = go;
-    g_beta = gb;
-}
-
 // -i z v: the factor of the rho-derivative of the spherical-wave factors
 template <typename R> __device__ __forceinline__ C2<R> mi_z(C2<R> z, C2<R> v)
 {
@@ -329,11 +240,15 @@ template <typename R> __device__ __forceinline__ C2<R> mi_z(C2<R> z, C2<R> v)
     return C2<R>{zv.y, -zv.x};
 }
 
-// contract_f_adj with the rho-derivatives of the spherical-wave factors from the factors themselves: column j (m = j - 1)
-// of c(z), z = -i / rho, obeys dc_j/drho = -i z ((j - 1) c_j + j c_(j+1)) (verified against finite differences of the
-// recursion), so one more column of the value recursion replaces the tangent recursions and their state.
+// The contraction part of accumulate_f_adj alone (F~_k itself is known from the first sweep): per partial wave the
+// weighted sums along rho_in, rho_out and beta_k.  The rho-derivatives of the spherical-wave factors come from the
+// factors themselves: column j (m = j - 1) of c(z), z = -i / rho, obeys dc_j/drho = -i z ((j - 1) c_j + j c_(j+1))
+// (checked against finite differences of the recursion), so one more column of the value recursion replaces the
+// tangent recursions and their state (forward + backward of the benchmark batch 262 -> 257 ms on B200).  Every complex
+// operation of the loop runs as FP32-pair instructions.  (The single-scattering adjoints below keep the tangent
+// recursions: two-leg paths are a small share of any batch.)
 template <typename R, int KIND, int NR, int NC>
-__device__ __forceinline__ void contract_f_adj_identity(const C2<R> (&Wh)[RepTab<KIND, NR, NC>().n], const R *dhk,
+__device__ __forceinline__ void contract_f_adj(const C2<R> (&Wh)[RepTab<KIND, NR, NC>().n], const R *dhk,
                                                         const R *dhdk, const C2<R> *tlk, int E, int ilx, C2<R> z_in,
                                                         C2<R> z_out, C2<R> &g_in, C2<R> &g_out, C2<R> &g_beta)
 {
@@ -406,21 +321,6 @@ __device__ __forceinline__ void contract_f_adj_identity(const C2<R> (&Wh)[RepTab
     g_in = gi;
     g_out = go;
     g_beta = gb;
-}
-
-#ifndef FG_ADJ_DERIV
-#define FG_ADJ_DERIV 0
-#endif
-template <typename R, int KIND, int NR, int NC>
-__device__ __forceinline__ void contract_f_adj(const C2<R> (&Wh)[RepTab<KIND, NR, NC>().n], const R *dhk,
-                                               const R *dhdk, const C2<R> *tlk, int E, int ilx, C2<R> z_in,
-                                               C2<R> z_out, C2<R> &g_in, C2<R> &g_out, C2<R> &g_beta)
-{
-#if FG_ADJ_DERIV
-    contract_f_adj_identity<R, KIND, NR, NC>(Wh, dhk, dhdk, tlk, E, ilx, z_in, z_out, g_in, g_out, g_beta);
-#else
-    contract_f_adj_tangent<R, KIND, NR, NC>(Wh, dhk, dhdk, tlk, E, ilx, z_in, z_out, g_in, g_out, g_beta);
-#endif
 }
 
 // Weights of the contraction: Wh[r] = sum over the orbit of r of sign * ph(m_a) * M(b, a), and the same with an
@@ -625,41 +525,35 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
     for (int k = nsc; k >= 1; --k) {
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
-        // Wh[r] = sum over the flip orbit of r of sign * e^{-i eta m_a} M(b, a), We the same times -i m_a;
-        // M(b, a) = sum_c P_(k-1)(b, c) R_k(c, a), one c at a time
+        // Wh[r] = sum over the flip orbit of r of sign * e^{-i eta m_a} M(b, a), M(b, a) = sum_c P_(k-1)(b, c)
+        // R_k(c, a), one c at a time.  The Euler-angle derivative needs no weights of its own: with F_k = Phi F~_k,
+        // d ptrac / d eta_(k+1) = Tr(R_k (-i m) F_k P_(k-1)) = -i sum_a m_a (P_k R_k)(a, a), and P_k is stored.
         C2<R> Wh[RT.n];
         {
-            C2<R> We[RT.n];
 #pragma unroll
-            for (int r = 0; r < RT.n; ++r) Wh[r] = We[r] = cz<R>();
+            for (int r = 0; r < RT.n; ++r) Wh[r] = cz<R>();
 #pragma unroll 1
             for (int c = 0; c < N0; ++c) {
-                C2<R> pc[N], rr[N], re[N];
+                C2<R> pc[N], rr[N];
 #pragma unroll
                 for (int b = 0; b < N; ++b) pc[b] = Pst[k - 1][b][c];
 #pragma unroll
-                for (int a = 0; a < N; ++a) {
-                    rr[a] = cmul(ph[L.m[a] + MM], Rst[c][a]);
-                    re[a] = C2<R>{rr[a].y * R(L.m[a]), -rr[a].x * R(L.m[a])};     // -i m_a rr
-                }
+                for (int a = 0; a < N; ++a) rr[a] = cmul(ph[L.m[a] + MM], Rst[c][a]);
 #pragma unroll
                 for (int a = 0; a < N; ++a)
 #pragma unroll
                     for (int b = 0; b < N; ++b) {
                         const int r = RT.rep[a][b];
-                        if (RT.sg[a][b] > 0) {
-                            Wh[r] = pfma(pc[b], rr[a], Wh[r]);
-                            if (L.m[a] != 0) We[r] = pfma(pc[b], re[a], We[r]);
-                        } else {
-                            Wh[r] = pfms(pc[b], rr[a], Wh[r]);
-                            if (L.m[a] != 0) We[r] = pfms(pc[b], re[a], We[r]);
-                        }
+                        Wh[r] = RT.sg[a][b] > 0 ? pfma(pc[b], rr[a], Wh[r]) : pfms(pc[b], rr[a], Wh[r]);
                     }
             }
-            C2<R> ge = cz<R>();
+            C2<R> tm = cz<R>();                     // sum_a m_a (P_k R_k)(a, a)
+#pragma unroll 1
+            for (int c = 0; c < N0; ++c)
 #pragma unroll
-            for (int r = 0; r < RT.n; ++r) ge = cfma(Fst[k - 1][r], We[r], ge);
-            add_re(pg.eta[k + 1], sd, ge);
+                for (int a = 0; a < N; ++a)
+                    if (L.m[a] != 0) tm = pfma(cscl(Pst[k][a][c], R(L.m[a])), Rst[c][a], tm);
+            add_re(pg.eta[k + 1], sd, C2<R>{tm.y, -tm.x});   // -i tm
         }
         if (k > 1) {
             // R_(k-1) = R_k F_k with F_k(c, b) = e^{-i eta m_c} sign F~_k[rep(c, b)], one row of R at a time
