@@ -3,8 +3,9 @@
 // then sum |chi_R - target_R|^2 / sum |target_R|^2).
 //
 // The transform restricted to the kept R points is a dense complex matrix F (NR, NK) built once by the host; one block
-// per row evaluates chi_R = F x, the misfit and, in the same pass, its gradient dR/dx_k = 2/norm Re sum_m conj(d_m)
-// F[m][k] -- so a refinement step needs no further launch for the loss's backward.  FP64, fixed-order sums.
+// per row evaluates chi_R = F x (a warp per R point, coalesced over k), the misfit and, in the same pass, its
+// gradient dR/dx_k = 2/norm Re sum_m conj(d_m) F[m][k] (a thread per k, coalesced over k) -- so a refinement step
+// needs no further launch for the loss's backward.  FP64, fixed-order sums.
 #include <cuda_runtime.h>
 
 #include "fg_launch.h"
@@ -25,19 +26,28 @@ __global__ void k_rspace(int NK, int NR, const double *__restrict__ rows, const 
     const int64_t b = blockIdx.x;
     for (int k = threadIdx.x; k < NK; k += blockDim.x) x[k] = rows[b * NK + k];
     __syncthreads();
+    // chi_R - target: one warp per R point, lanes over k (coalesced rows of F), a fixed-order shuffle reduction
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     double s = 0.0;
-    for (int m = threadIdx.x; m < NR; m += blockDim.x) {
+    for (int m = warp; m < NR; m += nwarps) {
         const double2 *f = F + (int64_t)m * NK;
         double re = 0.0, im = 0.0;
-        for (int k = 0; k < NK; ++k) {
+        for (int k = lane; k < NK; k += 32) {
             const double2 v = f[k];
             re = fma(v.x, x[k], re);
             im = fma(v.y, x[k], im);
         }
-        const double2 t = target[m];
-        const double2 dm = make_double2(re - t.x, im - t.y);
-        d[m] = dm;
-        s = fma(dm.x, dm.x, fma(dm.y, dm.y, s));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, o);
+            im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+        if (lane == 0) {
+            const double2 t = target[m];
+            const double2 dm = make_double2(re - t.x, im - t.y);
+            d[m] = dm;
+            s = fma(dm.x, dm.x, fma(dm.y, dm.y, s));
+        }
     }
     red[threadIdx.x] = s;
     __syncthreads();

@@ -113,8 +113,10 @@ class GPUPathStage:
 
     # -- per-path signal ------------------------------------------------------------------------------------
     def _check_ipots(self, ipots: torch.Tensor) -> None:
-        if ipots.numel() and (int(ipots.min()) < 0 or int(ipots.max()) > self.P.nph):
-            raise IndexError(f"potential index out of range 0..{self.P.nph}")
+        if ipots.numel():
+            lo, hi = (int(v) for v in torch.stack(torch.aminmax(ipots)).cpu())    # one synchronisation
+            if lo < 0 or hi > self.P.nph:
+                raise IndexError(f"potential index out of range 0..{self.P.nph}")
 
     def cchi(self, coords, ipots):
         """coords (B, nleg, 3) A, absorber first; ipots (B, nleg) long with the absorber 0.  Returns cchi (B, E) of

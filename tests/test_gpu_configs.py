@@ -5,10 +5,10 @@
 3. Adjoint on an 800-atom Fe/O/Pt packing: the path finder's paths, the gradient of the reference's R-space misfit
    with respect to every position against the reference's own autograd, per-path sigma^2 against central
    differences, FP32-vs-FP64 gradient error stated.
-4. MD batch: frames of a thermally displaced bcc Fe supercell x absorbers in one launch, chi averaged per frame,
-   against the oracle's FP64 sums.
-5. Two-edge refinement (Ni K + O K of a rock-salt NiO model with vacancies): the step captured as a CUDA graph equals
-   the eager step and the misfit falls.
+4. MD batch: frames of the thermally displaced bcc Fe 16^3 supercell x 32 absorbers, the finder's paths in one
+   launch, chi averaged per frame, against the oracle's FP64 sums.
+5. Two-edge refinement (Ni K + O K of the 8^3 rock-salt NiO model with vacancies, finder paths): the step captured
+   as a CUDA graph equals the eager step and the misfit falls.
 """
 import numpy as np
 import pytest
@@ -109,73 +109,71 @@ def test_cfg3_adjoint_800_atoms():
 
 
 def test_cfg4_md_frames_times_absorbers():
-    from feffgpu_b200 import GPUPathStage
-    from feffgpu_b200.model import PathModel
+    """Configuration 4 at its per-frame size: frames of the thermally displaced bcc Fe 16^3 supercell (8192 atoms,
+    sigma 0.08 A) x 32 absorbers each, every path of up to 3 legs within 5.5 A from the CUDA path finder (all frames
+    and absorbers in one call, as the benchmark's MD leg), all paths in one fused launch with chi averaged per frame;
+    each frame's row against the oracle's FP64 sum of the same paths (R <= 1e-6 mixed, 1e-12 FP64).  Four frames
+    (about 33,000 paths) keep the oracle's share of the test to seconds."""
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    from feffgpu_b200.pathfinder import GPUPathFinder
     P = phase("cfg4_fe_phase")
-    st = GPUPathStage(P, device="cuda", dtype=torch.complex64)
-    base, box = W.bcc_supercell(6, 2.87)
-    frames, A = 3, 4
+    frames, A = 4, 32
+    base, box = W.bcc_supercell(16, 2.87)
     rng = np.random.default_rng(12)
-    gs, allpos = [], []
-    N = len(base)
-    for f in range(frames):
-        pos = W.thermal(base, 0.08, seed=100 + f)
-        allpos.append(pos)
-        for a in rng.choice(N, size=A, replace=False):
-            paths = W.random_paths(pos, box, int(a), {2: 14, 3: 60}, rmax=5.5, leg_max=5.5, seed=int(a) + 7 * f)
-            for nleg, (c, ip, atoms) in paths.items():
-                full = np.concatenate([np.full((len(atoms), 1), a), atoms], 1) + f * N
-                gs.append((full, ip, np.full(len(atoms), 1.0 / A), np.full(len(atoms), f)))
-    allpos = np.concatenate(allpos)
-    model = PathModel(st, gs, allpos, nrows=frames, box=box)      # every path stays within its own frame
-    q = torch.tensor(K401, device="cuda")
-    S = st.linear_matrix(K401).double()
-    with torch.no_grad():
-        rows = model.rows(torch.tensor(allpos, device="cuda"), q, S).cpu().numpy()
+    pos = np.stack([W.thermal(base, 0.08, seed=100 + f) for f in range(frames)]).astype(np.float32)
+    abs_ = np.stack([rng.choice(len(base), size=A, replace=False) for _ in range(frames)])
+    res = GPUPathFinder(P, device="cuda", rmax=5.5, nlegmax=3, critpw=0.0).enumerate_many(
+        pos, box, abs_, np.ones(len(base), int))
+    groups = []
+    for nleg, (coords, ipots, deg, _xp, _atoms, slot) in sorted(res["paths"].items()):
+        groups.append((coords.double().cpu().numpy(), ipots.cpu().numpy(), deg.double().cpu().numpy() / A,
+                       torch.div(slot, A, rounding_mode="floor").cpu().numpy()))
+    assert sum(len(g[0]) for g in groups) > 25000
     orc = O.Oracle(P)
     So = orc.linear_matrix(K401)
-    coords = model.coords(torch.tensor(allpos, device="cuda")).cpu().numpy()
-    nl, deg, row = model.batch.nleg.cpu().numpy(), model.batch.deg.cpu().numpy(), model.batch.row.cpu().numpy()
-    ip = model.batch.ipots.cpu().numpy()
-    chi = np.zeros((len(nl), len(K401)))
-    for n in np.unique(nl):
-        sel = np.nonzero(nl == n)[0]
-        cc, rf = orc.cchi(coords[sel, :n], ip[sel, :n])
-        chi[sel] = O.chi_fine(cc, rf, K401, So)
-    ref = O.chi_rows(chi, deg, row, frames, K401)
-    for f in range(frames):
-        R = _R(K401, ref[f], rows[f])
-        print(f"cfg4 frame {f}: R {R:.2e}")
-        assert R <= 1e-6
+    ref = np.zeros((frames, len(K401)))
+    for coords, ipots, deg, row in groups:
+        cc, rf = orc.cchi(coords, ipots)
+        np.add.at(ref, row, deg[:, None] * O.chi_fine(cc, rf, K401, So))
+    batch = PathBatch(groups, nrows=frames, device="cuda")
+    for dtype, tol in ((torch.complex64, 1e-6), (torch.complex128, 1e-12)):
+        rows = GPUPathStage(P, device="cuda", dtype=dtype).chi_reduce(batch, K401).cpu().numpy()
+        for f in range(frames):
+            R = _R(K401, ref[f], rows[f])
+            print(f"cfg4 {dtype} frame {f}: R {R:.2e}")
+            assert R <= tol
 
 
 def test_cfg5_two_edge_refinement_graph():
+    """Configuration 5 at its stated size: rock-salt NiO 8^3 cells (4096 sites, 5 % vacancies, 0.1 A disorder), Ni K
+    and O K edges, 32 absorbers each with the CUDA finder's paths (rmax 5 A, 4 legs, importance cut 2 %, unmerged
+    single scattering: the reference GpuRmc's defaults); the refinement step captured as one CUDA graph equals the
+    same steps run eagerly (losses and positions to 1e-9) and the misfit falls over 15 steps."""
     from feffgpu_b200 import GPUPathStage
-    from feffgpu_b200.model import GraphedRefinement, PathModel
+    from feffgpu_b200.model import GraphedRefinement, PathModel, finder_groups
+    from feffgpu_b200.pathfinder import GPUPathFinder
     from feffgpu_b200.rspace import FitWindow, RSpaceMisfit
-    pos0, lab, box = W.rock_salt_supercell(3, 4.177)
+    pos0, lab, box = W.rock_salt_supercell(8, 4.177)
     rng = np.random.default_rng(5)
     keep = rng.random(len(pos0)) >= 0.05
     pos0, lab = pos0[keep], lab[keep]
     pos = W.thermal(pos0, 0.1, seed=6)
     hidden = W.thermal(pos, 0.03, seed=7)
     q = torch.tensor(K401, device="cuda")
-    models = []
-    for edge, fname, ipmap in (("Ni", "cfg5_nik_phase", {"Ni": 1, "O": 2}), ("O", "cfg5_ok_phase", {"Ni": 1, "O": 2})):
-        st = GPUPathStage(phase(fname), device="cuda", dtype=torch.complex64)
-        ipot_of = np.array([ipmap[x] for x in lab])
-        gs = []
-        for a in W.central_atom(pos, box, lab, edge, 2):
-            paths = W.random_paths(pos, box, int(a), {2: 12, 3: 60, 4: 60}, rmax=5.0, leg_max=5.0, seed=int(a),
-                                   ipot_of=ipot_of)
-            for nleg, (c, ip, atoms) in paths.items():
-                gs.append((np.concatenate([np.full((len(atoms), 1), a), atoms], 1), ip, np.ones(len(atoms)),
-                           np.zeros(len(atoms), int)))
+    ipot_of = np.array([{"Ni": 1, "O": 2}[x] for x in lab])
+    models, npaths = [], 0
+    for edge, fname in (("Ni", "cfg5_nik_phase"), ("O", "cfg5_ok_phase")):
+        P = phase(fname)
+        st = GPUPathStage(P, device="cuda", dtype=torch.complex64)
+        finder = GPUPathFinder(P, device="cuda", rmax=5.0, nlegmax=4, critpw=2.0, merge_degenerate=False)
+        gs = finder_groups(finder, pos, box, W.central_atom(pos, box, lab, edge, 32), ipot_of)
         model = PathModel(st, gs, pos, nrows=1, box=box)
+        npaths += model.batch.n
         S = st.linear_matrix(K401).double().contiguous()
         with torch.no_grad():
             target = model.rows(torch.tensor(hidden, device="cuda"), q, S)[0]
         models.append((model, q, S, RSpaceMisfit(len(K401), target, FitWindow(kmin=3.0, kmax=14.0, rmin=1.0, rmax=5.0))))
+    assert len(pos) > 3800 and npaths > 5000
     g = GraphedRefinement(models, pos, lr=0.002)
     eager_pos = torch.tensor(pos, device="cuda", requires_grad=True)        # the same steps without the graph
     opt = torch.optim.Adam([eager_pos], lr=0.002, capturable=True)
@@ -190,7 +188,7 @@ def test_cfg5_two_edge_refinement_graph():
         losses.append(float(g.loss))
         assert abs(float(g.loss) - float(loss)) <= 1e-9 * abs(float(loss)), (it, float(g.loss), float(loss))
     assert torch.allclose(g.pos.detach(), eager_pos.detach(), rtol=0, atol=1e-9)
-    print(f"cfg5: misfit {losses[0]:.4e} -> {losses[-1]:.4e}")
+    print(f"cfg5: {npaths} paths, misfit {losses[0]:.4e} -> {losses[-1]:.4e}")
     assert losses[-1] < 0.8 * losses[0]
 
 
