@@ -75,6 +75,14 @@ fg_status launch_row_finish(const fg_paths *P, int NK, const unsigned long long 
 // without waiting (the rows of a replay that meets a bad input are NaN).
 fg_status read_status(const int *status, cudaStream_t st);
 
+// The path finder's description of B paths with a warp per path (fg_paths.cu), for a call on one absorber; paths with
+// keep[b] == 0 are skipped (keep may be null)
+fg_status describe_paths_warp(int64_t B, int32_t nleg, const int32_t *seq, const int32_t *slot, const int64_t *cand_off,
+                              const float *cand_rel, const int64_t *cand_atom, const int64_t *ipot_of,
+                              const int64_t *absorbers, const fg_pf_tables *T, const uint8_t *keep, float *coords,
+                              int64_t *ipots, int64_t *atoms, float *rtot, float *xport, int64_t *key,
+                              cudaStream_t st);
+
 // Events around the main kernel of a call when kernel timing is on (fg_set_kernel_timing)
 void timer_begin(cudaStream_t st);
 void timer_end(cudaStream_t st);

@@ -192,6 +192,97 @@ __device__ __forceinline__ int indbet(float c)
     return i < 0 ? 0 : (i > 2 * kNBeta ? 2 * kNBeta : i);
 }
 
+// Geometry of path b: its atoms' positions and potentials (written out when `write`), leg lengths, unit legs, closed
+// length and the cosines of the scattering angles -- the arithmetic of the reference's FP32 description.
+struct PathGeom {
+    float px[kMaxLeg + 1], py[kMaxLeg + 1], pz[kMaxLeg + 1];
+    int ip[kMaxLeg + 1];
+    float ri[kMaxLeg], cb[kMaxLeg], rt;
+};
+
+__device__ __forceinline__ void path_geom(int64_t b, int nleg, const int32_t *__restrict__ seq,
+                                          const int32_t *__restrict__ slot, const Cands &C,
+                                          const int64_t *__restrict__ cand_atom, const int64_t *__restrict__ ipot_of,
+                                          const int64_t *__restrict__ absorbers, bool write, float *__restrict__ coords,
+                                          int64_t *__restrict__ ipots, int64_t *__restrict__ atoms,
+                                          float *__restrict__ rtot_out, PathGeom &G)
+{
+    const int m = nleg - 1;
+    const int a = slot[b];
+    const int64_t base = C.off[a];
+    const int nc = (int)(C.off[a + 1] - base);
+    G.px[0] = G.py[0] = G.pz[0] = 0.f;
+    G.ip[0] = 0;
+    if (write) {
+        coords[b * nleg * 3 + 0] = coords[b * nleg * 3 + 1] = coords[b * nleg * 3 + 2] = 0.f;
+        ipots[b * nleg] = 0;
+    }
+    for (int q = 0; q < m; ++q) {
+        const int j = seq[b * m + q];
+        cand_xyz(C, base, nc, j, G.px[q + 1], G.py[q + 1], G.pz[q + 1]);
+        const int64_t atom = j == nc ? absorbers[a] : cand_atom[base + j];
+        G.ip[q + 1] = j == nc ? 0 : (int)ipot_of[atom];
+        if (write) {
+            atoms[b * m + q] = atom;
+            ipots[b * nleg + q + 1] = G.ip[q + 1];
+            coords[(b * nleg + q + 1) * 3 + 0] = G.px[q + 1];
+            coords[(b * nleg + q + 1) * 3 + 1] = G.py[q + 1];
+            coords[(b * nleg + q + 1) * 3 + 2] = G.pz[q + 1];
+        }
+    }
+    // legs j = 0..nleg-1: atom j -> atom j+1 (atom nleg = the absorber)
+    float ux[kMaxLeg], uy[kMaxLeg], uz[kMaxLeg];
+    G.rt = 0.f;
+    for (int j = 0; j < nleg; ++j) {
+        const int k = j + 1 < nleg ? j + 1 : 0;
+        const float dx = __fsub_rn(G.px[k], G.px[j]), dy = __fsub_rn(G.py[k], G.py[j]), dz = __fsub_rn(G.pz[k], G.pz[j]);
+        G.ri[j] = len3(dx, dy, dz);
+        G.rt = __fadd_rn(G.rt, G.ri[j]);
+        const float r = fmaxf(G.ri[j], 1e-12f);
+        ux[j] = __fdiv_rn(dx, r); uy[j] = __fdiv_rn(dy, r); uz[j] = __fdiv_rn(dz, r);
+    }
+    if (write) rtot_out[b] = G.rt;
+    // cos(beta) at atom j+1 between leg j and leg j+1 (j = nleg - 1: at the absorber, last leg -> first leg)
+    for (int j = 0; j < nleg; ++j) {
+        const int k = j + 1 < nleg ? j + 1 : 0;
+        G.cb[j] = __fadd_rn(__fadd_rn(__fmul_rn(ux[j], ux[k]), __fmul_rn(uy[j], uy[k])), __fmul_rn(uz[j], uz[k]));
+    }
+}
+
+// |crit| trap of energy e, the term the importance sums over e (pathfinder.py:75-100)
+__device__ __forceinline__ float importance_term(const PathGeom &G, int nleg, const int *ib, float cabs,
+                                                 const fg_pf_tables &T, int e)
+{
+    const int m = nleg - 1;
+    const float k = T.cksp[e];
+    float crit = __fdiv_rn(cabs, __fmul_rn(G.ri[nleg - 1], k));
+    for (int j = 0; j < m; ++j) {
+        const float f = T.fbeta[((int64_t)e * T.nph1 + G.ip[j + 1]) * (2 * kNBeta + 1) + ib[j]];
+        crit = __fdiv_rn(__fmul_rn(crit, f), __fmul_rn(G.ri[j], k));
+    }
+    crit = __fmul_rn(crit, expf(-__fdiv_rn(G.rt, T.xlam[e])));
+    return __fmul_rn(fabsf(crit), T.trap[e - T.ik0]);
+}
+
+// forward key (ri..., cos...) and its reverse (ri reversed, cos of the scatterers reversed, the absorber's cos last),
+// each rounded to 1e-3; the lexicographically smaller one (pathfinder.py:134-157)
+__device__ __forceinline__ void path_key(const PathGeom &G, int nleg, int64_t *__restrict__ key)
+{
+    int64_t kf[2 * kMaxLeg], kr[2 * kMaxLeg];
+    for (int j = 0; j < nleg; ++j) {
+        kf[j] = (int64_t)rintf(__fmul_rn(G.ri[j], 1000.f));
+        kf[nleg + j] = (int64_t)rintf(__fmul_rn(G.cb[j], 1000.f));
+        kr[j] = (int64_t)rintf(__fmul_rn(G.ri[nleg - 1 - j], 1000.f));
+    }
+    for (int j = 0; j < nleg - 1; ++j) kr[nleg + j] = (int64_t)rintf(__fmul_rn(G.cb[nleg - 2 - j], 1000.f));
+    kr[2 * nleg - 1] = kf[2 * nleg - 1];
+    int cmp = 0;
+    for (int j = 0; j < 2 * nleg && cmp == 0; ++j) cmp = kr[j] < kf[j] ? -1 : (kr[j] > kf[j] ? 1 : 0);
+    for (int j = 0; j < 2 * nleg; ++j) key[j] = cmp < 0 ? kr[j] : kf[j];
+}
+
+// One thread per path: coordinates (absorber at the origin), potentials, atom indices, closed length, the plane-wave
+// importance (pathfinder.py:75-100) and, for nleg > 2, the degeneracy key (pathfinder.py:134-157).
 __global__ void k_describe(int64_t B, int nleg, const int32_t *__restrict__ seq, const int32_t *__restrict__ slot,
                            Cands C, const int64_t *__restrict__ cand_atom, const int64_t *__restrict__ ipot_of,
                            const int64_t *__restrict__ absorbers, fg_pf_tables T, float *__restrict__ coords,
@@ -200,76 +291,54 @@ __global__ void k_describe(int64_t B, int nleg, const int32_t *__restrict__ seq,
 {
     const int m = nleg - 1;
     for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < B; b += (int64_t)gridDim.x * blockDim.x) {
-        const int a = slot[b];
-        const int64_t base = C.off[a];
-        const int nc = (int)(C.off[a + 1] - base);
-        float px[kMaxLeg + 1], py[kMaxLeg + 1], pz[kMaxLeg + 1];
-        int ip[kMaxLeg + 1];
-        px[0] = py[0] = pz[0] = 0.f;
-        ip[0] = 0;
-        coords[b * nleg * 3 + 0] = coords[b * nleg * 3 + 1] = coords[b * nleg * 3 + 2] = 0.f;
-        ipots[b * nleg] = 0;
-        for (int q = 0; q < m; ++q) {
-            const int j = seq[b * m + q];
-            cand_xyz(C, base, nc, j, px[q + 1], py[q + 1], pz[q + 1]);
-            const int64_t atom = j == nc ? absorbers[a] : cand_atom[base + j];
-            ip[q + 1] = j == nc ? 0 : (int)ipot_of[atom];
-            atoms[b * m + q] = atom;
-            ipots[b * nleg + q + 1] = ip[q + 1];
-            coords[(b * nleg + q + 1) * 3 + 0] = px[q + 1];
-            coords[(b * nleg + q + 1) * 3 + 1] = py[q + 1];
-            coords[(b * nleg + q + 1) * 3 + 2] = pz[q + 1];
-        }
-        // legs j = 0..nleg-1: atom j -> atom j+1 (atom nleg = the absorber)
-        float ri[kMaxLeg], ux[kMaxLeg], uy[kMaxLeg], uz[kMaxLeg];
-        float rt = 0.f;
-        for (int j = 0; j < nleg; ++j) {
-            const int k = j + 1 < nleg ? j + 1 : 0;
-            const float dx = __fsub_rn(px[k], px[j]), dy = __fsub_rn(py[k], py[j]), dz = __fsub_rn(pz[k], pz[j]);
-            ri[j] = len3(dx, dy, dz);
-            rt = __fadd_rn(rt, ri[j]);
-            const float r = fmaxf(ri[j], 1e-12f);
-            ux[j] = __fdiv_rn(dx, r); uy[j] = __fdiv_rn(dy, r); uz[j] = __fdiv_rn(dz, r);
-        }
-        rtot_out[b] = rt;
-        // cos(beta) at atom j+1 between leg j and leg j+1 (j = nleg - 1: at the absorber, last leg -> first leg)
-        float cb[kMaxLeg];
-        for (int j = 0; j < nleg; ++j) {
-            const int k = j + 1 < nleg ? j + 1 : 0;
-            cb[j] = __fadd_rn(__fadd_rn(__fmul_rn(ux[j], ux[k]), __fmul_rn(uy[j], uy[k])), __fmul_rn(uz[j], uz[k]));
-        }
+        PathGeom G;
+        path_geom(b, nleg, seq, slot, C, cand_atom, ipot_of, absorbers, true, coords, ipots, atoms, rtot_out, G);
         if (xport) {
             int ib[kMaxLeg];
-            for (int j = 0; j < m; ++j) ib[j] = indbet(cb[j]);
-            const float cabs = fmaxf(fabsf(cb[nleg - 1]), 0.3f);
+            for (int j = 0; j < m; ++j) ib[j] = indbet(G.cb[j]);
+            const float cabs = fmaxf(fabsf(G.cb[nleg - 1]), 0.3f);
             float s = 0.f;
-            for (int e = T.ik0; e < T.E; ++e) {
-                const float k = T.cksp[e];
-                float crit = __fdiv_rn(cabs, __fmul_rn(ri[nleg - 1], k));
-                for (int j = 0; j < m; ++j) {
-                    const float f = T.fbeta[((int64_t)e * T.nph1 + ip[j + 1]) * (2 * kNBeta + 1) + ib[j]];
-                    crit = __fdiv_rn(__fmul_rn(crit, f), __fmul_rn(ri[j], k));
-                }
-                crit = __fmul_rn(crit, expf(-__fdiv_rn(rt, T.xlam[e])));
-                s = __fadd_rn(s, __fmul_rn(fabsf(crit), T.trap[e - T.ik0]));
-            }
+            for (int e = T.ik0; e < T.E; ++e) s = __fadd_rn(s, importance_term(G, nleg, ib, cabs, T, e));
             xport[b] = s;
         }
-        if (key && nleg > 2) {
-            // forward key (ri..., cos...) and its reverse (ri reversed, cos of the scatterers reversed, the absorber's
-            // cos last), each rounded to 1e-3; the lexicographically smaller one
-            int64_t kf[2 * kMaxLeg], kr[2 * kMaxLeg];
-            for (int j = 0; j < nleg; ++j) {
-                kf[j] = (int64_t)rintf(__fmul_rn(ri[j], 1000.f));
-                kf[nleg + j] = (int64_t)rintf(__fmul_rn(cb[j], 1000.f));
-                kr[j] = (int64_t)rintf(__fmul_rn(ri[nleg - 1 - j], 1000.f));
+        if (key && nleg > 2) path_key(G, nleg, key + b * 2 * nleg);
+    }
+}
+
+// The same description, one warp per path (a few thousand paths of one absorber would leave most of the GPU idle
+// with a thread each): the lanes form the importance's per-energy terms, one lane sums them in energy order -- the
+// thread-per-path kernel's order, so the importance is bit for bit the same.  Paths whose keep flag is 0 (sequences
+// that are not paths) are skipped.
+constexpr int kDescribeWarps = 4;
+__global__ void __launch_bounds__(32 * kDescribeWarps)
+    k_describe_warp(int64_t B, int nleg, const int32_t *__restrict__ seq, const int32_t *__restrict__ slot, Cands C,
+                    const int64_t *__restrict__ cand_atom, const int64_t *__restrict__ ipot_of,
+                    const int64_t *__restrict__ absorbers, fg_pf_tables T, const uint8_t *__restrict__ keep,
+                    float *__restrict__ coords, int64_t *__restrict__ ipots, int64_t *__restrict__ atoms,
+                    float *__restrict__ rtot_out, float *__restrict__ xport, int64_t *__restrict__ key)
+{
+    extern __shared__ float terms_all[];                       // (kDescribeWarps, E)
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float *terms = terms_all + (size_t)w * T.E;
+    const int m = nleg - 1;
+    for (int64_t b = (int64_t)blockIdx.x * kDescribeWarps + w; b < B; b += (int64_t)gridDim.x * kDescribeWarps) {
+        if (keep && !keep[b]) continue;                        // warp-uniform
+        PathGeom G;
+        path_geom(b, nleg, seq, slot, C, cand_atom, ipot_of, absorbers, lane == 0, coords, ipots, atoms, rtot_out, G);
+        if (xport) {
+            int ib[kMaxLeg];
+            for (int j = 0; j < m; ++j) ib[j] = indbet(G.cb[j]);
+            const float cabs = fmaxf(fabsf(G.cb[nleg - 1]), 0.3f);
+            for (int e = T.ik0 + lane; e < T.E; e += 32) terms[e] = importance_term(G, nleg, ib, cabs, T, e);
+            __syncwarp();
+            if (lane == 0) {
+                float s = 0.f;
+                for (int e = T.ik0; e < T.E; ++e) s = __fadd_rn(s, terms[e]);
+                xport[b] = s;
             }
-            for (int j = 0; j < nleg - 1; ++j) kr[nleg + j] = (int64_t)rintf(__fmul_rn(cb[nleg - 2 - j], 1000.f));
-            kr[2 * nleg - 1] = kf[2 * nleg - 1];
-            int cmp = 0;
-            for (int j = 0; j < 2 * nleg && cmp == 0; ++j) cmp = kr[j] < kf[j] ? -1 : (kr[j] > kf[j] ? 1 : 0);
-            for (int j = 0; j < 2 * nleg; ++j) key[b * 2 * nleg + j] = cmp < 0 ? kr[j] : kf[j];
+            __syncwarp();
         }
+        if (lane == 0 && key && nleg > 2) path_key(G, nleg, key + b * 2 * nleg);
     }
 }
 
@@ -293,14 +362,17 @@ extern "C" fg_status fg_pf_candidates(const float *pos, int64_t n, float box, co
     if (A == 0) return FG_OK;
     if (!pos || !absorbers) return fail(FG_ERR_VALUE, "null argument");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // a block per absorber slot; a few slots (one absorber's call) get wide blocks so that the scan over the atoms
+    // is short (the compaction is ordered by warps, so the result does not depend on the width)
+    const int threads = A < 64 ? 1024 : 256;
     if (!offset) {
         if (!count) return fail(FG_ERR_VALUE, "null count");
-        k_candidates<false><<<A, 256, 0, st>>>(pos, n, box, cell, absorbers, per_frame, rmax, count, nullptr, nullptr,
-                                               nullptr);
+        k_candidates<false><<<A, threads, 0, st>>>(pos, n, box, cell, absorbers, per_frame, rmax, count, nullptr,
+                                                   nullptr, nullptr);
     } else {
         if (!cand_atom || !cand_rel) return fail(FG_ERR_VALUE, "null output");
-        k_candidates<true><<<A, 256, 0, st>>>(pos, n, box, cell, absorbers, per_frame, rmax, nullptr, offset, cand_atom,
-                                              cand_rel);
+        k_candidates<true><<<A, threads, 0, st>>>(pos, n, box, cell, absorbers, per_frame, rmax, nullptr, offset,
+                                                  cand_atom, cand_rel);
     }
     FG_CUDA(cudaGetLastError());
     return FG_OK;
@@ -364,6 +436,27 @@ extern "C" fg_status fg_pf_describe(int64_t B, int32_t nleg, const int32_t *seq,
     FG_CUDA(cudaGetLastError());
     return FG_OK;
 }
+
+namespace fg {
+fg_status describe_paths_warp(int64_t B, int32_t nleg, const int32_t *seq, const int32_t *slot, const int64_t *cand_off,
+                              const float *cand_rel, const int64_t *cand_atom, const int64_t *ipot_of,
+                              const int64_t *absorbers, const fg_pf_tables *T, const uint8_t *keep, float *coords,
+                              int64_t *ipots, int64_t *atoms, float *rtot, float *xport, int64_t *key,
+                              cudaStream_t st)
+{
+    if (B == 0) return FG_OK;
+    const fg_pf_tables t = *T;
+    const size_t smem = (size_t)kDescribeWarps * t.E * sizeof(float);
+    if (smem > 48 * 1024) FG_CUDA(cudaFuncSetAttribute(k_describe_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)smem));
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((B + kDescribeWarps - 1) / kDescribeWarps, 148 * 16));
+    k_describe_warp<<<blocks, 32 * kDescribeWarps, smem, st>>>(B, nleg, seq, slot, Cands{cand_off, cand_rel}, cand_atom,
+                                                                ipot_of, absorbers, t, keep, coords, ipots, atoms,
+                                                                rtot, xport, key);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+}  // namespace fg
 
 extern "C" fg_status fg_pf_windows(const float *sorted_len, const int64_t *seg_off, int64_t nseg, float eps,
                                    int64_t *window)

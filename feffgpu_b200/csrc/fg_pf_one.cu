@@ -344,6 +344,7 @@ extern "C" fg_status fg_pf_enumerate_one(const float *pos, int64_t n, float box,
         k_cand_len<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(nc, cand_rel, len, seq, slot);
         FG_TRY(cuda(cudaGetLastError(), "launch"));
     }
+    // a warp per path; sequences that are not paths (terminal flag 0) are skipped
     auto describe = [&](fg_pf_leg &l, const int32_t *s, const int32_t *sl, bool want_key) -> fg_status {
         const int64_t B = l.nb;
         if (fg_status rc = S.get(B * l.nleg * 3, &l.coords)) return rc;
@@ -353,9 +354,8 @@ extern "C" fg_status fg_pf_enumerate_one(const float *pos, int64_t n, float box,
         if (fg_status rc = S.get(B, &l.xport)) return rc;
         if (want_key)
             if (fg_status rc = S.get(B * 2 * l.nleg, &l.key)) return rc;
-        if (B == 0) return FG_OK;
-        return fg_pf_describe(B, l.nleg, s, sl, d_off, cand_rel, cand_atom, ipot_of, d_ab, T, l.coords, l.ipots,
-                              l.atoms, l.rtot, l.xport, l.key, stream);
+        return describe_paths_warp(B, l.nleg, s, sl, d_off, cand_rel, cand_atom, ipot_of, d_ab, T, l.keep, l.coords,
+                                   l.ipots, l.atoms, l.rtot, l.xport, l.key, st);
     };
     std::vector<fg_pf_leg> &legs = r->legs;
     legs.reserve(kMaxLeg);

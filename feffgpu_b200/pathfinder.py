@@ -104,6 +104,30 @@ class GPUPathFinder:
         self.trap = torch.tensor(w / 2, device=dev, dtype=torch.float32)
         self._tables = _lib.PfTables(E, P.nph + 1, self.ik0, self.fbeta.data_ptr(), self.cksp.data_ptr(),
                                      self.xlam.data_ptr(), self.trap.data_ptr())
+        self._cells: dict = {}
+
+    def _cell(self, box):
+        """(cubic length or -1, the cell words on the device or None) of a box, kept per box: the reference's front
+        ends pass the same box (often a device tensor) on every call, and converting it costs a synchronisation and a
+        matrix inverse on the host.  A tensor is known by its identity and version counter (an in-place change makes a
+        new entry); the entry holds the tensor, so its identity cannot pass to another one while it is cached."""
+        if torch.is_tensor(box):
+            key = ("t", id(box), box._version)
+        elif box is None or np.isscalar(box):
+            key = ("s", None if box is None else float(box))
+        else:
+            a = np.asarray(box, np.float64)
+            key = ("a", a.shape, a.tobytes())
+        hit = self._cells.get(key)
+        if hit is None:
+            cell = as_cell(box)
+            cellw = (torch.as_tensor(cell_words(cell, np.float32), device=self.device)
+                     if isinstance(cell, np.ndarray) else None)
+            hit = (cell if isinstance(cell, float) else -1.0, cellw, box if torch.is_tensor(box) else None)
+            if len(self._cells) > 32:
+                self._cells.clear()
+            self._cells[key] = hit
+        return hit[0], hit[1]
 
     def _stream(self) -> int:
         return torch.cuda.current_stream(self.device).cuda_stream
@@ -162,9 +186,7 @@ class GPUPathFinder:
         n = int(posd.shape[0])
         if not 0 <= int(absorber) < n:
             raise IndexError(f"absorber {int(absorber)} outside the {n} atoms")
-        cell = as_cell(box)
-        cellw = torch.as_tensor(cell_words(cell, np.float32), device=dev) if isinstance(cell, np.ndarray) else None
-        boxf = cell if isinstance(cell, float) else -1.0
+        boxf, cellw = self._cell(box)
         ipot_of = (ipot.to(dev, torch.int64) if torch.is_tensor(ipot)
                    else torch.as_tensor(np.asarray(ipot), device=dev, dtype=torch.int64)).contiguous()
         h = C.c_void_p()
@@ -209,11 +231,7 @@ class GPUPathFinder:
         if ab_np.shape[0] != F:
             raise ValueError("absorbers must be (A,) or (frames, A)")
         per_frame = max(int(ab_np.shape[1]), 1)
-        cell = as_cell(box)
-        cellw = None
-        if isinstance(cell, np.ndarray):
-            cellw = torch.as_tensor(cell_words(cell, np.float32), device=dev)
-        boxf = cell if isinstance(cell, float) else -1.0
+        boxf, cellw = self._cell(box)
         cptr = cellw.data_ptr() if cellw is not None else None
         ab = torch.as_tensor(ab_np.reshape(-1), device=dev).contiguous()
         A = int(ab.shape[0])
