@@ -75,6 +75,22 @@ fg_status launch_row_finish(const fg_paths *P, int NK, const unsigned long long 
 // without waiting (the rows of a replay that meets a bad input are NaN).
 fg_status read_status(const int *status, cudaStream_t st);
 
+// The one-absorber path finder's device steps (fg_paths.cu).  candidates_one: the candidates of one absorber in atom
+// order (cand_atom, cand_rel; n entries at most), their number in *nc and off = {0, nc}, the single-scattering partial
+// paths (len, seq, slot) and absorbers[0] = absorber, with no host round trip; tmp_atom / tmp_rel (n rounded up to 256
+// entries), bcnt and boff (n / 256 + 2) are scratch.  extend_count: children per partial path (k_extend's count
+// pass) for min(P, *P_dev) parents when P_dev is given.  scan_counts: off[0] = 0, off[i + 1] = the inclusive sum of
+// count[0..i] over min(P, *P_dev) entries, the sum in *total.
+fg_status candidates_one(const float *pos, int64_t n, float box, const float *cell, int64_t absorber, float rmax,
+                         int64_t *tmp_atom, float *tmp_rel, int32_t *bcnt, int64_t *boff, int64_t *cand_atom,
+                         float *cand_rel, float *len, int32_t *seq, int32_t *slot, int64_t *off, int64_t *absorbers,
+                         int64_t *nc, cudaStream_t st);
+fg_status extend_count(int64_t P, const int64_t *P_dev, int32_t m, const int32_t *seq, const float *len,
+                       const int32_t *slot, const int64_t *cand_off, const float *cand_rel, float two_r,
+                       int32_t *count, cudaStream_t st);
+fg_status scan_counts(int64_t P, const int64_t *P_dev, const int32_t *count, int64_t *off, int64_t *total,
+                      cudaStream_t st);
+
 // The path finder's description of B paths with a warp per path (fg_paths.cu), for a call on one absorber; paths with
 // keep[b] == 0 are skipped (keep may be null)
 fg_status describe_paths_warp(int64_t B, int32_t nleg, const int32_t *seq, const int32_t *slot, const int64_t *cand_off,

@@ -51,6 +51,24 @@ __device__ __forceinline__ void wrap_cell(const float *__restrict__ c, float &x,
 }
 
 // ------------------------------------------------------------------------------------------------ candidates
+// Whether atom i is a candidate of the absorber ab at (ax, ay, az), and its minimum-image position relative to it
+__device__ __forceinline__ bool candidate(const float *__restrict__ pos, int64_t i, int64_t ab, float ax, float ay,
+                                          float az, float box, const float *__restrict__ cell, float rmax, float &rx,
+                                          float &ry, float &rz)
+{
+    if (cell) {
+        rx = __fsub_rn(pos[3 * i], ax);
+        ry = __fsub_rn(pos[3 * i + 1], ay);
+        rz = __fsub_rn(pos[3 * i + 2], az);
+        wrap_cell(cell, rx, ry, rz);
+    } else {
+        rx = wrap1(__fsub_rn(pos[3 * i], ax), box);
+        ry = wrap1(__fsub_rn(pos[3 * i + 1], ay), box);
+        rz = wrap1(__fsub_rn(pos[3 * i + 2], az), box);
+    }
+    return i != ab && len3(rx, ry, rz) <= rmax;
+}
+
 // One block per absorber slot.  count: number of candidates; with out != null the candidates are written in atom
 // order at off[a] (ordered compaction: warp ballots, then the warps' counts in order).
 template <bool WRITE>
@@ -71,20 +89,7 @@ __global__ void k_candidates(const float *__restrict__ pos_all, int64_t n, float
     for (int64_t i0 = 0; i0 < n; i0 += blockDim.x) {
         const int64_t i = i0 + threadIdx.x;
         float rx = 0.f, ry = 0.f, rz = 0.f;
-        bool c = false;
-        if (i < n) {
-            if (cell) {
-                rx = __fsub_rn(pos[3 * i], ax);
-                ry = __fsub_rn(pos[3 * i + 1], ay);
-                rz = __fsub_rn(pos[3 * i + 2], az);
-                wrap_cell(cell, rx, ry, rz);
-            } else {
-                rx = wrap1(__fsub_rn(pos[3 * i], ax), box);
-                ry = wrap1(__fsub_rn(pos[3 * i + 1], ay), box);
-                rz = wrap1(__fsub_rn(pos[3 * i + 2], az), box);
-            }
-            c = i != ab && len3(rx, ry, rz) <= rmax;
-        }
+        const bool c = i < n && candidate(pos, i, ab, ax, ay, az, box, cell, rmax, rx, ry, rz);
         const unsigned m = __ballot_sync(0xffffffffu, c);
         if (lane == 0) warp_n[w] = __popc(m);
         __syncthreads();
@@ -106,6 +111,112 @@ __global__ void k_candidates(const float *__restrict__ pos_all, int64_t n, float
     if (!WRITE && threadIdx.x == 0) count[a] = (int32_t)total;
 }
 
+// The candidates of one absorber over many blocks, in two passes without a host round trip: block b compacts the
+// candidates among atoms [b kCandChunk, (b + 1) kCandChunk) in atom order to the same offset of a scratch and counts
+// them; after a scan of the counts (k_scan_counts) k_cand_place moves each block's run to its place, so the result is
+// k_candidates' order.  A one-absorber call cannot fill the GPU with a block per absorber.
+constexpr int kCandChunk = 256;
+
+__global__ void __launch_bounds__(kCandChunk)
+    k_cand_blocks(const float *__restrict__ pos, int64_t n, float box, const float *__restrict__ cell, int64_t ab,
+                  float rmax, int64_t *__restrict__ tmp_atom, float *__restrict__ tmp_rel, int32_t *__restrict__ bcnt)
+{
+    __shared__ int warp_n[kCandChunk / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const float ax = pos[3 * ab], ay = pos[3 * ab + 1], az = pos[3 * ab + 2];
+    const int64_t i = (int64_t)blockIdx.x * kCandChunk + threadIdx.x;
+    float rx = 0.f, ry = 0.f, rz = 0.f;
+    const bool c = i < n && candidate(pos, i, ab, ax, ay, az, box, cell, rmax, rx, ry, rz);
+    const unsigned m = __ballot_sync(0xffffffffu, c);
+    if (lane == 0) warp_n[w] = __popc(m);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int q = 0; q < kCandChunk / 32; ++q) {
+        if (q < w) before += warp_n[q];
+        total += warp_n[q];
+    }
+    if (c) {
+        const int64_t o = (int64_t)blockIdx.x * kCandChunk + before + __popc(m & ((1u << lane) - 1u));
+        tmp_atom[o] = i;
+        tmp_rel[3 * o] = rx;
+        tmp_rel[3 * o + 1] = ry;
+        tmp_rel[3 * o + 2] = rz;
+    }
+    if (threadIdx.x == 0) bcnt[blockIdx.x] = total;
+}
+
+// Block b's run to its place (boff: the scan of the block counts), with the single-scattering partial paths: length,
+// sequence (the candidate itself) and slot 0.  Also off = {0, nc} and absorbers[0] = ab for the later kernels.
+__global__ void __launch_bounds__(kCandChunk)
+    k_cand_place(int64_t ab, const int64_t *__restrict__ tmp_atom, const float *__restrict__ tmp_rel,
+                 const int32_t *__restrict__ bcnt, const int64_t *__restrict__ boff, int64_t nblocks,
+                 int64_t *__restrict__ cand_atom, float *__restrict__ cand_rel, float *__restrict__ len,
+                 int32_t *__restrict__ seq, int32_t *__restrict__ slot, int64_t *__restrict__ off,
+                 int64_t *__restrict__ absorbers)
+{
+    const int64_t b = blockIdx.x;
+    if (threadIdx.x < bcnt[b]) {
+        const int64_t src = b * kCandChunk + threadIdx.x, o = boff[b] + threadIdx.x;
+        const float x = tmp_rel[3 * src], y = tmp_rel[3 * src + 1], z = tmp_rel[3 * src + 2];
+        cand_atom[o] = tmp_atom[src];
+        cand_rel[3 * o] = x;
+        cand_rel[3 * o + 1] = y;
+        cand_rel[3 * o + 2] = z;
+        len[o] = len3(x, y, z);
+        seq[o] = (int32_t)o;
+        slot[o] = 0;
+    }
+    if (b == 0 && threadIdx.x == 0) {
+        off[0] = 0;
+        off[1] = boff[nblocks];
+        absorbers[0] = ab;
+    }
+}
+
+// off[0] = 0, off[i + 1] = cnt[0] + ... + cnt[i] for i < P (P = min(P, *P_dev) when P_dev is given), and the sum in
+// *total: one block, chunks of its width, warp scans carried across chunks.
+constexpr int kScanThreads = 1024;
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_scan_counts(int64_t P, const int64_t *__restrict__ P_dev, const int32_t *__restrict__ cnt,
+                  int64_t *__restrict__ off, int64_t *__restrict__ total)
+{
+    __shared__ long long warp_s[kScanThreads / 32];
+    __shared__ long long carry_s;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (P_dev) P = min(P, *P_dev);
+    if (threadIdx.x == 0) {
+        off[0] = 0;
+        carry_s = 0;
+    }
+    __syncthreads();
+    for (int64_t i0 = 0; i0 < P; i0 += kScanThreads) {
+        const int64_t i = i0 + threadIdx.x;
+        long long x = i < P ? cnt[i] : 0;
+        for (int d = 1; d < 32; d <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= d) x += y;
+        }
+        if (lane == 31) warp_s[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            long long v = warp_s[lane];
+            for (int d = 1; d < 32; d <<= 1) {
+                const long long y = __shfl_up_sync(0xffffffffu, v, d);
+                if (lane >= d) v += y;
+            }
+            warp_s[lane] = v;
+        }
+        __syncthreads();
+        const long long incl = carry_s + (w > 0 ? warp_s[w - 1] : 0) + x;
+        if (i < P) off[i + 1] = incl;
+        __syncthreads();
+        if (threadIdx.x == kScanThreads - 1) carry_s = incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry_s;
+}
+
 // ------------------------------------------------------------------------------------------------ extension
 struct Cands {
     const int64_t *off;     // (A + 1) candidate offsets per absorber slot
@@ -125,8 +236,9 @@ template <bool WRITE>
 __global__ void k_extend(int64_t P, int m, const int32_t *__restrict__ seq, const float *__restrict__ len,
                          const int32_t *__restrict__ slot, Cands C, float two_r, int32_t *__restrict__ count,
                          const int64_t *__restrict__ child_off, int32_t *__restrict__ cseq, float *__restrict__ clen,
-                         int32_t *__restrict__ cslot)
+                         int32_t *__restrict__ cslot, const int64_t *__restrict__ P_dev = nullptr)
 {
+    if (P_dev) P = min(P, *P_dev);     // the parents' number where only the device knows it (P: its upper bound)
     const int lane = threadIdx.x & 31;
     const int64_t wg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwg = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t p = wg; p < P; p += nwg) {
@@ -438,6 +550,42 @@ extern "C" fg_status fg_pf_describe(int64_t B, int32_t nleg, const int32_t *seq,
 }
 
 namespace fg {
+fg_status candidates_one(const float *pos, int64_t n, float box, const float *cell, int64_t absorber, float rmax,
+                         int64_t *tmp_atom, float *tmp_rel, int32_t *bcnt, int64_t *boff, int64_t *cand_atom,
+                         float *cand_rel, float *len, int32_t *seq, int32_t *slot, int64_t *off, int64_t *absorbers,
+                         int64_t *nc, cudaStream_t st)
+{
+    const int64_t G = (n + kCandChunk - 1) / kCandChunk;
+    if (G > INT32_MAX) return fail(FG_ERR_VALUE, "too many atoms");
+    k_cand_blocks<<<(unsigned)G, kCandChunk, 0, st>>>(pos, n, box, cell, absorber, rmax, tmp_atom, tmp_rel, bcnt);
+    FG_CUDA(cudaGetLastError());
+    k_scan_counts<<<1, kScanThreads, 0, st>>>(G, nullptr, bcnt, boff, nc);
+    FG_CUDA(cudaGetLastError());
+    k_cand_place<<<(unsigned)G, kCandChunk, 0, st>>>(absorber, tmp_atom, tmp_rel, bcnt, boff, G, cand_atom, cand_rel,
+                                                     len, seq, slot, off, absorbers);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+fg_status extend_count(int64_t P, const int64_t *P_dev, int32_t m, const int32_t *seq, const float *len,
+                       const int32_t *slot, const int64_t *cand_off, const float *cand_rel, float two_r,
+                       int32_t *count, cudaStream_t st)
+{
+    if (P <= 0) return FG_OK;
+    k_extend<false><<<grid_of(P * 32, 256), 256, 0, st>>>(P, m, seq, len, slot, Cands{cand_off, cand_rel}, two_r,
+                                                          count, nullptr, nullptr, nullptr, nullptr, P_dev);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+fg_status scan_counts(int64_t P, const int64_t *P_dev, const int32_t *count, int64_t *off, int64_t *total,
+                      cudaStream_t st)
+{
+    k_scan_counts<<<1, kScanThreads, 0, st>>>(P, P_dev, count, off, total);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
 fg_status describe_paths_warp(int64_t B, int32_t nleg, const int32_t *seq, const int32_t *slot, const int64_t *cand_off,
                               const float *cand_rel, const int64_t *cand_atom, const int64_t *ipot_of,
                               const int64_t *absorbers, const fg_pf_tables *T, const uint8_t *keep, float *coords,

@@ -1,8 +1,9 @@
 // fg_pf_one.cu -- the path finder for one absorber, driven from the host in C++ (the reference's front ends call the
 // finder once per absorber: src/feffgpu/exafs/forward.py:122-123, md/spectrum.py:275-277).  The kernels are the
 // batched finder's (fg_paths.cu); what changes is the driver: one call runs candidates, growth, description, merges
-// and importance cut with one synchronisation per growth level plus two, instead of a Python sequence of small torch
-// operations whose launch and dispatch latency dominated a call of a few hundred paths.  The merges and the cut run
+// and importance cut with two synchronisations (the numbers of candidates and of three-leg sequences; the result
+// fields) plus one per growth level past three legs, instead of a Python sequence of small torch operations whose
+// launch and dispatch latency dominated a call of a few hundred paths.  The merges and the cut run
 // on the host in FP32 with the arithmetic and order of the batched path (and so of the reference, pathfinder.py:
 // 102-157, 271-279), so the kept paths are bit for bit those of fg_pf_* driven by feffgpu_b200/pathfinder.py.
 #include <cuda_runtime.h>
@@ -68,35 +69,22 @@ struct Scratch {
     }
 };
 
-__global__ void k_cand_len(int64_t nc, const float *__restrict__ rel, float *__restrict__ len, int32_t *__restrict__ seq,
-                           int32_t *__restrict__ slot)
+// The kept paths of one leg count into the caller's arrays: path b of the output is described path idx[b], with the
+// degeneracy deg_k[b] of the merges
+__global__ void k_gather_paths(int64_t B, int nleg, const int64_t *__restrict__ idx, const float *__restrict__ deg_k,
+                               const float *__restrict__ c_in, const int64_t *__restrict__ ip_in,
+                               const float *__restrict__ x_in, const int64_t *__restrict__ at_in,
+                               float *__restrict__ coords, int64_t *__restrict__ ipots, float *__restrict__ deg,
+                               float *__restrict__ xport, int64_t *__restrict__ atoms)
 {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nc) return;
-    const float x = rel[3 * i], y = rel[3 * i + 1], z = rel[3 * i + 2];
-    len[i] = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
-    seq[i] = (int32_t)i;
-    slot[i] = 0;
-}
-
-// out[i] = in[idx[i]] for rows of w elements
-template <typename T>
-__global__ void k_gather_rows(int64_t B, int w, const int64_t *__restrict__ idx, const T *__restrict__ in,
-                              T *__restrict__ out)
-{
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= B * w) return;
-    const int64_t b = t / w, j = t % w;
-    out[t] = in[idx[b] * w + j];
-}
-
-template <typename T> fg_status gather(int64_t B, int w, const int64_t *idx, const T *in, T *out, cudaStream_t st)
-{
-    if (B == 0 || !out) return FG_OK;
-    const int64_t n = B * w;
-    k_gather_rows<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(B, w, idx, in, out);
-    FG_CUDA(cudaGetLastError());
-    return FG_OK;
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    const int64_t j = idx[b];
+    for (int q = 0; q < 3 * nleg; ++q) coords[b * 3 * nleg + q] = c_in[j * 3 * nleg + q];
+    for (int q = 0; q < nleg; ++q) ipots[b * nleg + q] = ip_in[j * nleg + q];
+    for (int q = 0; q < nleg - 1; ++q) atoms[b * (nleg - 1) + q] = at_in[j * (nleg - 1) + q];
+    xport[b] = x_in[j];
+    deg[b] = deg_k[b];
 }
 
 // indices that sort v ascending, equal values in index order (numpy's argsort(kind="stable"))
@@ -145,6 +133,8 @@ struct fg_pf_leg {
     uint8_t *keep = nullptr;            // terminal flags (nleg > 2), null for single scattering
     std::vector<int64_t> kept;          // indices into the described paths
     std::vector<float> kept_deg;        // degeneracies of the kept paths
+    const int64_t *d_kept = nullptr;    // the same two on the device
+    const float *d_kept_deg = nullptr;
 };
 
 struct fg_pf_result {
@@ -312,38 +302,42 @@ extern "C" fg_status fg_pf_enumerate_one(const float *pos, int64_t n, float box,
         return e == cudaSuccess ? FG_OK : fail(FG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
     };
     unsigned char *hp = nullptr;
-    // candidates: count, then write (one synchronisation for the count)
-    int64_t *d_ab = nullptr, *d_off = nullptr;
-    int32_t *d_cnt = nullptr;
+    // Candidates and the first level's child counts without a host round trip (sized by the atom count, an upper
+    // bound of the candidates'), then one synchronisation for both numbers.
+    const int64_t G = (n + 255) / 256;
+    int64_t *d_ab = nullptr, *d_off = nullptr, *d_counts = nullptr, *tmp_atom = nullptr, *boff = nullptr;
+    int64_t *cand_atom = nullptr, *d_coff = nullptr;
+    int32_t *bcnt = nullptr, *seq = nullptr, *slot = nullptr, *cc = nullptr;
+    float *tmp_rel = nullptr, *cand_rel = nullptr, *len = nullptr;
     FG_TRY(S.get(1, &d_ab));
     FG_TRY(S.get(2, &d_off));
-    FG_TRY(S.get(1, &d_cnt));
-    FG_TRY(cuda(cudaMemcpyAsync(d_ab, &absorber, sizeof(int64_t), cudaMemcpyHostToDevice, st), "copy"));
-    FG_TRY(fg_pf_candidates(pos, n, box, cell, d_ab, 1, 1, rmax, d_cnt, nullptr, nullptr, nullptr, stream));
-    FG_TRY(pinned(64, &hp));
-    FG_TRY(cuda(cudaMemcpyAsync(hp, d_cnt, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "copy"));
-    FG_TRY(cuda(cudaStreamSynchronize(st), "synchronize"));
-    int32_t nc32 = 0;
-    std::memcpy(&nc32, hp, sizeof(int32_t));
-    const int64_t nc = nc32;
-    const int64_t off_h[2] = {0, nc};
-    FG_TRY(cuda(cudaMemcpyAsync(d_off, off_h, sizeof(off_h), cudaMemcpyHostToDevice, st), "copy"));
-    int64_t *cand_atom = nullptr;
-    float *cand_rel = nullptr;
-    FG_TRY(S.get(nc, &cand_atom));
-    FG_TRY(S.get(3 * nc, &cand_rel));
-    if (nc > 0)
-        FG_TRY(fg_pf_candidates(pos, n, box, cell, d_ab, 1, 1, rmax, nullptr, d_off, cand_atom, cand_rel, stream));
-    // single scattering: every candidate
-    int32_t *seq = nullptr, *slot = nullptr;
-    float *len = nullptr;
-    FG_TRY(S.get(nc, &seq));
-    FG_TRY(S.get(nc, &slot));
-    FG_TRY(S.get(nc, &len));
-    if (nc > 0) {
-        k_cand_len<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(nc, cand_rel, len, seq, slot);
-        FG_TRY(cuda(cudaGetLastError(), "launch"));
+    FG_TRY(S.get(2, &d_counts));
+    FG_TRY(S.get(G * 256, &tmp_atom));
+    FG_TRY(S.get(G * 256 * 3, &tmp_rel));
+    FG_TRY(S.get(G, &bcnt));
+    FG_TRY(S.get(G + 1, &boff));
+    FG_TRY(S.get(n, &cand_atom));
+    FG_TRY(S.get(3 * n, &cand_rel));
+    FG_TRY(S.get(n, &seq));
+    FG_TRY(S.get(n, &slot));
+    FG_TRY(S.get(n, &len));
+    FG_TRY(candidates_one(pos, n, box, cell, absorber, rmax, tmp_atom, tmp_rel, bcnt, boff, cand_atom, cand_rel, len,
+                          seq, slot, d_off, d_ab, d_counts, st));
+    const float two_r = 2.f * rmax;
+    if (nlegmax > 2) {
+        FG_TRY(S.get(n, &cc));
+        FG_TRY(S.get(n + 1, &d_coff));
+        FG_TRY(extend_count(n, d_counts, 1, seq, len, slot, d_off, cand_rel, two_r, cc, st));
+        FG_TRY(scan_counts(n, d_counts, cc, d_coff, d_counts + 1, st));
+    } else {
+        FG_TRY(cuda(cudaMemsetAsync(d_counts + 1, 0, sizeof(int64_t), st), "memset"));
     }
+    FG_TRY(pinned(64, &hp));
+    FG_TRY(cuda(cudaMemcpyAsync(hp, d_counts, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, st), "copy"));
+    FG_TRY(cuda(cudaStreamSynchronize(st), "synchronize"));
+    int64_t counts_h[2];
+    std::memcpy(counts_h, hp, sizeof(counts_h));
+    const int64_t nc = counts_h[0];
     // a warp per path; sequences that are not paths (terminal flag 0) are skipped
     auto describe = [&](fg_pf_leg &l, const int32_t *s, const int32_t *sl, bool want_key) -> fg_status {
         const int64_t B = l.nb;
@@ -363,34 +357,29 @@ extern "C" fg_status fg_pf_enumerate_one(const float *pos, int64_t n, float box,
     legs[0].nleg = 2;
     legs[0].nb = nc;
     FG_TRY(describe(legs[0], seq, slot, false));
-    // growth, one level per extra leg: one synchronisation per level (the number of children sizes the next)
+    // growth, one level per extra leg; past the first, one synchronisation per level (the number of children sizes
+    // the next)
     int64_t P = nc > 1 ? nc : 0;     // multiple scattering needs two candidates (pathfinder.py:237, 243, 262)
-    const float two_r = 2.f * rmax;
     for (int m = 1; m <= nlegmax - 2 && P > 0; ++m) {
-        int32_t *cc = nullptr;
-        FG_TRY(S.get(P, &cc));
-        FG_TRY(fg_pf_extend(P, m, seq, len, slot, d_off, cand_rel, two_r, cc, nullptr, nullptr, nullptr, nullptr,
-                            stream));
-        FG_TRY(pinned((size_t)P * sizeof(int32_t), &hp));
-        FG_TRY(cuda(cudaMemcpyAsync(hp, cc, (size_t)P * sizeof(int32_t), cudaMemcpyDeviceToHost, st), "copy"));
-        FG_TRY(cuda(cudaStreamSynchronize(st), "synchronize"));
-        std::vector<int64_t> coff((size_t)P + 1, 0);
-        const int32_t *ch = reinterpret_cast<const int32_t *>(hp);
-        for (int64_t i = 0; i < P; ++i) coff[i + 1] = coff[i] + ch[i];
-        const int64_t Cn = coff[P];
+        int64_t Cn = counts_h[1];
+        if (m > 1) {
+            FG_TRY(S.get(P, &cc));
+            FG_TRY(S.get(P + 1, &d_coff));
+            FG_TRY(extend_count(P, nullptr, m, seq, len, slot, d_off, cand_rel, two_r, cc, st));
+            FG_TRY(scan_counts(P, nullptr, cc, d_coff, d_counts + 1, st));
+            FG_TRY(cuda(cudaMemcpyAsync(hp, d_counts + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "copy"));
+            FG_TRY(cuda(cudaStreamSynchronize(st), "synchronize"));
+            std::memcpy(&Cn, hp, sizeof(int64_t));
+        }
         if (Cn > kPartialLimit || Cn * (4 * (m + 2) + 8) > (int64_t(8) << 30))
             return bail(fail(FG_ERR_VALUE, std::to_string(Cn) + " partial paths of " + std::to_string(m + 2) +
                                                " legs: lower the path cutoff or the largest number of legs"));
         if (Cn == 0) break;
-        int64_t *d_coff = nullptr;
         int32_t *cseq = nullptr, *cslot = nullptr;
         float *clen = nullptr;
-        FG_TRY(S.get(P + 1, &d_coff));
         FG_TRY(S.get(Cn * (m + 1), &cseq));
         FG_TRY(S.get(Cn, &cslot));
         FG_TRY(S.get(Cn, &clen));
-        FG_TRY(cuda(cudaMemcpyAsync(d_coff, coff.data(), coff.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st),
-                    "copy"));
         FG_TRY(fg_pf_extend(P, m, seq, len, slot, d_off, cand_rel, two_r, nullptr, d_coff, cseq, clen, cslot, stream));
         fg_pf_leg l;
         l.nleg = m + 2;
@@ -472,11 +461,29 @@ extern "C" fg_status fg_pf_enumerate_one(const float *pos, int64_t n, float box,
     std::vector<fg_pf_leg> kept;
     merge_and_cut(H, nc, c1, ip1, merge != 0, critpw, kept, r->ref);
     for (int i = 0; i <= kMaxLeg; ++i) counts[i] = -1;
+    size_t nkept = 0;
     for (size_t i = 0; i < legs.size(); ++i) {
         legs[i].kept = std::move(kept[i].kept);
         legs[i].kept_deg = std::move(kept[i].kept_deg);
         counts[legs[i].nleg] = (int64_t)legs[i].kept.size();
+        nkept += legs[i].kept.size();
     }
+    // every leg's kept indices, then their degeneracies, to the device in one copy
+    std::vector<int64_t> packed(2 * nkept);
+    int64_t *d_packed = nullptr;
+    FG_TRY(S.get(packed.size(), &d_packed));
+    size_t o = 0;
+    for (fg_pf_leg &l : legs) {
+        std::copy(l.kept.begin(), l.kept.end(), packed.begin() + o);
+        float *dg = reinterpret_cast<float *>(packed.data() + nkept + o);
+        std::copy(l.kept_deg.begin(), l.kept_deg.end(), dg);
+        l.d_kept = d_packed + o;
+        l.d_kept_deg = reinterpret_cast<const float *>(d_packed + nkept + o);
+        o += l.kept.size();
+    }
+    if (nkept)
+        FG_TRY(cuda(cudaMemcpyAsync(d_packed, packed.data(), packed.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                    st), "copy"));
     *ref = r->ref;
     *out = r;
     return FG_OK;
@@ -493,14 +500,10 @@ extern "C" fg_status fg_pf_result_gather(fg_pf_result *r, int32_t nleg, float *c
         const int64_t B = (int64_t)l.kept.size();
         if (B == 0) return FG_OK;
         if (!coords || !ipots || !deg || !xport || !atoms) return fail(FG_ERR_VALUE, "null output");
-        int64_t *d_idx = nullptr;
-        if (fg_status rc = r->scratch.get(B, &d_idx)) return rc;
-        FG_CUDA(cudaMemcpyAsync(d_idx, l.kept.data(), B * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-        FG_CUDA(cudaMemcpyAsync(deg, l.kept_deg.data(), B * sizeof(float), cudaMemcpyHostToDevice, st));
-        if (fg_status rc = gather<float>(B, nleg * 3, d_idx, l.coords, coords, st)) return rc;
-        if (fg_status rc = gather<int64_t>(B, nleg, d_idx, l.ipots, ipots, st)) return rc;
-        if (fg_status rc = gather<float>(B, 1, d_idx, l.xport, xport, st)) return rc;
-        return gather<int64_t>(B, nleg - 1, d_idx, l.atoms, atoms, st);
+        k_gather_paths<<<(unsigned)((B + 127) / 128), 128, 0, st>>>(B, nleg, l.d_kept, l.d_kept_deg, l.coords, l.ipots,
+                                                                   l.xport, l.atoms, coords, ipots, deg, xport, atoms);
+        FG_CUDA(cudaGetLastError());
+        return FG_OK;
     }
     return fail(FG_ERR_VALUE, "no paths of " + std::to_string(nleg) + " legs in the result");
 }
