@@ -794,7 +794,7 @@ def main():
     import torch.distributed as dist
     from feffgpu_b200 import GPUPathStage, PathBatch, _lib
     from feffgpu_b200.roofline import batch_flops
-    from feffgpu_b200.autotune import default_tuner
+    from feffgpu_b200.autotune import default_tuner, shape_key
     tuner = default_tuner()
 
     if world > 1:
@@ -931,8 +931,9 @@ def main():
         "dtype": "fp32 (complex chain) + fp64 (phase argument, sums)", "data": "synthetic",
         "config": workload_config(all_groups, world),
         "autotune": {"fwd_warps": stage._launch[0], "bwd_warps": stage._launch[1],
-                     "timed": [{"kind": k, "warps": w_, "ms": round(t_, 3)} for sig, k, w_, t_ in tuner.log
-                               if sig.split("|")[1] == "p0"]},
+                     "fwd_regs_alt": stage._launch[2], "fwd_stage_t": stage._launch[3],
+                     "timed": [{"kind": k, "shape": shape_key(w_) if k == "fwd" else w_, "ms": round(t_, 3)}
+                               for sig, k, w_, t_ in tuner.log if sig.split("|")[1] == "p0"]},
         "reference_cpu": ref_cpu, "pair_tables": pairs, "path_finder": pf, "md_batch": md, "rmc_refinement": rmc,
         "reference_gpu": ref_gpu, "plain_fp64": plain, "fwd_bwd": fwd_bwd,
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "parity": parity,

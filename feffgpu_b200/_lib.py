@@ -26,7 +26,7 @@ EXPORTS = ("fg_stage_create", "fg_stage_destroy", "fg_stage_get_info", "fg_stage
            "fg_chi_fine_backward", "fg_chi_reduce_workspace", "fg_chi_reduce", "fg_chi_reduce_noalloc",
            "fg_chi_reduce_backward_workspace",
            "fg_chi_reduce_backward", "fg_set_kernel_timing", "fg_kernel_time_ms", "fg_fp32_fma_peak", "fg_set_launch",
-           "fg_stage_set_launch", "fg_pf_candidates", "fg_pf_extend", "fg_pf_terminal", "fg_pf_describe",
+           "fg_stage_set_launch", "fg_stage_set_fused_variant", "fg_pf_candidates", "fg_pf_extend", "fg_pf_terminal", "fg_pf_describe",
            "fg_pf_windows", "fg_pair_histogram", "fg_pair_ss_grad", "fg_rspace_misfit",
            "fg_path_columns", "fg_shard_lpt", "fg_pf_enumerate_one", "fg_pf_result_gather", "fg_pf_result_destroy")
 
@@ -79,6 +79,7 @@ _SIGS = {
     "fg_fp32_fma_peak": (C.c_int, [C.POINTER(C.c_double), _P]),
     "fg_set_launch": (C.c_int, [C.c_int32, C.c_int32]),
     "fg_stage_set_launch": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "fg_stage_set_fused_variant": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "fg_pf_candidates": (C.c_int, [_P, C.c_int64, C.c_float, _P, _P, C.c_int32, C.c_int32, C.c_float, _P, _P, _P,
                                    _P, _P]),
     "fg_pf_extend": (C.c_int, [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, C.c_float, _P, _P, _P, _P, _P, _P]),

@@ -1,14 +1,21 @@
 """Launch-shape autotuner of the persistent per-path kernels.
 
-The forward (fused stage) and the adjoint kernels keep one path per warp and take their launch shape -- warps per
-CTA, i.e. paths in flight per CTA -- at launch.  The shape sets the shared-memory granule of a CTA (the per-warp
-rotation tables grow with the batch's longest path and double in FP64) and with it how many paths an SM keeps
-resident under the register and shared-memory limits; which shape is fastest depends on the precision, the leg mix
-and the energy count.  The autotuner times every candidate shape on the device (CUDA events on the current stream,
-one warm-up and three timed launches each, on a stratified sample of the batch), keeps the fastest per workload
-signature, and persists the choice per GPU model in a JSON file (``$FEFFGPU_B200_TUNE_CACHE``, default
-``~/.cache/feffgpu_b200/autotune.json``), so a workload is tuned once.  Results do not depend on the shape: the
-cross-path sums run in a fixed order whatever the schedule.
+The forward (fused stage) and the adjoint kernels keep one path per warp and take their launch shape at launch.
+The adjoint's shape is its warps per CTA, i.e. paths in flight per CTA.  The forward's has three parts:
+
+* warps per CTA (1, 2, 4): the shared-memory granule of a CTA (the per-warp rotation tables grow with the batch's
+  longest path and double in FP64) and with it how many paths an SM keeps resident;
+* the register budget: the default (two CTAs of 128 threads per SM in FP32, one in FP64) or three CTAs per SM --
+  more warps to hide latency against fewer registers for the partial-wave loop's instruction-level parallelism;
+* the t-matrix source: read through L1, or each scatterer's column copied into a shared-memory tile per warp first
+  (asynchronous copies), which takes shared memory from L1.
+
+Which shape is fastest depends on the precision, the leg mix and the energy count.  The autotuner times every
+candidate on the device (CUDA events on the current stream, one warm-up and three timed launches each, on a
+stratified sample of the batch), keeps the fastest per workload signature, and persists the choice per GPU model in
+a JSON file (``$FEFFGPU_B200_TUNE_CACHE``, default ``~/.cache/feffgpu_b200/autotune.json``), so a workload is tuned
+once.  Results do not depend on the shape: the cross-path sums are exact and every path's arithmetic is the same
+whatever the schedule.
 
 ``GPUPathStage(..., autotune=True)`` tunes on the first call of each new workload signature (never inside CUDA
 graph capture: a signature first met during capture runs with the default shape); ``GPUPathStage.tune`` tunes
@@ -28,6 +35,8 @@ from . import _lib
 
 FWD_WARPS = (1, 2, 4)
 BWD_WARPS = (1, 2, 4)
+FWD_VARIANTS = ((0, 0), (1, 0), (0, 1))      # (register budget, t-matrix staging): default, 3 CTAs per SM, staged
+FWD_SHAPES = tuple((w, r, t) for r, t in FWD_VARIANTS for w in FWD_WARPS)
 SAMPLE_PATHS = 32768
 _lock = threading.Lock()
 
@@ -50,16 +59,24 @@ def signature(stage, batch, nk: int, prec: int) -> str:
     return f"{name}|p{prec}|l{stage.ilinit}|E{stage.E}|K{nk}|n{batch.nleg_max}|{mix}"
 
 
+def shape_key(shape) -> str:
+    """'w4r0t0' for a forward shape (warps, register budget, t staging)."""
+    w, r, t = shape
+    return f"w{w}r{r}t{t}"
+
+
 class Autotuner:
-    """Chooses (forward warps, adjoint warps) per workload signature.  ``timer(kind, stage, batch, q, S, prec, w)``
-    returns milliseconds for one candidate (the default times the library's calls with CUDA events)."""
+    """Chooses the launch per workload signature: (forward warps, adjoint warps, forward register budget, forward t
+    staging).  ``timer(kind, stage, batch, q, S, prec, shape)`` returns milliseconds for one candidate, ``shape`` a
+    (warps, register budget, t staging) tuple for 'fwd' and the warps for 'bwd' (the default times the library's
+    calls with CUDA events)."""
 
     def __init__(self, path: Path | None = None, timer=None, sample_paths: int = SAMPLE_PATHS):
         self.path = Path(path) if path is not None else cache_path()
         self.timer = timer or _time_candidate
         self.sample_paths = sample_paths
         self.table: dict = self._load()
-        self.log: list = []          # (signature, kind, warps, ms) of the candidates timed by this process
+        self.log: list = []          # (signature, kind, shape, ms) of the candidates timed by this process
 
     def _load(self) -> dict:
         try:
@@ -80,10 +97,12 @@ class Autotuner:
         e = self.table.get(sig)
         if e is None or (backward and "bwd" not in e):
             return None
-        return int(e["fwd"]), int(e.get("bwd", 0))
+        f = e["fwd"]
+        w, r, t = (int(f), 0, 0) if isinstance(f, int) else (int(x) for x in f)
+        return w, int(e.get("bwd", 0)), r, t
 
     def tune(self, stage, batch, q, S, prec: int, backward: bool = True):
-        """Times the candidates and records the fastest; returns (fwd_warps, bwd_warps)."""
+        """Times the candidates and records the fastest; returns (fwd_warps, bwd_warps, regs_alt, stage_t)."""
         nk = int(q.shape[0])
         sig = signature(stage, batch, nk, prec)
         with _lock:
@@ -91,36 +110,51 @@ class Autotuner:
             if hit is not None:
                 return hit
             sample = batch.sample(self.sample_paths)
-            times = {}
-            for w in FWD_WARPS:
-                times[("fwd", w)] = self.timer("fwd", stage, sample, q, S, prec, w)
-            fwd = _pick({w: times[("fwd", w)] for w in FWD_WARPS})
-            entry = {"fwd": fwd, "ms_fwd": {str(w): round(times[("fwd", w)], 4) for w in FWD_WARPS},
-                     "sample_paths": sample.n}
+            entry = self.table.get(sig, {})
+            if "fwd" in entry and "ms_fwd" in entry:
+                fwd = self.lookup(sig, False)
+                fwd = (fwd[0], fwd[2], fwd[3])
+            else:
+                tf = {sh: self.timer("fwd", stage, sample, q, S, prec, sh) for sh in FWD_SHAPES}
+                fwd = _pick(tf)
+                entry = {"fwd": list(fwd), "ms_fwd": {shape_key(sh): round(ms, 4) for sh, ms in tf.items()},
+                         "sample_paths": sample.n}
+                self.log += [(sig, "fwd", sh, ms) for sh, ms in tf.items()]
             if backward:
-                for w in BWD_WARPS:
-                    times[("bwd", w)] = self.timer("bwd", stage, sample, q, S, prec, w)
-                entry["bwd"] = _pick({w: times[("bwd", w)] for w in BWD_WARPS})
-                entry["ms_bwd"] = {str(w): round(times[("bwd", w)], 4) for w in BWD_WARPS}
-            for (kind, w), ms in times.items():
-                self.log.append((sig, kind, w, ms))
+                tb = {w: self.timer("bwd", stage, sample, q, S, prec, w) for w in BWD_WARPS}
+                entry["bwd"] = _pick(tb)
+                entry["ms_bwd"] = {str(w): round(ms, 4) for w, ms in tb.items()}
+                self.log += [(sig, "bwd", w, ms) for w, ms in tb.items()]
             self.table[sig] = entry
             self._save()
-            return entry["fwd"], entry.get("bwd", 0)
+            return fwd[0], entry.get("bwd", 0), fwd[1], fwd[2]
 
 
-def _pick(ms: dict, tol: float = 0.01) -> int:
-    """The widest shape within tol of the fastest (timing noise does not move the choice off the default)."""
+def _preference(shape):
+    """Order among near-ties: the default variant first, then the widest CTA."""
+    if isinstance(shape, tuple):
+        w, r, t = shape
+        return (r + t, -w)
+    return (0, -shape)
+
+
+def _pick(ms: dict, tol: float = 0.01):
+    """The preferred shape within tol of the fastest (timing noise does not move the choice off the default)."""
     best = min(ms.values())
-    return max(w for w, t in ms.items() if t <= best * (1 + tol))
+    return min((sh for sh, t in ms.items() if t <= best * (1 + tol)), key=_preference)
 
 
-def _time_candidate(kind: str, stage, batch, q, S, prec: int, warps: int, reps: int = 3) -> float:
-    """Milliseconds of the forward (kind 'fwd') or adjoint ('bwd') call on batch with `warps` warps per CTA."""
+def _time_candidate(kind: str, stage, batch, q, S, prec: int, shape, reps: int = 3) -> float:
+    """Milliseconds of the forward (kind 'fwd', shape = (warps, register budget, t staging)) or adjoint ('bwd',
+    shape = warps) call on batch."""
     lib = stage._lib
     coords = batch.coords.contiguous()
-    fw, bw = (warps, 0) if kind == "fwd" else (0, warps)
+    if kind == "fwd":
+        fw, bw, r, t = shape[0], 0, shape[1], shape[2]
+    else:
+        fw, bw, r, t = 0, shape, 0, 0
     _lib.check(lib.fg_stage_set_launch(stage._h, fw, bw))
+    _lib.check(lib.fg_stage_set_fused_variant(stage._h, r, t))
     try:
         with torch.no_grad():
             if kind == "fwd":
@@ -143,7 +177,9 @@ def _time_candidate(kind: str, stage, batch, q, S, prec: int, warps: int, reps: 
                 ms.append(e0.elapsed_time(e1))
         return float(np.median(ms))
     finally:
-        _lib.check(lib.fg_stage_set_launch(stage._h, *stage._launch))
+        fw, bw, r, t = stage._launch
+        _lib.check(lib.fg_stage_set_launch(stage._h, fw, bw))
+        _lib.check(lib.fg_stage_set_fused_variant(stage._h, r, t))
 
 
 _default = None

@@ -37,8 +37,8 @@ def _headers_mtime() -> float:
 
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False, out: Path | None = None,
           defines: dict | None = None) -> Path:
-    """Compile (if stale) and return the library path.  out/defines build a variant elsewhere (preprocessor
-    definitions such as FG_FUSED_MIN_BLOCKS) for the autotuner's offline comparisons."""
+    """Compile (if stale) and return the library path.  out/defines build a variant elsewhere (with preprocessor
+    definitions) for offline comparisons."""
     out_dir = OUT if out is None else Path(out)
     lib = out_dir / LIB.name
     out_dir.mkdir(parents=True, exist_ok=True)

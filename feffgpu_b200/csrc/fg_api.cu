@@ -35,6 +35,7 @@ struct fg_stage {
     int num_sms = 148;
     int max_smem = 227 * 1024;
     int fwd_warps = 0, bwd_warps = 0;   // launch shape of this stage's calls, 0 = the process default
+    int fused_regs_alt = 0, fused_stage_t = 0;   // the fused forward's register budget and t-matrix staging
     // device address of the no-allocation scratch in this stage's context, looked up by its first
     // fg_chi_reduce_noalloc call (a device reset invalidates the stage, and with it this address)
     void *noalloc_scratch = nullptr;
@@ -183,6 +184,16 @@ extern "C" fg_status fg_stage_set_launch(fg_stage *s, int32_t fwd_warps, int32_t
     if (fwd_warps < 0 || fwd_warps > 8 || bwd_warps < 0 || bwd_warps > 8) return fail(FG_ERR_VALUE, "warps must be 0..8");
     s->fwd_warps = fwd_warps;
     s->bwd_warps = bwd_warps;
+    return FG_OK;
+}
+
+extern "C" fg_status fg_stage_set_fused_variant(fg_stage *s, int32_t regs_alt, int32_t stage_t)
+{
+    if (!s) return fail(FG_ERR_VALUE, "null stage");
+    if ((regs_alt != 0 && regs_alt != 1) || (stage_t != 0 && stage_t != 1))
+        return fail(FG_ERR_VALUE, "regs_alt and stage_t must be 0 or 1");
+    s->fused_regs_alt = regs_alt;
+    s->fused_stage_t = stage_t;
     return FG_OK;
 }
 
@@ -363,6 +374,14 @@ fg_status set_device(const fg_stage *s)
 
 int fwd_warps(const fg_stage *s) { return s->fwd_warps ? s->fwd_warps : g_fwd_warps; }
 int bwd_warps(const fg_stage *s) { return s->bwd_warps ? s->bwd_warps : g_bwd_warps; }
+FusedShape fused_shape(const fg_stage *s)
+{
+    FusedShape f;
+    f.warps = fwd_warps(s);
+    f.regs_alt = s->fused_regs_alt != 0;
+    f.stage_t = s->fused_stage_t != 0;
+    return f;
+}
 
 StageView view(const fg_stage *s) { return StageView{s->E, s->L1, s->nph1, s->num_sms, s->ilinit, s->max_smem}; }
 
@@ -508,7 +527,7 @@ extern "C" fg_status fg_chi_reduce(const fg_stage *s, fg_precision prec, const f
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (fg_status rc = by_kind(s, prec, [&](auto L, const auto &T) {
             return decltype(L)::fused(sv, T, P, NK, q, S, span, rows, cchi_save, reff_save,
-                                      static_cast<unsigned char *>(workspace), fwd_warps(s), st);
+                                      static_cast<unsigned char *>(workspace), fused_shape(s), st);
         }))
         return rc;
     return read_status(reinterpret_cast<const int *>(static_cast<unsigned char *>(workspace) + kStatusOffset), st);
@@ -594,7 +613,7 @@ extern "C" fg_status fg_chi_reduce_noalloc(const fg_stage *s, fg_precision prec,
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (fg_status rc = by_kind(s, prec, [&](auto L, const auto &T) {
             return decltype(L)::fused(sv, T, P, NK, q, S, span, rows, nullptr, nullptr,
-                                      static_cast<unsigned char *>(ws), fwd_warps(s), st);
+                                      static_cast<unsigned char *>(ws), fused_shape(s), st);
         }))
         return rc;
     return read_status(reinterpret_cast<const int *>(static_cast<unsigned char *>(ws) + kStatusOffset), st);

@@ -143,7 +143,7 @@ template <typename R, int NCAN> __device__ __forceinline__ void load_row(const R
 // measured slower).
 template <typename R, int KIND, int NR, int NC, int UNR = 1>
 __device__ __forceinline__ void accumulate_f(C2<R> (&acc)[RepTab<KIND, NR, NC>().n], const R *dhk,
-                                             const C2<R> *tlk, int E, int ilx, C2<R> z_in, C2<R> z_out)
+                                             const C2<R> *tlk, int tstride, int ilx, C2<R> z_in, C2<R> z_out)
 {
     constexpr RepTab<KIND, NR, NC> RT{};
     constexpr LamTab L = lamtab(KIND);
@@ -164,12 +164,12 @@ __device__ __forceinline__ void accumulate_f(C2<R> (&acc)[RepTab<KIND, NR, NC>()
     po[1] = C2<R>{R(1), R(0)};
     co[1] = C2<R>{R(1), R(0)};
     // t-matrix of the next two partial waves in flight (the table is read from L2)
-    C2<R> t1 = tlk[E], t2 = ilx >= 2 ? tlk[(size_t)2 * E] : cz<R>();
+    C2<R> t1 = tlk[tstride], t2 = ilx >= 2 ? tlk[(size_t)2 * tstride] : cz<R>();
 #pragma unroll UNR
     for (int il = 1; il <= ilx; ++il) {
         const C2<R> t = t1;
         t1 = t2;
-        if (il + 2 <= ilx) t2 = tlk[(size_t)(il + 2) * E];
+        if (il + 2 <= ilx) t2 = tlk[(size_t)(il + 2) * tstride];
         R d[NCAN];
         load_row<R, NCAN>(dhk + (size_t)il * DS, d);
         C2<R> tco[CO + 1];
@@ -322,8 +322,26 @@ __device__ __forceinline__ C2<R> cfac(const WarpPath<R> &g, const Tables<R> &T, 
 // matrix -- the first matrix's columns beyond laml0x and the last one's rows beyond laml0x are computed and not
 // used -- so that one unrolled loop serves the whole chain: measured on B200 the smaller instruction footprint
 // outweighs the extra entries (57.4 vs 62.4 ms for the 2e5-path benchmark launch).
+// One lane's t-matrix column t(ip, l, e), l = 1..ilx, into its column of a warp's staging tile (row stride 32
+// entries), by asynchronous copies to shared memory; the lane waits for its own copies only.
+template <typename R>
+__device__ __forceinline__ void stage_t_column(C2<R> *tile_col, const C2<R> *tg, int E, int ilx)
+{
+    for (int il = 1; il <= ilx; ++il) {
+        const unsigned s = (unsigned)__cvta_generic_to_shared(tile_col + il * 32);
+        if constexpr (sizeof(C2<R>) == 8)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(tg + (size_t)il * E) : "memory");
+        else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(tg + (size_t)il * E) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// tst: the warp's t-matrix staging tile ((L1 + 1) x 32 entries, shared memory) or null to read the table through L1.
 template <typename R, int KIND>
-__device__ C2<R> energy_ms(const WarpPath<R> &g, const R *dh, const Tables<R> &T, int e, int nleg)
+__device__ C2<R> energy_ms(const WarpPath<R> &g, const R *dh, const Tables<R> &T, int e, int nleg,
+                           C2<R> *tst = nullptr)
 {
     constexpr LamTab L = lamtab(KIND);
     constexpr int N = L.N, N0 = L.N0, MM = L.MM, DS = dstride(MM);
@@ -336,8 +354,17 @@ __device__ C2<R> energy_ms(const WarpPath<R> &g, const R *dh, const Tables<R> &T
     for (int k = 1; k <= nsc; ++k) {
         C2<R> acc[RT.n];
         const int ip = g.ip[k];
-        accumulate_f<R, KIND, N, N, sizeof(R) == 4 ? 2 : 1>(acc, dh + (k - 1) * dleg, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
-                                    zfac(cscl(ck, (R)g.ri[k + 1])), zfac(cscl(ck, (R)g.ri[k])));
+        const int ilx = T.lmax[ip * E + e] + 1;
+        const C2<R> *tk = T.tl + ip * tlip + e;
+        int tstride = E;
+        if (tst) {
+            C2<R> *col = tst + (threadIdx.x & 31);
+            stage_t_column<R>(col, tk, E, ilx);
+            tk = col;
+            tstride = 32;
+        }
+        accumulate_f<R, KIND, N, N, sizeof(R) == 4 ? 2 : 1>(acc, dh + (k - 1) * dleg, tk, tstride, ilx,
+                                                           zfac(cscl(ck, (R)g.ri[k + 1])), zfac(cscl(ck, (R)g.ri[k])));
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
         C2<R> Pn[N][N0];

@@ -20,10 +20,13 @@ template <typename R> __host__ __device__ inline size_t table_bytes(int L1, int 
     const size_t p = with_signal ? 2 * align_up((size_t)E * sizeof(double), 16) : 0;
     return d > p ? d : p;
 }
-template <typename R> inline size_t warp_bytes(int L1, int nsc_max, int MM, int E, bool with_signal)
+// (fused kernel: then the signal and, with stage_t, the t-matrix staging tile of (L1 + 1) x 32 entries)
+template <typename R> inline size_t warp_bytes(int L1, int nsc_max, int MM, int E, bool with_signal,
+                                               bool stage_t = false)
 {
     size_t b = geo_bytes<R>() + table_bytes<R>(L1, nsc_max, MM, E, with_signal);
     if (with_signal) b += align_up((size_t)E * sizeof(C2<R>), 16);
+    if (with_signal && stage_t) b += (size_t)(L1 + 1) * 32 * sizeof(C2<R>);
     return b;
 }
 
@@ -36,7 +39,8 @@ template <int EDGE> struct Kinds {
 };
 
 template <typename R, int EDGE>
-__device__ __forceinline__ C2<R> path_energy(const WarpPath<R> &g, const R *dh, const Tables<R> &T, int e, int nleg)
+__device__ __forceinline__ C2<R> path_energy(const WarpPath<R> &g, const R *dh, const Tables<R> &T, int e, int nleg,
+                                             C2<R> *tst = nullptr)
 {
     using K = Kinds<EDGE>;
     if (nleg == 2) {
@@ -45,7 +49,7 @@ __device__ __forceinline__ C2<R> path_energy(const WarpPath<R> &g, const R *dh, 
         else
             return energy_ss_col<R, K::SS>(g, dh, T, e);
     }
-    return energy_ms<R, K::MS>(g, dh, T, e, nleg);
+    return energy_ms<R, K::MS>(g, dh, T, e, nleg, tst);
 }
 
 // One warp per path, grid-stride over the paths of one leg count: cchi (B, E) and reff (B).
@@ -168,14 +172,20 @@ struct PathsDev {
 // signal at all E, its amplitude and unwrapped phase, and the weighted fine-grid terms
 // deg exp(-2 sigma2 q^2) a(q) sin(phi(q) + 2 q reff), each added exactly to its row (fixed_add).  The batch's
 // indices were checked by k_validate before the launch: with a malformed batch the kernel returns at once.
-#ifndef FG_FUSED_MIN_BLOCKS
-#define FG_FUSED_MIN_BLOCKS 2
-#endif
-template <typename R, int EDGE>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
+//
+// MINB, the blocks of 128 threads per SM the registers are budgeted for, and stage_t, whether the t-matrix columns of
+// a scatterer go through a shared-memory tile (asynchronous copies) or are read through L1, are tunable (FusedShape);
+// neither changes a result bit.
+template <typename R> struct FusedMinBlocks {
+    static constexpr int def = sizeof(R) == 4 ? 2 : 1;   // measured fastest on B200 for the benchmark workloads
+    static constexpr int alt = 3;                         // FP64 at 2 compiles as at 1 (255 registers fit two CTAs)
+};
+template <typename R, int EDGE, int MINB>
+__global__ void __launch_bounds__(128, MINB)
     k_fused(Tables<R> T, PathsDev P, int NK, const double *__restrict__ q, const double *__restrict__ S,
             const int *__restrict__ span, unsigned long long *__restrict__ racc, C2<R> *__restrict__ cchi_save,
-            double *__restrict__ reff_save, unsigned long long *counter, int *status, int nsc_max, size_t wbytes)
+            double *__restrict__ reff_save, unsigned long long *counter, int *status, int nsc_max, size_t wbytes,
+            int stage_t)
 {
     using K = Kinds<EDGE>;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -186,6 +196,9 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
     WarpPath<R> &g = *reinterpret_cast<WarpPath<R> *>(base);
     R *dh = reinterpret_cast<R *>(base + geo_bytes<R>());
     C2<R> *cbuf = reinterpret_cast<C2<R> *>(base + geo_bytes<R>() + table_bytes<R>(L1, nsc_max, K::MM, E, true));
+    C2<R> *tst = stage_t ? reinterpret_cast<C2<R> *>(reinterpret_cast<unsigned char *>(cbuf) +
+                                                     align_up((size_t)E * sizeof(C2<R>), 16))
+                         : nullptr;
     double *pha = reinterpret_cast<double *>(dh);   // the tables are dead once the path's energies are done
     double *amp = pha + align_up((size_t)E, 2);
     for (;;) {
@@ -200,7 +213,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FG_FUSED_MIN_BLOCKS : 1)
         for (int e0 = first_chunk(E); e0 < E; e0 += 32) {
             const int e = e0 + lane;
             if (e >= 0 && e < E) {
-                const C2<R> v = path_energy<R, EDGE>(g, dh, T, e, nleg);
+                const C2<R> v = path_energy<R, EDGE>(g, dh, T, e, nleg, tst);
                 cbuf[e] = v;
                 if (cchi_save) cchi_save[p * E + e] = v;
             }
@@ -276,7 +289,7 @@ fg_status Launch<R, EDGE>::cchi(const StageView &sv, const Tables<R> &T, int64_t
 template <typename R, int EDGE>
 fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const fg_paths *P, int NK, const double *q,
                                  const double *S, const int *span, double *rows, void *cchi_save, double *reff_save,
-                                 unsigned char *ws, int warps, cudaStream_t st)
+                                 unsigned char *ws, const FusedShape &shape, cudaStream_t st)
 {
     using K = Kinds<EDGE>;
     unsigned long long *counter = reinterpret_cast<unsigned long long *>(ws);
@@ -286,16 +299,16 @@ fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const 
     if (fg_status rc = launch_validate(P, sv.nph1, status, st)) return rc;
     if (P->n > 0) {
         const int nsc_max = P->nleg_max - 1;
-        const size_t wb = warp_bytes<R>(sv.L1, nsc_max, K::MM, sv.E, true);
-        warps = fit_warps(warps > 4 ? 4 : warps, wb, sv.max_smem);
+        const size_t wb = warp_bytes<R>(sv.L1, nsc_max, K::MM, sv.E, true, shape.stage_t);
+        const int warps = fit_warps(shape.warps > 4 ? 4 : shape.warps, wb, sv.max_smem);
         const int threads = warps * 32;
-        auto kern = k_fused<R, EDGE>;
+        auto kern = shape.regs_alt ? k_fused<R, EDGE, FusedMinBlocks<R>::alt> : k_fused<R, EDGE, FusedMinBlocks<R>::def>;
         int blocks = 0;
         if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, P->n, blocks)) return rc;
         PathsDev pd{P->n, P->nleg_max, P->nrows, P->coords, P->ipots, P->nleg, P->deg, P->sigma2, P->order, P->row};
         timer_begin(st);
         kern<<<blocks, threads, wb * warps, st>>>(T, pd, NK, q, S, span, racc, static_cast<C2<R> *>(cchi_save),
-                                                  reff_save, counter, status, nsc_max, wb);
+                                                  reff_save, counter, status, nsc_max, wb, shape.stage_t ? 1 : 0);
         timer_end(st);
         FG_CUDA(cudaGetLastError());
     }

@@ -31,6 +31,15 @@ inline int fit_warps(int want, size_t per_warp, int max_smem)
     return w;
 }
 
+// Launch shape of the fused forward kernel: warps per block (paths per CTA), the register budget (regs_alt: three
+// blocks of 128 threads per SM instead of the default two in FP32, one in FP64) and whether the t-matrix columns of each scatterer are staged
+// in a shared-memory tile (stage_t) or read through L1.  No shape changes a result bit.
+struct FusedShape {
+    int warps = 4;
+    bool regs_alt = false;
+    bool stage_t = false;
+};
+
 // Per precision R and initial-state class EDGE (l_init + 1 = 1, 2, 3: K/L1, L2/L3/M2/M3, M4/M5/N4/N5 edges).
 template <typename R, int EDGE> struct Launch {
     static fg_status cchi(const StageView &sv, const Tables<R> &T, int64_t B, int nleg, const void *coords,
@@ -38,7 +47,7 @@ template <typename R, int EDGE> struct Launch {
                           cudaStream_t st);
     static fg_status fused(const StageView &sv, const Tables<R> &T, const fg_paths *P, int NK, const double *q,
                            const double *S, const int *span, double *rows, void *cchi_save, double *reff_save,
-                           unsigned char *ws, int warps, cudaStream_t st);
+                           unsigned char *ws, const FusedShape &shape, cudaStream_t st);
     static fg_status cchi_bwd(const StageView &sv, const Tables<R> &T, int64_t B, int nleg, const void *coords,
                               int coords_f64, const int64_t *ipots, const void *grad_cchi, const void *grad_reff,
                               void *grad_coords, unsigned char *ws, int warps, cudaStream_t st);

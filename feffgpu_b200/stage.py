@@ -100,7 +100,7 @@ class GPUPathStage:
         # launch shape (warps per CTA of the forward and adjoint kernels; 0 = the library default), per workload
         # when autotuning (feffgpu_b200.autotune)
         self.autotune = bool(autotune)
-        self._launch = (0, 0)
+        self._launch = (0, 0, 0, 0)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -278,14 +278,19 @@ class GPUPathStage:
         return dict(shared, mag=mag, phase=phase)
 
     # -- launch shape ---------------------------------------------------------------------------------------
-    def set_launch(self, fwd_warps: int = 0, bwd_warps: int = 0) -> None:
-        """Warps per CTA of this stage's forward and adjoint kernels (0 = the library default)."""
-        if (fwd_warps, bwd_warps) != self._launch:
-            _lib.check(self._lib.fg_stage_set_launch(self._h, int(fwd_warps), int(bwd_warps)))
-            self._launch = (int(fwd_warps), int(bwd_warps))
+    def set_launch(self, fwd_warps: int = 0, bwd_warps: int = 0, regs_alt: int = 0, stage_t: int = 0) -> None:
+        """Warps per CTA of this stage's forward and adjoint kernels (0 = the library default), and the fused
+        forward's register budget (1: three CTAs of 128 threads per SM) and t-matrix staging (1: through shared
+        memory)."""
+        want = (int(fwd_warps), int(bwd_warps), int(regs_alt), int(stage_t))
+        if want != self._launch:
+            _lib.check(self._lib.fg_stage_set_launch(self._h, want[0], want[1]))
+            _lib.check(self._lib.fg_stage_set_fused_variant(self._h, want[2], want[3]))
+            self._launch = want
 
     def tune(self, batch: "PathBatch", q, S=None, backward: bool = True, dtype=None, tuner=None):
-        """Times the launch shapes on (a sample of) batch, applies and returns the fastest (fwd, bwd) warps."""
+        """Times the launch shapes on (a sample of) batch, applies and returns the fastest
+        (fwd_warps, bwd_warps, regs_alt, stage_t)."""
         from .autotune import default_tuner
         if S is None:
             S = self.linear_matrix(q)

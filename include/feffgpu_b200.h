@@ -196,6 +196,13 @@ FG_API fg_status fg_fp32_fma_peak(double *tflops, void *stream);
 FG_API fg_status fg_set_launch(int32_t fwd_warps, int32_t bwd_warps);
 FG_API fg_status fg_stage_set_launch(fg_stage *stage, int32_t fwd_warps, int32_t bwd_warps);
 
+/* Variant of the fused forward (fg_chi_reduce, fg_chi_reduce_noalloc) on one stage, for the autotuner: regs_alt = 1
+ * budgets the registers for three blocks of 128 threads per SM (12 warps; the default budget is for two in FP32 and
+ * one in FP64); stage_t = 1 copies each scatterer's t-matrix column into a shared-memory tile per warp (asynchronous
+ * copies) instead of reading it through L1.  Both 0 (the default) are the fastest measured on B200 for the benchmark
+ * workloads.  No variant changes a result bit.  No reference counterpart. */
+FG_API fg_status fg_stage_set_fused_variant(fg_stage *stage, int32_t regs_alt, int32_t stage_t);
+
 /* ---------------------------------------------------------------------------------------------- path finder
  * The enumeration of the reference's GPUPathFinder.enumerate (src/feffgpu/pathfinder.py:213-271; its _longer_paths,
  * :159-211, for five and more legs), batched over absorber slots; the host driver (feffgpu_b200/pathfinder.py)

@@ -24,26 +24,44 @@ def _batch(counts, seed=0):
 def test_choice_and_persistence(tmp_path, monkeypatch):
     monkeypatch.setattr(A, "gpu_name", lambda d: "FakeGPU")
     calls = []
+    fwd_ms = {(1, 0, 0): 3.0, (2, 0, 0): 2.0, (4, 0, 0): 2.5, (1, 1, 0): 2.6, (2, 1, 0): 1.995, (4, 1, 0): 2.9,
+              (1, 0, 1): 3.3, (2, 0, 1): 2.8, (4, 0, 1): 3.1}
 
-    def timer(kind, stage, batch, q, S, prec, w):
-        calls.append((kind, w))
-        return {("fwd", 1): 3.0, ("fwd", 2): 2.0, ("fwd", 4): 2.5, ("bwd", 1): 9.0, ("bwd", 2): 9.5,
-                ("bwd", 4): 9.05}[(kind, w)]
+    def timer(kind, stage, batch, q, S, prec, shape):
+        calls.append((kind, shape))
+        if kind == "fwd":
+            return fwd_ms[shape]
+        return {1: 9.0, 2: 9.5, 4: 9.05}[shape]
 
     b = _batch({2: 10, 5: 30, 8: 4})
     q = torch.arange(401) * 0.05
     t = A.Autotuner(tmp_path / "t.json", timer=timer)
-    assert t.tune(_Stage(), b, q, None, 0, backward=True) == (2, 4)     # near-ties go to the wider shape
-    assert len(calls) == 6
+    # near-ties go to the default variant, then to the wider shape
+    assert t.tune(_Stage(), b, q, None, 0, backward=True) == (2, 4, 0, 0)
+    assert len(calls) == len(A.FWD_SHAPES) + len(A.BWD_WARPS)
     # a second tuner reads the file: no timing
     t2 = A.Autotuner(tmp_path / "t.json", timer=timer)
-    assert t2.tune(_Stage(), b, q, None, 0, backward=True) == (2, 4)
-    assert len(calls) == 6
-    # forward-only entries are completed when the adjoint is asked for later
+    assert t2.tune(_Stage(), b, q, None, 0, backward=True) == (2, 4, 0, 0)
+    assert len(calls) == len(A.FWD_SHAPES) + len(A.BWD_WARPS)
+    # forward-only entries are completed when the adjoint is asked for later, without timing the forward again
     b2 = _batch({3: 20})
-    assert t2.tune(_Stage(), b2, q, None, 0, backward=False) == (2, 0)
+    fwd_ms[(4, 0, 1)] = 1.0                      # a clear winner off the default variant is taken
+    assert t2.tune(_Stage(), b2, q, None, 0, backward=False) == (4, 0, 0, 1)
     assert t2.lookup(A.signature(_Stage(), b2, 401, 0), backward=True) is None
-    assert t2.tune(_Stage(), b2, q, None, 0, backward=True) == (2, 4)
+    n = len(calls)
+    assert t2.tune(_Stage(), b2, q, None, 0, backward=True) == (4, 4, 0, 1)
+    assert len(calls) == n + len(A.BWD_WARPS)
+
+
+def test_reads_entries_of_warps_only(tmp_path, monkeypatch):
+    """A cache entry holding the forward warps alone (no variant) reads as the default variant."""
+    import json
+    monkeypatch.setattr(A, "gpu_name", lambda d: "FakeGPU")
+    b = _batch({3: 20})
+    sig = A.signature(_Stage(), b, 401, 0)
+    (tmp_path / "t.json").write_text(json.dumps({sig: {"fwd": 2, "bwd": 1, "ms_fwd": {"2": 1.0}}}))
+    t = A.Autotuner(tmp_path / "t.json", timer=None)
+    assert t.lookup(sig, backward=True) == (2, 1, 0, 0)
 
 
 def test_signature_separates_workloads(monkeypatch):

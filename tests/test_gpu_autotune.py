@@ -25,31 +25,31 @@ def _batch(seed=3):
 @pytest.mark.parametrize("dtype", [torch.complex64, torch.complex128])
 def test_shapes_bit_identical_and_tuner_choice(dtype, tmp_path):
     from feffgpu_b200 import GPUPathStage
-    from feffgpu_b200.autotune import BWD_WARPS, FWD_WARPS, Autotuner
+    from feffgpu_b200.autotune import BWD_WARPS, FWD_SHAPES, Autotuner
     st = GPUPathStage(cfg2_phase(), device="cuda", dtype=dtype)
     b = _batch()
     S = st.linear_matrix(Q)
     s2 = torch.full((b.n,), 0.002, dtype=torch.float64, device="cuda")
     w = torch.randn(b.nrows, len(Q), dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
     ref = None
-    for fw in FWD_WARPS:
-        for bw in BWD_WARPS:
-            st.set_launch(fw, bw)
-            x = b.coords.clone().requires_grad_(True)
-            s = s2.clone().requires_grad_(True)
-            rows = st.chi_reduce(b, Q, S, coords=x, sigma2=s)
-            (rows * w).sum().backward()
-            out = (rows.detach(), x.grad, s.grad)
-            if ref is None:
-                ref = out
-            else:
-                assert all(torch.equal(a, r) for a, r in zip(out, ref)), (fw, bw)
+    shapes = [(fw, 4, r, t_) for fw, r, t_ in FWD_SHAPES] + [(4, bw, 0, 0) for bw in BWD_WARPS]
+    for shape in shapes:                         # every forward shape, every adjoint shape
+        st.set_launch(*shape)
+        x = b.coords.clone().requires_grad_(True)
+        s = s2.clone().requires_grad_(True)
+        rows = st.chi_reduce(b, Q, S, coords=x, sigma2=s)
+        (rows * w).sum().backward()
+        out = (rows.detach(), x.grad, s.grad)
+        if ref is None:
+            ref = out
+        else:
+            assert all(torch.equal(a, r) for a, r in zip(out, ref)), shape
     t = Autotuner(tmp_path / "tune.json")
     st.set_launch(0, 0)
-    fw, bw = st.tune(b, Q, S, backward=True, tuner=t)
-    assert fw in FWD_WARPS and bw in BWD_WARPS and st._launch == (fw, bw)
-    assert len(t.log) == len(FWD_WARPS) + len(BWD_WARPS) and all(ms > 0 for *_, ms in t.log)
-    print(f"{dtype}: tuned fwd {fw} bwd {bw}; " + ", ".join(f"{k}{w_}={ms:.3f}ms" for _, k, w_, ms in t.log))
+    fw, bw, r, t_ = st.tune(b, Q, S, backward=True, tuner=t)
+    assert (fw, r, t_) in FWD_SHAPES and bw in BWD_WARPS and st._launch == (fw, bw, r, t_)
+    assert len(t.log) == len(FWD_SHAPES) + len(BWD_WARPS) and all(ms > 0 for *_, ms in t.log)
+    print(f"{dtype}: tuned fwd {fw}/{r}/{t_} bwd {bw}; " + ", ".join(f"{k}{w_}={ms:.3f}ms" for _, k, w_, ms in t.log))
     # a stage that tunes itself on first use returns the same numbers
     auto = GPUPathStage(cfg2_phase(), device="cuda", dtype=dtype, autotune=True)
     import feffgpu_b200.autotune as A
@@ -58,6 +58,6 @@ def test_shapes_bit_identical_and_tuner_choice(dtype, tmp_path):
     s = s2.clone().requires_grad_(True)
     rows = auto.chi_reduce(b, Q, S, coords=x, sigma2=s)
     (rows * w).sum().backward()
-    assert auto._launch != (0, 0)
+    assert auto._launch != (0, 0, 0, 0)
     assert torch.equal(rows.detach(), ref[0]) and torch.equal(x.grad, ref[1]) and torch.equal(s.grad, ref[2])
     A._default = None
