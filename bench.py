@@ -560,7 +560,7 @@ def frontends_leg(dev):
     * RMC: MultipleScattering.full_pass and full_gradient of the same frame for 32 absorbers, 3 legs, critpw 2
       (src/feffgpu/exafs/forward.py:691-723).
     The front ends' own orchestration (per-absorber finder calls, chunk loops, host syncs) is timed too: this is what
-    the one-line drop-in buys, not the fused API's figure."""
+    the one-line drop-in buys, not the fused API's figure.  Each figure is the median of three timed calls."""
     import dataclasses
     import torch
     ref = ROOT / "baseline" / "_ref"
@@ -585,13 +585,16 @@ def frontends_leg(dev):
     symbols = np.array(["Fe"] * len(pos))
     k = np.arange(401) * 0.05
 
-    def wall(fn):
+    def wall(fn, reps=3):
         fn()
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        fn()
-        torch.cuda.synchronize(dev)
-        return (time.perf_counter() - t0) * 1e3
+        ms = []
+        for _ in range(reps):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize(dev)
+            ms.append((time.perf_counter() - t0) * 1e3)
+        return float(np.median(ms))
 
     def md():
         es = EdgeSpectra(P, "Fe", {"Fe": 1}, ["Fe"], k, rpath=5.5, nleg=3, criteria=2.0, device=str(dev))

@@ -101,12 +101,13 @@ fg_status scan_counts(int64_t P, const int64_t *P_dev, const int32_t *count, int
                       cudaStream_t st);
 
 // The path finder's description of B paths with a warp per path (fg_paths.cu), for a call on one absorber; paths with
-// keep[b] == 0 are skipped (keep may be null)
+// keep[b] == 0 are skipped (keep may be null); c1 (B, 3) and ip1 (B), when given, receive each path's first atom
+// (for single scattering: the candidate) and its potential.
 fg_status describe_paths_warp(int64_t B, int32_t nleg, const int32_t *seq, const int32_t *slot, const int64_t *cand_off,
                               const float *cand_rel, const int64_t *cand_atom, const int64_t *ipot_of,
                               const int64_t *absorbers, const fg_pf_tables *T, const uint8_t *keep, float *coords,
-                              int64_t *ipots, int64_t *atoms, float *rtot, float *xport, int64_t *key,
-                              cudaStream_t st);
+                              int64_t *ipots, int64_t *atoms, float *rtot, float *xport, int64_t *key, float *c1,
+                              int64_t *ip1, cudaStream_t st);
 
 // Events around the main kernel of a call when kernel timing is on (fg_set_kernel_timing)
 void timer_begin(cudaStream_t st);

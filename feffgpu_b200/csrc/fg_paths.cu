@@ -427,7 +427,8 @@ __global__ void __launch_bounds__(32 * kDescribeWarps)
                     const int64_t *__restrict__ cand_atom, const int64_t *__restrict__ ipot_of,
                     const int64_t *__restrict__ absorbers, fg_pf_tables T, const uint8_t *__restrict__ keep,
                     float *__restrict__ coords, int64_t *__restrict__ ipots, int64_t *__restrict__ atoms,
-                    float *__restrict__ rtot_out, float *__restrict__ xport, int64_t *__restrict__ key)
+                    float *__restrict__ rtot_out, float *__restrict__ xport, int64_t *__restrict__ key,
+                    float *__restrict__ c1, int64_t *__restrict__ ip1)
 {
     extern __shared__ float terms_all[];                       // (kDescribeWarps, E)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -437,6 +438,12 @@ __global__ void __launch_bounds__(32 * kDescribeWarps)
         if (keep && !keep[b]) continue;                        // warp-uniform
         PathGeom G;
         path_geom(b, nleg, seq, slot, C, cand_atom, ipot_of, absorbers, lane == 0, coords, ipots, atoms, rtot_out, G);
+        if (lane == 0 && c1) {
+            c1[3 * b] = G.px[1];
+            c1[3 * b + 1] = G.py[1];
+            c1[3 * b + 2] = G.pz[1];
+        }
+        if (lane == 0 && ip1) ip1[b] = G.ip[1];
         if (xport) {
             int ib[kMaxLeg];
             for (int j = 0; j < m; ++j) ib[j] = indbet(G.cb[j]);
@@ -589,8 +596,8 @@ fg_status scan_counts(int64_t P, const int64_t *P_dev, const int32_t *count, int
 fg_status describe_paths_warp(int64_t B, int32_t nleg, const int32_t *seq, const int32_t *slot, const int64_t *cand_off,
                               const float *cand_rel, const int64_t *cand_atom, const int64_t *ipot_of,
                               const int64_t *absorbers, const fg_pf_tables *T, const uint8_t *keep, float *coords,
-                              int64_t *ipots, int64_t *atoms, float *rtot, float *xport, int64_t *key,
-                              cudaStream_t st)
+                              int64_t *ipots, int64_t *atoms, float *rtot, float *xport, int64_t *key, float *c1,
+                              int64_t *ip1, cudaStream_t st)
 {
     if (B == 0) return FG_OK;
     const fg_pf_tables t = *T;
@@ -600,7 +607,7 @@ fg_status describe_paths_warp(int64_t B, int32_t nleg, const int32_t *seq, const
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((B + kDescribeWarps - 1) / kDescribeWarps, 148 * 16));
     k_describe_warp<<<blocks, 32 * kDescribeWarps, smem, st>>>(B, nleg, seq, slot, Cands{cand_off, cand_rel}, cand_atom,
                                                                 ipot_of, absorbers, t, keep, coords, ipots, atoms,
-                                                                rtot, xport, key);
+                                                                rtot, xport, key, c1, ip1);
     FG_CUDA(cudaGetLastError());
     return FG_OK;
 }

@@ -47,25 +47,57 @@ fg_status finder_pool(cudaMemPool_t *out)
     return FG_OK;
 }
 
-// device scratch of one call, stream-ordered from the finder's pool
+// Device scratch of one call, stream-ordered from the finder's pool and handed out from a few large blocks (a call
+// needs about thirty arrays; one pool allocation each cost more host time than the kernels that fill them).  Two
+// regions: `get` for arrays that stay on the device, `get_host` for the fields the host reads after the last
+// synchronisation, which so lie in a few contiguous blocks that are copied to the host in one copy each.
 struct Scratch {
+    struct Block {
+        unsigned char *base = nullptr;
+        size_t used = 0, cap = 0;
+    };
+    static constexpr size_t kBlock = size_t(4) << 20;
     cudaStream_t st = nullptr;
     cudaMemPool_t pool = nullptr;
-    std::vector<void *> bufs;
+    std::vector<Block> dev, host;
+    fg_status take(std::vector<Block> &region, size_t bytes, void **out)
+    {
+        bytes = align_up(std::max<size_t>(bytes, 1), 256);
+        if (region.empty() || region.back().cap - region.back().used < bytes) {
+            if (!pool)
+                if (fg_status rc = finder_pool(&pool)) return rc;
+            Block b;
+            b.cap = std::max(bytes, kBlock);
+            void *p = nullptr;
+            FG_CUDA(cudaMallocFromPoolAsync(&p, b.cap, pool, st));
+            b.base = static_cast<unsigned char *>(p);
+            region.push_back(b);
+        }
+        Block &b = region.back();
+        *out = b.base + b.used;
+        b.used += bytes;
+        return FG_OK;
+    }
     template <typename T> fg_status get(size_t count, T **out)
     {
-        if (!pool)
-            if (fg_status rc = finder_pool(&pool)) return rc;
         void *p = nullptr;
-        FG_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(count, 1) * sizeof(T), pool, st));
-        bufs.push_back(p);
+        if (fg_status rc = take(dev, count * sizeof(T), &p)) return rc;
+        *out = static_cast<T *>(p);
+        return FG_OK;
+    }
+    template <typename T> fg_status get_host(size_t count, T **out)
+    {
+        void *p = nullptr;
+        if (fg_status rc = take(host, count * sizeof(T), &p)) return rc;
         *out = static_cast<T *>(p);
         return FG_OK;
     }
     void release()
     {
-        for (void *p : bufs) cudaFreeAsync(p, st);
-        bufs.clear();
+        for (const Block &b : dev) cudaFreeAsync(b.base, st);
+        for (const Block &b : host) cudaFreeAsync(b.base, st);
+        dev.clear();
+        host.clear();
     }
 };
 
@@ -338,18 +370,26 @@ extern "C" fg_status fg_pf_enumerate_one(const float *pos, int64_t n, float box,
     int64_t counts_h[2];
     std::memcpy(counts_h, hp, sizeof(counts_h));
     const int64_t nc = counts_h[0];
-    // a warp per path; sequences that are not paths (terminal flag 0) are skipped
+    // a warp per path; sequences that are not paths (terminal flag 0) are skipped.  The single-scattering call also
+    // writes each candidate's position and potential (c1, ip1) for the merges.
+    float *c1_dev = nullptr;
+    int64_t *ip1_dev = nullptr;
     auto describe = [&](fg_pf_leg &l, const int32_t *s, const int32_t *sl, bool want_key) -> fg_status {
         const int64_t B = l.nb;
         if (fg_status rc = S.get(B * l.nleg * 3, &l.coords)) return rc;
         if (fg_status rc = S.get(B * l.nleg, &l.ipots)) return rc;
         if (fg_status rc = S.get(B * (l.nleg - 1), &l.atoms)) return rc;
-        if (fg_status rc = S.get(B, &l.rtot)) return rc;
-        if (fg_status rc = S.get(B, &l.xport)) return rc;
+        if (fg_status rc = S.get_host(B, &l.rtot)) return rc;
+        if (fg_status rc = S.get_host(B, &l.xport)) return rc;
         if (want_key)
-            if (fg_status rc = S.get(B * 2 * l.nleg, &l.key)) return rc;
+            if (fg_status rc = S.get_host(B * 2 * l.nleg, &l.key)) return rc;
+        if (l.nleg == 2) {
+            if (fg_status rc = S.get_host(B * 3, &c1_dev)) return rc;
+            if (fg_status rc = S.get_host(B, &ip1_dev)) return rc;
+        }
         return describe_paths_warp(B, l.nleg, s, sl, d_off, cand_rel, cand_atom, ipot_of, d_ab, T, l.keep, l.coords,
-                                   l.ipots, l.atoms, l.rtot, l.xport, l.key, st);
+                                   l.ipots, l.atoms, l.rtot, l.xport, l.key, l.nleg == 2 ? c1_dev : nullptr,
+                                   l.nleg == 2 ? ip1_dev : nullptr, st);
     };
     std::vector<fg_pf_leg> &legs = r->legs;
     legs.reserve(kMaxLeg);
@@ -384,8 +424,8 @@ extern "C" fg_status fg_pf_enumerate_one(const float *pos, int64_t n, float box,
         fg_pf_leg l;
         l.nleg = m + 2;
         l.nb = Cn;
-        FG_TRY(S.get(Cn, &l.keep));
-        FG_TRY(S.get(Cn, &l.deg));
+        FG_TRY(S.get_host(Cn, &l.keep));
+        FG_TRY(S.get_host(Cn, &l.deg));
         FG_TRY(fg_pf_terminal(Cn, m + 1, cseq, cslot, d_off, l.keep, l.deg, stream));
         FG_TRY(describe(l, cseq, cslot, merge != 0));
         legs.push_back(l);
@@ -394,54 +434,37 @@ extern "C" fg_status fg_pf_enumerate_one(const float *pos, int64_t n, float box,
         len = clen;
         P = Cn;
     }
-    // the fields the merges and the cut read, in one copy through pinned memory
+    // the fields the merges and the cut read: one copy per block of the host region, through pinned memory
     size_t bytes = 0;
-    auto reserve = [&](size_t b) {
-        const size_t at = bytes;
-        bytes += (b + 15) / 16 * 16;
-        return at;
-    };
-    struct At { size_t xport, deg, rtot, keep, key; };
-    std::vector<At> at(legs.size());
-    for (size_t i = 0; i < legs.size(); ++i) {
-        const fg_pf_leg &l = legs[i];
-        at[i].xport = reserve(l.nb * sizeof(float));
-        at[i].rtot = reserve(l.nb * sizeof(float));
-        at[i].deg = l.deg ? reserve(l.nb * sizeof(float)) : 0;
-        at[i].keep = l.keep ? reserve(l.nb) : 0;
-        at[i].key = l.key ? reserve(l.nb * 2 * l.nleg * sizeof(int64_t)) : 0;
+    std::vector<size_t> at_block(S.host.size());
+    for (size_t i = 0; i < S.host.size(); ++i) {
+        at_block[i] = bytes;
+        bytes += align_up(S.host[i].used, 256);
     }
-    const size_t at_c1 = reserve(nc * 3 * sizeof(float)), at_ip1 = reserve(nc * sizeof(int64_t));
     FG_TRY(pinned(bytes, &hp));
-    auto d2h = [&](size_t o, const void *src, size_t b) {
-        return b ? cuda(cudaMemcpyAsync(hp + o, src, b, cudaMemcpyDeviceToHost, st), "copy") : FG_OK;
-    };
-    for (size_t i = 0; i < legs.size(); ++i) {
-        const fg_pf_leg &l = legs[i];
-        FG_TRY(d2h(at[i].xport, l.xport, l.nb * sizeof(float)));
-        FG_TRY(d2h(at[i].rtot, l.rtot, l.nb * sizeof(float)));
-        if (l.deg) FG_TRY(d2h(at[i].deg, l.deg, l.nb * sizeof(float)));
-        if (l.keep) FG_TRY(d2h(at[i].keep, l.keep, l.nb));
-        if (l.key) FG_TRY(d2h(at[i].key, l.key, l.nb * 2 * l.nleg * sizeof(int64_t)));
-    }
-    if (nc > 0) {
-        // candidate j's coordinates are row 1 of single-scattering path j; its potential likewise
-        FG_TRY(cuda(cudaMemcpy2DAsync(hp + at_c1, 3 * sizeof(float), legs[0].coords + 3, 6 * sizeof(float),
-                                      3 * sizeof(float), nc, cudaMemcpyDeviceToHost, st), "copy"));
-        FG_TRY(cuda(cudaMemcpy2DAsync(hp + at_ip1, sizeof(int64_t), legs[0].ipots + 1, 2 * sizeof(int64_t),
-                                      sizeof(int64_t), nc, cudaMemcpyDeviceToHost, st), "copy"));
-    }
+    for (size_t i = 0; i < S.host.size(); ++i)
+        FG_TRY(cuda(cudaMemcpyAsync(hp + at_block[i], S.host[i].base, S.host[i].used, cudaMemcpyDeviceToHost, st),
+                    "copy"));
     FG_TRY(cuda(cudaStreamSynchronize(st), "synchronize"));
+    // the host copy of a device pointer of the host region
+    auto on_host = [&](const void *d) -> const unsigned char * {
+        if (!d) return nullptr;
+        const unsigned char *p = static_cast<const unsigned char *>(d);
+        for (size_t i = 0; i < S.host.size(); ++i)
+            if (p >= S.host[i].base && p < S.host[i].base + S.host[i].used) return hp + at_block[i] + (p - S.host[i].base);
+        return nullptr;
+    };
     std::vector<LegHost> H(legs.size());
     for (size_t i = 0; i < legs.size(); ++i) {
         const fg_pf_leg &l = legs[i];
         LegHost &h = H[i];
         h.nleg = l.nleg;
-        const float *xp = reinterpret_cast<const float *>(hp + at[i].xport);
-        const float *rt = reinterpret_cast<const float *>(hp + at[i].rtot);
-        const float *dg = l.deg ? reinterpret_cast<const float *>(hp + at[i].deg) : nullptr;
-        const uint8_t *kp = l.keep ? hp + at[i].keep : nullptr;
-        const int64_t *ky = l.key ? reinterpret_cast<const int64_t *>(hp + at[i].key) : nullptr;
+        if (l.nb == 0) continue;
+        const float *xp = reinterpret_cast<const float *>(on_host(l.xport));
+        const float *rt = reinterpret_cast<const float *>(on_host(l.rtot));
+        const float *dg = reinterpret_cast<const float *>(on_host(l.deg));
+        const uint8_t *kp = on_host(l.keep);
+        const int64_t *ky = reinterpret_cast<const int64_t *>(on_host(l.key));
         for (int64_t j = 0; j < l.nb; ++j) {
             if (kp && !kp[j]) continue;              // not a path (ends at the absorber, or after its reverse)
             h.idx.push_back(j);
@@ -455,8 +478,8 @@ extern "C" fg_status fg_pf_enumerate_one(const float *pos, int64_t n, float box,
     std::vector<float> c1(nc * 3);
     std::vector<int64_t> ip1(nc);
     if (nc > 0) {
-        std::memcpy(c1.data(), hp + at_c1, c1.size() * sizeof(float));
-        std::memcpy(ip1.data(), hp + at_ip1, ip1.size() * sizeof(int64_t));
+        std::memcpy(c1.data(), on_host(c1_dev), c1.size() * sizeof(float));
+        std::memcpy(ip1.data(), on_host(ip1_dev), ip1.size() * sizeof(int64_t));
     }
     std::vector<fg_pf_leg> kept;
     merge_and_cut(H, nc, c1, ip1, merge != 0, critpw, kept, r->ref);
