@@ -22,6 +22,8 @@ The reference is imported read-only from its source tree and run on the CPU in F
   k = 0..20 A^-1 step 0.05.
 * cfg4_fe_phase.npz, cfg5_nik_phase.npz, cfg5_ok_phase.npz -- bcc Fe (K edge) and rock-salt NiO (Ni K and O K
   edges) phase tables of 6 A clusters through the reference chain, for the MD-batch and two-edge refinement cases.
+* finder_lone/one/two/blk/ss.npz -- the same for the enumeration's edge cases: an absorber with no candidate, with one
+  (single scattering only) and with two, a 600-atom packing in a box (3 legs), and single scattering alone (2 legs);
 * finder_cu.npz, finder_pack.npz, finder_bcc.npz -- the reference's path finder on the Cu cluster (rmax 6, 4 legs),
   a 400-atom periodic Fe/O/Pt packing (rmax 6.5, 7 legs) and a thermal bcc Fe frame (rmax 5.5, 3 legs), each without
   and with an importance cut; finder_feopt.npz -- the reference finder's paths on the benchmark packing (counts,
@@ -350,6 +352,13 @@ FINDER_CASES = {
     "pack": ("pack", "cfg2_phase", "Fe", 6.5, 7, (0.0, 1.0)),
     "bcc": ("bcc", "cfg4_fe_phase", None, 5.5, 3, (0.0, 2.0)),
     "tri": ("tri", "cfg4_fe_phase", None, 5.0, 4, (0.0, 2.0)),
+    # edge cases of the enumeration: no candidate, one candidate (single scattering only), two candidates, a packing
+    # whose 600 atoms span several blocks of the one-absorber candidate scan, and single scattering alone
+    "lone": ("lone", "cfg4_fe_phase", None, 5.0, 4, (0.0,)),
+    "one": ("one", "cfg4_fe_phase", None, 5.0, 4, (0.0, 2.0)),
+    "two": ("two", "cfg4_fe_phase", None, 5.0, 5, (0.0, 2.0)),
+    "blk": ("blk", "cfg2_phase", "Fe", 5.0, 3, (0.0, 2.0)),
+    "ss": ("blk", "cfg2_phase", "Fe", 5.0, 2, (0.0, 2.0)),
 }
 
 # triclinic cells of the fixtures: a cubic supercell of edge L sheared to these lattice vectors (rows, units of L)
@@ -369,6 +378,18 @@ def finder_structure(kind):
         return pts, None, 0, np.ones(len(pts), int)
     if kind == "pack":
         pos, lab, box = W.random_packing(400, 0.08, 1.8, seed=77)
+        ab = int(W.central_atom(pos, box, lab, "Fe", 1)[0])
+        return pos, box, ab, np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
+    if kind == "lone":
+        return np.zeros((1, 3)), None, 0, np.ones(1, int)
+    if kind == "one":
+        pts = np.array([[0.0, 0.0, 0.0], [2.5, 0.1, -0.2], [20.0, 0.0, 0.0]])
+        return pts, None, 0, np.ones(3, int)
+    if kind == "two":
+        pts = np.array([[0.0, 0.0, 0.0], [2.5, 0.1, -0.2], [0.3, 2.6, 0.1], [20.0, 0.0, 0.0]])
+        return pts, None, 0, np.ones(4, int)
+    if kind == "blk":
+        pos, lab, box = W.random_packing(600, 0.08, 1.8, seed=91)
         ab = int(W.central_atom(pos, box, lab, "Fe", 1)[0])
         return pos, box, ab, np.array([{"Fe": 1, "O": 2, "Pt": 3}[x] for x in lab])
     if kind == "tri":
@@ -704,6 +725,8 @@ def main():
             make_finder_feopt()
         if "finder_tri" in want:
             make_finder(["tri"])
+        if "finder_edges" in want:
+            make_finder(["lone", "one", "two", "blk", "ss"])
         if "pairs" in want:
             make_pairs()
         if "pairs_tri" in want:

@@ -1,7 +1,9 @@
 """The CUDA path finder against the reference's finder (golden fixtures) and the oracle (B200).
 
-* finder_{cu,pack,bcc}: the same kept paths in the same order (atom sequences), the same degeneracies, importances
-  within 2e-5 relative (FP32 sums in another order), the same reference importance;
+* finder_{cu,pack,bcc,tri} and the edge cases finder_{lone,one,two,blk,ss} (no candidate, one, two, a 600-atom
+  packing over several candidate-scan blocks, single scattering alone): the same kept paths in the same order (atom
+  sequences), the same degeneracies, importances within 2e-5 relative (FP32 sums in another order), the same
+  reference importance, from the one-absorber call and from the batched call alike;
 * batched absorbers equal one call per absorber;
 * the benchmark's 3000-atom Fe/O/Pt packing (two absorbers, rmax 8 A, 8 legs, no importance cut, 1.9e5 paths) gives
   the reference finder's paths exactly;
@@ -46,6 +48,14 @@ def test_finder_equals_reference(name):
             assert np.allclose(xp, z[f"xport_{ci}_{nleg}"], rtol=2e-5, atol=0)
             assert coords.shape == (len(ra), nleg, 3) and np.all(coords[:, 0] == 0)
             print(f"finder_{name} critpw {crit} nleg {nleg}: {len(ra)} paths equal")
+        # the batched path (one absorber slot) gives the same paths bit for bit and the same reference importance
+        many = f.enumerate_many(z["pos"], box, [int(z["absorber"])], z["ipot"])
+        assert float(many["ref"][0]) == ref
+        got_many = {n: v for n, v in many["paths"].items() if v[0].shape[0] > 0}
+        assert set(got_many) == set(got), (name, crit)
+        for nleg, v in got.items():
+            for x, y in zip(v, got_many[nleg][:5]):
+                assert x.dtype == y.dtype and torch.equal(x, y), (name, crit, nleg)
 
 
 @pytest.mark.parametrize("merge,crit", [(True, 0.5), (True, 0.0), (False, 0.5)])

@@ -7,7 +7,10 @@ import pytest
 from oracle import pathfinder as OF
 from tests.fixtures import npz, phase
 
-CASES = {"cu": "cfg1_cu", "pack": "cfg2_phase", "bcc": "cfg4_fe_phase", "tri": "cfg4_fe_phase"}
+CASES = {"cu": "cfg1_cu", "pack": "cfg2_phase", "bcc": "cfg4_fe_phase", "tri": "cfg4_fe_phase",
+         # edge cases: no candidate, one, two; a 600-atom packing over several candidate-scan blocks; 2 legs only
+         "lone": "cfg4_fe_phase", "one": "cfg4_fe_phase", "two": "cfg4_fe_phase", "blk": "cfg2_phase",
+         "ss": "cfg2_phase"}
 
 
 def finder_case(name):
