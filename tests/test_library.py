@@ -63,6 +63,16 @@ def test_new_entry_points_refuse_bad_arguments_on_the_host():
     assert lib.fg_rspace_misfit(1, 401, 100, None, None, None, 1.0, None, None, None) == V                  # nulls
     assert lib.fg_path_columns(1, 0, 0, None, None, None, None, None, None) == V                            # E 0
     assert lib.fg_path_columns(1, 60, 7, None, None, None, None, None, None) == V
+    assert lib.fg_stage_set_fused_variant(None, 0, 0) == V                                           # null stage
+    assert lib.fg_stage_set_launch(None, 4, 4) == V
+    assert lib.fg_pf_enumerate_one(None, 10, 1.0, None, 0, None, None, 5.0, 3, 0.0, 1, None, None, None, None) == V
+    assert lib.fg_pf_result_gather(None, 2, None, None, None, None, None, None) == V
+    lib.fg_pf_result_destroy(None)                                                                      # a no-op
+    cost = (C.c_double * 4)(3.0, 1.0, 2.0, 2.0)
+    owner = (C.c_int32 * 4)()
+    assert lib.fg_shard_lpt(cost, 4, 0, owner) == V                                                    # no ranks
+    assert lib.fg_shard_lpt(cost, 4, 2, owner) == _lib.FG_OK
+    assert sorted(sum(cost[i] for i in range(4) if owner[i] == r) for r in range(2)) == [4.0, 4.0]
     w = (C.c_int64 * 3)()
     sl = (C.c_float * 3)(1.0, 1.0005, 1.5)
     off = (C.c_int64 * 2)(0, 3)
