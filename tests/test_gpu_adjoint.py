@@ -3,7 +3,7 @@
 Oracles: the reference stage's gradient under torch.utils.checkpoint(use_reentrant=False) (golden fixtures,
 tests/golden/grad_*.npz) and central finite differences (h = 1e-4 A) of the oracle / of the stage itself.
 Tolerances (relative to the largest gradient component): FP64 form 1e-7 against the reference's autograd (its own
-agreement with finite differences is ~1e-6), mixed form 1e-4 (the north-star gradient bar); finite differences 1e-4.
+agreement with finite differences is ~1e-6), mixed form 1e-4 (the gradient bar of the mixed form); finite differences 1e-4.
 """
 import numpy as np
 import pytest

@@ -8,7 +8,7 @@ Here this package's CUDA path finder regenerates the batch, must give the same a
 the fused stage's rows of the sample -- one row per absorber and leg count -- are compared with the reference's rows
 and with the oracle's:
 
-  mixed form (complex64): R <= 1e-6 per row (the north-star gate), per-path cchi within 2e-5 of max|cchi|;
+  mixed form (complex64): R <= 1e-6 per row (the parity gate), per-path cchi within 2e-5 of max|cchi|;
   FP64 form (complex128): R <= 1e-12 per row, per-path cchi within 1e-10 of max|cchi|.
 
 R is the reference's R-factor (compare.py:17-27) with k 3-19 1/A, R 1-8 A, k weight 2.

@@ -55,7 +55,7 @@ def test_cfg3_adjoint_800_atoms():
     displacement).  This package: the CUDA finder's paths (the same lists), PathModel + chi_reduce, the misfit with
     PathSpectra's FP32 k grid; the loss and the gradient with respect to all 3 x 800 positions against the reference's
     (FP64 form: 1e-7 relative to the largest component, the rounding of PathSpectra's FP32 window cosines, measured
-    2e-9; mixed form: 1e-4), and per-path
+    2e-9; mixed form: 1e-4, the gradient bar of the mixed form), and per-path
     sigma^2 gradients (no reference counterpart) against central differences.  The FP32-vs-FP64 gradient error is
     printed."""
     from feffgpu_b200 import GPUPathStage

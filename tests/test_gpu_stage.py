@@ -4,7 +4,7 @@ Tolerances (written here, checked here):
   FP64 form (complex128): per-path cchi within 1e-10 of max|cchi| of the reference stage below k = 20 1/A (the
     reference's own bar against its literal port is 1e-8, tests/test_pathfinder.py:226); chi R < 1e-12.
   Mixed form (complex64): per-path cchi within 2e-5 of max|cchi|; chi R <= 1e-6 against the reference's FP64 chi
-    (the parity gate of the north-star target).
+    (the parity gate of the path stage).
   Both: FEFF's chi.dat to the reference's bars (R < 1e-9 for W, tests/test_xsph.py:122; R < 2e-5 otherwise,
     tests/test_validation_cases.py:50).
 """
