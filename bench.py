@@ -262,8 +262,12 @@ def extras(args, stage, batch, P, S, dev, timed, n_total, ms):
     import torch
     from feffgpu_b200 import GPUPathStage
     from feffgpu_b200.sharded import allreduce_rows
-    coords_h = batch.coords.cpu().pin_memory()
-    coords_d = torch.empty_like(batch.coords)
+    # the path coordinates come from the FP32 path finder: sent as FP32 when that is exact (the stage widens them to
+    # FP64 on the device, the same values), else as FP64
+    c64 = batch.coords.cpu()
+    c32 = c64.to(torch.float32)
+    coords_h = (c32 if torch.equal(c32.to(torch.float64), c64) else c64).pin_memory()
+    coords_d = torch.empty(coords_h.shape, dtype=coords_h.dtype, device=dev)
     rows_h = torch.empty(batch.nrows, NK, dtype=torch.float64).pin_memory()
 
     def e2e_step():
