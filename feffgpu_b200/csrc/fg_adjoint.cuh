@@ -451,7 +451,10 @@ __device__ __forceinline__ void cfac_grad(const WarpPath<R> &g, const Tables<R> 
 // pairing measured slower and is not used).  Keeping only every second or third prefix and recomputing the others
 // from F~_k (1.5-2.3 KB instead of 3.7 KB of local memory per lane) measured 1-3 % slower on B200: the local memory is
 // not what bounds this kernel.
-template <typename R, int KIND>
+//
+// MASK: the stage's lambda order is below 2 (T.nlam < N); a separate instantiation, so that the order-2 code carries
+// none of the masking (with it inline the order-2 adjoint measured 4 % slower).
+template <typename R, int KIND, bool MASK = false>
 __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, const R (*dterm_db)[49],
                               const Tables<R> &T, int e, int nleg, C2<R> gbar, ParGrad &pg)
 {
@@ -481,6 +484,7 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
         const int ip = g.ip[k];
         accumulate_f<R, KIND, N, N>(acc, dh + (k - 1) * dleg, T.tl + ip * tlip + e, E, T.lmax[ip * E + e] + 1,
                                     zfac(cscl(ck, (R)g.ri[k + 1])), zfac(cscl(ck, (R)g.ri[k])));
+        if constexpr (MASK) mask_lambda<R, KIND, N, N>(acc, T.nlam);
 #pragma unroll
         for (int r = 0; r < RT.n; ++r) Fst[k - 1][r] = acc[r];
         C2<R> ph[2 * MM + 1];
@@ -547,6 +551,7 @@ __device__ void energy_ms_adj(const WarpPath<R> &g, const R *dh, const R *dhd, c
                         Wh[r] = RT.sg[a][b] > 0 ? pfma(pc[b], rr[a], Wh[r]) : pfms(pc[b], rr[a], Wh[r]);
                     }
             }
+            if constexpr (MASK) mask_lambda<R, KIND, N, N>(Wh, T.nlam);   // entries outside the set are constants
             C2<R> tm = cz<R>();                     // sum_a m_a (P_k R_k)(a, a)
 #pragma unroll 1
             for (int c = 0; c < N0; ++c)
@@ -763,7 +768,7 @@ __device__ void energy_ss_col_adj(const WarpPath<R> &g, const R *dh, const R *dh
     cfac_grad(g, T, e, 2, gbar, cmul(ptrac, cf), pg);
 }
 
-template <typename R, int EDGE>
+template <typename R, int EDGE, bool MASK = false>
 __device__ __forceinline__ void path_energy_adj(const WarpPath<R> &g, const R *dh, const R *dhd,
                                                 const R (*dterm_db)[49], const Tables<R> &T, int e, int nleg,
                                                 C2<R> gbar, ParGrad &pg)
@@ -776,7 +781,7 @@ __device__ __forceinline__ void path_energy_adj(const WarpPath<R> &g, const R *d
             energy_ss_col_adj<R, K::SS>(g, dh, dhd, dterm_db, T, e, gbar, pg);
         return;
     }
-    energy_ms_adj<R, K::MS>(g, dh, dhd, dterm_db, T, e, nleg, gbar, pg);
+    energy_ms_adj<R, K::MS, MASK>(g, dh, dhd, dterm_db, T, e, nleg, gbar, pg);
 }
 
 // ------------------------------------------------------------------------------------------------ kernels
@@ -935,7 +940,7 @@ __device__ __forceinline__ double coord_grad(const WarpPath<R> &g, const double 
 
 // The adjoint over a set of paths: per path the seeds gbar (E, complex) and dL/dreff (A), out dL/dcoords.
 // Paths come from `order` (or are 0..B-1), coordinates/ipots with a row stride of `stride` legs.
-template <typename R, int EDGE, typename CT>
+template <typename R, int EDGE, typename CT, bool MASK = false>
 __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restrict__ coords,
                                                   const int64_t *__restrict__ ipots, int stride,
                                                   const int *__restrict__ nlegs, int nleg_uniform, int64_t B,
@@ -972,7 +977,8 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
         for (int j = 0; j <= kMaxLeg; ++j) pg.ri[j] = pg.beta[j] = pg.eta[j] = 0.0;
         for (int e0 = first_chunk(E); e0 < E; e0 += 32) {
             const int e = e0 + lane;
-            if (e >= 0 && e < E) path_energy_adj<R, EDGE>(g, dh, dhd, as.dterm_db, T, e, nleg, gbar[p * E + e], pg);
+            if (e >= 0 && e < E)
+                path_energy_adj<R, EDGE, MASK>(g, dh, dhd, as.dterm_db, T, e, nleg, gbar[p * E + e], pg);
         }
         // fixed-order warp reduction of the per-lane sums
         for (int j = 1; j <= nleg; ++j) {
@@ -1114,7 +1120,8 @@ fg_status launch_adjoint(const StageView &sv, const Tables<R> &T, const CT *coor
     const size_t wb = adj_warp_bytes<R>(sv.L1, nsc_max, K::MM);
     warps = fit_warps(warps, wb, sv.max_smem);
     const int threads = warps * 32;
-    auto kern = k_adjoint<R, EDGE, CT>;
+    constexpr int N = lamtab(K::MS).N;
+    auto kern = T.nlam < N ? k_adjoint<R, EDGE, CT, true> : k_adjoint<R, EDGE, CT, false>;
     int blocks = 0;
     if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;
     timer_begin(st);

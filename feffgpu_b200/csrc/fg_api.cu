@@ -120,6 +120,7 @@ template <typename R> fg_status build_tables(fg_stage *s, Tables<R> &T, const st
     if ((st = upload(s, rc, &T.rc))) return st;
     if ((st = upload(s, lmax_t, &T.lmax))) return st;
     T.MMd = 3;
+    T.nlam = s->iorder == 0 ? 1 : (s->iorder == 1 ? 3 : 6);
     return FG_OK;
 }
 }  // namespace
@@ -204,7 +205,11 @@ extern "C" fg_status fg_stage_create(const fg_phase_desc *d, int device, fg_stag
     *out = nullptr;
     if (d->nsp != 1) return fail(FG_ERR_NOT_IMPLEMENTED, "spin-dependent phase files are not ported");
     if (d->iorder >= 10) return fail(FG_ERR_NOT_IMPLEMENTED, "icalc >= 10 not ported");
-    if (d->iorder != 2) return fail(FG_ERR_NOT_IMPLEMENTED, "only iorder = 2 (the path stage's default) is built");
+    if (d->iorder == 3)
+        return fail(FG_ERR_NOT_IMPLEMENTED, "iorder 3 (the 10-entry lambda set) is not built; orders 0, 1 and 2 are");
+    if (d->iorder < 0 || d->iorder > 3)
+        return fail(FG_ERR_VALUE, "iorder " + std::to_string(d->iorder) +
+                                      ": the lambda set exceeds the rotation tables (|m| <= 3)");
     if (d->ne1 < 2 || d->nph < 0 || d->ltot < 0 || !d->lmax0 || !d->em || !d->eref || !d->ph || !d->rkk)
         return fail(FG_ERR_VALUE, "incomplete phase description");
     fg_stage *s = new fg_stage();

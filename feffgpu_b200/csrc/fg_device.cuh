@@ -235,11 +235,26 @@ template <int KIND, int NR, int NC> struct RepTab {
     }
 };
 
+// The multiple-scattering lambda set of a lower order (setlam, genfmt.py:115-153): iorder 1 keeps (m, n) = (0, 0),
+// (-1, 0), (1, 0) and iorder 0 (0, 0), the first 3 and 1 entries of the order-2 sets here, a flip-closed subset.
+// A scattering matrix (or its adjoint weights) restricted to it: the canonical entries with a row or column beyond
+// the first nlam are zero, so the chain product, the termination and the trace are those of the smaller set.
+template <typename R, int KIND, int NR, int NC>
+__device__ __forceinline__ void mask_lambda(C2<R> (&acc)[RepTab<KIND, NR, NC>().n], int nlam)
+{
+    constexpr RepTab<KIND, NR, NC> RT{};
+    if (nlam >= NR && nlam >= NC) return;
+#pragma unroll
+    for (int r = 0; r < RT.n; ++r)
+        if (RT.a[r] >= nlam || RT.b[r] >= nlam) acc[r] = C2<R>{R(0), R(0)};
+}
+
 // ------------------------------------------------------------------------------------------------ stage tables
 // Device tables of one phase file (built by fg_stage_create).
 template <typename R> struct Tables {
     int E, nph1, L1, nterm, MMd;
     int term_l[2];              // l of the termination terms (distinct final-state l of bcoef, genfmt.py:230)
+    int nlam;                   // multiple-scattering lambda entries of the stage's order: 6 (iorder 2), 3 (1), 1 (0)
     const C2<R> *tl;            // (nph1, L1+1, E) j-averaged t-matrix, index il = l + 1 (stage.py:111-118)
     const int *lmax;            // (nph1, E)
     const C2<R> *ck;            // (E) complex momentum, bohr^-1

@@ -365,6 +365,7 @@ __device__ C2<R> energy_ms(const WarpPath<R> &g, const R *dh, const Tables<R> &T
         }
         accumulate_f<R, KIND, N, N, sizeof(R) == 4 ? 2 : 1>(acc, dh + (k - 1) * dleg, tk, tstride, ilx,
                                                            zfac(cscl(ck, (R)g.ri[k + 1])), zfac(cscl(ck, (R)g.ri[k])));
+        mask_lambda<R, KIND, N, N>(acc, T.nlam);
         C2<R> ph[2 * MM + 1];
         phase_powers<R, MM>(g.phs[k + 1], ph);
         C2<R> Pn[N][N0];

@@ -22,6 +22,8 @@ The reference is imported read-only from its source tree and run on the CPU in F
   k = 0..20 A^-1 step 0.05.
 * cfg4_fe_phase.npz, cfg5_nik_phase.npz, cfg5_ok_phase.npz -- bcc Fe (K edge) and rock-salt NiO (Ni K and O K
   edges) phase tables of 6 A clusters through the reference chain, for the MD-batch and two-edge refinement cases.
+* grad_L001_io0/io1.npz, grad_A014_io0/io1.npz -- as grad_*.npz with the reference stage at lambda-set orders 0
+  and 1 (GPUPathStage(..., iorder=k)), with its cchi of every path;
 * finder_lone/one/two/blk/ss.npz -- the same for the enumeration's edge cases: an absorber with no candidate, with one
   (single scattering only) and with two, a 600-atom packing in a box (3 legs), and single scattering alone (2 legs);
 * finder_cu.npz, finder_pack.npz, finder_bcc.npz -- the reference's path finder on the Cu cluster (rmax 6, 4 legs),
@@ -97,9 +99,9 @@ def parse_chi(fname):
     return tab[:, 0], tab[:, 1]
 
 
-def ref_stage(P):
+def ref_stage(P, iorder=2):
     from feffgpu.stage import GPUPathStage
-    return GPUPathStage(P, device="cpu", dtype=torch.complex128)
+    return GPUPathStage(P, device="cpu", dtype=torch.complex128, iorder=iorder)
 
 
 def make_case(name):
@@ -181,12 +183,13 @@ def make_walks():
     print("walks_W written")
 
 
-def make_grad(name, nlegs=(2, 3, 4, 5, 6), per=3, seed=11):
-    """Reference gradients: the stage under checkpoint(use_reentrant=False) as the reference's callers use it."""
+def make_grad(name, nlegs=(2, 3, 4, 5, 6), per=3, seed=11, iorder=2):
+    """Reference gradients: the stage under checkpoint(use_reentrant=False) as the reference's callers use it.  With
+    iorder != 2 the fixture is grad_<name>_io<iorder>.npz and also holds the reference's cchi of every path."""
     from feffgpu.pad import read_phase_pad
     from torch.utils.checkpoint import checkpoint
     P = read_phase_pad(str(CASES[name] / "phase.pad"))
-    g = ref_stage(P)
+    g = ref_stage(P, iorder)
     rng = np.random.default_rng(seed)
     q = np.arange(1, 401) * 0.05
     S = g.linear_matrix(q)
@@ -211,9 +214,14 @@ def make_grad(name, nlegs=(2, 3, 4, 5, 6), per=3, seed=11):
         (gx,) = torch.autograd.grad(loss, x)
         out[f"coords_{nleg}"], out[f"ipots_{nleg}"], out[f"deg_{nleg}"] = coords, ipots, deg
         out[f"grad_{nleg}"], out[f"loss_{nleg}"] = gx.numpy(), np.asarray(float(loss.detach()))
+        if iorder != 2:
+            with torch.no_grad():
+                out[f"cchi_{nleg}"] = g.cchi(torch.tensor(coords), torch.tensor(ipots))[0].numpy()
     out.update(phase_to_arrays(P, prefix="ph_"))
-    np.savez_compressed(HERE / f"grad_{name}.npz", **out)
-    print(f"grad_{name} written")
+    out["iorder"] = np.asarray(iorder)
+    tag = name if iorder == 2 else f"{name}_io{iorder}"
+    np.savez_compressed(HERE / f"grad_{tag}.npz", **out)
+    print(f"grad_{tag} written")
 
 
 def make_grad_walks():
@@ -725,6 +733,10 @@ def main():
             make_finder_feopt()
         if "finder_tri" in want:
             make_finder(["tri"])
+        if "iorder" in want:
+            for io in (0, 1):
+                make_grad("L001", nlegs=(2, 3, 4, 5), per=2, iorder=io)       # K edge
+                make_grad("A014", nlegs=(2, 3, 4), per=2, iorder=io)          # L3 edge
         if "finder_edges" in want:
             make_finder(["lone", "one", "two", "blk", "ss"])
         if "pairs" in want:

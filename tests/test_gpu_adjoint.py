@@ -383,3 +383,48 @@ def test_axial_legs_gradient_matches_finite_differences(dtype):
         print(f"{name} {dtype}: gradient vs finite differences {e:.2e} (fused {ef:.2e})")
         assert np.isfinite(e) and e < tol, (name, e)
         assert np.isfinite(ef) and ef < tol, (name, ef)
+
+
+IORDER_CASES = ["grad_L001_io0", "grad_L001_io1", "grad_A014_io0", "grad_A014_io1"]   # K and L3 edges
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+@pytest.mark.parametrize("name", IORDER_CASES)
+def test_lower_lambda_orders_equal_reference(name, dtype):
+    """GPUPathStage(..., iorder=0 or 1), the reference's smaller multiple-scattering lambda sets (setlam,
+    genfmt.py:115-153): per-path cchi against the reference stage at the same order, and the gradient of the
+    weighted fine-grid sum, per-path and fused, against its checkpointed autograd."""
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    z = npz(name)
+    io = int(z["iorder"])
+    st = GPUPathStage(phase(name), device="cuda", dtype=dtype, iorder=io)
+    q = z["q"]
+    S = st.linear_matrix(q)
+    w = torch.tensor(z["w"], device="cuda")
+    legs = sorted(int(k.split("_")[1]) for k in z if k.startswith("coords_"))
+    tol_c = {torch.complex128: 1e-10, torch.complex64: 2e-5}[dtype]
+    for n in legs:
+        x = torch.tensor(z[f"coords_{n}"], device="cuda", dtype=st.rdtype, requires_grad=True)
+        cc, rf = st.cchi(x, torch.tensor(z[f"ipots_{n}"]))
+        ec = _rel(cc.detach().cpu().numpy(), z[f"cchi_{n}"])
+        chi = st.chi_fine(cc, rf, q, S)
+        (torch.tensor(z[f"deg_{n}"], device="cuda")[:, None] * chi.double() * w[None]).sum().backward()
+        eg = _rel(x.grad.double().cpu().numpy(), z[f"grad_{n}"])
+        print(f"{name} nleg {n} {dtype}: cchi {ec:.2e}, gradient {eg:.2e}")
+        assert ec < tol_c and eg < TOL[dtype], (n, ec, eg)
+    b = PathBatch([(z[f"coords_{n}"], z[f"ipots_{n}"], z[f"deg_{n}"]) for n in legs], nrows=1, device="cuda")
+    x = b.coords.clone().requires_grad_(True)
+    rows = st.chi_reduce(b, q, coords=x)
+    (rows[0] * w).sum().backward()
+    g = x.grad.cpu().numpy()
+    s = 0
+    for n in legs:
+        m = len(z[f"coords_{n}"])
+        assert _rel(g[s:s + m, :n], z[f"grad_{n}"]) < TOL[dtype], n
+        s += m
+    # the order is a property of the multiple-scattering paths only: two-leg paths are the same at every order
+    if 2 in legs:
+        ref2 = GPUPathStage(phase(name), device="cuda", dtype=dtype).cchi(torch.tensor(z["coords_2"], dtype=st.rdtype),
+                                                                            torch.tensor(z["ipots_2"]))[0]
+        got2 = st.cchi(torch.tensor(z["coords_2"], dtype=st.rdtype), torch.tensor(z["ipots_2"]))[0]
+        assert torch.equal(ref2, got2)
