@@ -2,12 +2,14 @@
 //
 // Per path (one warp) and energy (one lane), with the upstream gradient gbar = dL/dRe(cchi) + i dL/dIm(cchi):
 //   dL = Re(conj(gbar) dcchi),  cchi = ptrac cfac,  ptrac = Tr(T F_nsc ... F_1).
-// T does not depend on the chain, so it is formed first.  Sweep 1 stores the prefix products P_k = F_k ... F_1
-// (k < nsc) in local memory; sweep 2 runs k = nsc .. 1 with the suffix R_k = T F_nsc ... F_(k+1) in registers,
-// recomputes F_k and, in the same partial-wave loop, contracts dF_k against M_k = P_(k-1) R_k:
-//   d/drho_(k+1), d/drho_k  through tangent recursions of the spherical-wave factors (dz/drho = -i z^2),
-//   d/dbeta_k               through the tangent recursion of d^l(beta) (a second rotation table),
-//   d/deta_(k+1)            from F~_k after the loop (F = e^{-i eta m1} F~).
+// Multiple scattering: sweep 1 forms every F~_k (the forward's partial-wave loop) and stores F~_k and the prefix
+// products P_k = F_k ... F_1 P_0 in per-lane local memory; the termination is differentiated with P_nsc and gives the
+// start of the suffix R_nsc = [T 0]; sweep 2 runs k = nsc .. 1: the orbit weights Wh (dL/dF~_k folded over the flip
+// symmetry) from M_k = P_(k-1) R_k, the Euler-angle derivative d/deta_(k+1) = -i sum_a m_a (P_k R_k)(a, a), the
+// update R_(k-1) = R_k F_k, and one partial-wave loop that contracts the derivatives of F~_k against Wh:
+//   d/drho_(k+1), d/drho_k  from the spherical-wave factors themselves (dc_j/drho = -i z ((j - 1) c_j + j c_(j+1))),
+//   d/dbeta_k               through d'(beta) (a second rotation table).
+// Single scattering differentiates its one matrix the same way, with tangent recursions of the spherical waves.
 // The termination's parameters (rho_1, rho_nleg, beta_nleg, eta_1) are differentiated with P_nsc, and cfac gives
 // d/dri_j = cfac (i (ck - xk) - 1/ri_j).  The per-energy gradients of (ri, beta, eta) are summed over the energies
 // (lane accumulators, then a fixed-order warp reduction) and carried to the coordinates by forward-mode dual numbers
