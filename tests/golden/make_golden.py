@@ -706,8 +706,9 @@ def main():
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
     set_reference(args.reference)
-    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder", "pairs", "pairs_tri",
-                             "feffdat", "larch", "bench_sample", "rspace", "cfg3"])
+    want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder", "finder_tri",
+                             "finder_edges", "pairs", "pairs_tri", "feffdat", "larch", "bench_sample", "rspace", "cfg3",
+                             "iorder"])
     with tempfile.TemporaryDirectory() as tmp:
         if "cases" in want:
             import shutil
