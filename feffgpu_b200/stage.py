@@ -7,7 +7,8 @@ MD-EXAFS and RMC-EXAFS front ends and their forward model (``src/feffgpu/exafs/f
   form (FP32 scattering-matrix chain, FP64 geometry, 2kR + phase argument and sums), complex128 the plain FP64 form;
 * ``cchi(coords, ipots) -> (cchi (B, E) complex, reff (B,) A)``, differentiable in ``coords`` through the hand-written
   adjoint (a plain ``backward()`` works; the reference needs ``checkpoint(use_reentrant=False)``, which also works);
-* ``linear_matrix(q)``, ``spline_matrix(q)``, ``unwrap(phase)``, ``chi_fine(cchi, reff, q, S=None, convention)``;
+* ``linear_matrix(q)``, ``spline_matrix(q)``, ``unwrap(phase)``, ``chi_fine(cchi, reff, q, S=None, convention)``,
+  ``geometry(coords_bohr) -> (ri, beta, eta)``;
 * attributes ``P``, ``E``, ``rdtype``, ``cdtype``, ``device``, ``iorder``, ``L1``, ``lmax``, ``xk``, ``ck``.
 
 New beside them: ``chi_reduce(batch, q, ...)``, the fused stage: every path of a ``PathBatch`` (mixed leg counts,
@@ -256,6 +257,15 @@ class GPUPathStage:
                             "rep": ck.real / BOHR}, torch.tensor(table, device=self.device, dtype=torch.float64))
         return self._ecols
 
+    def geometry(self, coords_bohr):
+        """ri (B, nleg), beta (B, nleg), eta (B, nleg) for legs 1..nleg of paths coords (B, nleg, 3) in bohr, absorber
+        first -- the reference's GPUPathStage.geometry (stage.py:170-206), with its branch choices: FP64 on the
+        device (fg_path_geometry), returned in the coordinates' dtype, differentiable in the coordinates."""
+        x = torch.as_tensor(coords_bohr)
+        if x.dim() != 3 or x.shape[2] != 3:
+            raise ValueError("coords must be (B, nleg, 3)")
+        return _Geometry.apply(x, self)
+
     def columns(self, cchi, reff) -> dict:
         """FEFF's feffNNNN.dat columns of paths from their signals (the reference's PathStage._columns,
         genfmt.py:449-461): cchi (B, E) and reff (B,) A as cchi() returns them.  Per path mag (B, E) (A) and phase
@@ -395,6 +405,33 @@ class _Cchi(torch.autograd.Function):
         if not ctx.needs_input_grad[0]:
             return None, None, None
         return ctx.stage._cchi_backward(coords, ipots, g_cchi, g_reff), None, None
+
+
+class _Geometry(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, stage):
+        x64 = x.detach().to(stage.device, torch.float64).contiguous()
+        B, nleg = int(x64.shape[0]), int(x64.shape[1])
+        ri, beta, eta = (torch.empty(B, nleg, device=stage.device, dtype=torch.float64) for _ in range(3))
+        _lib.check(stage._lib.fg_path_geometry(B, nleg, x64.data_ptr(), ri.data_ptr(), beta.data_ptr(),
+                                               eta.data_ptr(), _stream(stage.device)))
+        ctx.save_for_backward(x64)
+        ctx.stage, ctx.dtype, ctx.in_device = stage, x.dtype, x.device
+        return ri.to(x.dtype), beta.to(x.dtype), eta.to(x.dtype)
+
+    @staticmethod
+    def backward(ctx, g_ri, g_beta, g_eta):
+        (x64,) = ctx.saved_tensors
+        if not ctx.needs_input_grad[0]:
+            return None, None
+        B, nleg = int(x64.shape[0]), int(x64.shape[1])
+        gs = [torch.zeros(B, nleg, device=x64.device, dtype=torch.float64) if g is None
+              else g.to(torch.float64).contiguous() for g in (g_ri, g_beta, g_eta)]
+        grad = torch.empty_like(x64)
+        st = ctx.stage
+        _lib.check(st._lib.fg_path_geometry_backward(B, nleg, x64.data_ptr(), gs[0].data_ptr(), gs[1].data_ptr(),
+                                                     gs[2].data_ptr(), grad.data_ptr(), _stream(st.device)))
+        return grad.to(ctx.in_device, ctx.dtype), None
 
 
 class _ChiFine(torch.autograd.Function):

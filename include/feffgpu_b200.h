@@ -308,6 +308,16 @@ FG_API fg_status fg_pair_ss_grad(const double *pos, int32_t C, int64_t n, double
 FG_API fg_status fg_path_columns(int64_t B, int32_t E, fg_precision prec, const void *cchi, const void *reff,
                                  const double *cols, double *mag, double *phase, void *stream);
 
+/* The path geometry of GPUPathStage.geometry (src/feffgpu/stage.py:170-206): coords (B, nleg, 3) FP64 in bohr,
+ * absorber first -> ri, beta, eta (B, nleg) FP64 for legs 1..nleg (leg lengths in bohr, scattering angles, Euler sums
+ * eta_j = alpha_(j-1) + gamma_j), with the reference's branch choices; the backward gives dL/dcoords (B, nleg, 3) from
+ * dL/dri, dL/dbeta, dL/deta.  nleg 2..9. */
+FG_API fg_status fg_path_geometry(int64_t B, int32_t nleg, const double *coords, double *ri, double *beta, double *eta,
+                                  void *stream);
+FG_API fg_status fg_path_geometry_backward(int64_t B, int32_t nleg, const double *coords, const double *grad_ri,
+                                           const double *grad_beta, const double *grad_eta, double *grad_coords,
+                                           void *stream);
+
 /* ---------------------------------------------------------------------------------------------- R-space misfit
  * The loss of the refinement (src/feffgpu/exafs/transform.py:104-145): per row b of rows (B, NK) FP64,
  * R[b] = inv_norm * sum_m |(F x_b)_m - target_m|^2 with F (NR, NK) the windowed, k-weighted FFT restricted to the R

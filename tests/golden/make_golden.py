@@ -22,6 +22,8 @@ The reference is imported read-only from its source tree and run on the CPU in F
   k = 0..20 A^-1 step 0.05.
 * cfg4_fe_phase.npz, cfg5_nik_phase.npz, cfg5_ok_phase.npz -- bcc Fe (K edge) and rock-salt NiO (Ni K and O K
   edges) phase tables of 6 A clusters through the reference chain, for the MD-batch and two-edge refinement cases.
+* geometry_ref.npz -- the reference stage's geometry (ri, beta, eta) of 2-8-leg paths, degenerate ones included, and
+  the gradient of a weighted sum of it by its autograd;
 * grad_L001_io0/io1.npz, grad_A014_io0/io1.npz -- as grad_*.npz with the reference stage at lambda-set orders 0
   and 1 (GPUPathStage(..., iorder=k)), with its cchi of every path;
 * finder_lone/one/two/blk/ss.npz -- the same for the enumeration's edge cases: an absorber with no candidate, with one
@@ -439,6 +441,34 @@ def make_finder(names=None):
         print(f"finder_{name}: {time.time() - t:.1f} s")
 
 
+def make_geometry(seed=5):
+    """geometry_ref.npz -- the reference stage's geometry (stage.py:170-206) of 2-8-leg paths in bohr: random paths,
+    and the degenerate cases its branch choices define (a leg along z, collinear atoms, a revisit), per leg count the
+    coordinates, ri, beta, eta and the gradient of sum(w_r ri + w_b beta + w_e eta) by its autograd."""
+    from feffgpu.pad import BOHR
+    g = ref_stage(phase_from_npz(np.load(HERE / "cfg1_cu.npz"), prefix="ph_"))
+    rng = np.random.default_rng(seed)
+    out = {}
+    for nleg in range(2, 9):
+        c = np.concatenate([np.zeros((6, 1, 3)), rng.normal(0, 2.0, (6, nleg - 1, 3))], 1) / BOHR
+        if nleg == 3:
+            c[0, 1] = [0.0, 0.0, 4.0]                     # first leg along z
+            c[1, 1], c[1, 2] = [2.0, 0.0, 0.0], [4.5, 0.0, 0.0]   # collinear atoms
+        if nleg == 4:
+            c[0, 3] = c[0, 1]                             # a revisit: A -> B -> C -> B
+        x = torch.tensor(c, requires_grad=True)
+        ri, beta, eta = g.geometry(x)
+        w = [torch.tensor(rng.normal(size=(6, nleg))) for _ in range(3)]
+        loss = (w[0] * ri + w[1] * beta + w[2] * eta).sum()
+        (gx,) = torch.autograd.grad(loss, x)
+        out[f"coords_{nleg}"] = c
+        out[f"ri_{nleg}"], out[f"beta_{nleg}"], out[f"eta_{nleg}"] = (t.detach().numpy() for t in (ri, beta, eta))
+        out[f"wr_{nleg}"], out[f"wb_{nleg}"], out[f"we_{nleg}"] = (t.numpy() for t in w)
+        out[f"grad_{nleg}"] = gx.numpy()
+    np.savez_compressed(HERE / "geometry_ref.npz", **out)
+    print("geometry_ref written")
+
+
 def make_finder_feopt():
     """finder_feopt.npz -- the reference's path finder on the benchmark structure (the seeded 3000-atom Fe/O/Pt
     packing of feffgpu_b200.workloads, its two most central Fe absorbers, rmax 8 A, 8 legs, no importance cut): per
@@ -708,7 +738,7 @@ def main():
     set_reference(args.reference)
     want = set(args.only or ["cases", "walks", "grad", "cfg1", "cfg2", "cfg45", "finder", "finder_tri",
                              "finder_edges", "pairs", "pairs_tri", "feffdat", "larch", "bench_sample", "rspace", "cfg3",
-                             "iorder"])
+                             "iorder", "geometry"])
     with tempfile.TemporaryDirectory() as tmp:
         if "cases" in want:
             import shutil
@@ -734,6 +764,8 @@ def main():
             make_finder_feopt()
         if "finder_tri" in want:
             make_finder(["tri"])
+        if "geometry" in want:
+            make_geometry()
         if "iorder" in want:
             for io in (0, 1):
                 make_grad("L001", nlegs=(2, 3, 4, 5), per=2, iorder=io)       # K edge

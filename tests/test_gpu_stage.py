@@ -323,3 +323,34 @@ def test_gaussian_frames_damp_the_first_shell_like_the_sigma2_factor():
     e = np.abs(env(avg)[w] / env(damped)[w] - 1.0).max()
     print(f"envelope of the frame average vs the sigma^2 factor on the ideal lattice: {e:.3f}")
     assert e < 0.03
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_geometry_equals_reference(dtype):
+    """GPUPathStage.geometry (stage.py:170-206): ri, beta, eta of 2-8-leg paths -- random ones and the degenerate
+    cases the reference's branch choices define (a leg along z, collinear atoms, a revisit) -- and the gradient of a
+    weighted sum of them, against the reference's values and autograd (tests/golden/geometry_ref.npz).  For the leg
+    along z the reference's autograd gives NaN in the components that pass through its small-vector branch (its
+    Euler angles are constants there); those are left out, and this gradient is finite everywhere."""
+    from feffgpu_b200 import GPUPathStage
+    z = npz("geometry_ref")
+    st = GPUPathStage(phase("case_L001"), device="cuda", dtype=dtype)
+    for nleg in range(2, 9):
+        x = torch.tensor(z[f"coords_{nleg}"], device="cuda", requires_grad=True)
+        ri, beta, eta = st.geometry(x)
+        assert ri.dtype == torch.float64 and ri.shape == (len(x), nleg)
+        for got, key in ((ri, "ri"), (beta, "beta"), (eta, "eta")):
+            ref = z[f"{key}_{nleg}"]
+            assert np.abs(got.detach().cpu().numpy() - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()), (nleg, key)
+        w = [torch.tensor(z[f"{k}_{nleg}"], device="cuda") for k in ("wr", "wb", "we")]
+        (w[0] * ri + w[1] * beta + w[2] * eta).sum().backward()
+        g, ref = x.grad.cpu().numpy(), z[f"grad_{nleg}"]
+        ok = np.isfinite(ref)
+        assert np.all(np.isfinite(g)) and ok.mean() > 0.9, nleg
+        assert np.abs(g - np.where(ok, ref, g)).max() <= 1e-10 * np.abs(ref[ok]).max(), nleg
+    # float32 coordinates come back as float32, still differentiable
+    x32 = torch.tensor(z["coords_3"], dtype=torch.float32, requires_grad=True)
+    ri32 = st.geometry(x32)[0]
+    assert ri32.dtype == torch.float32
+    ri32.sum().backward()
+    assert x32.grad is not None and x32.grad.dtype == torch.float32
