@@ -891,10 +891,20 @@ def main():
                 traffic = float(line.split("=")[1])
             if line.startswith("captured"):
                 traffic_src = line.split("=", 1)[1].strip()
+    pipe, pipe_src = None, None
+    pf_ = ROOT / "profiles" / "k_fused_fma_pipe_full_size.md"
+    if pf_.exists():
+        for line in pf_.read_text().splitlines():
+            if line.startswith("captured=") and "fma_pipe_pct=" in line:
+                kv = dict(x.split("=", 1) for x in line.split())
+                pipe, pipe_src = float(kv["fma_pipe_pct"]), kv["captured"]
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
             "frac": achieved / peak.value if achieved else None, "traffic": traffic,
             "traffic_source": f"not measured in this run: ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                               f"full-size launch, profiles/k_fused_feopt_traffic.txt ({traffic_src})",
+            "fma_pipe_active_pct": pipe,
+            "fma_pipe_source": f"not measured in this run: ncu sm__pipe_fma_cycles_active of one full-size launch, "
+                               f"profiles/k_fused_fma_pipe_full_size.md ({pipe_src})",
             "kernel": "k_fused (per-path signal, all leg counts, one persistent launch)",
             "kernel_ms": kern_ms, "flops_per_launch": flops,
             "peak_source": "measured on this GPU by fg_fp32_fma_peak (FFMA chains on every SM); "
