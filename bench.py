@@ -261,7 +261,7 @@ def extras(args, stage, batch, P, S, dev, timed, n_total, ms):
     headline's (this GPU's share of the paths, rows all-reduced over the GPUs)."""
     import torch
     from feffgpu_b200 import GPUPathStage
-    from feffgpu_b200.sharded import allreduce_rows
+    from feffgpu_b200.sharded import chi_reduce_all_ranks
     # the path coordinates come from the FP32 path finder: sent as FP32 when that is exact (the stage widens them to
     # FP64 on the device, the same values), else as FP64
     c64 = batch.coords.cpu()
@@ -272,7 +272,7 @@ def extras(args, stage, batch, P, S, dev, timed, n_total, ms):
 
     def e2e_step():
         coords_d.copy_(coords_h, non_blocking=True)
-        rows = allreduce_rows(stage.chi_reduce(batch, Q, S, coords=coords_d))
+        rows = chi_reduce_all_ranks(stage, batch, Q, S, coords=coords_d)
         rows_h.copy_(rows, non_blocking=True)
 
     with torch.no_grad():
@@ -289,7 +289,7 @@ def extras(args, stage, batch, P, S, dev, timed, n_total, ms):
         w = torch.randn(batch.nrows, NK, dtype=torch.float64, device=dev, generator=torch.Generator(dev).manual_seed(0))
 
         def fb():
-            rows = allreduce_rows(stage.chi_reduce(batch, Q, S, coords=cg, sigma2=s2))
+            rows = chi_reduce_all_ranks(stage, batch, Q, S, coords=cg, sigma2=s2)
             (rows * w).sum().backward()
 
         ms_fb, _ = timed(fb, max(2, args.steps // 2), 1)
@@ -300,7 +300,7 @@ def extras(args, stage, batch, P, S, dev, timed, n_total, ms):
     # the plain FP64 drop-in (complex128) on the same batch
     stage64 = GPUPathStage(P, device=dev, dtype=torch.complex128, autotune=not args.no_autotune)
     with torch.no_grad():
-        ms64, _ = timed(lambda: allreduce_rows(stage64.chi_reduce(batch, Q, S)), 2, 1)
+        ms64, _ = timed(lambda: chi_reduce_all_ranks(stage64, batch, Q, S), 2, 1)
     plain = {"value": n_total * NK / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
              "speedup_mixed_over_fp64": ms64 / ms, "launch_warps": list(stage64._launch)}
 
@@ -811,13 +811,14 @@ def main():
     torch.cuda.set_device(dev)
     P, all_groups = workload(world, args.paths_scale)
     stage = GPUPathStage(P, device=dev, dtype=torch.complex64, autotune=not args.no_autotune)
-    from feffgpu_b200.sharded import allreduce_rows, split_groups
+    from feffgpu_b200.sharded import chi_reduce_all_ranks, split_groups
     groups = split_groups(all_groups, world, rank, lmax=stage.lmax.cpu().numpy()) if world > 1 else all_groups
     batch = PathBatch(groups, nrows=2 * world, device=dev)
     n_total = sum(len(g[0]) for g in all_groups)
 
     def step_rows(**kw):
-        return allreduce_rows(stage.chi_reduce(batch, Q, S, **kw))
+        # one rank: the fused call itself; several: each rank's share, exact row sums summed as integers
+        return chi_reduce_all_ranks(stage, batch, Q, S, **kw) if world > 1 else stage.chi_reduce(batch, Q, S, **kw)
     S = stage.linear_matrix(Q)
     lib = _lib.load()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2, written between steps

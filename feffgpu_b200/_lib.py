@@ -28,7 +28,7 @@ EXPORTS = ("fg_stage_create", "fg_stage_destroy", "fg_stage_get_info", "fg_stage
            "fg_chi_reduce_backward", "fg_set_kernel_timing", "fg_kernel_time_ms", "fg_fp32_fma_peak", "fg_set_launch",
            "fg_stage_set_launch", "fg_stage_set_fused_variant", "fg_pf_candidates", "fg_pf_extend", "fg_pf_terminal", "fg_pf_describe",
            "fg_pf_windows", "fg_pair_histogram", "fg_pair_ss_grad", "fg_rspace_misfit",
-           "fg_path_columns", "fg_path_geometry", "fg_path_geometry_backward", "fg_shard_lpt", "fg_pf_enumerate_one", "fg_pf_result_gather", "fg_pf_result_destroy")
+           "fg_path_columns", "fg_chi_reduce_words", "fg_rows_from_words", "fg_path_geometry", "fg_path_geometry_backward", "fg_shard_lpt", "fg_pf_enumerate_one", "fg_pf_result_gather", "fg_pf_result_destroy")
 
 
 class PhaseDesc(C.Structure):
@@ -93,6 +93,9 @@ _SIGS = {
                                   C.c_double, C.c_int32, C.c_double, C.c_double, _P, _P]),
     "fg_rspace_misfit": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, _P, _P, _P, C.c_double, _P, _P, _P]),
     "fg_path_columns": (C.c_int, [C.c_int64, C.c_int32, C.c_int, _P, _P, _P, _P, _P, _P]),
+    "fg_chi_reduce_words": (C.c_int, [_P, C.c_int, C.POINTER(Paths), C.c_int32, _P, _P, _P, _P, _P, _P, _P,
+                                      C.c_size_t, _P]),
+    "fg_rows_from_words": (C.c_int, [C.c_int64, C.c_int32, _P, _P, _P]),
     "fg_path_geometry": (C.c_int, [C.c_int64, C.c_int32, _P, _P, _P, _P, _P]),
     "fg_path_geometry_backward": (C.c_int, [C.c_int64, C.c_int32, _P, _P, _P, _P, _P, _P]),
     "fg_shard_lpt": (C.c_int, [_P, C.c_int64, C.c_int32, _P]),

@@ -538,6 +538,40 @@ extern "C" fg_status fg_chi_reduce(const fg_stage *s, fg_precision prec, const f
     return read_status(reinterpret_cast<const int *>(static_cast<unsigned char *>(workspace) + kStatusOffset), st);
 }
 
+extern "C" fg_status fg_chi_reduce_words(const fg_stage *s, fg_precision prec, const fg_paths *P, int32_t NK,
+                                         const double *q, const double *S, const int32_t *span, uint64_t *words,
+                                         void *cchi_save, double *reff_save, void *workspace, size_t workspace_bytes,
+                                         void *stream)
+{
+    g_err.clear();
+    if (!s) return fail(FG_ERR_VALUE, "null stage");
+    if (fg_status rc = check_paths(P)) return rc;
+    if (NK < 0) return fail(FG_ERR_VALUE, "negative NK");
+    if (NK == 0 || P->nrows == 0) return FG_OK;
+    if (!q || !S || !span || !words) return fail(FG_ERR_VALUE, "null array");
+    if (!workspace || workspace_bytes < kCounterBytes)
+        return fail(FG_ERR_WORKSPACE, "workspace needs " + std::to_string(kCounterBytes) + " bytes");
+    if (fg_status rc = set_device(s)) return rc;
+    const StageView sv = view(s);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (fg_status rc = by_kind(s, prec, [&](auto L, const auto &T) {
+            return decltype(L)::fused(sv, T, P, NK, q, S, span, nullptr, cchi_save, reff_save,
+                                      static_cast<unsigned char *>(workspace), fused_shape(s), st,
+                                      reinterpret_cast<unsigned long long *>(words));
+        }))
+        return rc;
+    return read_status(reinterpret_cast<const int *>(static_cast<unsigned char *>(workspace) + kStatusOffset), st);
+}
+
+extern "C" fg_status fg_rows_from_words(int64_t nrows, int32_t NK, const uint64_t *words, double *rows, void *stream)
+{
+    if (nrows < 0 || NK < 0) return fail(FG_ERR_VALUE, "bad size");
+    if (nrows == 0 || NK == 0) return FG_OK;
+    if (!words || !rows) return fail(FG_ERR_VALUE, "null array");
+    return launch_row_finish(nrows, NK, reinterpret_cast<const unsigned long long *>(words), rows, nullptr,
+                             static_cast<cudaStream_t>(stream));
+}
+
 extern "C" size_t fg_chi_reduce_backward_workspace(const fg_stage *s, const fg_paths *P, int32_t NK)
 {
     if (!s || !P || NK < 0) return 0;

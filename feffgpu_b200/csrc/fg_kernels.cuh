@@ -289,13 +289,19 @@ fg_status Launch<R, EDGE>::cchi(const StageView &sv, const Tables<R> &T, int64_t
 template <typename R, int EDGE>
 fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const fg_paths *P, int NK, const double *q,
                                  const double *S, const int *span, double *rows, void *cchi_save, double *reff_save,
-                                 unsigned char *ws, const FusedShape &shape, cudaStream_t st)
+                                 unsigned char *ws, const FusedShape &shape, cudaStream_t st,
+                                 unsigned long long *words)
 {
     using K = Kinds<EDGE>;
     unsigned long long *counter = reinterpret_cast<unsigned long long *>(ws);
     int *status = reinterpret_cast<int *>(ws + kStatusOffset);
-    unsigned long long *racc = reinterpret_cast<unsigned long long *>(ws + kCounterBytes);
-    FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes + row_sum_bytes(P->nrows, NK), st));
+    unsigned long long *racc = words ? words : reinterpret_cast<unsigned long long *>(ws + kCounterBytes);
+    if (words) {
+        FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes, st));
+        FG_CUDA(cudaMemsetAsync(words, 0, (size_t)2 * P->nrows * NK * sizeof(unsigned long long), st));
+    } else {
+        FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes + row_sum_bytes(P->nrows, NK), st));
+    }
     if (fg_status rc = launch_validate(P, sv.nph1, status, st)) return rc;
     if (P->n > 0) {
         const int nsc_max = P->nleg_max - 1;
@@ -312,7 +318,8 @@ fg_status Launch<R, EDGE>::fused(const StageView &sv, const Tables<R> &T, const 
         timer_end(st);
         FG_CUDA(cudaGetLastError());
     }
-    return launch_row_finish(P, NK, racc, rows, status, st);
+    if (!rows) return FG_OK;
+    return launch_row_finish(P->nrows, NK, racc, rows, status, st);
 }
 
 template <typename R>

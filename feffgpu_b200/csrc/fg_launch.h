@@ -45,9 +45,11 @@ template <typename R, int EDGE> struct Launch {
     static fg_status cchi(const StageView &sv, const Tables<R> &T, int64_t B, int nleg, const void *coords,
                           int coords_f64, const int64_t *ipots, void *cchi, void *reff, int *bad, int warps,
                           cudaStream_t st);
+    // rows null: the exact sums are left in words (2 x nrows x NK, see fg_chi_reduce_words) instead of finished
     static fg_status fused(const StageView &sv, const Tables<R> &T, const fg_paths *P, int NK, const double *q,
                            const double *S, const int *span, double *rows, void *cchi_save, double *reff_save,
-                           unsigned char *ws, const FusedShape &shape, cudaStream_t st);
+                           unsigned char *ws, const FusedShape &shape, cudaStream_t st,
+                           unsigned long long *words = nullptr);
     static fg_status cchi_bwd(const StageView &sv, const Tables<R> &T, int64_t B, int nleg, const void *coords,
                               int coords_f64, const int64_t *ipots, const void *grad_cchi, const void *grad_reff,
                               void *grad_coords, unsigned char *ws, int warps, cudaStream_t st);
@@ -75,8 +77,9 @@ fg_status launch_validate(const fg_paths *P, int nph1, int *status, cudaStream_t
 // Bytes of the exact row sums of nrows x NK (two 64-bit words per entry)
 size_t row_sum_bytes(int nrows, int NK);
 
-// Rows (nrows, NK) from the exact fixed-point sums (two word arrays of nrows * NK), NaN where the status is set.
-fg_status launch_row_finish(const fg_paths *P, int NK, const unsigned long long *racc, double *rows, const int *status,
+// Rows (nrows, NK) from the exact fixed-point sums (two word arrays of nrows * NK), NaN where the status is set
+// (status may be null).
+fg_status launch_row_finish(int64_t nrows, int NK, const unsigned long long *racc, double *rows, const int *status,
                             cudaStream_t st);
 
 // The status word of a call's kernels (device int) turned into a return code: outside stream capture the call waits

@@ -38,7 +38,7 @@ __global__ void k_row_finish(int64_t count, const unsigned long long *__restrict
     const long long hi = (long long)(racc[i] + (lo >> 32));   // value * 2^32 (integer part), wraps modulo 2^64
     lo &= 0xffffffffull;
     const double v = (double)(hi >> 32) + ((double)(hi & 0xffffffffll) + (double)lo * 0x1p-32) * 0x1p-32;
-    rows[i] = *(volatile const int *)status ? __longlong_as_double(0x7ff8000000000000ll) : v;
+    rows[i] = (status && *(volatile const int *)status) ? __longlong_as_double(0x7ff8000000000000ll) : v;
 }
 }  // namespace
 
@@ -54,10 +54,10 @@ fg_status launch_validate(const fg_paths *P, int nph1, int *status, cudaStream_t
 
 size_t row_sum_bytes(int nrows, int NK) { return align_up((size_t)2 * nrows * NK * sizeof(unsigned long long), 256); }
 
-fg_status launch_row_finish(const fg_paths *P, int NK, const unsigned long long *racc, double *rows,
-                            const int *status, cudaStream_t st)
+fg_status launch_row_finish(int64_t nrows, int NK, const unsigned long long *racc, double *rows, const int *status,
+                            cudaStream_t st)
 {
-    const int64_t count = (int64_t)P->nrows * NK;
+    const int64_t count = nrows * NK;
     if (count > 0) {
         k_row_finish<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(count, racc, rows, status);
         FG_CUDA(cudaGetLastError());
@@ -78,8 +78,8 @@ fg_status read_status(const int *status, cudaStream_t st)
         return fail(FG_ERR_VALUE, "a weighted path term is not finite or its magnitude is 2^31 or more (the rows are "
                                   "NaN)");
     if (v & kBadLayout)
-        return fail(FG_ERR_VALUE, "malformed path batch: a path index, leg count, summation index or chunk offset is "
-                                  "outside its range (the rows are NaN)");
+        return fail(FG_ERR_VALUE, "malformed path batch: a launch-order entry, leg count or row is outside its range "
+                                  "(the rows are NaN)");
     return FG_OK;
 }
 

@@ -2,10 +2,12 @@
 
 The paths of a job are independent; the only exchange is the final sum of every rank's partial rows (rows x NK FP64,
 e.g. 2 x 401 x 8 B per absorber pair).  ``shard`` splits a path list across ranks by cost (longest-processing-time
-first over the ranks, deterministic); ``allreduce_rows`` sums partial rows over the process group (NCCL on GPUs, gloo
-elsewhere) and is differentiable: every rank computes the loss from the same summed rows, so the gradient reaching
-each rank's partial rows is the upstream gradient itself.  Gradients of positions shared by all ranks (an RMC model)
-are then summed with ``allreduce_grad``.
+first over the ranks, deterministic); ``chi_reduce_all_ranks`` evaluates each rank's share with the fused stage and
+sums the exact row sums over the process group as 64-bit integers (NCCL on GPUs, gloo elsewhere) before the rows are
+formed, so the rows are bit for bit those of one process over all the paths; ``allreduce_rows`` sums finished FP64
+partial rows instead.  Both are differentiable: every rank computes the loss from the same summed rows, so the
+gradient reaching each rank's paths is the upstream gradient itself.  Gradients of positions shared by all ranks (an
+RMC model) are then summed with ``allreduce_grad``.
 
 The reference runs multi-GPU jobs as independent processes per MD-frame shard (``src/feffgpu/parallel/__init__.py:
 78-133``); this module adds the path-level split with one collective.
@@ -72,6 +74,37 @@ class _AllReduceSum(torch.autograd.Function):
     def backward(ctx, g):
         # every rank holds the same loss of the summed rows: its partial rows receive the upstream gradient
         return g, None
+
+
+class _ChiReduceAllRanks(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coords, sigma2, q, S, stage, batch, prec, group):
+        need = ctx.needs_input_grad[0] or (sigma2 is not None and ctx.needs_input_grad[1])
+        words, cchi, reff = stage._chi_reduce_words(batch, coords, sigma2, q, S, prec, save=need)
+        if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
+            dist.all_reduce(words, op=dist.ReduceOp.SUM, group=group)     # 64-bit integers: exact, any order
+        if need:
+            ctx.save_for_backward(coords, sigma2, q, S, cchi, reff)
+        ctx.stage, ctx.batch, ctx.prec = stage, batch, prec
+        return stage.rows_from_words(words)
+
+    @staticmethod
+    def backward(ctx, g):
+        # every rank holds the same loss of the summed rows: its paths receive the upstream gradient
+        coords, sigma2, q, S, cchi, reff = ctx.saved_tensors
+        want_s2 = sigma2 is not None and ctx.needs_input_grad[1]
+        gc, gs = ctx.stage._chi_reduce_backward(ctx.batch, coords, sigma2, q, S, ctx.prec, g, cchi, reff, want_s2)
+        return (gc if ctx.needs_input_grad[0] else None), (gs if want_s2 else None), None, None, None, None, None, None
+
+
+def chi_reduce_all_ranks(stage, batch, q, S=None, coords=None, sigma2=None, dtype=None, group=None) -> torch.Tensor:
+    """The rows of every rank's paths: each rank evaluates its own batch (its share of the paths, e.g. from
+    split_groups) with the fused stage, the exact row sums are summed over the ranks as 64-bit integers, and the rows
+    are formed from the total -- bit for bit the rows one process computes over all the paths, whatever the number of
+    ranks or the split.  Same arguments as GPUPathStage.chi_reduce; differentiable in coords and sigma2 (each rank
+    receives the gradient of its own paths).  One all-reduce of 2 x nrows x NK int64 per call."""
+    crd, s2, qt, Sd, prec = stage._reduce_args(batch, q, S, coords, sigma2, dtype)
+    return _ChiReduceAllRanks.apply(crd, s2, qt, Sd, stage, batch, prec, group)
 
 
 def allreduce_rows(rows: torch.Tensor, group=None) -> torch.Tensor:

@@ -350,10 +350,53 @@ class GPUPathStage:
             return _ChiReduce.apply(crd, qt, Sd, self, batch, prec)
         return _ChiReduceS2.apply(crd, s2, qt, Sd, self, batch, prec)
 
+    def _reduce_args(self, batch, q, S, coords, sigma2, dtype):
+        """chi_reduce's argument preparation: (coords, sigma2, q, S, prec) on the device."""
+        if S is None:
+            S = self.linear_matrix(q)
+        Sd = torch.as_tensor(S).to(self.device, torch.float64).contiguous()
+        qt = torch.as_tensor(q, device=self.device, dtype=torch.float64).contiguous()
+        crd = (batch.coords if coords is None else coords).to(self.device, torch.float64)
+        s2 = None if sigma2 is None else torch.as_tensor(sigma2).to(self.device, torch.float64)
+        prec = self.prec if dtype is None else (_lib.FG_FP64 if dtype == torch.complex128 else _lib.FG_MIXED)
+        if batch.max_ipot > self.P.nph:
+            raise IndexError(f"potential index {batch.max_ipot} out of range 0..{self.P.nph}")
+        grad = torch.is_grad_enabled() and (crd.requires_grad or (s2 is not None and s2.requires_grad))
+        self._pick_launch(batch, qt, Sd, prec, backward=grad)
+        return crd, s2, qt, Sd, prec
+
     def _paths_struct(self, batch, coords, sigma2):
         return _lib.Paths(batch.n, batch.nleg_max, batch.nrows, coords.data_ptr(), batch.ipots.data_ptr(),
                           batch.nleg.data_ptr(), batch.deg.data_ptr(), _ptr(sigma2), batch.row.data_ptr(),
                           batch.order.data_ptr())
+
+    def rows_from_words(self, words: torch.Tensor) -> torch.Tensor:
+        """rows (nrows, NK) FP64 from exact row-sum words (2, nrows, NK) int64 as chi_reduce_words leaves them, or
+        their integer sum over ranks (fg_rows_from_words)."""
+        w = words.contiguous()
+        if w.dim() != 3 or w.shape[0] != 2 or w.dtype != torch.int64:
+            raise ValueError("words must be (2, nrows, NK) int64")
+        rows = torch.empty(int(w.shape[1]), int(w.shape[2]), device=w.device, dtype=torch.float64)
+        _lib.check(self._lib.fg_rows_from_words(int(w.shape[1]), int(w.shape[2]), w.data_ptr(), rows.data_ptr(),
+                                                _stream(self.device)))
+        return rows
+
+    def _chi_reduce_words(self, batch, coords, sigma2, q, S, prec, save: bool):
+        """The fused forward with its exact row sums left as words (2, nrows, NK) int64 (fg_chi_reduce_words)."""
+        coords = coords.contiguous()
+        NK = q.shape[0]
+        ps = self._paths_struct(batch, coords, sigma2)
+        words = torch.empty(2, batch.nrows, NK, device=self.device, dtype=torch.int64)
+        ws = batch.workspace(256)
+        cchi = reff = None
+        if save:
+            cchi = torch.empty(batch.n, self.E, device=self.device,
+                               dtype=torch.complex128 if prec == _lib.FG_FP64 else torch.complex64)
+            reff = torch.empty(batch.n, device=self.device, dtype=torch.float64)
+        _lib.check(self._lib.fg_chi_reduce_words(self._h, prec, C.byref(ps), NK, q.data_ptr(), S.data_ptr(),
+                                                 self._span(S).data_ptr(), words.data_ptr(), _ptr(cchi), _ptr(reff),
+                                                 ws.data_ptr(), 256, _stream(self.device)))
+        return words, cchi, reff
 
     def _chi_reduce_forward(self, batch, coords, sigma2, q, S, prec, save: bool):
         coords = coords.contiguous()

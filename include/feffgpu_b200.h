@@ -150,6 +150,19 @@ FG_API fg_status fg_chi_reduce(const fg_stage *stage, fg_precision prec, const f
                         const double *S, const int32_t *span, double *rows, void *cchi_save, double *reff_save,
                         void *workspace, size_t workspace_bytes, void *stream);
 
+/* fg_chi_reduce without the last step: the exact row sums are left in words (2 x nrows x NK 64-bit words, caller
+ * owned, zeroed by the call): words[r * NK + k] the signed high word (the sum scaled by 2^32, integer part, modulo
+ * 2^64) and words[nrows * NK + r * NK + k] the low word (the next 32 bits of every term, summed).  Words of partial
+ * sums add exactly as 64-bit integers, so summing them over several GPUs (an integer all-reduce) and then calling
+ * fg_rows_from_words gives rows bit for bit equal to one call over all the paths, whatever the number of GPUs or
+ * the split.  The workspace needs only its 256-byte head.  No reference counterpart. */
+FG_API fg_status fg_chi_reduce_words(const fg_stage *stage, fg_precision prec, const fg_paths *paths, int32_t NK,
+                                     const double *q, const double *S, const int32_t *span, uint64_t *words,
+                                     void *cchi_save, double *reff_save, void *workspace, size_t workspace_bytes,
+                                     void *stream);
+/* rows (nrows, NK) FP64 from words as fg_chi_reduce_words leaves them (or their integer sum over calls). */
+FG_API fg_status fg_rows_from_words(int64_t nrows, int32_t NK, const uint64_t *words, double *rows, void *stream);
+
 /* Scratch-free variant of fg_chi_reduce.  No counterpart in the reference: it exists for callers that must not
  * allocate device memory -- for example a host program whose GPU memory is handed out by an allocator it does not
  * control (a simulation code that reserves the whole device for its own pool at start-up) and so cannot provide

@@ -92,3 +92,61 @@ def test_two_ranks_on_the_cuda_stage_equal_one_process():
         mine = np.nonzero(owner == r)[0]          # split_groups keeps every group's paths in order
         assert np.array_equal(out[r][2], nl[mine])
         np.testing.assert_allclose(out[r][1], full[mine], rtol=0, atol=1e-12 * np.abs(full).max())
+
+
+def _worker_exact(rank, world, port, out, dtype_name):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from feffgpu_b200 import GPUPathStage, PathBatch
+        from feffgpu_b200.sharded import chi_reduce_all_ranks, split_groups
+        from tests.fixtures import phase
+        st = GPUPathStage(phase("case_L001"), device="cuda:0", dtype=getattr(torch, dtype_name))
+        mine = split_groups(_groups(), world, rank, lmax=st.lmax.cpu().numpy())
+        b = PathBatch(mine, nrows=2, device="cuda:0")
+        cg = b.coords.clone().requires_grad_(True)
+        s2 = torch.full((b.n,), 0.003, dtype=torch.float64, device="cuda:0", requires_grad=True)
+        total = chi_reduce_all_ranks(st, b, Q, coords=cg, sigma2=s2)
+        (total * torch.tensor(_weights(), device="cuda:0")).sum().backward()
+        out[rank] = (total.detach().cpu().numpy(), cg.grad.cpu().numpy(), s2.grad.cpu().numpy(), b.nleg.cpu().numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("dtype_name", ["complex64", "complex128"])
+def test_two_ranks_exact_rows_equal_one_process_bit_for_bit(dtype_name):
+    """chi_reduce_all_ranks: the ranks' exact row sums are summed as 64-bit integers before the rows are formed, so
+    the rows of two ranks equal one process's chi_reduce over all the paths bit for bit (mixed and FP64 forms), and
+    every path's coordinate and sigma^2 gradient equals the one-process one."""
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    from feffgpu_b200.roofline import path_flops
+    from feffgpu_b200.sharded import shard
+    from tests.fixtures import phase
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_worker_exact, args=(r, world, port, out, dtype_name)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=600)
+        assert p.exitcode == 0
+    gs = _groups()
+    st = GPUPathStage(phase("case_L001"), device="cuda:0", dtype=getattr(torch, dtype_name))
+    b = PathBatch(gs, nrows=2, device="cuda:0")
+    cg = b.coords.clone().requires_grad_(True)
+    s2 = torch.full((b.n,), 0.003, dtype=torch.float64, device="cuda:0", requires_grad=True)
+    rows = st.chi_reduce(b, Q, coords=cg, sigma2=s2)
+    (rows * torch.tensor(_weights(), device="cuda:0")).sum().backward()
+    ref = rows.detach().cpu().numpy()
+    for r in range(world):
+        assert np.array_equal(out[r][0], ref), r          # bit for bit
+    nl = b.nleg.cpu().numpy()
+    owner = shard(nl, world, path_flops(nl, b.ipots.cpu().numpy(), st.lmax.cpu().numpy()))
+    full_c, full_s = cg.grad.cpu().numpy(), s2.grad.cpu().numpy()
+    for r in range(world):
+        mine = np.nonzero(owner == r)[0]
+        assert np.array_equal(out[r][3], nl[mine])
+        assert np.array_equal(out[r][1], full_c[mine]) and np.array_equal(out[r][2], full_s[mine])
