@@ -68,6 +68,12 @@ def test_new_entry_points_refuse_bad_arguments_on_the_host():
     assert lib.fg_path_columns(1, 0, 0, None, None, None, None, None, None) == V                            # E 0
     assert lib.fg_path_columns(1, 60, 7, None, None, None, None, None, None) == V
     assert lib.fg_stage_set_fused_variant(None, 0, 0) == V                                           # null stage
+    assert lib.fg_chi_reduce_words(None, 0, None, 401, None, None, None, None, None, None, None, 0, None) == V
+    assert lib.fg_rows_from_words(-1, 401, None, None, None) == V
+    assert lib.fg_rows_from_words(2, 401, None, None, None) == V                                       # null words
+    assert lib.fg_rows_from_words(0, 401, None, None, None) == _lib.FG_OK                              # nothing to do
+    assert lib.fg_path_geometry(1, 10, None, None, None, None, None) == V                              # nleg 10
+    assert lib.fg_path_geometry_backward(1, 3, None, None, None, None, None, None) == V
     assert lib.fg_stage_set_launch(None, 4, 4) == V
     assert lib.fg_pf_enumerate_one(None, 10, 1.0, None, 0, None, None, 5.0, 3, 0.0, 1, None, None, None, None) == V
     assert lib.fg_pf_result_gather(None, 2, None, None, None, None, None, None) == V
