@@ -777,7 +777,7 @@ __device__ __forceinline__ void path_energy_adj(const WarpPath<R> &g, const R *d
 {
     using K = Kinds<EDGE>;
     if (nleg == 2) {
-        if constexpr (EDGE == 1)
+        if constexpr (K::SS_SYM)
             energy_ss_sym_adj<R, K::SS>(g, dh, dhd, dterm_db, T, e, gbar, pg);
         else
             energy_ss_col_adj<R, K::SS>(g, dh, dhd, dterm_db, T, e, gbar, pg);
@@ -1122,8 +1122,9 @@ fg_status launch_adjoint(const StageView &sv, const Tables<R> &T, const CT *coor
     const size_t wb = adj_warp_bytes<R>(sv.L1, nsc_max, K::MM);
     warps = fit_warps(warps, wb, sv.max_smem);
     const int threads = warps * 32;
-    constexpr int N = lamtab(K::MS).N;
-    auto kern = T.nlam < N ? k_adjoint<R, EDGE, CT, true> : k_adjoint<R, EDGE, CT, false>;
+    auto kern = k_adjoint<R, EDGE, CT, false>;
+    if constexpr (K::MS <= 1)                       // orders 0 and 1 restrict the order-2 sets
+        if (T.nlam < lamtab(K::MS).N) kern = k_adjoint<R, EDGE, CT, true>;
     int blocks = 0;
     if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;
     timer_begin(st);

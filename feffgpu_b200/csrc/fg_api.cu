@@ -120,7 +120,7 @@ template <typename R> fg_status build_tables(fg_stage *s, Tables<R> &T, const st
     if ((st = upload(s, rc, &T.rc))) return st;
     if ((st = upload(s, lmax_t, &T.lmax))) return st;
     T.MMd = 3;
-    T.nlam = s->iorder == 0 ? 1 : (s->iorder == 1 ? 3 : 6);
+    T.nlam = s->iorder == 0 ? 1 : (s->iorder == 1 ? 3 : (s->iorder == 3 ? 10 : 6));
     return FG_OK;
 }
 }  // namespace
@@ -205,8 +205,6 @@ extern "C" fg_status fg_stage_create(const fg_phase_desc *d, int device, fg_stag
     *out = nullptr;
     if (d->nsp != 1) return fail(FG_ERR_NOT_IMPLEMENTED, "spin-dependent phase files are not ported");
     if (d->iorder >= 10) return fail(FG_ERR_NOT_IMPLEMENTED, "icalc >= 10 not ported");
-    if (d->iorder == 3)
-        return fail(FG_ERR_NOT_IMPLEMENTED, "iorder 3 (the 10-entry lambda set) is not built; orders 0, 1 and 2 are");
     if (d->iorder < 0 || d->iorder > 3)
         return fail(FG_ERR_VALUE, "iorder " + std::to_string(d->iorder) +
                                       ": the lambda set exceeds the rotation tables (|m| <= 3)");
@@ -391,20 +389,28 @@ FusedShape fused_shape(const fg_stage *s)
 StageView view(const fg_stage *s) { return StageView{s->E, s->L1, s->nph1, s->num_sms, s->ilinit, s->max_smem}; }
 
 // Calls F::template run<R, EDGE>(tables) for the stage's precision and initial-state class.
+// The kernels of the stage's edge class (l_init + 1) and lambda order (EDGE + 3 at order 3)
 template <class F> fg_status by_kind(const fg_stage *s, fg_precision prec, F &&f)
 {
+    const int edge = (s->ilinit < 1 ? 1 : (s->ilinit > 3 ? 3 : s->ilinit)) + (s->iorder == 3 ? 3 : 0);
     if (prec == FG_FP64) {
-        switch (s->ilinit) {
+        switch (edge) {
         case 1: return f(Launch<double, 1>{}, s->td);
         case 2: return f(Launch<double, 2>{}, s->td);
-        default: return f(Launch<double, 3>{}, s->td);
+        case 3: return f(Launch<double, 3>{}, s->td);
+        case 4: return f(Launch<double, 4>{}, s->td);
+        case 5: return f(Launch<double, 5>{}, s->td);
+        default: return f(Launch<double, 6>{}, s->td);
         }
     }
     if (prec != FG_MIXED) return fail(FG_ERR_VALUE, "precision must be FG_MIXED or FG_FP64");
-    switch (s->ilinit) {
+    switch (edge) {
     case 1: return f(Launch<float, 1>{}, s->tf);
     case 2: return f(Launch<float, 2>{}, s->tf);
-    default: return f(Launch<float, 3>{}, s->tf);
+    case 3: return f(Launch<float, 3>{}, s->tf);
+    case 4: return f(Launch<float, 4>{}, s->tf);
+    case 5: return f(Launch<float, 5>{}, s->tf);
+    default: return f(Launch<float, 6>{}, s->tf);
     }
 }
 

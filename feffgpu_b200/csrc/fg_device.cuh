@@ -138,7 +138,9 @@ template <typename R> __device__ __forceinline__ C2<R> zfac(C2<R> rho)
 // The lambda index sets of setlam (genfmt.py:115-153) in the order setlam leaves them: the laml0x entries that
 // reach the final state lead.  kind 0: K edge, two or more scatterers; 1: L and M edges, two or more scatterers
 // (iorder 2 gives the same six entries, all of them within the final state); 2/3/4: single scattering at K/L/M
-// edges (mmax = nmax = l_init + 1, FEFF's LAMTOT = 15 truncates the M set).
+// edges (mmax = nmax = l_init + 1, FEFF's LAMTOT = 15 truncates the M set); 5/6/7: two or more scatterers at
+// iorder 3 (ten entries) at K/L/M edges.  Orders 0 and 1 use kinds 0 and 1 restricted to their first 3 and 1
+// entries (mask_lambda).
 struct LamTab {
     int N, N0, MM, CI, CO;
     int IT;                     // largest il = l + 1 of a final-state term: l_init + 2 (K and L1: 2, L2/L3: 3, M: 4)
@@ -159,6 +161,21 @@ __host__ __device__ constexpr LamTab lamtab(int kind)
             t.m[i] = kind == 0 ? mK[i] : (kind == 1 ? mL[i] : mS[i]);
             t.n[i] = kind == 0 ? nK[i] : (kind == 1 ? nL[i] : nS[i]);
         }
+    } else if (kind >= 5 && kind <= 7) {
+        // multiple scattering at order 3 (setlam, genfmt.py:115-153: m = 0, +-1, +-2, +-3 with n = 0 and m = 0, +-1
+        // with n = 1), the entries within the final state of edge l_init + 1 = kind - 4 (n, |m| <= l_init + 1) first
+        const int m0[10] = {0, -1, 1, -2, 2, -3, 3, 0, -1, 1}, n0[10] = {0, 0, 0, 0, 0, 0, 0, 1, 1, 1};
+        const int il = kind - 4;
+        int c = 0;
+        for (int pass = 0; pass < 2; ++pass) {
+            for (int i = 0; i < 10; ++i) {
+                const int am = m0[i] < 0 ? -m0[i] : m0[i];
+                const bool first = n0[i] <= il && am <= il;
+                if (first == (pass == 0)) { t.m[c] = m0[i]; t.n[c] = n0[i]; ++c; }
+            }
+            if (pass == 0) t.N0 = c;
+        }
+        t.N = 10;
     } else {
         const int mmax = kind == 3 ? 2 : 3;
         int c = 0;
@@ -172,8 +189,8 @@ __host__ __device__ constexpr LamTab lamtab(int kind)
         t.N = c;
         t.N0 = c;
     }
-    t.IT = (kind == 0 || kind == 2) ? 2 : (kind == 3 ? 3 : 4);
-    t.NT = (kind == 0 || kind == 2) ? 1 : 2;
+    t.IT = (kind == 0 || kind == 2 || kind == 5) ? 2 : ((kind == 3 || kind == 6) ? 3 : 4);
+    t.NT = (kind == 0 || kind == 2 || kind == 5) ? 1 : 2;
     t.MM = 0; t.CI = 0; t.CO = 0;
     for (int i = 0; i < t.N; ++i) {
         int am = t.m[i] < 0 ? -t.m[i] : t.m[i];

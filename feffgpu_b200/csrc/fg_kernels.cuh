@@ -30,9 +30,13 @@ template <typename R> inline size_t warp_bytes(int L1, int nsc_max, int MM, int 
     return b;
 }
 
+// EDGE 1..3: l_init + 1 of the edge (K/L1, L2/L3/M2/M3, M4/M5/N4/N5) at lambda orders 0..2; EDGE 4..6: the same
+// edges at order 3.  MS and SS: the lambda kinds of multiple and single scattering (lamtab).
 template <int EDGE> struct Kinds {
-    static constexpr int MS = EDGE == 1 ? 0 : 1;
-    static constexpr int SS = EDGE + 1;
+    static constexpr int EL = EDGE > 3 ? EDGE - 3 : EDGE;
+    static constexpr int MS = EDGE > 3 ? 4 + EL : (EL == 1 ? 0 : 1);
+    static constexpr int SS = EL + 1;
+    static constexpr bool SS_SYM = SS == 2;      // the K-edge single-scattering set (flip-symmetric accumulation)
     static constexpr int MMMS = lamtab(MS).MM;
     static constexpr int MMSS = lamtab(SS).MM;
     static constexpr int MM = MMMS > MMSS ? MMMS : MMSS;
@@ -44,7 +48,7 @@ __device__ __forceinline__ C2<R> path_energy(const WarpPath<R> &g, const R *dh, 
 {
     using K = Kinds<EDGE>;
     if (nleg == 2) {
-        if constexpr (EDGE == 1)
+        if constexpr (K::SS_SYM)
             return energy_ss_sym<R, K::SS>(g, dh, T, e);
         else
             return energy_ss_col<R, K::SS>(g, dh, T, e);

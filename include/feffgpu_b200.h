@@ -50,8 +50,8 @@ typedef struct fg_phase_desc {
     int32_t ltot;         /* ph index offset: entry l + ltot holds l = -lmax0..lmax0 */
     int32_t nsp;          /* spin channels; only 1 is supported */
     int32_t ihole;        /* FEFF hole index (1 = K, 4 = L3, 9 = M5, ...) */
-    int32_t iorder;       /* lambda-set order (GPUPathStage's iorder): 0, 1 or 2 (the default); 3 is not built
-                           * (FG_ERR_NOT_IMPLEMENTED), 4 and above exceed the rotation tables (FG_ERR_VALUE) */
+    int32_t iorder;       /* lambda-set order (GPUPathStage's iorder): 0..3, 2 by default; 4 and above exceed the
+                           * rotation tables (FG_ERR_VALUE) */
     double edge;          /* edge energy (hartree), for xk */
     const int32_t *lmax0; /* (nph+1) partial waves stored per potential */
     const double *em;     /* (ne1) complex energies (hartree), interleaved */

@@ -24,8 +24,8 @@ The reference is imported read-only from its source tree and run on the CPU in F
   edges) phase tables of 6 A clusters through the reference chain, for the MD-batch and two-edge refinement cases.
 * geometry_ref.npz -- the reference stage's geometry (ri, beta, eta) of 2-8-leg paths, degenerate ones included, and
   the gradient of a weighted sum of it by its autograd;
-* grad_L001_io0/io1.npz, grad_A014_io0/io1.npz -- as grad_*.npz with the reference stage at lambda-set orders 0
-  and 1 (GPUPathStage(..., iorder=k)), with its cchi of every path;
+* grad_L001_io0/io1/io3.npz, grad_A014_io0/io1/io3.npz, grad_A009_io3.npz -- as grad_*.npz with the reference
+  stage at lambda-set orders 0, 1 and 3 (GPUPathStage(..., iorder=k)), with its cchi of every path;
 * finder_lone/one/two/blk/ss.npz -- the same for the enumeration's edge cases: an absorber with no candidate, with one
   (single scattering only) and with two, a 600-atom packing in a box (3 legs), and single scattering alone (2 legs);
 * finder_cu.npz, finder_pack.npz, finder_bcc.npz -- the reference's path finder on the Cu cluster (rmax 6, 4 legs),
@@ -767,9 +767,10 @@ def main():
         if "geometry" in want:
             make_geometry()
         if "iorder" in want:
-            for io in (0, 1):
+            for io in (0, 1, 3):
                 make_grad("L001", nlegs=(2, 3, 4, 5), per=2, iorder=io)       # K edge
                 make_grad("A014", nlegs=(2, 3, 4), per=2, iorder=io)          # L3 edge
+            make_grad("A009", nlegs=(2, 3, 4), per=2, iorder=3)               # M5 edge
         if "finder_edges" in want:
             make_finder(["lone", "one", "two", "blk", "ss"])
         if "pairs" in want:

@@ -385,15 +385,16 @@ def test_axial_legs_gradient_matches_finite_differences(dtype):
         assert np.isfinite(ef) and ef < tol, (name, ef)
 
 
-IORDER_CASES = ["grad_L001_io0", "grad_L001_io1", "grad_A014_io0", "grad_A014_io1"]   # K and L3 edges
+IORDER_CASES = ["grad_L001_io0", "grad_L001_io1", "grad_A014_io0", "grad_A014_io1",    # K and L3 edges
+                "grad_L001_io3", "grad_A014_io3", "grad_A009_io3"]                      # order 3: K, L3, M5
 
 
 @pytest.mark.parametrize("dtype", DTYPES)
 @pytest.mark.parametrize("name", IORDER_CASES)
 def test_lower_lambda_orders_equal_reference(name, dtype):
-    """GPUPathStage(..., iorder=0 or 1), the reference's smaller multiple-scattering lambda sets (setlam,
-    genfmt.py:115-153): per-path cchi against the reference stage at the same order, and the gradient of the
-    weighted fine-grid sum, per-path and fused, against its checkpointed autograd."""
+    """GPUPathStage(..., iorder=0, 1 or 3), the reference's other multiple-scattering lambda sets (setlam,
+    genfmt.py:115-153; 1, 3 and 10 entries): per-path cchi against the reference stage at the same order, and the
+    gradient of the weighted fine-grid sum, per-path and fused, against its checkpointed autograd."""
     from feffgpu_b200 import GPUPathStage, PathBatch
     z = npz(name)
     io = int(z["iorder"])

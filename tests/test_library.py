@@ -44,9 +44,9 @@ def test_stage_create_rejects_spin_and_iorder():
     assert rc == _lib.FG_ERR_NOT_IMPLEMENTED
     d.nsp, d.iorder = 1, 12
     assert lib.fg_stage_create(C.byref(d), 0, C.byref(h)) == _lib.FG_ERR_NOT_IMPLEMENTED
-    d.iorder = 3                                     # the 10-entry lambda set: not built
-    assert lib.fg_stage_create(C.byref(d), 0, C.byref(h)) == _lib.FG_ERR_NOT_IMPLEMENTED
     d.iorder = 5                                     # beyond the reference's |m| <= 3 rotation tables
+    assert lib.fg_stage_create(C.byref(d), 0, C.byref(h)) == _lib.FG_ERR_VALUE
+    d.iorder = -1
     assert lib.fg_stage_create(C.byref(d), 0, C.byref(h)) == _lib.FG_ERR_VALUE
 
 
