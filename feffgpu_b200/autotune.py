@@ -51,12 +51,13 @@ def gpu_name(device) -> str:
 
 
 def signature(stage, batch, nk: int, prec: int) -> str:
-    """Workload key: GPU model, precision, initial-state class, energies, k points, longest path and the leg mix
-    (fraction of paths per leg count, to 0.05)."""
+    """Workload key: GPU model, precision, initial-state class, lambda-set order (other orders run other kernels),
+    energies, k points, longest path and the leg mix (fraction of paths per leg count, to 0.05)."""
     name = gpu_name(stage.device)
     n = max(batch.n, 1)
     mix = ",".join(f"{k}:{round(20 * v / n) / 20:.2f}" for k, v in sorted(batch.counts.items()))
-    return f"{name}|p{prec}|l{stage.ilinit}|E{stage.E}|K{nk}|n{batch.nleg_max}|{mix}"
+    order = "" if getattr(stage, "iorder", 2) == 2 else f"|o{stage.iorder}"
+    return f"{name}|p{prec}|l{stage.ilinit}{order}|E{stage.E}|K{nk}|n{batch.nleg_max}|{mix}"
 
 
 def shape_key(shape) -> str:

@@ -73,6 +73,9 @@ def test_signature_separates_workloads(monkeypatch):
     assert a != A.signature(s, _batch({2: 10, 5: 30}), 201, 0)          # k grid
     assert a != A.signature(s, _batch({2: 30, 5: 10}), 401, 0)          # leg mix
     assert a != A.signature(s, _batch({2: 10, 5: 30, 7: 1}), 401, 0)    # longest path
+    s3 = _Stage()
+    s3.iorder = 3
+    assert a != A.signature(s3, _batch({2: 10, 5: 30}), 401, 0)         # lambda-set order
 
 
 def test_sample_is_stratified():
