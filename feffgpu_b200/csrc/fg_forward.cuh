@@ -376,7 +376,9 @@ __device__ C2<R> energy_ms(const WarpPath<R> &g, const R *dh, const Tables<R> &T
                 C2<R> s = cz<R>();
                 if (k == 1) {
                     s = RT.sg[a][b] > 0 ? acc[RT.rep[a][b]] : cscl(acc[RT.rep[a][b]], R(-1));
-                } else {
+                } else if (sizeof(R) == 8 || a < N0 || k < nsc) {
+                    // the termination reads rows < N0 of the last product only (skipping the others: 1.2 % faster
+                    // in FP32 on B200, 0.7 % slower in FP64, where it is not done)
 #pragma unroll
                     for (int c = 0; c < N; ++c) {
                         const C2<R> f = acc[RT.rep[a][c]];
