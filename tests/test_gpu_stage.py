@@ -354,3 +354,26 @@ def test_geometry_equals_reference(dtype):
     assert ri32.dtype == torch.float32
     ri32.sum().backward()
     assert x32.grad is not None and x32.grad.dtype == torch.float32
+
+
+@pytest.mark.parametrize("dtype", DTYPES)
+def test_fused_stage_reports_terms_out_of_range(dtype):
+    """A weighted path term that is not finite (a NaN coordinate) or reaches 2^31 in magnitude (a huge degeneracy)
+    cannot enter the exact fixed-point sums: nothing of it is added, the call raises ValueError naming the cause and
+    its rows are NaN; the stage works normally afterwards."""
+    from feffgpu_b200 import GPUPathStage, PathBatch
+    P = phase("case_L001")
+    st = GPUPathStage(P, device="cuda", dtype=dtype)
+    coords, ipots, deg = groups("case_L001")[3]
+    q = np.arange(1, 401) * 0.05
+    good = PathBatch([(coords[:5], ipots[:5], deg[:5])], device="cuda")
+    ref = st.chi_reduce(good, q)
+    huge = deg[:5].copy()
+    huge[2] = 1e14
+    with pytest.raises(ValueError, match="2\\^31"):
+        st.chi_reduce(PathBatch([(coords[:5], ipots[:5], huge)], device="cuda"), q)
+    bad = coords[:5].copy()
+    bad[1, 1, 0] = np.nan
+    with pytest.raises(ValueError, match="not finite"):
+        st.chi_reduce(PathBatch([(bad, ipots[:5], deg[:5])], device="cuda"), q)
+    assert torch.equal(st.chi_reduce(good, q), ref)
