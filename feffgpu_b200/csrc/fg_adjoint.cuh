@@ -21,10 +21,11 @@
 namespace fg {
 
 // ------------------------------------------------------------------------------------------------ setup
-// Rotation-table derivatives d/dbeta D^(k) for k = 1..nsc and the termination's d/dbeta d^{l_t}(beta_nleg).
+// Rotation tables D^(k) and their derivatives d/dbeta D^(k) for k = 1..nsc (one recursion for both; path_setup
+// then skips its own pass) and the termination's d/dbeta d^{l_t}(beta_nleg).
 template <typename R>
-__device__ void adj_setup(const WarpPath<R> &g, R *dhd, R (*dterm_db)[49], const Tables<R> &T, int nleg, int lane,
-                          int MM)
+__device__ void adj_setup(const WarpPath<R> &g, R *dh, R *dhd, R (*dterm_db)[49], const Tables<R> &T, int nleg,
+                          int lane, int MM)
 {
     const int nsc = nleg - 1;
     const int NC = ncanon(MM), DS = dstride(MM), L1 = T.L1;
@@ -34,21 +35,29 @@ __device__ void adj_setup(const WarpPath<R> &g, R *dhd, R (*dterm_db)[49], const
         canon_mn(MM, r, m1, m2);
         const double b = g.beta[k];
         const double c = cos(b), s = sin(b), c2 = cos(0.5 * b), s2 = sin(0.5 * b);
-        R *out = dhd + (size_t)(k - 1) * (L1 + 1) * DS + r;
+        const size_t o = (size_t)(k - 1) * (L1 + 1) * DS + r;
+        R *out = dh + o, *outd = dhd + o;
         const double *xf = T.xfac + (m1 + 3) * 7 + (m2 + 3);
         double dm1 = 0.0, d0 = 0.0, em1 = 0.0, e0 = 0.0;   // d and d/dbeta at l-2, l-1
-        for (int l = 0; l < L1; ++l) {
-            double dl, el;
-            if (l <= 3) {
-                dl = wigner_small(l, m1, m2, c2, s2);
-                el = wigner_small_dbeta(l, m1, m2, c2, s2);
-            } else {
-                const double *q = T.rc + (((size_t)(l - 1) * 7 + (m1 + 3)) * 7 + (m2 + 3)) * 3;
-                const double f = fma(q[0], c, -q[1]);
-                dl = fma(f, d0, -q[2] * dm1);
-                el = fma(f, e0, fma(-q[0] * s, d0, -q[2] * em1));
-            }
-            out[(size_t)(l + 1) * DS] = (R)(el * xf[(size_t)(l + 1) * 49]);
+        const int lseed = min(L1, 4);
+        for (int l = 0; l < lseed; ++l) {             // l <= 3: Wigner's explicit sum
+            const double dl = wigner_small(l, m1, m2, c2, s2), el = wigner_small_dbeta(l, m1, m2, c2, s2);
+            const double x = xf[(size_t)(l + 1) * 49];
+            out[(size_t)(l + 1) * DS] = (R)(dl * x);
+            outd[(size_t)(l + 1) * DS] = (R)(el * x);
+            dm1 = d0; d0 = dl;
+            em1 = e0; e0 = el;
+        }
+        // the three-term recursion, unrolled so that the coefficient loads issue ahead of the dependent steps
+#pragma unroll 4
+        for (int l = lseed; l < L1; ++l) {
+            const double *q = T.rc + (((size_t)(l - 1) * 7 + (m1 + 3)) * 7 + (m2 + 3)) * 3;
+            const double f = fma(q[0], c, -q[1]);
+            const double dl = fma(f, d0, -q[2] * dm1);
+            const double el = fma(f, e0, fma(-q[0] * s, d0, -q[2] * em1));
+            const double x = xf[(size_t)(l + 1) * 49];
+            out[(size_t)(l + 1) * DS] = (R)(dl * x);
+            outd[(size_t)(l + 1) * DS] = (R)(el * x);
             dm1 = d0; d0 = dl;
             em1 = e0; e0 = el;
         }
@@ -790,6 +799,7 @@ __device__ __forceinline__ void path_energy_adj(const WarpPath<R> &g, const R *d
 template <typename R> struct AdjShared {
     R dterm_db[2][49];
     double gpar[3 * (kMaxLeg + 1)];
+    double cg[9 * kMaxLeg];            // coordinate-gradient contributions per (leg, atom slot, component)
 };
 
 template <typename R> __host__ __device__ constexpr size_t adj_head_bytes()
@@ -912,31 +922,55 @@ __device__ __forceinline__ double unframe_grad(double gc, int lane, int f)
 }
 
 // Geometry adjoint: dL/dcoords (nleg, 3) of one path from the reduced parameter gradients in gpar (bohr units),
-// one coordinate direction per lane (dual numbers through leg_geometry).
+// returned one coordinate direction per lane (lane = 3 atom + component).  Leg j's geometry reads three atoms (j,
+// j + 1, j - 1; the absorber for 0 and nleg), so each (leg, atom slot, component) is one dual-number evaluation of
+// leg_geometry seeded along that coordinate: 9 nleg tasks spread over the warp (three rounds for eight legs) instead
+// of nleg + 1 evaluations in sequence on every lane.  Leg j's parameters enter the loss as gpar_ri[j] ri_j +
+// gpar_beta[j] beta_j + gpar_eta[j] gamma_j + gpar_eta[j'] alpha_j with j' = j + 1 (1 for j = nleg:
+// eta_1 = alpha_nleg + gamma_1).  The contributions pass through cg (9 kMaxLeg doubles of the warp's shared memory)
+// and each lane sums those of its coordinate in a fixed order (leg, then slot).
 template <typename R>
-__device__ __forceinline__ double coord_grad(const WarpPath<R> &g, const double *gpar, int nleg, int lane)
+__device__ __forceinline__ double coord_grad(const WarpPath<R> &g, const double *gpar, double *cg, int nleg, int lane)
 {
-    if (lane >= 3 * nleg) return 0.0;
-    const int atom = lane / 3, comp = lane % 3;
     const double inv = 1.0 / kBohr;
-    auto rat = [&](int i, Dual *o) {
-        const int a = (i == 0 || i == nleg) ? 0 : i;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) o[c] = Dual{g.xyz[a][c], (a == atom && c == comp) ? inv : 0.0};
+    auto amap = [nleg](int x) { return (x == 0 || x == nleg) ? 0 : x; };
+    // the atom in slot s of leg j (leg_geometry's i, ip1, im1) and whether an earlier slot holds the same atom
+    auto slot_atom = [&](int j, int s, bool &dup) {
+        const int i = j == nleg ? 0 : j, ip1 = j == nleg ? 1 : j + 1, im1 = j - 1;
+        const int a0 = amap(i), a1 = amap(ip1), a2 = amap(im1);
+        dup = (s == 1 && a1 == a0) || (s == 2 && (a2 == a0 || a2 == a1));
+        return s == 0 ? a0 : (s == 1 ? a1 : a2);
     };
-    Dual alpha_prev = Dual{0.0, 0.0};
+    for (int task = lane; task < 9 * nleg; task += 32) {
+        const int j = task / 9 + 1, s = (task % 9) / 3, comp = task % 3;
+        bool dup;
+        const int atom = slot_atom(j, s, dup);
+        double v = 0.0;
+        if (!dup) {
+            auto rat = [&](int i, Dual *o) {
+                const int a = amap(i);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) o[c] = Dual{g.xyz[a][c], (a == atom && c == comp) ? inv : 0.0};
+            };
+            const LegGeomT<Dual> lg = leg_geometry<Dual>(rat, j, nleg);
+            const int jn = j == nleg ? 1 : j + 1;
+            v = gpar[j] * lg.ri.d + gpar[(kMaxLeg + 1) + j] * lg.beta.d + gpar[2 * (kMaxLeg + 1) + j] * lg.gamma.d +
+                gpar[2 * (kMaxLeg + 1) + jn] * lg.alpha.d;
+        }
+        cg[task] = v;
+    }
+    __syncwarp();
     double out = 0.0;
-    // alpha_0 = alpha_nleg: evaluate leg nleg first
-    {
-        const LegGeomT<Dual> lg = leg_geometry<Dual>(rat, nleg, nleg);
-        alpha_prev = lg.alpha;
+    if (lane < 3 * nleg) {
+        const int atom = lane / 3, comp = lane % 3;
+        for (int j = 1; j <= nleg; ++j)
+#pragma unroll
+            for (int s = 0; s < 3; ++s) {
+                bool dup;
+                if (slot_atom(j, s, dup) == atom && !dup) out += cg[(j - 1) * 9 + 3 * s + comp];
+            }
     }
-    for (int j = 1; j <= nleg; ++j) {
-        const LegGeomT<Dual> lg = leg_geometry<Dual>(rat, j, nleg);
-        const double deta = alpha_prev.d + lg.gamma.d;
-        out += gpar[j] * lg.ri.d + gpar[(kMaxLeg + 1) + j] * lg.beta.d + gpar[2 * (kMaxLeg + 1) + j] * deta;
-        alpha_prev = lg.alpha;
-    }
+    __syncwarp();
     return out;
 }
 
@@ -970,8 +1004,8 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
         const int64_t p = order ? order[tk] : (int64_t)tk;
         const int nleg = nlegs ? nlegs[p] : nleg_uniform;
         const int MM = nleg == 2 ? K::MMSS : K::MMMS;
-        path_setup<R, CT>(g, dh, T, coords + p * stride * 3, ipots + p * stride, nleg, lane, status, MM);
-        adj_setup<R>(g, dhd, as.dterm_db, T, nleg, lane, MM);
+        path_setup<R, CT>(g, dh, T, coords + p * stride * 3, ipots + p * stride, nleg, lane, status, MM, false);
+        adj_setup<R>(g, dh, dhd, as.dterm_db, T, nleg, lane, MM);
         __syncwarp();
         const int frame = choose_frame<R>(g, nleg, lane);
         if (frame) reframe_path<R>(g, nleg, lane, frame);
@@ -1003,7 +1037,7 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
             for (int j = 1; j <= nleg; ++j) as.gpar[j] += gr * kBohr * 0.5;
         }
         __syncwarp();
-        double gc = coord_grad<R>(g, as.gpar, nleg, lane);
+        double gc = coord_grad<R>(g, as.gpar, as.cg, nleg, lane);
         if (frame) gc = unframe_grad(gc, lane, frame);
         if (lane < 3 * stride) {
             const int64_t o = p * stride * 3 + lane;

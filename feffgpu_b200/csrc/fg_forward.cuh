@@ -40,11 +40,12 @@ __device__ __forceinline__ void canon_mn(int MM, int r, int &m1, int &m2)
     m2 = r % (2 * MM + 1) - MM;
 }
 
-// Warp-cooperative setup of one path: geometry (FP64), Euler phases, rotation tables of legs 1..nsc and the
-// termination's rotation matrices.  coords: (nleg, 3) angstrom (float or double), ipots: (nleg).
+// Warp-cooperative setup of one path: geometry (FP64), Euler phases, rotation tables of legs 1..nsc (unless
+// tables is false: the adjoint forms them with their derivatives) and the termination's rotation matrices.
+// coords: (nleg, 3) angstrom (float or double), ipots: (nleg).
 template <typename R, typename CT>
 __device__ void path_setup(WarpPath<R> &g, R *dh, const Tables<R> &T, const CT *coords, const int64_t *ipots,
-                           int nleg, int lane, int *bad_ipot, int MM)
+                           int nleg, int lane, int *bad_ipot, int MM, bool tables = true)
 {
     const int nsc = nleg - 1;
     for (int i = lane; i < nleg * 3; i += 32) g.xyz[i / 3][i % 3] = (double)coords[i] / kBohr;
@@ -79,7 +80,7 @@ __device__ void path_setup(WarpPath<R> &g, R *dh, const Tables<R> &T, const CT *
     }
     // rotation tables D^(k), k = 1..nsc, il = 1..L1
     const int NC = ncanon(MM), DS = dstride(MM), L1 = T.L1;
-    for (int task = lane; task < nsc * NC; task += 32) {
+    for (int task = lane; tables && task < nsc * NC; task += 32) {
         const int k = task / NC + 1, r = task % NC;
         int m1, m2;
         canon_mn(MM, r, m1, m2);
@@ -88,14 +89,19 @@ __device__ void path_setup(WarpPath<R> &g, R *dh, const Tables<R> &T, const CT *
         R *out = dh + (size_t)(k - 1) * (L1 + 1) * DS + r;
         const double *xf = T.xfac + (m1 + 3) * 7 + (m2 + 3);
         double dm1 = 0.0, d0 = 0.0;
-        for (int l = 0; l < L1; ++l) {
-            double dl;
-            if (l <= 3) {
-                dl = wigner_small(l, m1, m2, c2, s2);
-            } else {
-                const double *q = T.rc + (((size_t)(l - 1) * 7 + (m1 + 3)) * 7 + (m2 + 3)) * 3;
-                dl = fma(fma(q[0], c, -q[1]), d0, -q[2] * dm1);
-            }
+        const int lseed = min(L1, 4);
+        for (int l = 0; l < lseed; ++l) {             // l <= 3: Wigner's explicit sum
+            const double dl = wigner_small(l, m1, m2, c2, s2);
+            out[(size_t)(l + 1) * DS] = (R)(dl * xf[(size_t)(l + 1) * 49]);
+            dm1 = d0;
+            d0 = dl;
+        }
+        // the three-term recursion: its coefficient loads do not depend on it, so the unrolled trips issue them
+        // ahead of the dependent multiply-adds
+#pragma unroll 4
+        for (int l = lseed; l < L1; ++l) {
+            const double *q = T.rc + (((size_t)(l - 1) * 7 + (m1 + 3)) * 7 + (m2 + 3)) * 3;
+            const double dl = fma(fma(q[0], c, -q[1]), d0, -q[2] * dm1);
             out[(size_t)(l + 1) * DS] = (R)(dl * xf[(size_t)(l + 1) * 49]);
             dm1 = d0;
             d0 = dl;
