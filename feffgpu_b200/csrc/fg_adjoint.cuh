@@ -41,7 +41,8 @@ __device__ void adj_setup(const WarpPath<R> &g, R *dh, R *dhd, R (*dterm_db)[49]
         double dm1 = 0.0, d0 = 0.0, em1 = 0.0, e0 = 0.0;   // d and d/dbeta at l-2, l-1
         const int lseed = min(L1, 4);
         for (int l = 0; l < lseed; ++l) {             // l <= 3: Wigner's explicit sum
-            const double dl = wigner_small(l, m1, m2, c2, s2), el = wigner_small_dbeta(l, m1, m2, c2, s2);
+            const double dl = wigner_small(l, m1, m2, c2, s2, seed_table(T));
+            const double el = wigner_small_dbeta(l, m1, m2, c2, s2, seed_table(T));
             const double x = xf[(size_t)(l + 1) * 49];
             out[(size_t)(l + 1) * DS] = (R)(dl * x);
             outd[(size_t)(l + 1) * DS] = (R)(el * x);
@@ -65,7 +66,8 @@ __device__ void adj_setup(const WarpPath<R> &g, R *dh, R *dhd, R (*dterm_db)[49]
     for (int task = lane; task < T.nterm * 49; task += 32) {
         const int t = task / 49, m1 = (task % 49) / 7 - 3, m2 = task % 7 - 3;
         const double b = g.beta[nleg];
-        dterm_db[t][task % 49] = (R)wigner_small_dbeta(T.term_l[t], m1, m2, cos(0.5 * b), sin(0.5 * b));
+        dterm_db[t][task % 49] = (R)wigner_small_dbeta(T.term_l[t], m1, m2, cos(0.5 * b), sin(0.5 * b),
+                                                        seed_table(T));
     }
 }
 

@@ -314,6 +314,26 @@ extern "C" fg_status fg_stage_create(const fg_phase_desc *d, int device, fg_stag
                 q[1] = (2 * l + 1) * m * n / den;
                 q[2] = (l + 1) * std::sqrt(std::max(a1, 0.0) * std::max(a2, 0.0)) / den;
             }
+    // then the seed coefficients of Wigner's explicit sum for l <= 3 (wigner_small), [l][m + 3][n + 3][k]: the
+    // same IEEE operations (a correctly rounded square root and division of exact factorial products) as the sum
+    // formed them term by term on the device
+    {
+        const size_t seed0 = (size_t)(L1 + 1) * 49 * 3;
+        rc.resize(seed0 + (size_t)4 * 49 * 8, 0.0);
+        const double fct[8] = {1, 1, 2, 6, 24, 120, 720, 5040};
+        for (int l = 0; l <= 3; ++l)
+            for (int m = -l; m <= l; ++m)
+                for (int n = -l; n <= l; ++n) {
+                    const double pref = std::sqrt(fct[l + m] * fct[l - m] * fct[l + n] * fct[l - n]);
+                    for (int k = 0; k <= 2 * l; ++k) {
+                        const int a = l + n - k, b = k, c = m - n + k, d = l - m - k;
+                        if (a < 0 || b < 0 || c < 0 || d < 0) continue;
+                        double term = pref / (fct[a] * fct[b] * fct[c] * fct[d]);
+                        if ((m - n + k) & 1) term = -term;
+                        rc[seed0 + (((size_t)l * 7 + m + 3) * 7 + n + 3) * 8 + k] = term;
+                    }
+                }
+    }
     // lmax on the device as (ip, e)
     std::vector<int> lmax_t((size_t)nph1 * E);
     for (int ip = 0; ip < nph1; ++ip)

@@ -279,7 +279,8 @@ template <typename R> struct Tables {
     const C2<R> *wt;            // (nterm, E) sum over k with lind_k = l of bdiag_k rkk_k^2 (mmtrxi, genfmt.py:378)
     const double *xfac;         // (L1+2, 7, 7) xnlm(il,|m1|+1) (-1)^|m1| / xnlm(il,|m2|+1), 0 where |m| >= il
     const double *xnlm;         // (L1+2, 8) Legendre normalisation, snlm (genfmt.py:41-53)
-    const double *rc;           // (L1+1, 7, 7, 3) three-term recursion coefficients for d^{l+1} (stage.py:80-86)
+    const double *rc;           // (L1+1, 7, 7, 3) three-term recursion coefficients for d^{l+1} (stage.py:80-86),
+                                // then the (4, 7, 7, 8) seed coefficients of wigner_small (seed_table)
 };
 
 // ------------------------------------------------------------------------------------------------ geometry
@@ -379,39 +380,32 @@ template <typename S, class Rat> __device__ __forceinline__ LegGeomT<S> leg_geom
 
 // ------------------------------------------------------------------------------------------------ rotation matrices
 // d^l_{mn}(beta) for l <= 3 from Wigner's explicit sum (the seeds; stage.py:26-38 and the closed forms of
-// stage.py:52-76 are its l = 1, 2 cases).
-__device__ __forceinline__ double wigner_small(int l, int m, int n, double c2, double s2)
+// stage.py:52-76 are its l = 1, 2 cases): sum over k of w_k c2^pc s2^ps, pc = 2l + n - m - 2k, ps = m - n + 2k, with
+// the signed coefficients w_k = (-1)^(m-n+k) sqrt((l+m)!(l-m)!(l+n)!(l-n)!) / ((l+n-k)! k! (m-n+k)! (l-m-k)!) read
+// from the stage's seed table ws (seed_table; built on the host by the same IEEE operations).  k runs over the terms
+// whose factorial arguments are all >= 0.
+__device__ __forceinline__ double wigner_small(int l, int m, int n, double c2, double s2, const double *ws)
 {
-    if (abs(m) > l || abs(n) > l) return 0.0;
-    const double f[8] = {1, 1, 2, 6, 24, 120, 720, 5040};
-    const double pref = sqrt(f[l + m] * f[l - m] * f[l + n] * f[l - n]);
+    if (l > 3 || abs(m) > l || abs(n) > l) return 0.0;      // the table holds l <= 3 (final states l_t <= 3)
+    const double *w = ws + ((l * 7 + m + 3) * 7 + n + 3) * 8;
     double out = 0.0;
-    for (int k = 0; k <= 2 * l; ++k) {
-        const int a = l + n - k, b = k, c = m - n + k, d = l - m - k;
-        if (a < 0 || b < 0 || c < 0 || d < 0) continue;
-        double term = pref / (f[a] * f[b] * f[c] * f[d]);
-        if ((m - n + k) & 1) term = -term;
+    for (int k = max(0, n - m); k <= min(l + n, l - m); ++k) {
         const int pc = 2 * l + n - m - 2 * k, ps = m - n + 2 * k;
         double pw = 1.0;
         for (int q = 0; q < pc; ++q) pw *= c2;
         for (int q = 0; q < ps; ++q) pw *= s2;
-        out += term * pw;
+        out += w[k] * pw;
     }
     return out;
 }
 
 // d/dbeta of d^l_{mn}(beta) for l <= 3 (the derivative of the half-angle powers of Wigner's sum)
-__device__ __forceinline__ double wigner_small_dbeta(int l, int m, int n, double c2, double s2)
+__device__ __forceinline__ double wigner_small_dbeta(int l, int m, int n, double c2, double s2, const double *ws)
 {
-    if (abs(m) > l || abs(n) > l) return 0.0;
-    const double f[8] = {1, 1, 2, 6, 24, 120, 720, 5040};
-    const double pref = sqrt(f[l + m] * f[l - m] * f[l + n] * f[l - n]);
+    if (l > 3 || abs(m) > l || abs(n) > l) return 0.0;      // the table holds l <= 3 (final states l_t <= 3)
+    const double *w = ws + ((l * 7 + m + 3) * 7 + n + 3) * 8;
     double out = 0.0;
-    for (int k = 0; k <= 2 * l; ++k) {
-        const int a = l + n - k, b = k, c = m - n + k, d = l - m - k;
-        if (a < 0 || b < 0 || c < 0 || d < 0) continue;
-        double term = pref / (f[a] * f[b] * f[c] * f[d]);
-        if ((m - n + k) & 1) term = -term;
+    for (int k = max(0, n - m); k <= min(l + n, l - m); ++k) {
         const int pc = 2 * l + n - m - 2 * k, ps = m - n + 2 * k;
         // d/dbeta c2^pc s2^ps = (ps c2^(pc+1) s2^(ps-1) - pc c2^(pc-1) s2^(ps+1)) / 2
         double t1 = 0.0, t2 = 0.0;
@@ -427,9 +421,16 @@ __device__ __forceinline__ double wigner_small_dbeta(int l, int m, int n, double
             for (int q = 0; q < ps + 1; ++q) pw *= s2;
             t2 = pc * pw;
         }
-        out += term * 0.5 * (t1 - t2);
+        out += w[k] * 0.5 * (t1 - t2);
     }
     return out;
+}
+
+// The seed coefficients, stored after the recursion coefficients in the rc buffer: (4, 7, 7, 8) doubles indexed
+// [l][m + 3][n + 3][k].
+template <typename R> __device__ __forceinline__ const double *seed_table(const Tables<R> &T)
+{
+    return T.rc + (size_t)(T.L1 + 1) * 49 * 3;
 }
 
 }  // namespace fg

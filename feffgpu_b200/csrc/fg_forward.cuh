@@ -91,7 +91,7 @@ __device__ void path_setup(WarpPath<R> &g, R *dh, const Tables<R> &T, const CT *
         double dm1 = 0.0, d0 = 0.0;
         const int lseed = min(L1, 4);
         for (int l = 0; l < lseed; ++l) {             // l <= 3: Wigner's explicit sum
-            const double dl = wigner_small(l, m1, m2, c2, s2);
+            const double dl = wigner_small(l, m1, m2, c2, s2, seed_table(T));
             out[(size_t)(l + 1) * DS] = (R)(dl * xf[(size_t)(l + 1) * 49]);
             dm1 = d0;
             d0 = dl;
@@ -111,7 +111,7 @@ __device__ void path_setup(WarpPath<R> &g, R *dh, const Tables<R> &T, const CT *
     for (int task = lane; task < T.nterm * 49; task += 32) {
         const int t = task / 49, m1 = (task % 49) / 7 - 3, m2 = task % 7 - 3;
         const double b = g.beta[nleg];
-        g.dterm[t][task % 49] = (R)wigner_small(T.term_l[t], m1, m2, cos(0.5 * b), sin(0.5 * b));
+        g.dterm[t][task % 49] = (R)wigner_small(T.term_l[t], m1, m2, cos(0.5 * b), sin(0.5 * b), seed_table(T));
     }
     __syncwarp();
 }
