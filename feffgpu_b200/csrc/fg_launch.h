@@ -16,6 +16,7 @@ __host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + 
 
 constexpr size_t kCounterBytes = 256;   // head of every fused workspace: work-queue counters and flags
 constexpr size_t kStatusOffset = 64;    // the int status word (kBadIpot | kBadLayout) within that head
+constexpr int kGparStride = 32;         // per path in the fused backward's workspace: parameter gradients, frame
 
 // What the launches need to know about a stage.
 struct StageView {

@@ -91,7 +91,8 @@ namespace fg {
 // counter, per-path seeds of the chain adjoint (n x E complex, sized for FP64), per-path dL/dreff
 size_t fused_bwd_workspace(const fg_paths *P, int, int E)
 {
-    return kCounterBytes + align_up((size_t)P->n * E * 2 * sizeof(double), 256) + align_up((size_t)P->n * sizeof(double), 256);
+    return kCounterBytes + align_up((size_t)P->n * E * 2 * sizeof(double), 256) + align_up((size_t)P->n * sizeof(double), 256) +
+           align_up((size_t)P->n * kGparStride * sizeof(double), 256);
 }
 size_t cchi_bwd_workspace(int64_t, int) { return kCounterBytes; }
 }  // namespace fg
