@@ -16,6 +16,8 @@
 // through the geometry (one coordinate direction per lane), with the reference's branch choices
 // (stage.py:148-206 under torch autograd).
 #pragma once
+#include <type_traits>
+
 #include "fg_kernels.cuh"
 
 namespace fg {
@@ -978,7 +980,9 @@ __device__ __forceinline__ double coord_grad(const double (*xyz)[3], const doubl
 
 // The adjoint over a set of paths: per path the seeds gbar (E, complex) and dL/dreff (A), out dL/dcoords.
 // Paths come from `order` (or are 0..B-1), coordinates/ipots with a row stride of `stride` legs.
-template <typename R, int EDGE, typename CT, bool MASK = false>
+// SPLIT: the coordinate gradient is k_coord_grad's (the fused backward); the kernel hands over each path's parameter
+// gradients and frame in gpar_out and carries none of that code.
+template <typename R, int EDGE, typename CT, bool MASK = false, bool SPLIT = false>
 __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restrict__ coords,
                                                   const int64_t *__restrict__ ipots, int stride,
                                                   const int *__restrict__ nlegs, int nleg_uniform, int64_t B,
@@ -1040,21 +1044,20 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
             for (int j = 1; j <= nleg; ++j) as.gpar[j] += gr * kBohr * 0.5;
         }
         __syncwarp();
-        if (gpar_out) {
+        if constexpr (SPLIT) {
             // the coordinate gradient is k_coord_grad's: hand over the parameter gradients and the frame
             double *o = gpar_out + p * kGparStride;
             for (int i = lane; i < 3 * (kMaxLeg + 1); i += 32) o[i] = as.gpar[i];
             if (lane == 0) o[3 * (kMaxLeg + 1)] = (double)frame;
-            __syncwarp();
-            continue;
-        }
-        double gc = coord_grad(g.xyz, as.gpar, as.cg, nleg, lane);
-        if (frame) gc = unframe_grad(gc, lane, frame);
-        if (lane < 3 * stride) {
-            const int64_t o = p * stride * 3 + lane;
-            const double v = lane < 3 * nleg ? gc : 0.0;
-            if (gout_d) gout_d[o] = v;
-            else gout_r[o] = (R)v;
+        } else {
+            double gc = coord_grad(g.xyz, as.gpar, as.cg, nleg, lane);
+            if (frame) gc = unframe_grad(gc, lane, frame);
+            if (lane < 3 * stride) {
+                const int64_t o = p * stride * 3 + lane;
+                const double v = lane < 3 * nleg ? gc : 0.0;
+                if (gout_d) gout_d[o] = v;
+                else gout_r[o] = (R)v;
+            }
         }
         __syncwarp();
     }
@@ -1064,8 +1067,8 @@ __global__ void __launch_bounds__(128) k_adjoint(Tables<R> T, const CT *__restri
 // parameter gradients and frames come from k_adjoint through gpar (kGparStride doubles per path), the atoms from the
 // batch, rotated into the path's frame exactly as reframe_path rotates them; then coord_grad and the rotation back,
 // as k_adjoint does inline for the drop-in cchi backward.  Inside k_adjoint this per-path code ran at 8 warps per SM
-// between long energy loops; here it runs at 20 (96 registers): forward + backward of the path-finder batch on B200
-// 218.9 -> 217.4 ms, gradients bit-identical.
+// between long energy loops; here it runs at 20 (96 registers), and the split k_adjoint carries none of it: forward +
+// backward of the path-finder batch on B200 219.3 -> 216.8 ms, gradients bit-identical.
 template <typename CT>
 __global__ void __launch_bounds__(128) k_coord_grad(const CT *__restrict__ coords, int stride,
                                                      const int *__restrict__ nlegs, int nleg_uniform, int64_t B,
@@ -1210,6 +1213,12 @@ fg_status launch_adjoint(const StageView &sv, const Tables<R> &T, const CT *coor
     auto kern = k_adjoint<R, EDGE, CT, false>;
     if constexpr (K::MS <= 1)                       // orders 0 and 1 restrict the order-2 sets
         if (T.nlam < lamtab(K::MS).N) kern = k_adjoint<R, EDGE, CT, true>;
+    if constexpr (std::is_same<CT, double>::value)  // the fused backward (FP64 coordinates) splits
+        if (gpar_out) {
+            kern = k_adjoint<R, EDGE, CT, false, true>;
+            if constexpr (K::MS <= 1)
+                if (T.nlam < lamtab(K::MS).N) kern = k_adjoint<R, EDGE, CT, true, true>;
+        }
     int blocks = 0;
     if (fg_status rc = grid_for(kern, threads, wb * warps, sv.num_sms, B, blocks)) return rc;
     timer_begin(st);
